@@ -1,0 +1,501 @@
+"""Python binding of the B200 traversal engine (libgg.so, C ABI in include/gg.h).
+
+The binding is a thin ctypes layer: graphs, frontiers and vertex arrays live
+on the GPU inside the library; results come back as numpy arrays.  There is
+no CPU fallback: importing works without a GPU (host-only functions such as
+the generators and the partitioner run anywhere), but every device call fails
+with a GGError when no CUDA device is present, and importing fails when the
+compiled library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libgg.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"graphgrind_b200: compiled library {LIB_PATH} is missing; build it with "
+        "`make -C graphgrind_b200` (or __graft_entry__.build())")
+
+lib = C.CDLL(LIB_PATH)
+
+# ------------------------------------------------------------------ status
+GG_OK = 0
+ERRORS = {
+    -1: "INVALID_ARG", -2: "CUDA", -3: "OOM", -4: "PARTITION", -5: "IO", -6: "FORMAT",
+    -7: "NO_DEVICE", -8: "UNSUPPORTED", -9: "TIMEOUT", -10: "SIZE",
+}
+W_NONE, W_INT32, W_FLOAT32 = 0, 1, 2
+BALANCE_EDGE, BALANCE_VERTEX = 0, 1
+PART_DEST, PART_SOURCE = 0, 1
+ORDER_CSR, ORDER_HILBERT = 0, 1
+EM_FORCE_SPARSE, EM_FORCE_CSC, EM_FORCE_COO, EM_NO_OUTPUT = 0x1, 0x2, 0x4, 0x8
+F_BFS, F_CC, F_PR, F_PRDELTA, F_SPMV, F_BF, F_BC, F_BC_BACK, F_BP = range(1, 10)
+
+
+class GGError(RuntimeError):
+    def __init__(self, code: int, where: str):
+        self.code = code
+        msg = lib.gg_last_error_string().decode(errors="replace")
+        super().__init__(f"{where}: GG_ERR_{ERRORS.get(code, code)} ({code}): {msg}")
+
+
+def check(rc: int, where: str) -> None:
+    if rc != GG_OK:
+        raise GGError(rc, where)
+
+
+# ----------------------------------------------------------------- structs
+class HostGraphC(C.Structure):
+    _fields_ = [("n", C.c_uint32), ("m", C.c_uint64), ("symmetric", C.c_int32),
+                ("weight_type", C.c_int32), ("offsets", C.POINTER(C.c_uint32)),
+                ("indices", C.POINTER(C.c_uint32)), ("weights", C.c_void_p)]
+
+
+class BuildOpts(C.Structure):
+    _fields_ = [("num_partitions", C.c_int32), ("balance", C.c_int32), ("part_how", C.c_int32),
+                ("relabel", C.c_int32), ("order", C.c_int32), ("tile_vertices", C.c_int32),
+                ("tile_edges", C.c_int32), ("build_coo", C.c_int32)]
+
+
+class GraphInfo(C.Structure):
+    _fields_ = [("n", C.c_uint32), ("m", C.c_uint64), ("symmetric", C.c_int32),
+                ("weight_type", C.c_int32), ("num_partitions", C.c_int32), ("has_coo", C.c_int32),
+                ("transposed", C.c_int32), ("num_csc_tiles", C.c_int32),
+                ("num_coo_tiles", C.c_int32), ("device_bytes", C.c_uint64)]
+
+
+class RunStats(C.Structure):
+    _fields_ = [("ms", C.c_double), ("rounds", C.c_int32), ("edges_traversed", C.c_uint64),
+                ("kernels", C.c_int32)]
+
+
+class EdgeMapStats(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("frontier_active", C.c_uint64),
+                ("frontier_out_edges", C.c_uint64), ("output_active", C.c_uint64),
+                ("output_out_edges", C.c_uint64)]
+
+
+class BfsArgs(C.Structure):
+    _fields_ = [("parents", C.c_void_p), ("levels", C.c_void_p), ("round", C.c_int32)]
+
+
+class CcArgs(C.Structure):
+    _fields_ = [("ids", C.c_void_p), ("prev_ids", C.c_void_p)]
+
+
+class PairArgs(C.Structure):  # gg_pr_args / gg_prdelta_args / gg_spmv_args / gg_bf_args / gg_bc_args
+    _fields_ = [("a", C.c_void_p), ("b", C.c_void_p)]
+
+
+_P = C.c_void_p
+_u32p = C.POINTER(C.c_uint32)
+_i64p = C.POINTER(C.c_int64)
+
+
+def _sig(name, res, *args):
+    f = getattr(lib, name)
+    f.restype = res
+    f.argtypes = list(args)
+    return f
+
+
+_sig("gg_last_error_string", C.c_char_p)
+_sig("gg_version", C.c_char_p)
+_sig("gg_gen_rmat", C.c_int, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_uint64,
+     C.c_int32, C.POINTER(HostGraphC))
+_sig("gg_gen_grid", C.c_int, C.c_int32, C.c_double, C.c_uint64, C.POINTER(HostGraphC))
+_sig("gg_gen_er", C.c_int, C.c_uint32, C.c_uint64, C.c_uint64, C.c_int32, C.POINTER(HostGraphC))
+_sig("gg_host_graph_add_weights", C.c_int, C.POINTER(HostGraphC), C.c_int32, C.c_uint64, C.c_int32, C.c_int32)
+_sig("gg_host_graph_write_adj", C.c_int, C.POINTER(HostGraphC), C.c_char_p)
+_sig("gg_host_graph_write_gr", C.c_int, C.POINTER(HostGraphC), C.c_char_p)
+_sig("gg_host_graph_read", C.c_int, C.c_char_p, C.c_int32, C.c_int32, C.c_int32, C.POINTER(HostGraphC))
+_sig("gg_host_graph_transpose", C.c_int, C.POINTER(HostGraphC), C.POINTER(HostGraphC))
+_sig("gg_host_graph_free", None, C.POINTER(HostGraphC))
+_sig("gg_partition_sizes", C.c_int, _u32p, _u32p, C.c_uint32, C.c_uint64, C.c_int32, C.c_int32, C.c_int32,
+     C.c_int32, _i64p, _i64p)
+_sig("gg_hilbert_key", C.c_int64, C.c_int64, C.c_int64, C.c_int64)
+_sig("gg_graph_build", C.c_int, C.POINTER(HostGraphC), C.POINTER(BuildOpts), C.POINTER(_P))
+_sig("gg_graph_destroy", C.c_int, _P)
+_sig("gg_graph_get_info", C.c_int, _P, C.POINTER(GraphInfo))
+_sig("gg_graph_partition_starts", C.c_int, _P, _i64p)
+_sig("gg_graph_transpose", C.c_int, _P)
+_sig("gg_frontier_single", C.c_int, _P, C.c_uint32, C.POINTER(_P))
+_sig("gg_frontier_all", C.c_int, _P, C.POINTER(_P))
+_sig("gg_frontier_empty", C.c_int, _P, C.POINTER(_P))
+_sig("gg_frontier_from_mask", C.c_int, _P, C.POINTER(C.c_uint8), C.POINTER(_P))
+_sig("gg_frontier_from_list", C.c_int, _P, _u32p, C.c_uint64, C.POINTER(_P))
+_sig("gg_frontier_destroy", C.c_int, _P)
+_sig("gg_frontier_stats", C.c_int, _P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64))
+_sig("gg_frontier_to_mask", C.c_int, _P, C.POINTER(C.c_uint8))
+_sig("gg_frontier_to_dense", C.c_int, _P)
+_sig("gg_frontier_to_sparse", C.c_int, _P)
+_sig("gg_frontier_repr", C.c_int, _P)
+_sig("gg_edge_map", C.c_int, _P, _P, C.c_int32, _P, C.c_int64, C.c_uint32, C.POINTER(_P))
+_sig("gg_last_edge_map_stats", C.c_int, _P, C.POINTER(EdgeMapStats))
+_sig("gg_vertex_map", C.c_int, _P, _P, C.c_int32, _P)
+_sig("gg_vertex_filter", C.c_int, _P, _P, C.c_int32, _P, C.POINTER(_P))
+_sig("gg_vertex_array_alloc", C.c_int, _P, C.c_size_t, C.POINTER(_P))
+_sig("gg_vertex_array_free", C.c_int, _P, _P)
+_sig("gg_memcpy_h2d", C.c_int, _P, _P, C.c_size_t)
+_sig("gg_memcpy_d2h", C.c_int, _P, _P, C.c_size_t)
+_sig("gg_bfs", C.c_int, _P, C.c_uint32, _P, _P, C.POINTER(RunStats))
+_sig("gg_components", C.c_int, _P, _P, C.POINTER(RunStats))
+_sig("gg_pagerank", C.c_int, _P, C.c_int32, C.c_int32, _P, C.POINTER(RunStats))
+_sig("gg_pagerank_delta", C.c_int, _P, _P, C.POINTER(RunStats))
+_sig("gg_spmv", C.c_int, _P, _P, _P, C.POINTER(RunStats))
+_sig("gg_bellman_ford", C.c_int, _P, C.c_uint32, _P, C.POINTER(RunStats))
+_sig("gg_bc", C.c_int, _P, C.c_uint32, _P, _P, C.POINTER(RunStats))
+_sig("gg_bp", C.c_int, _P, C.c_int32, _P, _P, _P, C.POINTER(RunStats))
+
+# Every symbol declared in include/gg.h (checked by the tests).
+EXPORTED = [
+    "gg_last_error_string", "gg_version", "gg_gen_rmat", "gg_gen_grid", "gg_gen_er",
+    "gg_host_graph_add_weights", "gg_host_graph_write_adj", "gg_host_graph_write_gr",
+    "gg_host_graph_read", "gg_host_graph_transpose", "gg_host_graph_free", "gg_partition_sizes",
+    "gg_hilbert_key", "gg_graph_build", "gg_graph_destroy", "gg_graph_get_info",
+    "gg_graph_partition_starts", "gg_graph_transpose", "gg_graph_device_arrays",
+    "gg_frontier_single", "gg_frontier_all", "gg_frontier_empty", "gg_frontier_from_mask",
+    "gg_frontier_from_list", "gg_frontier_destroy", "gg_frontier_stats", "gg_frontier_to_mask",
+    "gg_frontier_to_dense", "gg_frontier_to_sparse", "gg_frontier_repr", "gg_edge_map",
+    "gg_last_edge_map_stats", "gg_vertex_map", "gg_vertex_filter", "gg_vertex_array_alloc",
+    "gg_vertex_array_free", "gg_memcpy_h2d", "gg_memcpy_d2h", "gg_bfs", "gg_components",
+    "gg_pagerank", "gg_pagerank_delta", "gg_spmv", "gg_bellman_ford", "gg_bc", "gg_bp",
+]
+
+
+def _ptr(a: np.ndarray) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data)
+
+
+# -------------------------------------------------------------- host graph
+class HostGraph:
+    """A host CSR graph owned by the library (gg_host_graph)."""
+
+    def __init__(self, c: HostGraphC):
+        self.c = c
+
+    def __del__(self):
+        try:
+            lib.gg_host_graph_free(C.byref(self.c))
+        except Exception:
+            pass
+
+    @property
+    def n(self) -> int:
+        return int(self.c.n)
+
+    @property
+    def m(self) -> int:
+        return int(self.c.m)
+
+    @property
+    def symmetric(self) -> bool:
+        return bool(self.c.symmetric)
+
+    @property
+    def weight_type(self) -> int:
+        return int(self.c.weight_type) if self.c.weights else W_NONE
+
+    @property
+    def offsets(self) -> np.ndarray:
+        return np.ctypeslib.as_array(self.c.offsets, shape=(self.n + 1,))
+
+    @property
+    def indices(self) -> np.ndarray:
+        if self.m == 0:
+            return np.zeros(0, np.uint32)
+        return np.ctypeslib.as_array(self.c.indices, shape=(self.m,))
+
+    @property
+    def weights(self):
+        if not self.c.weights or self.m == 0:
+            return None
+        buf = (C.c_uint32 * self.m).from_address(self.c.weights)
+        a = np.frombuffer(buf, dtype=np.uint32)
+        return a.view(np.float32) if self.weight_type == W_FLOAT32 else a.view(np.int32)
+
+    def degrees(self) -> np.ndarray:
+        return np.diff(self.offsets.astype(np.int64)).astype(np.uint32)
+
+    @staticmethod
+    def rmat(scale, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=1, symmetric=True) -> "HostGraph":
+        g = HostGraphC()
+        check(lib.gg_gen_rmat(scale, edge_factor, a, b, c, seed, int(symmetric), C.byref(g)), "gg_gen_rmat")
+        return HostGraph(g)
+
+    @staticmethod
+    def grid(side, long_range_frac=0.001, seed=3) -> "HostGraph":
+        g = HostGraphC()
+        check(lib.gg_gen_grid(side, long_range_frac, seed, C.byref(g)), "gg_gen_grid")
+        return HostGraph(g)
+
+    @staticmethod
+    def er(n, m, seed=4, symmetric=False) -> "HostGraph":
+        g = HostGraphC()
+        check(lib.gg_gen_er(n, m, seed, int(symmetric), C.byref(g)), "gg_gen_er")
+        return HostGraph(g)
+
+    @staticmethod
+    def read(path, binary=False, symmetric=False, weighted=False) -> "HostGraph":
+        g = HostGraphC()
+        check(lib.gg_host_graph_read(str(path).encode(), int(binary), int(symmetric), int(weighted), C.byref(g)),
+              "gg_host_graph_read")
+        return HostGraph(g)
+
+    @staticmethod
+    def from_csr(offsets, indices, weights=None, symmetric=False) -> "HostGraph":
+        """Copy a CSR given as numpy arrays into a library-owned host graph."""
+        import tempfile
+        offsets = np.ascontiguousarray(offsets, dtype=np.uint32)
+        indices = np.ascontiguousarray(indices, dtype=np.uint32)
+        n = len(offsets) - 1
+        with tempfile.TemporaryDirectory() as d:  # round trip through the .gr writer/reader
+            p = os.path.join(d, "g.gr")
+            hdr = np.array([1, 4 if weights is not None else 0, n, len(indices)], np.uint64)
+            with open(p, "wb") as f:
+                f.write(hdr.tobytes())
+                f.write(offsets[1:].astype(np.uint64).tobytes())
+                f.write(indices.tobytes())
+                if len(indices) & 1:
+                    f.write(b"\0\0\0\0")
+                if weights is not None:
+                    f.write(np.ascontiguousarray(weights, dtype=np.int32).tobytes())
+            return HostGraph.read(p, binary=True, symmetric=symmetric, weighted=weights is not None)
+
+    def add_weights(self, weight_type=W_INT32, seed=7, lo=1, hi=100) -> "HostGraph":
+        check(lib.gg_host_graph_add_weights(C.byref(self.c), weight_type, seed, lo, hi), "gg_host_graph_add_weights")
+        return self
+
+    def write_adj(self, path):
+        check(lib.gg_host_graph_write_adj(C.byref(self.c), str(path).encode()), "gg_host_graph_write_adj")
+
+    def write_gr(self, path):
+        check(lib.gg_host_graph_write_gr(C.byref(self.c), str(path).encode()), "gg_host_graph_write_gr")
+
+    def transpose(self) -> "HostGraph":
+        t = HostGraphC()
+        check(lib.gg_host_graph_transpose(C.byref(self.c), C.byref(t)), "gg_host_graph_transpose")
+        return HostGraph(t)
+
+
+def partition_sizes(in_deg, out_deg, m, P, balance=BALANCE_EDGE, part_how=PART_DEST, relabel=False):
+    """Reference partition sizes (coo, csc); raises GGError(PARTITION) where the reference asserts."""
+    in_deg = np.ascontiguousarray(in_deg, np.uint32)
+    out_deg = np.ascontiguousarray(out_deg, np.uint32)
+    coo = np.zeros(P, np.int64)
+    csc = np.zeros(P, np.int64)
+    check(lib.gg_partition_sizes(in_deg.ctypes.data_as(_u32p), out_deg.ctypes.data_as(_u32p), len(in_deg), m, P,
+                                 balance, part_how, int(relabel), coo.ctypes.data_as(_i64p),
+                                 csc.ctypes.data_as(_i64p)), "gg_partition_sizes")
+    return coo, csc
+
+
+def hilbert_key(side_edges: int, x: int, y: int) -> int:
+    return int(lib.gg_hilbert_key(side_edges, x, y))
+
+
+# ------------------------------------------------------------ device graph
+@dataclass
+class Run:
+    ms: float
+    rounds: int
+    edges_traversed: int
+    kernels: int
+
+
+def _run(st: RunStats) -> Run:
+    return Run(st.ms, st.rounds, st.edges_traversed, st.kernels)
+
+
+class Frontier:
+    """partitioned_vertices on the device."""
+
+    def __init__(self, graph: "Graph", handle: C.c_void_p):
+        self.graph = graph
+        self.h = handle
+
+    def __del__(self):
+        self.close()
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.gg_frontier_destroy(self.h)
+            self.h = None
+
+    def stats(self):
+        a, b = C.c_uint64(), C.c_uint64()
+        check(lib.gg_frontier_stats(self.h, C.byref(a), C.byref(b)), "gg_frontier_stats")
+        return int(a.value), int(b.value)
+
+    def mask(self) -> np.ndarray:
+        out = np.zeros(self.graph.n, np.uint8)
+        check(lib.gg_frontier_to_mask(self.h, out.ctypes.data_as(C.POINTER(C.c_uint8))), "gg_frontier_to_mask")
+        return out
+
+    def to_dense(self):
+        check(lib.gg_frontier_to_dense(self.h), "gg_frontier_to_dense")
+
+    def to_sparse(self):
+        check(lib.gg_frontier_to_sparse(self.h), "gg_frontier_to_sparse")
+
+    def repr(self) -> int:
+        return int(lib.gg_frontier_repr(self.h))
+
+
+class DeviceArray:
+    """A device vertex array (n entries) owned by a Graph."""
+
+    def __init__(self, graph: "Graph", dtype, init=None):
+        self.graph = graph
+        self.dtype = np.dtype(dtype)
+        p = C.c_void_p()
+        check(lib.gg_vertex_array_alloc(graph.h, self.dtype.itemsize, C.byref(p)), "gg_vertex_array_alloc")
+        self.ptr = p
+        if init is not None:
+            self.upload(np.full(graph.n, init, self.dtype) if np.isscalar(init) else init)
+
+    def upload(self, a):
+        a = np.ascontiguousarray(a, self.dtype)
+        check(lib.gg_memcpy_h2d(self.ptr, _ptr(a), a.nbytes), "gg_memcpy_h2d")
+
+    def download(self) -> np.ndarray:
+        out = np.empty(self.graph.n, self.dtype)
+        check(lib.gg_memcpy_d2h(_ptr(out), self.ptr, out.nbytes), "gg_memcpy_d2h")
+        return out
+
+    def __del__(self):
+        if getattr(self, "ptr", None) and getattr(self.graph, "h", None):
+            lib.gg_vertex_array_free(self.graph.h, self.ptr)
+            self.ptr = None
+
+
+class Graph:
+    """partitioned_graph on the device (gg_graph_build)."""
+
+    def __init__(self, host: HostGraph, partitions=384, balance=BALANCE_EDGE, part_how=PART_DEST, relabel=False,
+                 order=ORDER_HILBERT, tile_vertices=0, tile_edges=0, build_coo=0):
+        self.host = host
+        o = BuildOpts(partitions, balance, part_how, int(relabel), order, tile_vertices, tile_edges, build_coo)
+        h = C.c_void_p()
+        check(lib.gg_graph_build(C.byref(host.c), C.byref(o), C.byref(h)), "gg_graph_build")
+        self.h = h
+        self.n = host.n
+        self.m = host.m
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.gg_graph_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def info(self) -> GraphInfo:
+        i = GraphInfo()
+        check(lib.gg_graph_get_info(self.h, C.byref(i)), "gg_graph_get_info")
+        return i
+
+    def partition_starts(self) -> np.ndarray:
+        P = self.info().num_partitions
+        s = np.zeros(P + 1, np.int64)
+        check(lib.gg_graph_partition_starts(self.h, s.ctypes.data_as(_i64p)), "gg_graph_partition_starts")
+        return s
+
+    def transpose(self):
+        check(lib.gg_graph_transpose(self.h), "gg_graph_transpose")
+
+    # vertexSubset constructors
+    def frontier_single(self, v) -> Frontier:
+        h = C.c_void_p()
+        check(lib.gg_frontier_single(self.h, v, C.byref(h)), "gg_frontier_single")
+        return Frontier(self, h)
+
+    def frontier_all(self) -> Frontier:
+        h = C.c_void_p()
+        check(lib.gg_frontier_all(self.h, C.byref(h)), "gg_frontier_all")
+        return Frontier(self, h)
+
+    def frontier_from_mask(self, mask) -> Frontier:
+        mask = np.ascontiguousarray(mask, np.uint8)
+        h = C.c_void_p()
+        check(lib.gg_frontier_from_mask(self.h, mask.ctypes.data_as(C.POINTER(C.c_uint8)), C.byref(h)),
+              "gg_frontier_from_mask")
+        return Frontier(self, h)
+
+    def frontier_from_list(self, verts) -> Frontier:
+        verts = np.ascontiguousarray(verts, np.uint32)
+        h = C.c_void_p()
+        check(lib.gg_frontier_from_list(self.h, verts.ctypes.data_as(_u32p), len(verts), C.byref(h)),
+              "gg_frontier_from_list")
+        return Frontier(self, h)
+
+    def edge_map(self, frontier: Frontier, functor_id: int, args: C.Structure, threshold=-1, flags=0) -> Frontier:
+        h = C.c_void_p()
+        check(lib.gg_edge_map(self.h, frontier.h, functor_id, C.cast(C.byref(args), C.c_void_p), threshold, flags,
+                              C.byref(h)), "gg_edge_map")
+        return Frontier(self, h)
+
+    def last_edge_map_stats(self) -> EdgeMapStats:
+        s = EdgeMapStats()
+        check(lib.gg_last_edge_map_stats(self.h, C.byref(s)), "gg_last_edge_map_stats")
+        return s
+
+    # applications
+    def bfs(self, start=100):
+        par = np.empty(self.n, np.int32)
+        lev = np.empty(self.n, np.int32)
+        st = RunStats()
+        check(lib.gg_bfs(self.h, start, _ptr(par), _ptr(lev), C.byref(st)), "gg_bfs")
+        return par, lev, _run(st)
+
+    def components(self):
+        ids = np.empty(self.n, np.int32)
+        st = RunStats()
+        check(lib.gg_components(self.h, _ptr(ids), C.byref(st)), "gg_components")
+        return ids, _run(st)
+
+    def pagerank(self, max_iter=10, bit_all=False):
+        r = np.empty(self.n, np.float32)
+        st = RunStats()
+        check(lib.gg_pagerank(self.h, max_iter, int(bit_all), _ptr(r), C.byref(st)), "gg_pagerank")
+        return r, _run(st)
+
+    def pagerank_delta(self):
+        r = np.empty(self.n, np.float32)
+        st = RunStats()
+        check(lib.gg_pagerank_delta(self.h, _ptr(r), C.byref(st)), "gg_pagerank_delta")
+        return r, _run(st)
+
+    def spmv(self, x=None):
+        y = np.empty(self.n, np.float32)
+        st = RunStats()
+        xp = None
+        if x is not None:
+            x = np.ascontiguousarray(x, np.float32)
+            xp = _ptr(x)
+        check(lib.gg_spmv(self.h, xp, _ptr(y), C.byref(st)), "gg_spmv")
+        return y, _run(st)
+
+    def bellman_ford(self, start=100):
+        d = np.empty(self.n, np.int32)
+        st = RunStats()
+        check(lib.gg_bellman_ford(self.h, start, _ptr(d), C.byref(st)), "gg_bellman_ford")
+        return d, _run(st)
+
+    def bc(self, start=100):
+        dep = np.empty(self.n, np.float32)
+        npaths = np.empty(self.n, np.float32)
+        st = RunStats()
+        check(lib.gg_bc(self.h, start, _ptr(dep), _ptr(npaths), C.byref(st)), "gg_bc")
+        return dep, npaths, _run(st)
+
+
+def version() -> str:
+    return lib.gg_version().decode()

@@ -1,0 +1,663 @@
+// C ABI of edgeMap / vertexMap / vertexFilter with the built-in functors, and
+// the applications' Compute() loops (app/*.C) run on the device.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "gg_runtime.cuh"
+
+namespace gg {
+
+// ------------------------------------------------------------- helpers
+struct EventTimer {
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaStream_t s;
+  explicit EventTimer(cudaStream_t st) : s(st) {
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, s);
+  }
+  double stop() {
+    cudaEventRecord(b, s);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms;
+  }
+  ~EventTimer() {
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  }
+};
+
+template <class T>
+__global__ void k_fill(T* a, uint64_t n, T v) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    a[i] = v;
+}
+
+template <class T>
+static int fill(gg_graph_s* g, T* a, uint64_t n, T v) {
+  k_fill<T><<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(a, n, v);
+  GG_CUDA(cudaGetLastError());
+  g->kernels++;
+  return GG_OK;
+}
+
+template <class T>
+static int set_one(gg_graph_s* g, T* a, uint32_t i, T v) {
+  GG_CUDA(cudaMemcpyAsync(a + i, &v, sizeof(T), cudaMemcpyHostToDevice, g->stream));
+  return GG_OK;
+}
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  gg_graph_s* g = nullptr;
+  int alloc(gg_graph_s* gg_, uint64_t n) {
+    g = gg_;
+    GG_CUDA(cudaMallocAsync((void**)&p, sizeof(T) * (n + 4), g->stream));
+    return GG_OK;
+  }
+  ~DevBuf() {
+    if (p) cudaFreeAsync(p, g->stream);
+  }
+};
+
+struct FrontierHold {
+  gg_frontier_s* f = nullptr;
+  ~FrontierHold() { frontier_free(f); }
+  void reset(gg_frontier_s* x) {
+    frontier_free(f);
+    f = x;
+  }
+  gg_frontier_s* release() {
+    gg_frontier_s* x = f;
+    f = nullptr;
+    return x;
+  }
+};
+
+// contrib[s] = val[s] / outdeg(s)   (0 for out-degree 0, never gathered)
+__global__ void k_div_outdeg(uint32_t n, const float* val, const uint32_t* off, float* contrib) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t d = off[i + 1] - off[i];
+    contrib[i] = d ? val[i] / (float)d : 0.0f;
+  }
+}
+
+__device__ __forceinline__ void block_add_double(double v, double* out) {
+  __shared__ double s[32];
+  v = warp_sum(v);
+  if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double x = threadIdx.x < (blockDim.x >> 5) ? s[threadIdx.x] : 0.0;
+    x = warp_sum(x);
+    if (threadIdx.x == 0 && x != 0.0) atomicAdd(out, x);
+  }
+}
+
+// PageRank iteration epilogue (app/PageRank.C:361-371), fused:
+//   vertexMap(F, PR_Vertex_F)            p_next[i] = d*p_next[i] + (1-d)/n, i in F
+//   p_curr[j] = |p_curr[j] - p_next[j]|  for every j, L1 = sum
+//   vertexMap(F, PR_Vertex_Reset)        p_curr[i] = 0, i in F
+// plus the next iteration's contrib[j] = p_next[j]/outdeg(j).
+__global__ void k_pr_epilogue(uint32_t n, int all, const uint32_t* fbits, float* p_curr, float* p_next,
+                              const uint32_t* off, float damping, float added, float* contrib, double* l1) {
+  double acc = 0;
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x) {
+    const bool in = all || test_bit(fbits, (uint32_t)j);
+    float pn = p_next[j];
+    if (in) {
+      pn = damping * pn + added;
+      p_next[j] = pn;
+    }
+    const float diff = fabsf(p_curr[j] - pn);
+    acc += diff;
+    p_curr[j] = in ? 0.0f : diff;
+    const uint32_t d = off[j + 1] - off[j];
+    contrib[j] = d ? pn / (float)d : 0.0f;
+  }
+  block_add_double(acc, l1);
+}
+
+// PageRankDelta round epilogue (app/PageRankDelta.C:158-165): L1 = sum|Delta|,
+// nghSum reset to 0, next round's contrib = Delta/outdeg.
+__global__ void k_prd_epilogue(uint32_t n, const float* delta, float* ngh, const uint32_t* off, float* contrib,
+                               double* l1) {
+  double acc = 0;
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x) {
+    const float dl = delta[j];
+    acc += fabsf(dl);
+    ngh[j] = 0.0f;
+    const uint32_t d = off[j + 1] - off[j];
+    contrib[j] = d ? dl / (float)d : 0.0f;
+  }
+  block_add_double(acc, l1);
+}
+
+__global__ void k_invert(uint32_t n, float* a) {
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x)
+    a[j] = 1.0f / a[j];
+}
+__global__ void k_bc_final(uint32_t n, float* dep, const float* inv) {
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x)
+    dep[j] = (dep[j] - inv[j]) / inv[j];
+}
+
+static int read_red(gg_graph_s* g, double* v) {
+  GG_CUDA(cudaMemcpyAsync(g->ws.h_red, g->ws.d_red, sizeof(double), cudaMemcpyDeviceToHost, g->stream));
+  GG_CUDA(cudaStreamSynchronize(g->stream));
+  *v = g->ws.h_red[0];
+  return GG_OK;
+}
+
+static void fill_stats(gg_run_stats* st, double ms, int rounds, uint64_t trav, int kernels) {
+  if (!st) return;
+  st->ms = ms;
+  st->rounds = rounds;
+  st->edges_traversed = trav;
+  st->kernels = kernels;
+}
+
+template <class T>
+static int to_host(gg_graph_s* g, T* host, const T* dev, uint64_t n) {
+  if (!host) return GG_OK;
+  GG_CUDA(cudaMemcpyAsync(host, dev, sizeof(T) * n, cudaMemcpyDeviceToHost, g->stream));
+  GG_CUDA(cudaStreamSynchronize(g->stream));
+  return GG_OK;
+}
+
+// ================================================================== apps
+// app/BFS.C:77-101
+static int run_bfs(gg_graph_s* g, uint32_t start, int32_t* parents, int32_t* levels, gg_run_stats* st) {
+  const uint32_t n = g->n;
+  g->kernels = 0;
+  DevBuf<int32_t> par, lev;
+  GG_TRY(par.alloc(g, n));
+  GG_TRY(lev.alloc(g, n));
+  EventTimer tm(g->stream);
+  GG_TRY(fill<int32_t>(g, par.p, n, -1));
+  GG_TRY(fill<int32_t>(g, lev.p, n, -1));
+  GG_TRY(set_one<int32_t>(g, par.p, start, (int32_t)start));
+  GG_TRY(set_one<int32_t>(g, lev.p, start, 0));
+  FrontierHold F;
+  GG_TRY(gg_frontier_single(g, start, &F.f));
+  int32_t round = 0;
+  uint64_t trav = 0;
+  while (F.f->dm > 0) {
+    ++round;
+    BfsF f;
+    f.parents = par.p;
+    f.levels = lev.p;
+    f.round = round;
+    trav += F.f->out_edges;
+    gg_frontier_s* out = nullptr;
+    GG_TRY(edge_map(g, F.f, f, (int64_t)g->m / 20, 0, &out));
+    F.reset(out);
+  }
+  const double ms = tm.stop();
+  GG_TRY(to_host(g, parents, par.p, n));
+  GG_TRY(to_host(g, levels, lev.p, n));
+  fill_stats(st, ms, round, trav, g->kernels);
+  return GG_OK;
+}
+
+// app/Components.C:202-227
+static int run_cc(gg_graph_s* g, int32_t* ids_out, gg_run_stats* st) {
+  const uint32_t n = g->n;
+  g->kernels = 0;
+  DevBuf<int32_t> ids, prev;
+  GG_TRY(ids.alloc(g, n));
+  GG_TRY(prev.alloc(g, n));
+  EventTimer tm(g->stream);
+  k_iota<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>((uint32_t*)ids.p, n);
+  FrontierHold F;
+  GG_TRY(gg_frontier_all(g, &F.f));
+  int rounds = 0;
+  uint64_t trav = 0;
+  while (F.f->dm > 0) {
+    VCcCopy vc{ids.p, prev.p};
+    GG_TRY(vertex_map(g, F.f, vc));
+    CcF f;
+    f.ids = ids.p;
+    f.prev = prev.p;
+    trav += F.f->out_edges;
+    gg_frontier_s* out = nullptr;
+    GG_TRY(edge_map(g, F.f, f, (int64_t)g->m / 20, 0, &out));
+    F.reset(out);
+    ++rounds;
+  }
+  const double ms = tm.stop();
+  GG_TRY(to_host(g, ids_out, ids.p, n));
+  fill_stats(st, ms, rounds, trav, g->kernels);
+  return GG_OK;
+}
+
+// app/PageRank.C:330-378 (bit_all: app/PageRankBit.C:145)
+static int run_pagerank(gg_graph_s* g, int max_iter, int bit_all, float* ranks, gg_run_stats* st,
+                        const float* x_dev_init = nullptr) {
+  const uint32_t n = g->n;
+  g->kernels = 0;
+  DevBuf<float> a, b, contrib;
+  GG_TRY(a.alloc(g, n));
+  GG_TRY(b.alloc(g, n));
+  GG_TRY(contrib.alloc(g, n));
+  const float damping = 0.85f;
+  const float added = (float)((1 - 0.85) * (1 / (double)n));
+  const double eps = 0.0000001;
+  EventTimer tm(g->stream);
+  float* p_curr = a.p;
+  float* p_next = b.p;
+  if (x_dev_init) GG_CUDA(cudaMemcpyAsync(p_curr, x_dev_init, 4ull * n, cudaMemcpyDeviceToDevice, g->stream));
+  else GG_TRY(fill<float>(g, p_curr, n, (float)(1 / (double)n)));
+  GG_TRY(fill<float>(g, p_next, n, 0.0f));
+  k_div_outdeg<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(n, p_curr, g->out_off(), contrib.p);
+  g->kernels++;
+  FrontierHold F;
+  GG_TRY(gg_frontier_all(g, &F.f));
+  int count = 0;
+  uint64_t trav = 0;
+  float* last = p_next;
+  while (count < max_iter) {
+    ++count;
+    PrF f;
+    f.contrib = contrib.p;
+    f.acc_out = p_next;
+    trav += F.f->out_edges;
+    gg_frontier_s* out = nullptr;
+    GG_TRY(edge_map(g, F.f, f, (int64_t)g->m / 20, 0, &out));
+    FrontierHold O;
+    O.f = out;
+    if (!F.f->bit && !F.f->has_dense) GG_TRY(frontier_to_dense(F.f));
+    GG_CUDA(cudaMemsetAsync(g->ws.d_red, 0, sizeof(double), g->stream));
+    k_pr_epilogue<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(
+        n, F.f->bit ? 1 : 0, F.f->d_bits, p_curr, p_next, g->out_off(), damping, added, contrib.p, g->ws.d_red);
+    GG_CUDA(cudaGetLastError());
+    g->kernels++;
+    last = p_next;
+    double l1;
+    GG_TRY(read_red(g, &l1));
+    if (l1 < eps) break;
+    std::swap(p_curr, p_next);
+    gg_frontier_s* o = O.release();
+    if (bit_all) o->bit = true;  // output.bit = true
+    F.reset(o);
+  }
+  const double ms = tm.stop();
+  GG_TRY(to_host(g, ranks, last, n));
+  fill_stats(st, ms, count, trav, g->kernels);
+  return GG_OK;
+}
+
+// app/PageRankDelta.C:120-174
+static int run_pagerank_delta(gg_graph_s* g, float* ranks, gg_run_stats* st) {
+  const uint32_t n = g->n;
+  g->kernels = 0;
+  DevBuf<float> p, delta, ngh, contrib;
+  GG_TRY(p.alloc(g, n));
+  GG_TRY(delta.alloc(g, n));
+  GG_TRY(ngh.alloc(g, n));
+  GG_TRY(contrib.alloc(g, n));
+  const float damping = 0.85f, eps2 = 0.01f;
+  const double eps = 0.0000001;
+  const float one_over_n = (float)(1 / (double)n);
+  const float added = (float)((1 - 0.85) * (1 / (double)n));
+  EventTimer tm(g->stream);
+  GG_TRY(fill<float>(g, p.p, n, 0.0f));
+  GG_TRY(fill<float>(g, delta.p, n, one_over_n));
+  GG_TRY(fill<float>(g, ngh.p, n, 0.0f));
+  k_div_outdeg<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(n, delta.p, g->out_off(), contrib.p);
+  g->kernels++;
+  FrontierHold F, All;
+  GG_TRY(gg_frontier_all(g, &F.f));
+  GG_TRY(gg_frontier_all(g, &All.f));
+  int round = 0;
+  uint64_t trav = 0;
+  for (;;) {
+    ++round;
+    PrF f;
+    f.contrib = contrib.p;
+    f.acc_out = ngh.p;
+    trav += F.f->out_edges;
+    gg_frontier_s* out = nullptr;
+    GG_TRY(edge_map(g, F.f, f, (int64_t)g->m / 20, 0, &out));
+    frontier_free(out);
+    gg_frontier_s* active = nullptr;
+    if (round == 1) {
+      VPrdFirst vf{p.p, delta.p, ngh.p, damping, added, one_over_n, eps2};
+      GG_TRY(vertex_filter(g, All.f, vf, &active));
+    } else {
+      VPrd vf{p.p, delta.p, ngh.p, damping, eps2};
+      GG_TRY(vertex_filter(g, All.f, vf, &active));
+    }
+    FrontierHold A;
+    A.f = active;
+    GG_CUDA(cudaMemsetAsync(g->ws.d_red, 0, sizeof(double), g->stream));
+    k_prd_epilogue<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(n, delta.p, ngh.p, g->out_off(),
+                                                                          contrib.p, g->ws.d_red);
+    GG_CUDA(cudaGetLastError());
+    g->kernels++;
+    double l1;
+    GG_TRY(read_red(g, &l1));
+    if (l1 < eps) break;
+    F.reset(A.release());
+  }
+  const double ms = tm.stop();
+  GG_TRY(to_host(g, ranks, p.p, n));
+  fill_stats(st, ms, round, trav, g->kernels);
+  return GG_OK;
+}
+
+// app/SPMV.C:65-93
+static int run_spmv(gg_graph_s* g, const float* x_in, float* y_out, gg_run_stats* st) {
+  const uint32_t n = g->n;
+  g->kernels = 0;
+  DevBuf<float> x, y;
+  GG_TRY(x.alloc(g, n));
+  GG_TRY(y.alloc(g, n));
+  EventTimer tm(g->stream);
+  if (x_in) GG_CUDA(cudaMemcpyAsync(x.p, x_in, 4ull * n, cudaMemcpyHostToDevice, g->stream));
+  else GG_TRY(fill<float>(g, x.p, n, (float)(1 / (double)n)));
+  GG_TRY(fill<float>(g, y.p, n, 0.0f));
+  FrontierHold F;
+  GG_TRY(gg_frontier_all(g, &F.f));
+  SpmvF f;
+  f.x = x.p;
+  f.y = y.p;
+  f.float_w = g->wtype == GG_W_FLOAT32;
+  gg_frontier_s* out = nullptr;
+  GG_TRY(edge_map(g, F.f, f, (int64_t)g->m / 20, 0, &out));
+  frontier_free(out);
+  const double ms = tm.stop();
+  GG_TRY(to_host(g, y_out, y.p, n));
+  fill_stats(st, ms, 1, g->m, g->kernels);
+  return GG_OK;
+}
+
+// app/BellmanFord.C:106-145
+static int run_bf(gg_graph_s* g, uint32_t start, int32_t* dist, gg_run_stats* st) {
+  const uint32_t n = g->n;
+  g->kernels = 0;
+  DevBuf<int32_t> sp, vis;
+  GG_TRY(sp.alloc(g, n));
+  GG_TRY(vis.alloc(g, n));
+  const int32_t inf = 2147483647 / 2;
+  EventTimer tm(g->stream);
+  GG_TRY(fill<int32_t>(g, sp.p, n, inf));
+  GG_TRY(set_one<int32_t>(g, sp.p, start, 0));
+  GG_TRY(fill<int32_t>(g, vis.p, n, 0));
+  FrontierHold F;
+  GG_TRY(gg_frontier_single(g, start, &F.f));
+  int64_t round = 0;
+  uint64_t trav = 0;
+  while (F.f->dm > 0) {
+    if (round == (int64_t)n) {  // negative weight cycle
+      GG_TRY(fill<int32_t>(g, sp.p, n, -inf));
+      break;
+    }
+    BfF f;
+    f.sp = sp.p;
+    f.visited = vis.p;
+    trav += F.f->out_edges;
+    gg_frontier_s* out = nullptr;
+    GG_TRY(edge_map(g, F.f, f, (int64_t)g->m / 20, 0, &out));
+    VFill<int32_t> vf{vis.p, 0};
+    GG_TRY(vertex_map(g, out, vf));
+    F.reset(out);
+    ++round;
+  }
+  const double ms = tm.stop();
+  GG_TRY(to_host(g, dist, sp.p, n));
+  fill_stats(st, ms, (int)round, trav, g->kernels);
+  return GG_OK;
+}
+
+// app/BC.C:156-226 (single source, FP32 like fType)
+static int run_bc(gg_graph_s* g, uint32_t start, float* dep_out, float* np_out, gg_run_stats* st) {
+  const uint32_t n = g->n;
+  g->kernels = 0;
+  DevBuf<float> np, dep;
+  DevBuf<uint8_t> vis;
+  GG_TRY(np.alloc(g, n));
+  GG_TRY(dep.alloc(g, n));
+  GG_TRY(vis.alloc(g, n));
+  EventTimer tm(g->stream);
+  GG_TRY(fill<float>(g, np.p, n, 0.0f));
+  GG_TRY(fill<uint8_t>(g, vis.p, n, 0));
+  GG_TRY(set_one<float>(g, np.p, start, 1.0f));
+  GG_TRY(set_one<uint8_t>(g, vis.p, start, 1));
+  std::vector<gg_frontier_s*> levels;
+  struct LevelsHold {
+    std::vector<gg_frontier_s*>* v;
+    ~LevelsHold() {
+      for (auto* f : *v) frontier_free(f);
+    }
+  } lh{&levels};
+  gg_frontier_s* F0 = nullptr;
+  GG_TRY(gg_frontier_single(g, start, &F0));
+  levels.push_back(F0);
+  int round = 0;
+  uint64_t trav = 0;
+  gg_frontier_s* F = F0;
+  while (F->dm > 0) {
+    ++round;
+    BcF f;
+    f.values = np.p;
+    f.visited = vis.p;
+    trav += F->out_edges;
+    gg_frontier_s* out = nullptr;
+    GG_TRY(edge_map(g, F, f, (int64_t)g->m / 20, 0, &out));
+    VBcMark vm{vis.p};
+    GG_TRY(vertex_map(g, out, vm));
+    levels.push_back(out);
+    F = out;
+  }
+  if (np_out) GG_TRY(to_host(g, np_out, np.p, n));
+  GG_TRY(fill<float>(g, dep.p, n, 0.0f));
+  k_invert<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(n, np.p);  // inverseNumPaths aliases NumPaths
+  g->kernels++;
+  GG_TRY(fill<uint8_t>(g, vis.p, n, 0));
+  F = levels[round - 1];
+  VBcBack vb{vis.p, dep.p, np.p};
+  GG_TRY(vertex_map(g, F, vb));
+  GG_TRY(gg_graph_transpose(g));
+  int rc = GG_OK;
+  for (int r = round - 2; r >= 0 && !rc; --r) {
+    BcF f;
+    f.values = dep.p;
+    f.visited = vis.p;
+    trav += F->out_edges;
+    gg_frontier_s* out = nullptr;
+    rc = edge_map(g, F, f, (int64_t)g->m / 20, 0, &out);
+    if (rc) break;
+    frontier_free(out);
+    F = levels[r];
+    rc = vertex_map(g, F, vb);
+  }
+  gg_graph_transpose(g);
+  if (rc) return rc;
+  k_bc_final<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(n, dep.p, np.p);
+  g->kernels++;
+  const double ms = tm.stop();
+  GG_TRY(to_host(g, dep_out, dep.p, n));
+  fill_stats(st, ms, round, trav, g->kernels);
+  return GG_OK;
+}
+
+}  // namespace gg
+
+using namespace gg;
+
+extern "C" {
+
+int gg_edge_map(gg_graph_t g, gg_frontier_t in, int32_t fid, const void* args, int64_t threshold, uint32_t flags,
+                gg_frontier_t* out) {
+  if (!g || !in || !out || !args || in->g != g) return fail(GG_ERR_INVALID_ARG, "gg_edge_map: bad arguments");
+  switch (fid) {
+    case GG_F_BFS: {
+      const gg_bfs_args* a = (const gg_bfs_args*)args;
+      BfsF f;
+      f.parents = a->parents;
+      f.levels = a->levels;
+      f.round = a->round;
+      return edge_map(g, in, f, threshold, flags, out);
+    }
+    case GG_F_CC: {
+      const gg_cc_args* a = (const gg_cc_args*)args;
+      CcF f;
+      f.ids = a->ids;
+      f.prev = a->prev_ids;
+      return edge_map(g, in, f, threshold, flags, out);
+    }
+    case GG_F_PR:
+    case GG_F_PRDELTA: {
+      const float* src;
+      float* acc;
+      if (fid == GG_F_PR) {
+        src = ((const gg_pr_args*)args)->p_curr;
+        acc = ((const gg_pr_args*)args)->p_next;
+      } else {
+        src = ((const gg_prdelta_args*)args)->delta;
+        acc = ((const gg_prdelta_args*)args)->ngh_sum;
+      }
+      DevBuf<float> contrib;
+      GG_TRY(contrib.alloc(g, g->n));
+      k_div_outdeg<<<generic_grid(g, g->n), kGenericThreads, 0, g->stream>>>(g->n, src, g->out_off(), contrib.p);
+      PrF f;
+      f.contrib = contrib.p;
+      f.acc_out = acc;
+      return edge_map(g, in, f, threshold, flags, out);
+    }
+    case GG_F_SPMV: {
+      const gg_spmv_args* a = (const gg_spmv_args*)args;
+      SpmvF f;
+      f.x = a->p_curr;
+      f.y = a->p_next;
+      f.float_w = g->wtype == GG_W_FLOAT32;
+      return edge_map(g, in, f, threshold, flags, out);
+    }
+    case GG_F_BF: {
+      const gg_bf_args* a = (const gg_bf_args*)args;
+      BfF f;
+      f.sp = a->sp_len;
+      f.visited = a->visited;
+      return edge_map(g, in, f, threshold, flags, out);
+    }
+    case GG_F_BC:
+    case GG_F_BC_BACK: {
+      const gg_bc_args* a = (const gg_bc_args*)args;
+      BcF f;
+      f.values = a->values;
+      f.visited = a->visited;
+      return edge_map(g, in, f, threshold, flags, out);
+    }
+    default:
+      return fail(GG_ERR_UNSUPPORTED, "gg_edge_map: unknown functor id %d", fid);
+  }
+}
+
+int gg_last_edge_map_stats(gg_graph_t g, gg_edge_map_stats* st) {
+  if (!g || !st) return fail(GG_ERR_INVALID_ARG, "gg_last_edge_map_stats: bad arguments");
+  *st = g->last;
+  return GG_OK;
+}
+
+int gg_vertex_map(gg_graph_t g, gg_frontier_t f, int32_t vid, const void* args) {
+  if (!g || !f || !args || f->g != g) return fail(GG_ERR_INVALID_ARG, "gg_vertex_map: bad arguments");
+  int rc;
+  switch (vid) {
+    case GG_V_CC_COPY: {
+      const gg_cc_args* a = (const gg_cc_args*)args;
+      rc = vertex_map(g, f, VCcCopy{a->ids, a->prev_ids});
+      break;
+    }
+    case GG_V_PR_UPDATE: {
+      const gg_pr_vertex_args* a = (const gg_pr_vertex_args*)args;
+      const float added = (float)((1 - (double)a->damping) * (1 / (double)a->n));
+      rc = vertex_map(g, f, VPrUpdate{a->p_next, a->damping, added});
+      break;
+    }
+    case GG_V_FILL_F32: {
+      const gg_fill_args* a = (const gg_fill_args*)args;
+      rc = vertex_map(g, f, VFill<float>{(float*)a->array, (float)a->value});
+      break;
+    }
+    case GG_V_FILL_I32: {
+      const gg_fill_args* a = (const gg_fill_args*)args;
+      rc = vertex_map(g, f, VFill<int32_t>{(int32_t*)a->array, (int32_t)a->value});
+      break;
+    }
+    case GG_V_FILL_U8: {
+      const gg_fill_args* a = (const gg_fill_args*)args;
+      rc = vertex_map(g, f, VFill<uint8_t>{(uint8_t*)a->array, (uint8_t)a->value});
+      break;
+    }
+    case GG_V_BC_MARK: {
+      const gg_bc_args* a = (const gg_bc_args*)args;
+      rc = vertex_map(g, f, VBcMark{a->visited});
+      break;
+    }
+    case GG_V_BC_BACK: {
+      const gg_bc_back_vertex_args* a = (const gg_bc_back_vertex_args*)args;
+      rc = vertex_map(g, f, VBcBack{a->visited, a->dependencies, a->inv_num_paths});
+      break;
+    }
+    default:
+      return fail(GG_ERR_UNSUPPORTED, "gg_vertex_map: unknown vertex functor id %d", vid);
+  }
+  if (rc) return rc;
+  GG_CUDA(cudaStreamSynchronize(g->stream));
+  return GG_OK;
+}
+
+int gg_vertex_filter(gg_graph_t g, gg_frontier_t f, int32_t vid, const void* args, gg_frontier_t* out) {
+  if (!g || !f || !args || !out || f->g != g) return fail(GG_ERR_INVALID_ARG, "gg_vertex_filter: bad arguments");
+  const gg_prdelta_vertex_args* a = (const gg_prdelta_vertex_args*)args;
+  switch (vid) {
+    case GG_V_PRDELTA_FIRST: {
+      const float added = (float)((1 - (double)a->damping) * (double)a->one_over_n);
+      return vertex_filter(g, f, VPrdFirst{a->p, a->delta, a->ngh_sum, a->damping, added, a->one_over_n, a->epsilon2},
+                           out);
+    }
+    case GG_V_PRDELTA:
+      return vertex_filter(g, f, VPrd{a->p, a->delta, a->ngh_sum, a->damping, a->epsilon2}, out);
+    default:
+      return fail(GG_ERR_UNSUPPORTED, "gg_vertex_filter: unknown filter id %d", vid);
+  }
+}
+
+int gg_bfs(gg_graph_t g, uint32_t start, int32_t* parents, int32_t* levels, gg_run_stats* st) {
+  if (!g || start >= g->n) return fail(GG_ERR_INVALID_ARG, "gg_bfs: bad arguments");
+  return run_bfs(g, start, parents, levels, st);
+}
+int gg_components(gg_graph_t g, int32_t* ids, gg_run_stats* st) {
+  if (!g) return fail(GG_ERR_INVALID_ARG, "gg_components: null graph");
+  return run_cc(g, ids, st);
+}
+int gg_pagerank(gg_graph_t g, int32_t max_iter, int32_t bit_all, float* ranks, gg_run_stats* st) {
+  if (!g || max_iter < 1) return fail(GG_ERR_INVALID_ARG, "gg_pagerank: bad arguments");
+  return run_pagerank(g, max_iter, bit_all, ranks, st);
+}
+int gg_pagerank_delta(gg_graph_t g, float* ranks, gg_run_stats* st) {
+  if (!g) return fail(GG_ERR_INVALID_ARG, "gg_pagerank_delta: null graph");
+  return run_pagerank_delta(g, ranks, st);
+}
+int gg_spmv(gg_graph_t g, const float* x, float* y, gg_run_stats* st) {
+  if (!g) return fail(GG_ERR_INVALID_ARG, "gg_spmv: null graph");
+  return run_spmv(g, x, y, st);
+}
+int gg_bellman_ford(gg_graph_t g, uint32_t start, int32_t* dist, gg_run_stats* st) {
+  if (!g || start >= g->n) return fail(GG_ERR_INVALID_ARG, "gg_bellman_ford: bad arguments");
+  return run_bf(g, start, dist, st);
+}
+int gg_bc(gg_graph_t g, uint32_t start, float* dep, float* np, gg_run_stats* st) {
+  if (!g || start >= g->n) return fail(GG_ERR_INVALID_ARG, "gg_bc: bad arguments");
+  return run_bc(g, start, dep, np, st);
+}
+int gg_bp(gg_graph_t, int32_t, const float*, const float*, float*, gg_run_stats*) {
+  return fail(GG_ERR_UNSUPPORTED, "gg_bp: not built yet");
+}
+
+}  // extern "C"

@@ -1,0 +1,680 @@
+// Traversal engine for B200 (sm_100a): graph / vertexSubset state and the
+// kernels behind edgeMap, vertexMap and vertexFilter.
+//
+//   k_pull      dense pull over CTA-owned destination tiles (CSC or the
+//               partitioned COO): edges stream into shared memory by bulk
+//               copies (cp.async.bulk + mbarrier ring), contributions reduce
+//               into per-tile shared-memory accumulators, each destination is
+//               committed once.  No global atomics on vertex values: the GPU
+//               form of PART96's "one owner per destination range"
+//               (graphgrind/ligra-numa.h:558-562, 810-832).
+//   k_pull_early  dense pull for functors whose cond() turns false after one
+//               successful update (BFS): one thread per destination stops at
+//               the first frontier in-neighbour, as edgeMapDenseCSC's break
+//               (graphgrind/ligra-numa.h:621-626).
+//   k_push      sparse push over CSR (edgeMapSparseWithG, :868-916): the
+//               frontier's degrees are prefix-summed, every thread takes
+//               edges of the scanned range (load-balanced search), applies
+//               cond && updateAtomic, and appends winners to a bitmap-
+//               de-duplicated queue with warp-aggregated atomics.
+//   k_bits_to_queue / k_queue_to_bits  vertexSubset conversion (toSparse
+//               :246 by ballot/popc compaction, toDense :228).
+//   k_vertex_map / k_vertex_filter      vertexMap :1023, vertexFilter :1053.
+//
+// Device functor protocol (the reference's update/updateAtomic/cond and
+// functor-cache protocol, :364-543, in reduction form):
+//   using value_t;                       32-bit contribution type
+//   static constexpr bool kEarlyExit;    cond(d) is false after one update
+//   bool    cond(d)                      = F::cond
+//   value_t gather(s, w)                 contribution of source s (the read
+//                                        half of update(cache, s[, w]))
+//   static value_t identity(), combine(a, b), atomic_combine(smem*, v)
+//   bool    commit(d, acc)               create_cache + updates + commit_cache:
+//                                        applies the reduced contribution,
+//                                        returns "d joins the output"
+//   bool    update_atomic(s, d, w)       = F::updateAtomic (push)
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "gg_common.h"
+#include "gg_device.cuh"
+
+#define GG_CUDA(call)                                                                       \
+  do {                                                                                      \
+    cudaError_t e__ = (call);                                                               \
+    if (e__ != cudaSuccess)                                                                 \
+      return ::gg::fail(GG_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call,            \
+                        cudaGetErrorString(e__));                                           \
+  } while (0)
+
+#define GG_TRY(expr)          \
+  do {                        \
+    int r__ = (expr);         \
+    if (r__ != GG_OK) return r__; \
+  } while (0)
+
+namespace gg {
+
+// ------------------------------------------------------------ constants
+constexpr int kPullThreads = 256;
+constexpr int kPullK = 8;                                   // edges per thread per chunk
+constexpr int kPullSlots = kPullThreads * kPullK;           // 2048 stage slots
+constexpr int kPullChunk = kPullSlots - 8;                  // edges per chunk (8-aligned slack)
+constexpr int kPullStages = 3;
+constexpr int kMaxTileVertices = 4096;
+constexpr uint32_t kPad = 0xffffffffu;                      // COO padding source id
+
+constexpr int kPushThreads = 256;
+constexpr int kPushEdgesPerCta = 4096;
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;        // 2048 queue entries per block
+
+// -------------------------------------------------------- graph state
+struct TileSet {
+  uint4* d_tiles = nullptr;   // {v0, nv, e0, ne}, ordered by ne descending
+  uint32_t count = 0;
+  std::vector<uint4> host;
+};
+
+struct Workspace {
+  unsigned long long* d_stats = nullptr;  // [0] count [1] outdeg [2] queue len [3] err [4] tile ctr [5] total edges
+  unsigned long long* h_stats = nullptr;  // pinned mirror
+  uint32_t* d_dedup = nullptr;            // n bits, zero between calls
+  uint32_t* d_scan = nullptr;             // n+1 offsets of the push scan
+  uint32_t* d_bsum = nullptr;             // per-block sums of the scan
+  uint32_t bsum_cap = 0;
+  double* d_red = nullptr;                // reduction scratch (double)
+  double* h_red = nullptr;                // pinned
+};
+
+}  // namespace gg
+
+struct gg_graph_s {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int num_sms = 148;
+  uint32_t n = 0;
+  uint64_t m = 0;
+  bool symmetric = false;
+  int wtype = GG_W_NONE;
+  gg_build_opts opts{};
+  std::vector<int64_t> coo_sizes, coo_starts, csc_sizes, csc_starts;
+  // device CSR / CSC of the ORIGINAL orientation
+  uint32_t *d_csr_off = nullptr, *d_csr_idx = nullptr, *d_csr_w = nullptr;
+  uint32_t *d_csc_off = nullptr, *d_csc_idx = nullptr, *d_csc_w = nullptr;
+  std::vector<uint32_t> h_csr_off, h_csc_off;  // host copies of the offsets
+  gg::TileSet csc_tiles[2];  // [0]: pull over CSC (in-edges); [1]: transposed (pull over CSR)
+  gg::TileSet coo_tiles;
+  bool has_coo = false;
+  uint32_t *d_coo_src = nullptr, *d_coo_w = nullptr;
+  uint16_t* d_coo_dloc = nullptr;
+  uint64_t coo_len = 0;
+  bool transposed = false;
+  gg::Workspace ws;
+  gg_edge_map_stats last{};
+  uint64_t device_bytes = 0;
+  int kernels = 0;  // kernels launched since the counter was last reset
+  // current orientation views
+  const uint32_t* out_off() const { return transposed ? d_csc_off : d_csr_off; }
+  const uint32_t* out_idx() const { return transposed ? d_csc_idx : d_csr_idx; }
+  const uint32_t* out_w() const { return transposed ? d_csc_w : d_csr_w; }
+  const uint32_t* in_off() const { return transposed ? d_csr_off : d_csc_off; }
+  const uint32_t* in_idx() const { return transposed ? d_csr_idx : d_csc_idx; }
+  const uint32_t* in_w() const { return transposed ? d_csr_w : d_csc_w; }
+  const uint32_t* h_out_off() const { return transposed ? h_csc_off.data() : h_csr_off.data(); }
+  uint32_t words() const { return (n + 31) / 32; }
+};
+
+struct gg_frontier_s {
+  gg_graph_s* g = nullptr;
+  uint32_t n = 0;
+  bool bit = false;         // "all vertices active" (partitioned_vertices::bit)
+  bool has_dense = false;
+  bool has_sparse = false;
+  uint32_t* d_bits = nullptr;   // words()+4
+  uint32_t* d_queue = nullptr;  // n+4
+  uint64_t dm = 0;              // d_m
+  uint64_t out_edges = 0;       // num_out_edges
+};
+
+namespace gg {
+
+// ===================================================== kernel parameters
+struct PullParams {
+  const uint4* tiles;
+  uint32_t ntiles;
+  unsigned long long* tile_counter;
+  const uint32_t* src;      // CSC in-neighbour ids or COO sources
+  const uint16_t* dloc;     // COO destination offsets inside the tile
+  const uint32_t* wts;      // weights aligned with src (raw 32-bit)
+  const uint32_t* off;      // CSC offsets (absolute), CSC layout only
+  const uint32_t* fr_bits;  // frontier bitmap (unused when all active)
+  uint32_t* next_bits;      // output bitmap, zeroed by the caller
+  const uint32_t* deg_off;  // out-offsets of the current orientation (stats)
+  const uint32_t* member_off;  // original in-offsets: compressed-CSC membership, or null
+  unsigned long long* stats;   // [0] count [1] out-degree sum
+  unsigned long long* err;
+};
+
+__host__ __device__ constexpr size_t pull_smem_bytes(bool coo, bool hw, int vbytes) {
+  return 128                                                       // mbarriers
+         + (size_t)kPullStages * kPullSlots * 4                     // src
+         + (hw ? (size_t)kPullStages * kPullSlots * 4 : 0)          // weights
+         + (coo ? (size_t)kPullStages * kPullSlots * 2 : 0)         // dloc
+         + (size_t)kMaxTileVertices * vbytes                         // accumulators
+         + (coo ? 0 : (size_t)(kMaxTileVertices + 4) * 4)           // tile offsets
+         + (size_t)kMaxTileVertices * 2;                             // touched + cond flags
+}
+
+// One CTA per tile at a time; CTAs pull tiles from a global ticket counter
+// (tiles are ordered by edge count, largest first).
+template <class F, bool COO, bool HW, bool ALL>
+__global__ void __launch_bounds__(kPullThreads) k_pull(const PullParams p, const F f) {
+  using V = typename F::value_t;
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
+  uint32_t* s_src = reinterpret_cast<uint32_t*>(smem + 128);
+  uint32_t* s_w = s_src + kPullStages * kPullSlots;
+  uint16_t* s_dl = reinterpret_cast<uint16_t*>(s_w + (HW ? kPullStages * kPullSlots : 0));
+  V* s_acc = reinterpret_cast<V*>(s_dl + (COO ? kPullStages * kPullSlots : 0));
+  uint32_t* s_off = reinterpret_cast<uint32_t*>(s_acc + kMaxTileVertices);
+  uint8_t* s_touch = reinterpret_cast<uint8_t*>(s_off + (COO ? 0 : kMaxTileVertices + 4));
+  uint8_t* s_cond = s_touch + kMaxTileVertices;
+  __shared__ uint32_t s_tile;
+  __shared__ unsigned long long s_red[2][kPullThreads / 32];
+  __shared__ int s_fail;
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) {
+    for (int s = 0; s < kPullStages; ++s) mbar_init(&bars[s], 1);
+    fence_mbar_init();
+    s_fail = 0;
+  }
+  __syncthreads();
+  uint32_t parity = 0;  // bit s: parity of the next wait on stage s
+  unsigned long long my_cnt = 0, my_deg = 0;
+
+  for (;;) {
+    if (tid == 0) s_tile = (uint32_t)atomicAdd(p.tile_counter, 1ull);
+    __syncthreads();
+    const uint32_t t = s_tile;
+    if (t >= p.ntiles || s_fail) break;
+    const uint4 td = p.tiles[t];
+    const uint32_t v0 = td.x, nv = td.y, e0 = td.z, ne = td.w;
+    const uint32_t nchunks = (ne + kPullChunk - 1) / kPullChunk;
+
+    auto issue = [&](uint32_t c, int st) {
+      const uint32_t cs = e0 + c * kPullChunk;
+      const uint32_t ce = min(e0 + ne, cs + kPullChunk);
+      const uint32_t ca = cs & ~7u, cb = (ce + 7u) & ~7u;
+      const uint32_t nel = cb - ca;
+      const uint32_t bytes = nel * 4u * (HW ? 2u : 1u) + (COO ? nel * 2u : 0u);
+      mbar_arrive_expect_tx(&bars[st], bytes);
+      bulk_g2s(s_src + st * kPullSlots, p.src + ca, nel * 4u, &bars[st]);
+      if (HW) bulk_g2s(s_w + st * kPullSlots, p.wts + ca, nel * 4u, &bars[st]);
+      if (COO) bulk_g2s(s_dl + st * kPullSlots, p.dloc + ca, nel * 2u, &bars[st]);
+    };
+    if (tid == 0) {
+      for (uint32_t c = 0; c < nchunks && c < (uint32_t)kPullStages; ++c) issue(c, (int)c);
+    }
+    for (uint32_t i = tid; i < nv; i += kPullThreads) {
+      const uint32_t v = v0 + i;
+      s_acc[i] = F::identity();
+      s_touch[i] = 0;
+      bool c = f.cond(v);
+      if (p.member_off) c = c && (__ldg(p.member_off + v + 1) > __ldg(p.member_off + v));
+      s_cond[i] = c ? 1 : 0;
+      if (!COO) s_off[i] = __ldg(p.off + v);
+    }
+    if (!COO && tid == 0) s_off[nv] = __ldg(p.off + v0 + nv);
+    __syncthreads();
+
+    for (uint32_t c = 0; c < nchunks; ++c) {
+      const int st = (int)(c % kPullStages);
+      if (!mbar_wait_bounded(&bars[st], (parity >> st) & 1u)) {
+        atomicOr(p.err, (unsigned long long)DEV_ERR_TIMEOUT);
+        s_fail = 1;
+      }
+      parity ^= 1u << st;
+      const uint32_t cs = e0 + c * kPullChunk;
+      const uint32_t ce = min(e0 + ne, cs + kPullChunk);
+      const uint32_t ca = cs & ~7u;
+      // this thread's 8 stage slots: positions ca + 8*tid .. +7
+      const uint32_t pos0 = ca + (uint32_t)tid * kPullK;
+      const uint32_t* ssrc = s_src + st * kPullSlots + tid * kPullK;
+      uint32_t sv[kPullK], wv[kPullK];
+      uint16_t dv[kPullK];
+      {
+        const uint4 a = reinterpret_cast<const uint4*>(ssrc)[0];
+        const uint4 b = reinterpret_cast<const uint4*>(ssrc)[1];
+        sv[0] = a.x; sv[1] = a.y; sv[2] = a.z; sv[3] = a.w;
+        sv[4] = b.x; sv[5] = b.y; sv[6] = b.z; sv[7] = b.w;
+      }
+      if (HW) {
+        const uint32_t* sw = s_w + st * kPullSlots + tid * kPullK;
+        const uint4 a = reinterpret_cast<const uint4*>(sw)[0];
+        const uint4 b = reinterpret_cast<const uint4*>(sw)[1];
+        wv[0] = a.x; wv[1] = a.y; wv[2] = a.z; wv[3] = a.w;
+        wv[4] = b.x; wv[5] = b.y; wv[6] = b.z; wv[7] = b.w;
+      } else {
+#pragma unroll
+        for (int k = 0; k < kPullK; ++k) wv[k] = 1u;
+      }
+      if (COO) {
+        const uint4 a = reinterpret_cast<const uint4*>(s_dl + st * kPullSlots + tid * kPullK)[0];
+        dv[0] = a.x & 0xffff; dv[1] = a.x >> 16; dv[2] = a.y & 0xffff; dv[3] = a.y >> 16;
+        dv[4] = a.z & 0xffff; dv[5] = a.z >> 16; dv[6] = a.w & 0xffff; dv[7] = a.w >> 16;
+      }
+      int cur = -1;
+      V acc = F::identity();
+      uint32_t li = 0;
+      if (!COO && pos0 + kPullK > cs && pos0 < ce) {
+        // last tile-local vertex whose offset is <= max(pos0, cs)
+        const uint32_t key = max(pos0, cs);
+        uint32_t lo = 0, hi = nv;  // invariant: s_off[lo] <= key < s_off[hi]
+        while (hi - lo > 1) {
+          const uint32_t mid = (lo + hi) >> 1;
+          if (s_off[mid] <= key) lo = mid; else hi = mid;
+        }
+        li = lo;
+      }
+#pragma unroll
+      for (int k = 0; k < kPullK; ++k) {
+        const uint32_t pos = pos0 + k;
+        if (pos < cs || pos >= ce) continue;
+        const uint32_t s = sv[k];
+        uint32_t l;
+        if (COO) {
+          if (s == kPad) continue;
+          l = dv[k];
+        } else {
+          while (s_off[li + 1] <= pos) ++li;
+          l = li;
+        }
+        if (!s_cond[l]) continue;
+        if (!ALL && !test_bit(p.fr_bits, s)) continue;
+        const V val = f.gather(s, wv[k]);
+        if ((int)l != cur) {
+          if (cur >= 0) {
+            F::atomic_combine(&s_acc[cur], acc);
+            s_touch[cur] = 1;
+          }
+          cur = (int)l;
+          acc = val;
+        } else {
+          acc = F::combine(acc, val);
+        }
+      }
+      // final run: warp-aggregate when the whole warp ends on one destination
+      const int c0 = __shfl_sync(0xffffffffu, cur, 0);
+      if (__all_sync(0xffffffffu, cur == c0) && c0 >= 0) {
+        V r = acc;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) r = F::combine(r, __shfl_xor_sync(0xffffffffu, r, o));
+        if (lane == 0) {
+          F::atomic_combine(&s_acc[c0], r);
+          s_touch[c0] = 1;
+        }
+      } else if (cur >= 0) {
+        F::atomic_combine(&s_acc[cur], acc);
+        s_touch[cur] = 1;
+      }
+      __syncthreads();  // stage st fully consumed
+      if (tid == 0 && c + kPullStages < nchunks && !s_fail) {
+        fence_proxy_async_smem();
+        issue(c + kPullStages, st);
+      }
+    }
+    if (s_fail) break;
+    // commit: one thread per destination, warp-aligned on global vertex ids
+    const uint32_t base0 = v0 & ~31u;
+    for (uint32_t b = base0 + (uint32_t)warp * 32u; b < v0 + nv; b += kPullThreads) {
+      const uint32_t v = b + (uint32_t)lane;
+      bool act = false;
+      if (v >= v0 && v < v0 + nv) {
+        const uint32_t l = v - v0;
+        if (s_touch[l] && s_cond[l]) act = f.commit(v, s_acc[l]);
+      }
+      const uint32_t word = __ballot_sync(0xffffffffu, act);
+      if (act) my_deg += __ldg(p.deg_off + v + 1) - __ldg(p.deg_off + v);
+      if (lane == 0 && word) {
+        atomicOr(p.next_bits + (b >> 5), word);
+        my_cnt += __popc(word);
+      }
+    }
+    __syncthreads();
+  }
+  // block reduction of the output statistics
+  my_deg = warp_sum(my_deg);
+  my_cnt = warp_sum(my_cnt);
+  if (lane == 0) {
+    s_red[0][warp] = my_cnt;
+    s_red[1][warp] = my_deg;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    unsigned long long a = 0, b = 0;
+    for (int w = 0; w < kPullThreads / 32; ++w) {
+      a += s_red[0][w];
+      b += s_red[1][w];
+    }
+    if (a) atomicAdd(p.stats + 0, a);
+    if (b) atomicAdd(p.stats + 1, b);
+  }
+}
+
+// Dense pull with early exit (kEarlyExit functors): one lane per destination.
+template <class F, bool HW, bool ALL>
+__global__ void __launch_bounds__(256) k_pull_early(uint32_t n, const uint32_t* off, const uint32_t* idx,
+                                                    const uint32_t* wts, const uint32_t* fr_bits,
+                                                    uint32_t* next_bits, const uint32_t* deg_off,
+                                                    const uint32_t* member_off, unsigned long long* stats,
+                                                    const F f) {
+  unsigned long long my_cnt = 0, my_deg = 0;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); b < n; b += stride) {
+    const uint32_t v = (uint32_t)b + lane;
+    bool act = false;
+    if (v < n && f.cond(v) && (!member_off || member_off[v + 1] > member_off[v])) {
+      const uint32_t e1 = off[v + 1];
+      for (uint32_t j = off[v]; j < e1; ++j) {
+        const uint32_t s = idx[j];
+        if (ALL || test_bit(fr_bits, s)) {
+          act = f.commit(v, f.gather(s, HW ? wts[j] : 1u));
+          if (act || !f.cond(v)) break;
+        }
+      }
+    }
+    const uint32_t word = __ballot_sync(0xffffffffu, act);
+    if (act) my_deg += deg_off[v + 1] - deg_off[v];
+    if (lane == 0 && word) {
+      atomicOr(next_bits + (b >> 5), word);
+      my_cnt += __popc(word);
+    }
+  }
+  my_cnt = warp_sum(my_cnt);
+  my_deg = warp_sum(my_deg);
+  if (lane == 0) {
+    if (my_cnt) atomicAdd(stats + 0, my_cnt);
+    if (my_deg) atomicAdd(stats + 1, my_deg);
+  }
+}
+
+// ------------------------------------------------------------ push path
+// Block-level exclusive scan of up to kScanTile degrees (deg of queue[i]).
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* s_warp, uint32_t* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_warp[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = lane < (int)(blockDim.x >> 5) ? s_warp[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    s_warp[lane] = w;  // inclusive warp totals
+  }
+  __syncthreads();
+  const uint32_t before = warp ? s_warp[warp - 1] : 0;
+  *total = s_warp[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return before + x - v;
+}
+
+// pass 1: per-block degree sums
+static __global__ void __launch_bounds__(kScanThreads) k_scan_sums(const uint32_t* q, uint32_t k, const uint32_t* off,
+                                                            uint32_t* bsum) {
+  __shared__ uint32_t s_warp[32];
+  const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+  uint32_t t = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const uint32_t j = base + i;
+    if (j < k) {
+      const uint32_t v = q[j];
+      t += off[v + 1] - off[v];
+    }
+  }
+  uint32_t tot;
+  block_excl_scan(t, s_warp, &tot);
+  if (threadIdx.x == 0) bsum[blockIdx.x] = tot;
+}
+// pass 2: exclusive scan of the block sums (one block, serial over chunks);
+// writes the grand total to *total.
+static __global__ void __launch_bounds__(1024) k_scan_blocks(uint32_t* bsum, uint32_t nb, unsigned long long* total) {
+  __shared__ uint32_t s_warp[32];
+  uint32_t carry = 0;
+  for (uint32_t b0 = 0; b0 < nb; b0 += blockDim.x) {
+    const uint32_t j = b0 + threadIdx.x;
+    const uint32_t v = j < nb ? bsum[j] : 0;
+    uint32_t tot;
+    const uint32_t ex = block_excl_scan(v, s_warp, &tot);
+    if (j < nb) bsum[j] = carry + ex;
+    carry += tot;
+  }
+  if (threadIdx.x == 0) *total = carry;
+}
+// pass 3: exclusive offsets of every queue entry; offs[k] = total
+static __global__ void __launch_bounds__(kScanThreads) k_scan_write(const uint32_t* q, uint32_t k, const uint32_t* off,
+                                                             const uint32_t* bsum, uint32_t* offs) {
+  __shared__ uint32_t s_warp[32];
+  const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+  uint32_t d[kScanItems];
+  uint32_t t = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const uint32_t j = base + i;
+    d[i] = 0;
+    if (j < k) {
+      const uint32_t v = q[j];
+      d[i] = off[v + 1] - off[v];
+    }
+    t += d[i];
+  }
+  uint32_t tot;
+  uint32_t run = block_excl_scan(t, s_warp, &tot) + bsum[blockIdx.x];
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const uint32_t j = base + i;
+    if (j < k) offs[j] = run;
+    run += d[i];
+    if (j + 1 == k) offs[k] = run;
+  }
+}
+
+struct PushParams {
+  const uint32_t* q;        // frontier queue
+  uint32_t k;               // queue length
+  const uint32_t* offs;     // k+1 scanned degrees
+  const unsigned long long* total;
+  const uint32_t* off;      // out-offsets (current orientation)
+  const uint32_t* idx;      // out-neighbours
+  const uint32_t* wts;      // weights or null
+  const uint32_t* deg_off;  // out-offsets for output statistics
+  uint32_t* dedup;          // n-bit scratch, zero on entry and exit
+  uint32_t* out_q;          // output queue
+  unsigned long long* stats;  // [0] -, [1] out-degree sum, [2] queue length
+};
+
+template <class F, bool HW>
+__global__ void __launch_bounds__(kPushThreads) k_push(const PushParams p, const F f) {
+  __shared__ uint32_t s_q[2];
+  const uint64_t E = *p.total;
+  const int lane = threadIdx.x & 31;
+  unsigned long long my_deg = 0;
+  for (uint64_t c = blockIdx.x; c * kPushEdgesPerCta < E; c += gridDim.x) {
+    const uint32_t e_lo = (uint32_t)(c * kPushEdgesPerCta);
+    const uint64_t e_end = (uint64_t)e_lo + kPushEdgesPerCta;
+    const uint32_t e_hi = (uint32_t)(E < e_end ? E : e_end);
+    if (threadIdx.x < 2) {
+      const uint32_t key = threadIdx.x == 0 ? e_lo : e_hi - 1;
+      uint32_t lo = 0, hi = p.k;  // largest i with offs[i] <= key
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (p.offs[mid] <= key) lo = mid; else hi = mid;
+      }
+      s_q[threadIdx.x] = lo;
+    }
+    __syncthreads();
+    const uint32_t qlo = s_q[0], qhi = s_q[1];
+    const uint32_t iters = (e_hi - e_lo + kPushThreads - 1) / kPushThreads;
+    for (uint32_t it = 0; it < iters; ++it) {
+      const uint32_t e = e_lo + it * kPushThreads + threadIdx.x;
+      bool take = false;
+      uint32_t d = 0;
+      if (e < e_hi) {
+        uint32_t lo = qlo, hi = qhi + 1;
+        while (hi - lo > 1) {
+          const uint32_t mid = (lo + hi) >> 1;
+          if (p.offs[mid] <= e) lo = mid; else hi = mid;
+        }
+        const uint32_t s = p.q[lo];
+        const uint32_t ei = p.off[s] + (e - p.offs[lo]);
+        d = p.idx[ei];
+        const uint32_t w = HW ? p.wts[ei] : 1u;
+        if (f.cond(d) && f.update_atomic(s, d, w)) {
+          const uint32_t bit = 1u << (d & 31);
+          take = !(atomicOr(p.dedup + (d >> 5), bit) & bit);
+        }
+      }
+      const uint32_t ball = __ballot_sync(0xffffffffu, take);
+      if (ball) {
+        uint32_t base = 0;
+        if (lane == 0) base = (uint32_t)atomicAdd(p.stats + 2, (unsigned long long)__popc(ball));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (take) {
+          p.out_q[base + __popc(ball & ((1u << lane) - 1u))] = d;
+          my_deg += p.deg_off[d + 1] - p.deg_off[d];
+        }
+      }
+    }
+    __syncthreads();
+  }
+  my_deg = warp_sum(my_deg);
+  if (lane == 0 && my_deg) atomicAdd(p.stats + 1, my_deg);
+}
+
+// zero the dedup words touched by a queue
+static __global__ void k_clear_dedup(const uint32_t* q, const unsigned long long* len, uint32_t* dedup) {
+  const uint64_t k = *len;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < k; i += (uint64_t)gridDim.x * blockDim.x)
+    dedup[q[i] >> 5] = 0u;
+}
+
+// ------------------------------------------------------- vertexSubset ops
+static __global__ void k_queue_to_bits(const uint32_t* q, uint64_t k, uint32_t* bits) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < k; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t v = q[i];
+    atomicOr(bits + (v >> 5), 1u << (v & 31));
+  }
+}
+
+// ballot/popc compaction of a bitmap into a queue (one word per lane)
+static __global__ void k_bits_to_queue(const uint32_t* bits, uint32_t words, uint32_t* q, unsigned long long* len) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); b < words; b += stride) {
+    const uint64_t wi = b + lane;
+    const uint32_t w = wi < words ? bits[wi] : 0u;
+    const uint32_t c = __popc(w);
+    uint32_t x = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    const uint32_t tot = __shfl_sync(0xffffffffu, x, 31);
+    uint32_t base = 0;
+    if (lane == 31 && tot) base = (uint32_t)atomicAdd(len, (unsigned long long)tot);
+    base = __shfl_sync(0xffffffffu, base, 31);
+    uint32_t pos = base + x - c;
+    uint32_t ww = w;
+    while (ww) {
+      const int bpos = __ffs(ww) - 1;
+      ww &= ww - 1;
+      q[pos++] = (uint32_t)(wi * 32 + bpos);
+    }
+  }
+}
+
+// count and out-degree sum of a bitmap's members
+static __global__ void k_bits_stats(const uint32_t* bits, uint32_t n, const uint32_t* deg_off, unsigned long long* stats) {
+  unsigned long long c = 0, d = 0;
+  const uint32_t words = (n + 31) / 32;
+  for (uint64_t wi = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; wi < words; wi += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t w = bits[wi];
+    c += __popc(w);
+    while (w) {
+      const int b = __ffs(w) - 1;
+      w &= w - 1;
+      const uint32_t v = (uint32_t)(wi * 32 + b);
+      d += deg_off[v + 1] - deg_off[v];
+    }
+  }
+  c = warp_sum(c);
+  d = warp_sum(d);
+  if ((threadIdx.x & 31) == 0) {
+    if (c) atomicAdd(stats + 0, c);
+    if (d) atomicAdd(stats + 1, d);
+  }
+}
+
+// vertexMap: mode 0 all vertices, 1 dense members, 2 sparse list
+template <class VF, int MODE>
+__global__ void k_vertex_map(uint32_t n, const uint32_t* bits, const uint32_t* q, uint64_t k, const VF vf) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  if (MODE == 2) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < k; i += stride) vf(q[i]);
+  } else {
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride)
+      if (MODE == 0 || test_bit(bits, (uint32_t)v)) vf((uint32_t)v);
+  }
+}
+
+// vertexFilter over a dense (or all-active) subset: output bitmap + stats
+template <class VF, bool ALL>
+__global__ void k_vertex_filter(uint32_t n, const uint32_t* bits, uint32_t* out_bits, const uint32_t* deg_off,
+                                unsigned long long* stats, const VF vf) {
+  unsigned long long c = 0, d = 0;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); b < n; b += stride) {
+    const uint32_t v = (uint32_t)b + lane;
+    bool act = false;
+    if (v < n && (ALL || test_bit(bits, v))) act = vf(v);
+    const uint32_t word = __ballot_sync(0xffffffffu, act);
+    if (act) d += deg_off[v + 1] - deg_off[v];
+    if (lane == 0) {
+      out_bits[b >> 5] = word;
+      c += __popc(word);
+    }
+  }
+  c = warp_sum(c);
+  d = warp_sum(d);
+  if (lane == 0) {
+    if (c) atomicAdd(stats + 0, c);
+    if (d) atomicAdd(stats + 1, d);
+  }
+}
+
+}  // namespace gg
+
+namespace gg {
+static __global__ void k_iota(uint32_t* q, uint32_t n) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    q[i] = (uint32_t)i;
+}
+}  // namespace gg

@@ -1,0 +1,247 @@
+// Device forms of the applications' functor structs (app/*.C).  Each edge
+// functor states the reference member functions it replaces; the pull path
+// runs gather/combine/commit (the functor-cache protocol, create_cache /
+// update(cache, s) / commit_cache), the push path runs update_atomic.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace gg {
+
+struct MinI32 {
+  using value_t = int32_t;
+  __device__ static value_t identity() { return 0x7fffffff; }
+  __device__ static value_t combine(value_t a, value_t b) { return a < b ? a : b; }
+  __device__ static void atomic_combine(value_t* s, value_t v) { atomicMin(s, v); }
+};
+struct MinU32 {
+  using value_t = uint32_t;
+  __device__ static value_t identity() { return 0xffffffffu; }
+  __device__ static value_t combine(value_t a, value_t b) { return a < b ? a : b; }
+  __device__ static void atomic_combine(value_t* s, value_t v) { atomicMin(s, v); }
+};
+struct SumF32 {
+  using value_t = float;
+  __device__ static value_t identity() { return 0.0f; }
+  __device__ static value_t combine(value_t a, value_t b) { return a + b; }
+  __device__ static void atomic_combine(value_t* s, value_t v) { atomicAdd(s, v); }
+};
+
+// BFS_F, app/BFS.C:26-75.  cond = unvisited; update = first writer becomes
+// the parent (the pull keeps the smallest frontier in-neighbour; parents are
+// order-dependent in the reference too); updateAtomic = CAS(-1 -> s).
+// Also records the level (edgeMap round) of every newly reached vertex.
+struct BfsF : MinU32 {
+  static constexpr bool kEarlyExit = true;
+  static constexpr bool kUsesWeight = false;
+  int32_t* parents;
+  int32_t* levels;
+  int32_t round;
+  __device__ bool cond(uint32_t d) const { return __ldcg(parents + d) == -1; }
+  __device__ value_t gather(uint32_t s, uint32_t) const { return s; }
+  __device__ bool commit(uint32_t d, value_t acc) const {
+    parents[d] = (int32_t)acc;
+    if (levels) levels[d] = round;
+    return true;
+  }
+  __device__ bool update_atomic(uint32_t s, uint32_t d, uint32_t) const {
+    if (atomicCAS(parents + d, -1, (int32_t)s) == -1) {
+      if (levels) levels[d] = round;
+      return true;
+    }
+    return false;
+  }
+};
+
+// CC_F, app/Components.C:127-186.  Pull = the cached form (:158-180):
+// min over prevIDs[s]; output iff the label drops and IDs[d]==prevIDs[d].
+// Push = updateAtomic (:152-157): writeMin(IDs[d], IDs[s]) && orig==prevIDs[d].
+struct CcF : MinI32 {
+  static constexpr bool kEarlyExit = false;
+  static constexpr bool kUsesWeight = false;
+  int32_t* ids;
+  int32_t* prev;
+  __device__ bool cond(uint32_t) const { return true; }
+  __device__ value_t gather(uint32_t s, uint32_t) const { return __ldg(prev + s); }
+  __device__ bool commit(uint32_t d, value_t acc) const {
+    const int32_t orig = ids[d];
+    if (acc < orig) {
+      ids[d] = acc;
+      return orig == prev[d];
+    }
+    return false;
+  }
+  __device__ bool update_atomic(uint32_t s, uint32_t d, uint32_t) const {
+    const int32_t v = __ldcg(ids + s);
+    const int32_t old = atomicMin(ids + d, v);
+    return v < old && old == prev[d];
+  }
+};
+
+// PR_F, app/PageRank.C:256-298: p_next[d] += p_curr[s]/outdeg(s).  The
+// division is done once per source (contrib[s] = p_curr[s]/outdeg(s)) by the
+// iteration's vertex pass; the per-edge value is the same FP32 quotient.
+// Also PageRankDelta's PR_F (app/PageRankDelta.C:29-71) with contrib = Delta/outdeg.
+struct PrF : SumF32 {
+  static constexpr bool kEarlyExit = false;
+  static constexpr bool kUsesWeight = false;
+  const float* contrib;
+  float* acc_out;
+  __device__ bool cond(uint32_t) const { return true; }
+  __device__ value_t gather(uint32_t s, uint32_t) const { return __ldg(contrib + s); }
+  __device__ bool commit(uint32_t d, value_t acc) const {
+    acc_out[d] += acc;
+    return true;
+  }
+  __device__ bool update_atomic(uint32_t s, uint32_t d, uint32_t) const {
+    atomicAdd(acc_out + d, __ldg(contrib + s));
+    return true;
+  }
+};
+
+// SPMV_F, app/SPMV.C:7-47: p_next[d] += p_curr[s] * edgeLen.  Weights are
+// the reference's int edge lengths, or FP32 when the graph carries FP32 weights.
+struct SpmvF : SumF32 {
+  static constexpr bool kEarlyExit = false;
+  static constexpr bool kUsesWeight = true;
+  const float* x;
+  float* y;
+  int float_w;
+  __device__ float wv(uint32_t w) const { return float_w ? __uint_as_float(w) : (float)(int32_t)w; }
+  __device__ bool cond(uint32_t) const { return true; }
+  __device__ value_t gather(uint32_t s, uint32_t w) const { return __ldg(x + s) * wv(w); }
+  __device__ bool commit(uint32_t d, value_t acc) const {
+    y[d] += acc;
+    return true;
+  }
+  __device__ bool update_atomic(uint32_t s, uint32_t d, uint32_t w) const {
+    atomicAdd(y + d, __ldg(x + s) * wv(w));
+    return true;
+  }
+};
+
+// BF_F, app/BellmanFord.C:28-92.  Pull = cached form: min of SP[s]+w over the
+// frontier in-neighbours; output iff it lowers SP[d] and Visited[d] was 0.
+// Push = writeMin(SP[d], SP[s]+w) && CAS(Visited[d], 0, 1).
+struct BfF : MinI32 {
+  static constexpr bool kEarlyExit = false;
+  static constexpr bool kUsesWeight = true;
+  int32_t* sp;
+  int32_t* visited;
+  __device__ bool cond(uint32_t) const { return true; }
+  __device__ value_t gather(uint32_t s, uint32_t w) const { return __ldcg(sp + s) + (int32_t)w; }
+  __device__ bool commit(uint32_t d, value_t acc) const {
+    if (acc < sp[d]) {
+      sp[d] = acc;
+      if (visited[d] == 0) {
+        visited[d] = 1;
+        return true;
+      }
+    }
+    return false;
+  }
+  __device__ bool update_atomic(uint32_t s, uint32_t d, uint32_t w) const {
+    const int32_t nd = __ldcg(sp + s) + (int32_t)w;
+    const int32_t old = atomicMin(sp + d, nd);
+    if (nd < old) return atomicCAS(visited + d, 0, 1) == 0;
+    return false;
+  }
+};
+
+// BC_F / BC_Back_F, app/BC.C:28-117: value[d] += value[s] for unvisited d;
+// output iff value[d] was 0 before (first path reaching d).
+struct BcF : SumF32 {
+  static constexpr bool kEarlyExit = false;
+  static constexpr bool kUsesWeight = false;
+  float* values;
+  const uint8_t* visited;
+  __device__ bool cond(uint32_t d) const { return visited[d] == 0; }
+  __device__ value_t gather(uint32_t s, uint32_t) const { return __ldcg(values + s); }
+  __device__ bool commit(uint32_t d, value_t acc) const {
+    const float old = values[d];
+    values[d] = old + acc;
+    return old == 0.0f;
+  }
+  __device__ bool update_atomic(uint32_t s, uint32_t d, uint32_t) const {
+    return atomicAdd(values + d, __ldcg(values + s)) == 0.0f;
+  }
+};
+
+// ------------------------------------------------------- vertex functors
+// CC_Vertex_F, app/Components.C:189-200
+struct VCcCopy {
+  int32_t* ids;
+  int32_t* prev;
+  __device__ bool operator()(uint32_t i) const {
+    prev[i] = ids[i];
+    return true;
+  }
+};
+// PR_Vertex_F, app/PageRank.C:301-315
+struct VPrUpdate {
+  float* p_next;
+  float damping, added;
+  __device__ bool operator()(uint32_t i) const {
+    p_next[i] = damping * p_next[i] + added;
+    return true;
+  }
+};
+template <class T>
+struct VFill {
+  T* a;
+  T value;
+  __device__ bool operator()(uint32_t i) const {
+    a[i] = value;
+    return true;
+  }
+};
+// PR_Vertex_F_FirstRound, app/PageRankDelta.C:73-90
+struct VPrdFirst {
+  float* p;
+  float* delta;
+  const float* ngh;
+  float damping, added, one_over_n, eps2;
+  __device__ bool operator()(uint32_t i) const {
+    float d = damping * (p[i] + ngh[i]) + added - p[i];
+    const float pi = p[i] + d;
+    p[i] = pi;
+    d -= one_over_n;
+    delta[i] = d;
+    return fabsf(d) > eps2 * pi;
+  }
+};
+// PR_Vertex_F, app/PageRankDelta.C:92-106
+struct VPrd {
+  float* p;
+  float* delta;
+  const float* ngh;
+  float damping, eps2;
+  __device__ bool operator()(uint32_t i) const {
+    const float d = ngh[i] * damping;
+    delta[i] = d;
+    const float pi = p[i] + d;
+    p[i] = pi;
+    return fabsf(d) > eps2 * pi;
+  }
+};
+// BC_Vertex_F, app/BC.C:119-128
+struct VBcMark {
+  uint8_t* visited;
+  __device__ bool operator()(uint32_t i) const {
+    visited[i] = 1;
+    return true;
+  }
+};
+// BC_Back_Vertex_F, app/BC.C:131-143
+struct VBcBack {
+  uint8_t* visited;
+  float* dep;
+  const float* inv;
+  __device__ bool operator()(uint32_t i) const {
+    visited[i] = 1;
+    dep[i] += inv[i];
+    return true;
+  }
+};
+
+}  // namespace gg

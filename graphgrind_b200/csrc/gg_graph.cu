@@ -1,0 +1,680 @@
+// Device graph construction (partitioned_graph, graphgrind/graph-numa.h:642-685)
+// and the vertexSubset C API (partitioned_vertices, graphgrind/ligra-numa.h:91-272).
+//
+// Layout in HBM (uint32 ids and offsets):
+//   CSR  out_off[n+1], out_idx[m(+16 pad)], out_w[m]      (forward push)
+//   CSC  in_off[n+1],  in_idx[m(+16 pad)],  in_w[m]       (dense pull); shared with
+//        the CSR arrays when the graph is symmetric
+//   COO  per destination tile, Hilbert (or source-major) ordered inside the
+//        reference partition, padded to 8 edges: src[], dloc[] (u16 offset of
+//        the destination inside its tile), w[]
+//   tiles {v0, nv, e0, ne} per CTA work item, largest first.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <numeric>
+#include <vector>
+
+#include "gg_hilbert.h"
+#include "gg_runtime.cuh"
+
+namespace gg {
+
+template <class T>
+static int dev_alloc(gg_graph_s* g, T** p, size_t count) {
+  size_t bytes = sizeof(T) * std::max<size_t>(count, 1);
+  cudaError_t e = cudaMalloc((void**)p, bytes);
+  if (e != cudaSuccess) return fail(GG_ERR_OOM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+  g->device_bytes += bytes;
+  return GG_OK;
+}
+
+// ------------------------------------------------------------- frontiers
+int frontier_new(gg_graph_s* g, gg_frontier_s** out) {
+  gg_frontier_s* f = new (std::nothrow) gg_frontier_s;
+  if (!f) return fail(GG_ERR_OOM, "frontier: out of host memory");
+  f->g = g;
+  f->n = g->n;
+  *out = f;
+  return GG_OK;
+}
+
+int frontier_ensure_bits(gg_frontier_s* f, bool zero) {
+  gg_graph_s* g = f->g;
+  const size_t bytes = sizeof(uint32_t) * ((size_t)g->words() + 4);
+  if (!f->d_bits) GG_CUDA(cudaMallocAsync((void**)&f->d_bits, bytes, g->stream));
+  if (zero) GG_CUDA(cudaMemsetAsync(f->d_bits, 0, bytes, g->stream));
+  return GG_OK;
+}
+
+int frontier_ensure_queue(gg_frontier_s* f) {
+  gg_graph_s* g = f->g;
+  if (!f->d_queue) GG_CUDA(cudaMallocAsync((void**)&f->d_queue, sizeof(uint32_t) * ((size_t)g->n + 4), g->stream));
+  return GG_OK;
+}
+
+void frontier_free(gg_frontier_s* f) {
+  if (!f) return;
+  gg_graph_s* g = f->g;
+  if (f->d_bits) cudaFreeAsync(f->d_bits, g->stream);
+  if (f->d_queue) cudaFreeAsync(f->d_queue, g->stream);
+  delete f;
+}
+
+__global__ void k_all_bits(uint32_t* bits, uint32_t n) {
+  const uint32_t words = (n + 31) / 32;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < words; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t rem = n - (uint32_t)i * 32;
+    bits[i] = rem >= 32 ? 0xffffffffu : ((1u << rem) - 1u);
+  }
+}
+
+// toDense, graphgrind/ligra-numa.h:228-244
+int frontier_to_dense(gg_frontier_s* f) {
+  gg_graph_s* g = f->g;
+  if (f->has_dense) return GG_OK;
+  GG_TRY(frontier_ensure_bits(f, true));
+  if (f->bit) {
+    k_all_bits<<<generic_grid(g, g->words()), kGenericThreads, 0, g->stream>>>(f->d_bits, g->n);
+  } else if (f->has_sparse && f->dm) {
+    k_queue_to_bits<<<generic_grid(g, f->dm), kGenericThreads, 0, g->stream>>>(f->d_queue, f->dm, f->d_bits);
+  }
+  GG_CUDA(cudaGetLastError());
+  g->kernels++;
+  f->has_dense = true;
+  return GG_OK;
+}
+
+// toSparse, graphgrind/ligra-numa.h:246-260 (packIndex -> ballot compaction)
+int frontier_to_sparse(gg_frontier_s* f) {
+  gg_graph_s* g = f->g;
+  if (f->has_sparse) return GG_OK;
+  GG_TRY(frontier_ensure_queue(f));
+  if (f->bit) {
+    k_iota<<<generic_grid(g, g->n), kGenericThreads, 0, g->stream>>>(f->d_queue, g->n);
+    GG_CUDA(cudaGetLastError());
+    g->kernels++;
+    f->has_sparse = true;
+    return GG_OK;
+  }
+  if (!f->has_dense || f->dm == 0) {
+    f->has_sparse = true;
+    return GG_OK;
+  }
+  GG_TRY(reset_stats(g));
+  k_bits_to_queue<<<generic_grid(g, g->words()), kGenericThreads, 0, g->stream>>>(f->d_bits, g->words(), f->d_queue,
+                                                                                g->ws.d_stats + 2);
+  GG_CUDA(cudaGetLastError());
+  g->kernels++;
+  GG_TRY(read_stats(g));
+  if (g->ws.h_stats[2] != f->dm)
+    return fail(GG_ERR_INVALID_ARG, "bad stored value of m: frontier holds %llu vertices, stats say %llu",
+                (unsigned long long)g->ws.h_stats[2], (unsigned long long)f->dm);
+  f->has_sparse = true;
+  return GG_OK;
+}
+
+int reset_stats(gg_graph_s* g) {
+  GG_CUDA(cudaMemsetAsync(g->ws.d_stats, 0, sizeof(unsigned long long) * 8, g->stream));
+  return GG_OK;
+}
+
+int read_stats(gg_graph_s* g) {
+  GG_CUDA(cudaMemcpyAsync(g->ws.h_stats, g->ws.d_stats, sizeof(unsigned long long) * 8, cudaMemcpyDeviceToHost,
+                          g->stream));
+  GG_CUDA(cudaStreamSynchronize(g->stream));
+  if (g->ws.h_stats[3])
+    return fail(GG_ERR_TIMEOUT, "device wait budget exhausted (error word %llu)", (unsigned long long)g->ws.h_stats[3]);
+  return GG_OK;
+}
+
+// ------------------------------------------------------------------ tiles
+// Greedy destination tiles over [vbeg, vend): at most tv vertices and about
+// te edges (a single vertex above te gets its own tile); edge-less ranges
+// are dropped (their vertices can never be updated by a pull).
+static void make_tiles(const uint32_t* off, uint32_t vbeg, uint32_t vend, uint32_t tv, uint64_t te,
+                       std::vector<uint4>& out) {
+  uint32_t v = vbeg;
+  while (v < vend) {
+    const uint32_t t0 = v;
+    uint64_t ne = 0;
+    while (v < vend && v - t0 < tv) {
+      const uint64_t d = off[v + 1] - off[v];
+      if (v > t0 && ne + d > te) break;
+      ne += d;
+      ++v;
+    }
+    if (ne > 0) out.push_back(make_uint4(t0, v - t0, off[t0], (uint32_t)ne));
+  }
+}
+
+static int upload_tiles(gg_graph_s* g, TileSet& ts, std::vector<uint4>& tiles) {
+  std::stable_sort(tiles.begin(), tiles.end(), [](const uint4& a, const uint4& b) { return a.w > b.w; });
+  ts.host = tiles;
+  ts.count = (uint32_t)tiles.size();
+  GG_TRY(dev_alloc(g, &ts.d_tiles, tiles.size()));
+  if (!tiles.empty())
+    GG_CUDA(cudaMemcpy(ts.d_tiles, tiles.data(), sizeof(uint4) * tiles.size(), cudaMemcpyHostToDevice));
+  return GG_OK;
+}
+
+// ------------------------------------------------------- COO construction
+__global__ void k_edge_dst(const uint32_t* off, uint32_t n, uint32_t* dst) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x)
+    for (uint32_t j = off[v]; j < off[v + 1]; ++j) dst[j] = (uint32_t)v;
+}
+
+// sort key of every CSC edge inside its partition: Hilbert (EDGES_HILBERT=1,
+// graphgrind/graph-numa.h:482-490) or (src, dst) (CSRDestSort, :338-350)
+__global__ void k_coo_keys(const uint32_t* src, const uint32_t* dst, uint64_t m, const int64_t* starts, int P,
+                           const int64_t* part_side, int hilbert, uint64_t* keys, uint32_t* vals) {
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < m; j += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t d = dst[j], s = src[j];
+    uint64_t key;
+    if (hilbert) {
+      int lo = 0, hi = P;  // partition p with starts[p] <= d < starts[p+1]
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (starts[mid] <= (int64_t)d) lo = mid; else hi = mid;
+      }
+      key = (uint64_t)hilbert_xy2d(part_side[lo], (int64_t)s, (int64_t)d);
+    } else {
+      key = ((uint64_t)s << 32) | d;
+    }
+    keys[j] = key;
+    vals[j] = (uint32_t)j;
+  }
+}
+
+// scatter sorted tile segments into their padded COO slots
+__global__ void k_coo_scatter(const uint4* seg, const uint32_t* pad_start, uint32_t ntiles, const uint32_t* perm,
+                              const uint32_t* src, const uint32_t* dst, const uint32_t* w, uint32_t* coo_src,
+                              uint16_t* coo_dloc, uint32_t* coo_w) {
+  for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const uint4 s = seg[t];  // {v0, nv, e0 (CSC), ne}
+    const uint32_t base = pad_start[t];
+    for (uint32_t i = threadIdx.x; i < s.w; i += blockDim.x) {
+      const uint32_t j = perm[s.z + i];
+      coo_src[base + i] = src[j];
+      coo_dloc[base + i] = (uint16_t)(dst[j] - s.x);
+      if (w) coo_w[base + i] = w[j];
+    }
+  }
+}
+
+static int build_coo(gg_graph_s* g, const uint32_t* h_in_off) {
+  const uint32_t n = g->n;
+  const uint64_t m = g->m;
+  const int P = (int)g->coo_sizes.size();
+  const uint32_t tv = (uint32_t)g->opts.tile_vertices;
+  const uint64_t te = (uint64_t)g->opts.tile_edges;
+  std::vector<uint4> segs;  // in vertex order
+  for (int p = 0; p < P; ++p)
+    make_tiles(h_in_off, (uint32_t)g->coo_starts[p], (uint32_t)g->coo_starts[p + 1], tv, te, segs);
+  // padded placement
+  std::vector<uint32_t> pad_start(segs.size());
+  uint64_t pos = 0;
+  for (size_t t = 0; t < segs.size(); ++t) {
+    pad_start[t] = (uint32_t)pos;
+    pos += (segs[t].w + 7u) & ~7u;
+  }
+  if (pos + 16 >= (1ull << 31)) return fail(GG_ERR_SIZE, "padded COO exceeds the 2^31-edge sort limit");
+  g->coo_len = pos;
+  GG_TRY(dev_alloc(g, &g->d_coo_src, pos + 16));
+  GG_TRY(dev_alloc(g, &g->d_coo_dloc, pos + 16));
+  if (g->wtype != GG_W_NONE) GG_TRY(dev_alloc(g, &g->d_coo_w, pos + 16));
+  GG_CUDA(cudaMemset(g->d_coo_src, 0xff, sizeof(uint32_t) * (pos + 16)));
+  GG_CUDA(cudaMemset(g->d_coo_dloc, 0, sizeof(uint16_t) * (pos + 16)));
+  if (g->d_coo_w) GG_CUDA(cudaMemset(g->d_coo_w, 0, sizeof(uint32_t) * (pos + 16)));
+  // partition grid sides: roundUpPow2(edges of partition p)
+  std::vector<int64_t> side(P);
+  for (int p = 0; p < P; ++p) {
+    const int64_t ne = (int64_t)h_in_off[g->coo_starts[p + 1]] - (int64_t)h_in_off[g->coo_starts[p]];
+    side[p] = hilbert_side(ne);
+  }
+  uint32_t *d_dst = nullptr, *d_vals = nullptr, *d_perm = nullptr, *d_pad = nullptr;
+  uint64_t *d_keys = nullptr, *d_keys_out = nullptr;
+  int64_t *d_starts = nullptr, *d_side = nullptr;
+  uint4* d_segs = nullptr;
+  int* d_seg_begin = nullptr;
+  void* d_temp = nullptr;
+  size_t temp_bytes = 0;
+  int rc = GG_OK;
+  auto cleanup = [&]() {
+    cudaFree(d_dst); cudaFree(d_vals); cudaFree(d_perm); cudaFree(d_pad); cudaFree(d_keys);
+    cudaFree(d_keys_out); cudaFree(d_starts); cudaFree(d_side); cudaFree(d_segs); cudaFree(d_seg_begin);
+    cudaFree(d_temp);
+  };
+#define GG_BUILD(call)                                                                      \
+  do {                                                                                      \
+    cudaError_t e__ = (call);                                                               \
+    if (e__ != cudaSuccess) {                                                               \
+      rc = fail(GG_ERR_CUDA, "COO build: %s: %s", #call, cudaGetErrorString(e__));          \
+      cleanup();                                                                            \
+      return rc;                                                                            \
+    }                                                                                       \
+  } while (0)
+  const uint64_t mm = std::max<uint64_t>(m, 1);
+  GG_BUILD(cudaMalloc(&d_dst, 4 * mm));
+  GG_BUILD(cudaMalloc(&d_vals, 4 * mm));
+  GG_BUILD(cudaMalloc(&d_perm, 4 * mm));
+  GG_BUILD(cudaMalloc(&d_keys, 8 * mm));
+  GG_BUILD(cudaMalloc(&d_keys_out, 8 * mm));
+  GG_BUILD(cudaMalloc(&d_starts, 8 * (P + 1)));
+  GG_BUILD(cudaMalloc(&d_side, 8 * P));
+  GG_BUILD(cudaMalloc(&d_segs, sizeof(uint4) * std::max<size_t>(segs.size(), 1)));
+  GG_BUILD(cudaMalloc(&d_pad, 4 * std::max<size_t>(segs.size(), 1)));
+  GG_BUILD(cudaMalloc(&d_seg_begin, sizeof(int) * (segs.size() + 1)));
+  GG_BUILD(cudaMemcpy(d_starts, g->coo_starts.data(), 8 * (P + 1), cudaMemcpyHostToDevice));
+  GG_BUILD(cudaMemcpy(d_side, side.data(), 8 * P, cudaMemcpyHostToDevice));
+  if (!segs.empty()) {
+    GG_BUILD(cudaMemcpy(d_segs, segs.data(), sizeof(uint4) * segs.size(), cudaMemcpyHostToDevice));
+    GG_BUILD(cudaMemcpy(d_pad, pad_start.data(), 4 * segs.size(), cudaMemcpyHostToDevice));
+  }
+  // segment boundaries: tile edge ranges are contiguous and cover [0, m)
+  std::vector<int> seg_begin(segs.size() + 1);
+  for (size_t t = 0; t < segs.size(); ++t) seg_begin[t] = (int)segs[t].z;
+  seg_begin[segs.size()] = (int)m;
+  GG_BUILD(cudaMemcpy(d_seg_begin, seg_begin.data(), sizeof(int) * seg_begin.size(), cudaMemcpyHostToDevice));
+  const int grid = g->num_sms * 8;
+  k_edge_dst<<<grid, 256>>>(g->d_csc_off, n, d_dst);
+  k_coo_keys<<<grid, 256>>>(g->d_csc_idx, d_dst, m, d_starts, P, d_side, g->opts.order == GG_ORDER_HILBERT ? 1 : 0,
+                            d_keys, d_vals);
+  GG_BUILD(cudaGetLastError());
+  if (!segs.empty()) {
+    GG_BUILD(cub::DeviceSegmentedRadixSort::SortPairs(nullptr, temp_bytes, d_keys, d_keys_out, d_vals, d_perm, (int)m,
+                                                      (int)segs.size(), d_seg_begin, d_seg_begin + 1));
+    GG_BUILD(cudaMalloc(&d_temp, temp_bytes));
+    GG_BUILD(cub::DeviceSegmentedRadixSort::SortPairs(d_temp, temp_bytes, d_keys, d_keys_out, d_vals, d_perm, (int)m,
+                                                      (int)segs.size(), d_seg_begin, d_seg_begin + 1));
+    k_coo_scatter<<<grid, 256>>>(d_segs, d_pad, (uint32_t)segs.size(), d_perm, g->d_csc_idx, d_dst, g->d_csc_w,
+                                 g->d_coo_src, g->d_coo_dloc, g->d_coo_w);
+    GG_BUILD(cudaGetLastError());
+  }
+  GG_BUILD(cudaDeviceSynchronize());
+#undef GG_BUILD
+  cleanup();
+  // work items: padded segments
+  std::vector<uint4> tiles(segs.size());
+  for (size_t t = 0; t < segs.size(); ++t)
+    tiles[t] = make_uint4(segs[t].x, segs[t].y, pad_start[t], (segs[t].w + 7u) & ~7u);
+  GG_TRY(upload_tiles(g, g->coo_tiles, tiles));
+  g->has_coo = true;
+  return GG_OK;
+}
+
+static void graph_release(gg_graph_s* g) {
+  if (!g) return;
+  cudaFree(g->d_csr_off);
+  cudaFree(g->d_csr_idx);
+  cudaFree(g->d_csr_w);
+  if (!g->symmetric) {
+    cudaFree(g->d_csc_off);
+    cudaFree(g->d_csc_idx);
+    cudaFree(g->d_csc_w);
+  }
+  for (auto& t : g->csc_tiles) cudaFree(t.d_tiles);
+  cudaFree(g->coo_tiles.d_tiles);
+  cudaFree(g->d_coo_src);
+  cudaFree(g->d_coo_dloc);
+  cudaFree(g->d_coo_w);
+  cudaFree(g->ws.d_stats);
+  cudaFree(g->ws.d_dedup);
+  cudaFree(g->ws.d_scan);
+  cudaFree(g->ws.d_bsum);
+  cudaFree(g->ws.d_red);
+  if (g->ws.h_stats) cudaFreeHost(g->ws.h_stats);
+  if (g->ws.h_red) cudaFreeHost(g->ws.h_red);
+  if (g->stream) cudaStreamDestroy(g->stream);
+  delete g;
+}
+
+static int graph_build(const gg_host_graph* hg, const gg_build_opts* opts_in, gg_graph_s* g) {
+  const uint32_t n = hg->n;
+  const uint64_t m = hg->m;
+  gg_build_opts o{};
+  if (opts_in) o = *opts_in;
+  if (o.num_partitions <= 0) o.num_partitions = 384;
+  if (o.tile_vertices <= 0 || o.tile_vertices > kMaxTileVertices) o.tile_vertices = kMaxTileVertices;
+  if (o.tile_edges <= 0) o.tile_edges = 1 << 16;
+  if (o.order != GG_ORDER_CSR) o.order = GG_ORDER_HILBERT;
+  if (o.part_how == GG_PART_SOURCE)
+    return fail(GG_ERR_UNSUPPORTED, "-P source partitioning is not supported by this build");
+  g->opts = o;
+  g->n = n;
+  g->m = m;
+  g->symmetric = hg->symmetric != 0;
+  g->wtype = hg->weights ? hg->weight_type : GG_W_NONE;
+  GG_CUDA(cudaGetDevice(&g->device));
+  GG_CUDA(cudaDeviceGetAttribute(&g->num_sms, cudaDevAttrMultiProcessorCount, g->device));
+  GG_CUDA(cudaStreamCreate(&g->stream));
+  // CSC on the host: deterministic in-lists ordered by source id
+  gg_host_graph csc{};
+  const gg_host_graph* in = hg;
+  if (!g->symmetric) {
+    GG_TRY(gg_host_graph_transpose(hg, &csc));
+    in = &csc;
+  }
+  g->h_csr_off.assign(hg->offsets, hg->offsets + n + 1);
+  g->h_csc_off.assign(in->offsets, in->offsets + n + 1);
+  std::vector<uint32_t> indeg(n), outdeg(n);
+  for (uint32_t v = 0; v < n; ++v) {
+    outdeg[v] = hg->offsets[v + 1] - hg->offsets[v];
+    indeg[v] = in->offsets[v + 1] - in->offsets[v];
+  }
+  const int P = o.num_partitions;
+  g->coo_sizes.assign(P, 0);
+  g->csc_sizes.assign(P, 0);
+  int rc = gg_partition_sizes(indeg.data(), outdeg.data(), n, m, P, o.balance, o.part_how, o.relabel,
+                              g->coo_sizes.data(), g->csc_sizes.data());
+  if (rc) {
+    if (!g->symmetric) gg_host_graph_free(&csc);
+    return rc;
+  }
+  g->coo_starts.assign(P + 1, 0);
+  g->csc_starts.assign(P + 1, 0);
+  for (int p = 0; p < P; ++p) {
+    g->coo_starts[p + 1] = g->coo_starts[p] + g->coo_sizes[p];
+    g->csc_starts[p + 1] = g->csc_starts[p] + g->csc_sizes[p];
+  }
+  auto up = [&](uint32_t** d, const void* h, size_t count, size_t pad) -> int {
+    GG_TRY(dev_alloc(g, d, count + pad));
+    if (pad) GG_CUDA(cudaMemset(*d + count, 0, sizeof(uint32_t) * pad));
+    if (count) GG_CUDA(cudaMemcpy(*d, h, sizeof(uint32_t) * count, cudaMemcpyHostToDevice));
+    return GG_OK;
+  };
+  rc = up(&g->d_csr_off, hg->offsets, (size_t)n + 1, 4);
+  if (!rc) rc = up(&g->d_csr_idx, hg->indices, m, 16);
+  if (!rc && g->wtype != GG_W_NONE) rc = up(&g->d_csr_w, hg->weights, m, 16);
+  if (!rc) {
+    if (g->symmetric) {
+      g->d_csc_off = g->d_csr_off;
+      g->d_csc_idx = g->d_csr_idx;
+      g->d_csc_w = g->d_csr_w;
+    } else {
+      rc = up(&g->d_csc_off, in->offsets, (size_t)n + 1, 4);
+      if (!rc) rc = up(&g->d_csc_idx, in->indices, m, 16);
+      if (!rc && g->wtype != GG_W_NONE) rc = up(&g->d_csc_w, in->weights, m, 16);
+    }
+  }
+  // CTA tiles for the CSC pull, both orientations
+  if (!rc) {
+    std::vector<uint4> t0;
+    make_tiles(in->offsets, 0, n, (uint32_t)o.tile_vertices, (uint64_t)o.tile_edges, t0);
+    rc = upload_tiles(g, g->csc_tiles[0], t0);
+  }
+  if (!rc && !g->symmetric) {
+    std::vector<uint4> t1;
+    make_tiles(hg->offsets, 0, n, (uint32_t)o.tile_vertices, (uint64_t)o.tile_edges, t1);
+    rc = upload_tiles(g, g->csc_tiles[1], t1);
+  } else if (!rc) {
+    g->csc_tiles[1] = g->csc_tiles[0];
+    g->csc_tiles[1].d_tiles = nullptr;  // shared; released once
+  }
+  // partitioned COO: only for -v edge (graphgrind/graph-numa.h:661)
+  const bool want_coo = o.balance == GG_BALANCE_EDGE && o.build_coo >= 0;
+  if (!rc && want_coo && m > 0) rc = build_coo(g, in->offsets);
+  if (!g->symmetric) gg_host_graph_free(&csc);
+  if (rc) return rc;
+  // workspace
+  GG_TRY(dev_alloc(g, &g->ws.d_stats, 8));
+  GG_CUDA(cudaMemset(g->ws.d_stats, 0, 64));
+  GG_CUDA(cudaMallocHost((void**)&g->ws.h_stats, 64));
+  GG_TRY(dev_alloc(g, &g->ws.d_dedup, (size_t)g->words() + 4));
+  GG_CUDA(cudaMemset(g->ws.d_dedup, 0, sizeof(uint32_t) * ((size_t)g->words() + 4)));
+  GG_TRY(dev_alloc(g, &g->ws.d_scan, (size_t)n + 4));
+  GG_TRY(dev_alloc(g, &g->ws.d_red, 64));
+  GG_CUDA(cudaMallocHost((void**)&g->ws.h_red, 64 * sizeof(double)));
+  // keep stream-ordered allocations (frontiers) cached in the pool
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, g->device) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  GG_CUDA(cudaDeviceSynchronize());
+  return GG_OK;
+}
+
+}  // namespace gg
+
+using namespace gg;
+
+extern "C" {
+
+const char* gg_version(void) { return "graphgrind_b200 0.1 (sm_100a)"; }
+
+int gg_graph_build(const gg_host_graph* hg, const gg_build_opts* opts, gg_graph_t* out) {
+  if (!hg || !out || !hg->offsets || (hg->m && !hg->indices) || hg->n == 0)
+    return fail(GG_ERR_INVALID_ARG, "gg_graph_build: bad arguments");
+  if (hg->m >= (1ull << 32) - 64) return fail(GG_ERR_SIZE, "m=%llu exceeds uint32 offsets", (unsigned long long)hg->m);
+  if (hg->n > (1u << 31)) return fail(GG_ERR_SIZE, "n=%u exceeds the supported vertex range", hg->n);
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return fail(GG_ERR_NO_DEVICE, "no CUDA device is visible");
+  }
+  gg_graph_s* g = new (std::nothrow) gg_graph_s;
+  if (!g) return fail(GG_ERR_OOM, "graph: out of host memory");
+  int rc = graph_build(hg, opts, g);
+  if (rc) {
+    std::string keep = last_error();
+    graph_release(g);
+    set_error("%s", keep.c_str());
+    return rc;
+  }
+  *out = g;
+  return GG_OK;
+}
+
+int gg_graph_destroy(gg_graph_t g) {
+  if (!g) return fail(GG_ERR_INVALID_ARG, "gg_graph_destroy: null graph");
+  cudaStreamSynchronize(g->stream);
+  graph_release(g);
+  return GG_OK;
+}
+
+int gg_graph_get_info(gg_graph_t g, gg_graph_info* info) {
+  if (!g || !info) return fail(GG_ERR_INVALID_ARG, "gg_graph_get_info: bad arguments");
+  info->n = g->n;
+  info->m = g->m;
+  info->symmetric = g->symmetric;
+  info->weight_type = g->wtype;
+  info->num_partitions = (int32_t)g->coo_sizes.size();
+  info->has_coo = g->has_coo;
+  info->transposed = g->transposed;
+  info->num_csc_tiles = (int32_t)g->csc_tiles[0].count;
+  info->num_coo_tiles = (int32_t)g->coo_tiles.count;
+  info->device_bytes = g->device_bytes;
+  return GG_OK;
+}
+
+int gg_graph_partition_starts(gg_graph_t g, int64_t* starts) {
+  if (!g || !starts) return fail(GG_ERR_INVALID_ARG, "gg_graph_partition_starts: bad arguments");
+  std::copy(g->coo_starts.begin(), g->coo_starts.end(), starts);
+  return GG_OK;
+}
+
+int gg_graph_transpose(gg_graph_t g) {
+  if (!g) return fail(GG_ERR_INVALID_ARG, "gg_graph_transpose: null graph");
+  if (!g->symmetric) g->transposed = !g->transposed;  // graphgrind/graph-numa.h:598-611
+  return GG_OK;
+}
+
+int gg_graph_device_arrays(gg_graph_t g, const uint32_t** oo, const uint32_t** oi, const uint32_t** io,
+                           const uint32_t** ii) {
+  if (!g) return fail(GG_ERR_INVALID_ARG, "gg_graph_device_arrays: null graph");
+  if (oo) *oo = g->out_off();
+  if (oi) *oi = g->out_idx();
+  if (io) *io = g->in_off();
+  if (ii) *ii = g->in_idx();
+  return GG_OK;
+}
+
+// ---------------------------------------------------------- frontier API
+int gg_frontier_single(gg_graph_t g, uint32_t v, gg_frontier_t* out) {
+  if (!g || !out || v >= g->n) return fail(GG_ERR_INVALID_ARG, "gg_frontier_single: bad arguments");
+  gg_frontier_s* f;
+  GG_TRY(frontier_new(g, &f));
+  int rc = frontier_ensure_queue(f);
+  if (!rc && cudaMemcpyAsync(f->d_queue, &v, 4, cudaMemcpyHostToDevice, g->stream) != cudaSuccess)
+    rc = fail(GG_ERR_CUDA, "frontier upload failed");
+  if (rc) {
+    frontier_free(f);
+    return rc;
+  }
+  f->has_sparse = true;
+  f->dm = 1;
+  f->out_edges = g->h_out_off()[v + 1] - g->h_out_off()[v];
+  *out = f;
+  return GG_OK;
+}
+
+int gg_frontier_all(gg_graph_t g, gg_frontier_t* out) {
+  if (!g || !out) return fail(GG_ERR_INVALID_ARG, "gg_frontier_all: bad arguments");
+  gg_frontier_s* f;
+  GG_TRY(frontier_new(g, &f));
+  f->bit = true;
+  f->has_dense = false;
+  f->dm = g->n;
+  f->out_edges = g->m;  // bits(part, n, m)
+  *out = f;
+  return GG_OK;
+}
+
+int gg_frontier_empty(gg_graph_t g, gg_frontier_t* out) {
+  if (!g || !out) return fail(GG_ERR_INVALID_ARG, "gg_frontier_empty: bad arguments");
+  return frontier_new(g, out);
+}
+
+int gg_frontier_from_mask(gg_graph_t g, const uint8_t* mask, gg_frontier_t* out) {
+  if (!g || !mask || !out) return fail(GG_ERR_INVALID_ARG, "gg_frontier_from_mask: bad arguments");
+  std::vector<uint32_t> words((size_t)g->words() + 4, 0);
+  for (uint32_t v = 0; v < g->n; ++v)
+    if (mask[v]) words[v >> 5] |= 1u << (v & 31);
+  gg_frontier_s* f;
+  GG_TRY(frontier_new(g, &f));
+  int rc = frontier_ensure_bits(f, false);
+  if (!rc && cudaMemcpyAsync(f->d_bits, words.data(), 4 * words.size(), cudaMemcpyHostToDevice, g->stream) != cudaSuccess)
+    rc = fail(GG_ERR_CUDA, "frontier upload failed");
+  if (!rc) rc = reset_stats(g);
+  if (!rc) {
+    k_bits_stats<<<generic_grid(g, g->words()), kGenericThreads, 0, g->stream>>>(f->d_bits, g->n, g->out_off(),
+                                                                                g->ws.d_stats);
+    rc = read_stats(g);
+  }
+  if (rc) {
+    frontier_free(f);
+    return rc;
+  }
+  f->has_dense = true;
+  f->dm = g->ws.h_stats[0];
+  f->out_edges = g->ws.h_stats[1];
+  *out = f;
+  return GG_OK;
+}
+
+int gg_frontier_from_list(gg_graph_t g, const uint32_t* verts, uint64_t count, gg_frontier_t* out) {
+  if (!g || (!verts && count) || !out || count > g->n)
+    return fail(GG_ERR_INVALID_ARG, "gg_frontier_from_list: bad arguments");
+  const uint32_t* off = g->h_out_off();
+  uint64_t oe = 0;
+  for (uint64_t i = 0; i < count; ++i) {
+    if (verts[i] >= g->n) return fail(GG_ERR_INVALID_ARG, "vertex %u out of range", verts[i]);
+    oe += off[verts[i] + 1] - off[verts[i]];
+  }
+  gg_frontier_s* f;
+  GG_TRY(frontier_new(g, &f));
+  int rc = frontier_ensure_queue(f);
+  if (!rc && count &&
+      cudaMemcpyAsync(f->d_queue, verts, 4 * count, cudaMemcpyHostToDevice, g->stream) != cudaSuccess)
+    rc = fail(GG_ERR_CUDA, "frontier upload failed");
+  if (!rc && cudaStreamSynchronize(g->stream) != cudaSuccess) rc = fail(GG_ERR_CUDA, "sync failed");
+  if (rc) {
+    frontier_free(f);
+    return rc;
+  }
+  f->has_sparse = true;
+  f->dm = count;
+  f->out_edges = oe;
+  *out = f;
+  return GG_OK;
+}
+
+int gg_frontier_destroy(gg_frontier_t f) {
+  if (!f) return fail(GG_ERR_INVALID_ARG, "gg_frontier_destroy: null frontier");
+  frontier_free(f);
+  return GG_OK;
+}
+
+int gg_frontier_stats(gg_frontier_t f, uint64_t* active, uint64_t* out_edges) {
+  if (!f) return fail(GG_ERR_INVALID_ARG, "gg_frontier_stats: null frontier");
+  if (active) *active = f->dm;
+  if (out_edges) *out_edges = f->out_edges;
+  return GG_OK;
+}
+
+int gg_frontier_to_mask(gg_frontier_t f, uint8_t* mask) {
+  if (!f || !mask) return fail(GG_ERR_INVALID_ARG, "gg_frontier_to_mask: bad arguments");
+  gg_graph_s* g = f->g;
+  const uint32_t n = g->n;
+  if (f->bit) {
+    memset(mask, 1, n);
+    return GG_OK;
+  }
+  memset(mask, 0, n);
+  if (f->dm == 0) return GG_OK;
+  if (f->has_dense) {
+    std::vector<uint32_t> words(g->words());
+    GG_CUDA(cudaMemcpyAsync(words.data(), f->d_bits, 4ull * words.size(), cudaMemcpyDeviceToHost, g->stream));
+    GG_CUDA(cudaStreamSynchronize(g->stream));
+    for (uint32_t v = 0; v < n; ++v) mask[v] = (words[v >> 5] >> (v & 31)) & 1u;
+  } else {
+    std::vector<uint32_t> q(f->dm);
+    GG_CUDA(cudaMemcpyAsync(q.data(), f->d_queue, 4ull * f->dm, cudaMemcpyDeviceToHost, g->stream));
+    GG_CUDA(cudaStreamSynchronize(g->stream));
+    for (uint32_t v : q) mask[v] = 1;
+  }
+  return GG_OK;
+}
+
+int gg_frontier_to_dense(gg_frontier_t f) {
+  if (!f) return fail(GG_ERR_INVALID_ARG, "gg_frontier_to_dense: null frontier");
+  int rc = frontier_to_dense(f);
+  if (!rc) rc = cudaStreamSynchronize(f->g->stream) == cudaSuccess ? GG_OK : fail(GG_ERR_CUDA, "sync failed");
+  return rc;
+}
+
+int gg_frontier_to_sparse(gg_frontier_t f) {
+  if (!f) return fail(GG_ERR_INVALID_ARG, "gg_frontier_to_sparse: null frontier");
+  int rc = frontier_to_sparse(f);
+  if (!rc) rc = cudaStreamSynchronize(f->g->stream) == cudaSuccess ? GG_OK : fail(GG_ERR_CUDA, "sync failed");
+  return rc;
+}
+
+int gg_frontier_repr(gg_frontier_t f) {
+  if (!f) return fail(GG_ERR_INVALID_ARG, "gg_frontier_repr: null frontier");
+  if (f->bit) return 4;
+  return (f->has_dense ? 1 : 0) | (f->has_sparse ? 2 : 0);
+}
+
+int gg_vertex_array_alloc(gg_graph_t g, size_t elem_bytes, void** dev_ptr) {
+  if (!g || !dev_ptr || !elem_bytes) return fail(GG_ERR_INVALID_ARG, "gg_vertex_array_alloc: bad arguments");
+  GG_CUDA(cudaMalloc(dev_ptr, elem_bytes * ((size_t)g->n + 4)));
+  return GG_OK;
+}
+int gg_vertex_array_free(gg_graph_t g, void* p) {
+  if (!g) return fail(GG_ERR_INVALID_ARG, "gg_vertex_array_free: null graph");
+  cudaStreamSynchronize(g->stream);
+  GG_CUDA(cudaFree(p));
+  return GG_OK;
+}
+int gg_memcpy_h2d(void* d, const void* h, size_t bytes) {
+  GG_CUDA(cudaMemcpy(d, h, bytes, cudaMemcpyHostToDevice));
+  return GG_OK;
+}
+int gg_memcpy_d2h(void* h, const void* d, size_t bytes) {
+  GG_CUDA(cudaMemcpy(h, d, bytes, cudaMemcpyDeviceToHost));
+  return GG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,665 @@
+// Host-side graph preparation: seeded generators, CSR/CSC construction, the
+// reference's two input formats, and the reference partitioner restated.
+//
+// None of this is on the timed path; the reference likewise excludes graph
+// load and partition build from its "Running :" time
+// (graphgrind/ligra-numa.h:1155-1157).
+#include <fcntl.h>
+#include <omp.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cerrno>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <limits>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "gg_common.h"
+#include "gg_hilbert.h"
+
+namespace gg {
+
+static thread_local std::string g_err;
+
+void set_error(const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+}
+const char* last_error() { return g_err.c_str(); }
+int fail(int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+// ------------------------------------------------------------ CSR builder
+// Edges come from a generator callable gen(i, &u, &v) -> bool(valid) over
+// i in [0, count).  The builder runs the generator twice (count, scatter) so
+// that no edge list is materialised, then sorts and de-duplicates each row.
+template <class Gen>
+static int build_csr(uint32_t n, uint64_t count, bool symmetric, Gen gen, gg_host_graph* out) {
+  std::vector<uint64_t> deg(static_cast<size_t>(n) + 1, 0);
+  uint64_t* degp = deg.data();
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < (int64_t)count; i++) {
+    uint32_t u, v;
+    if (!gen((uint64_t)i, &u, &v) || u == v) continue;
+    __atomic_fetch_add(&degp[u], 1, __ATOMIC_RELAXED);
+    if (symmetric) __atomic_fetch_add(&degp[v], 1, __ATOMIC_RELAXED);
+  }
+  std::vector<uint64_t> off(static_cast<size_t>(n) + 1, 0);
+  for (uint32_t i = 0; i < n; i++) off[i + 1] = off[i] + deg[i];
+  const uint64_t raw = off[n];
+  std::vector<uint32_t> col;
+  try {
+    col.resize(raw);
+  } catch (...) {
+    return fail(GG_ERR_OOM, "generator: cannot hold %llu edges", (unsigned long long)raw);
+  }
+  std::vector<uint64_t> cur(off.begin(), off.end() - 1);
+  uint64_t* curp = cur.data();
+  uint32_t* colp = col.data();
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < (int64_t)count; i++) {
+    uint32_t u, v;
+    if (!gen((uint64_t)i, &u, &v) || u == v) continue;
+    colp[__atomic_fetch_add(&curp[u], 1, __ATOMIC_RELAXED)] = v;
+    if (symmetric) colp[__atomic_fetch_add(&curp[v], 1, __ATOMIC_RELAXED)] = u;
+  }
+  // sort + unique per row
+  std::vector<uint64_t> newdeg(n, 0);
+#pragma omp parallel for schedule(dynamic, 1024)
+  for (int64_t r = 0; r < (int64_t)n; r++) {
+    uint32_t* b = colp + off[r];
+    uint32_t* e = colp + off[r + 1];
+    std::sort(b, e);
+    newdeg[r] = (uint64_t)(std::unique(b, e) - b);
+  }
+  uint64_t m = 0;
+  for (uint32_t i = 0; i < n; i++) m += newdeg[i];
+  if (m >= (1ULL << 32) - 64)
+    return fail(GG_ERR_SIZE, "graph has %llu edges; offsets are uint32", (unsigned long long)m);
+  out->n = n;
+  out->m = m;
+  out->symmetric = symmetric ? 1 : 0;
+  out->weight_type = GG_W_NONE;
+  out->weights = nullptr;
+  out->offsets = static_cast<uint32_t*>(malloc(sizeof(uint32_t) * (static_cast<size_t>(n) + 1)));
+  out->indices = static_cast<uint32_t*>(malloc(sizeof(uint32_t) * (m ? m : 1)));
+  if (!out->offsets || !out->indices) return fail(GG_ERR_OOM, "generator: out of host memory");
+  std::vector<uint64_t> noff(static_cast<size_t>(n) + 1, 0);
+  for (uint32_t i = 0; i < n; i++) noff[i + 1] = noff[i] + newdeg[i];
+#pragma omp parallel for schedule(static)
+  for (int64_t r = 0; r < (int64_t)n; r++) {
+    out->offsets[r] = (uint32_t)noff[r];
+    memcpy(out->indices + noff[r], colp + off[r], newdeg[r] * sizeof(uint32_t));
+  }
+  out->offsets[n] = (uint32_t)m;
+  return GG_OK;
+}
+
+// R-MAT sampler: each edge draws `scale` quadrant choices from a SplitMix64
+// stream keyed by (seed, edge index); two 32-bit draws per 64-bit output.
+struct RmatGen {
+  int scale;
+  uint64_t ta, tab, tabc, base;
+  bool operator()(uint64_t i, uint32_t* u, uint32_t* v) const {
+    uint64_t key = mix64(base + i);
+    uint32_t s = 0, d = 0;
+    uint64_t r = 0;
+    for (int l = 0; l < scale; l++) {
+      if ((l & 1) == 0) r = mix64(key + (uint64_t)l);
+      uint64_t x = (l & 1) ? (r >> 32) : (r & 0xffffffffULL);
+      uint32_t sb, db;
+      if (x < ta) { sb = 0; db = 0; }
+      else if (x < tab) { sb = 0; db = 1; }
+      else if (x < tabc) { sb = 1; db = 0; }
+      else { sb = 1; db = 1; }
+      s = (s << 1) | sb;
+      d = (d << 1) | db;
+    }
+    *u = s;
+    *v = d;
+    return true;
+  }
+};
+
+}  // namespace gg
+
+using namespace gg;
+
+extern "C" {
+
+const char* gg_last_error_string(void) { return gg::last_error(); }
+
+void gg_host_graph_free(gg_host_graph* g) {
+  if (!g) return;
+  free(g->offsets);
+  free(g->indices);
+  free(g->weights);
+  g->offsets = nullptr;
+  g->indices = nullptr;
+  g->weights = nullptr;
+  g->n = 0;
+  g->m = 0;
+}
+
+int gg_gen_rmat(int32_t scale, int32_t edge_factor, double a, double b, double c, uint64_t seed,
+                int32_t symmetric, gg_host_graph* out) {
+  if (!out || scale < 1 || scale > 31 || edge_factor < 1 || a < 0 || b < 0 || c < 0 ||
+      a + b + c > 1.0)
+    return fail(GG_ERR_INVALID_ARG, "gg_gen_rmat: bad arguments");
+  memset(out, 0, sizeof *out);
+  RmatGen g;
+  g.scale = scale;
+  const double two32 = 4294967296.0;
+  g.ta = (uint64_t)(a * two32);
+  g.tab = (uint64_t)((a + b) * two32);
+  g.tabc = (uint64_t)((a + b + c) * two32);
+  g.base = mix64(seed ^ 0x52a1d3e7c4b9f601ULL);
+  uint32_t n = 1u << scale;
+  uint64_t cnt = (uint64_t)edge_factor << scale;
+  return build_csr(n, cnt, symmetric != 0, g, out);
+}
+
+int gg_gen_grid(int32_t side, double long_range_frac, uint64_t seed, gg_host_graph* out) {
+  if (!out || side < 2 || side > 46340 || long_range_frac < 0)
+    return fail(GG_ERR_INVALID_ARG, "gg_gen_grid: bad arguments");
+  memset(out, 0, sizeof *out);
+  const uint64_t S = (uint64_t)side;
+  const uint64_t n = S * S;
+  const uint64_t horiz = S * (S - 1), vert = S * (S - 1);
+  const uint64_t grid_edges = horiz + vert;  // undirected
+  const uint64_t extra = (uint64_t)llround(long_range_frac * (double)grid_edges);
+  const uint64_t base = mix64(seed ^ 0x3c6ef372fe94f82bULL);
+  auto gen = [=](uint64_t i, uint32_t* u, uint32_t* v) -> bool {
+    if (i < horiz) {  // (r, c) - (r, c+1)
+      uint64_t r = i / (S - 1), c = i % (S - 1);
+      *u = (uint32_t)(r * S + c);
+      *v = (uint32_t)(r * S + c + 1);
+      return true;
+    }
+    i -= horiz;
+    if (i < vert) {  // (r, c) - (r+1, c)
+      uint64_t r = i / S, c = i % S;
+      *u = (uint32_t)(r * S + c);
+      *v = (uint32_t)((r + 1) * S + c);
+      return true;
+    }
+    i -= vert;
+    uint64_t x = mix64(base + i);
+    *u = (uint32_t)(((x & 0xffffffffULL) * n) >> 32);
+    *v = (uint32_t)(((x >> 32) * n) >> 32);
+    return true;
+  };
+  return build_csr((uint32_t)n, grid_edges + extra, true, gen, out);
+}
+
+int gg_gen_er(uint32_t n, uint64_t m, uint64_t seed, int32_t symmetric, gg_host_graph* out) {
+  if (!out || n < 2) return fail(GG_ERR_INVALID_ARG, "gg_gen_er: bad arguments");
+  memset(out, 0, sizeof *out);
+  const uint64_t base = mix64(seed ^ 0x9b05688c2b3e6c1fULL);
+  auto gen = [=](uint64_t i, uint32_t* u, uint32_t* v) -> bool {
+    uint64_t x = mix64(base + i);
+    *u = (uint32_t)(((x & 0xffffffffULL) * (uint64_t)n) >> 32);
+    *v = (uint32_t)(((x >> 32) * (uint64_t)n) >> 32);
+    return true;
+  };
+  return build_csr(n, m, symmetric != 0, gen, out);
+}
+
+int gg_host_graph_add_weights(gg_host_graph* g, int32_t weight_type, uint64_t seed, int32_t lo,
+                              int32_t hi) {
+  if (!g || !g->offsets || (weight_type != GG_W_INT32 && weight_type != GG_W_FLOAT32) ||
+      (weight_type == GG_W_INT32 && hi < lo))
+    return fail(GG_ERR_INVALID_ARG, "gg_host_graph_add_weights: bad arguments");
+  free(g->weights);
+  g->weights = malloc(4 * (g->m ? g->m : 1));
+  if (!g->weights) return fail(GG_ERR_OOM, "weights: out of host memory");
+  g->weight_type = weight_type;
+  const uint64_t base = mix64(seed ^ 0x7f4a7c159e3779b9ULL);
+  const uint64_t span = (uint64_t)((int64_t)hi - (int64_t)lo + 1);
+  const bool sym = g->symmetric != 0;
+#pragma omp parallel for schedule(dynamic, 4096)
+  for (int64_t u = 0; u < (int64_t)g->n; u++) {
+    for (uint32_t j = g->offsets[u]; j < g->offsets[u + 1]; j++) {
+      uint64_t v = g->indices[j];
+      uint64_t a = (uint64_t)u, bb = v;
+      if (sym && bb < a) std::swap(a, bb);  // one weight per undirected edge
+      uint64_t h = mix64(base + ((a << 32) | bb));
+      if (weight_type == GG_W_INT32) {
+        ((int32_t*)g->weights)[j] = (int32_t)(lo + (int64_t)(h % span));
+      } else {
+        float w = (float)((double)((h >> 40) + 1) * (1.0 / 16777216.0));
+        ((float*)g->weights)[j] = w;
+      }
+    }
+  }
+  return GG_OK;
+}
+
+int gg_host_graph_transpose(const gg_host_graph* g, gg_host_graph* out) {
+  if (!g || !out || !g->offsets) return fail(GG_ERR_INVALID_ARG, "transpose: bad arguments");
+  const uint32_t n = g->n;
+  const uint64_t m = g->m;
+  memset(out, 0, sizeof *out);
+  out->n = n;
+  out->m = m;
+  out->symmetric = g->symmetric;
+  out->weight_type = g->weight_type;
+  out->offsets = (uint32_t*)calloc((size_t)n + 1, sizeof(uint32_t));
+  out->indices = (uint32_t*)malloc(4 * (m ? m : 1));
+  if (g->weights) out->weights = malloc(4 * (m ? m : 1));
+  if (!out->offsets || !out->indices || (g->weights && !out->weights))
+    return fail(GG_ERR_OOM, "transpose: out of host memory");
+  std::vector<uint32_t> cnt((size_t)n + 1, 0);
+  uint32_t* cp = cnt.data();
+#pragma omp parallel for schedule(static)
+  for (int64_t j = 0; j < (int64_t)m; j++) __atomic_fetch_add(&cp[g->indices[j]], 1, __ATOMIC_RELAXED);
+  for (uint32_t i = 0; i < n; i++) out->offsets[i + 1] = out->offsets[i] + cnt[i];
+  std::vector<uint32_t> cur(out->offsets, out->offsets + n);
+  uint32_t* curp = cur.data();
+  const uint32_t* w = (const uint32_t*)g->weights;
+  uint32_t* ow = (uint32_t*)out->weights;
+#pragma omp parallel for schedule(dynamic, 4096)
+  for (int64_t u = 0; u < (int64_t)n; u++) {
+    for (uint32_t j = g->offsets[u]; j < g->offsets[u + 1]; j++) {
+      uint32_t v = g->indices[j];
+      uint32_t pos = __atomic_fetch_add(&curp[v], 1, __ATOMIC_RELAXED);
+      out->indices[pos] = (uint32_t)u;
+      if (ow) ow[pos] = w[j];
+    }
+  }
+  // deterministic in-lists: ascending source id (ids are unique per list)
+#pragma omp parallel for schedule(dynamic, 1024)
+  for (int64_t v = 0; v < (int64_t)n; v++) {
+    uint32_t b = out->offsets[v], e = out->offsets[v + 1];
+    if (e - b < 2) continue;
+    if (!ow) {
+      std::sort(out->indices + b, out->indices + e);
+    } else {
+      std::vector<std::pair<uint32_t, uint32_t>> tmp(e - b);
+      for (uint32_t k = b; k < e; k++) tmp[k - b] = {out->indices[k], ow[k]};
+      std::sort(tmp.begin(), tmp.end());
+      for (uint32_t k = b; k < e; k++) {
+        out->indices[k] = tmp[k - b].first;
+        ow[k] = tmp[k - b].second;
+      }
+    }
+  }
+  return GG_OK;
+}
+
+// ------------------------------------------------------------- file formats
+static int write_all(FILE* f, const void* p, size_t bytes) {
+  return fwrite(p, 1, bytes, f) == bytes ? 0 : -1;
+}
+
+// PBBS text ("AdjacencyGraph" / "WeightedAdjacencyGraph"), the layout read by
+// readGraphFromFile (graphgrind/IO.h:136-199).  Weights are written as ints.
+static int write_adj_one(const uint32_t* off, const uint32_t* idx, const void* w, int wt, uint32_t n,
+                         uint64_t m, const char* path) {
+  FILE* f = fopen(path, "wb");
+  if (!f) return fail(GG_ERR_IO, "cannot open %s for writing: %s", path, strerror(errno));
+  std::string buf;
+  buf.reserve(1 << 22);
+  auto flush = [&]() {
+    if (!buf.empty()) {
+      if (write_all(f, buf.data(), buf.size())) return -1;
+      buf.clear();
+    }
+    return 0;
+  };
+  char tmp[32];
+  buf += (wt != GG_W_NONE) ? "WeightedAdjacencyGraph\n" : "AdjacencyGraph\n";
+  buf += std::to_string(n) + "\n" + std::to_string(m) + "\n";
+  auto put = [&](long long x) {
+    int k = snprintf(tmp, sizeof tmp, "%lld\n", x);
+    buf.append(tmp, k);
+    if (buf.size() > (1 << 22) - 64) return flush();
+    return 0;
+  };
+  int rc = 0;
+  for (uint32_t i = 0; i < n && !rc; i++) rc = put(off[i]);
+  for (uint64_t j = 0; j < m && !rc; j++) rc = put(idx[j]);
+  if (wt != GG_W_NONE)
+    for (uint64_t j = 0; j < m && !rc; j++) {
+      long long x = (wt == GG_W_INT32) ? (long long)((const int32_t*)w)[j]
+                                       : (long long)llround(((const float*)w)[j]);
+      rc = put(x);
+    }
+  if (!rc) rc = flush();
+  if (fclose(f) || rc) return fail(GG_ERR_IO, "write failed: %s", path);
+  return GG_OK;
+}
+
+// Galois .gr version 1 (graphgrind/IO.h:365-450): u64 header {1, edge data
+// size, n, m}, u64 end offsets[n], u32 destinations[m] padded to even m,
+// u32 weights[m].
+static int write_gr_one(const uint32_t* off, const uint32_t* idx, const void* w, int wt, uint32_t n,
+                        uint64_t m, const char* path) {
+  FILE* f = fopen(path, "wb");
+  if (!f) return fail(GG_ERR_IO, "cannot open %s for writing: %s", path, strerror(errno));
+  uint64_t hdr[4] = {1, (uint64_t)(wt != GG_W_NONE ? 4 : 0), n, m};
+  int rc = write_all(f, hdr, sizeof hdr);
+  std::vector<uint64_t> ends(n);
+  for (uint32_t i = 0; i < n; i++) ends[i] = off[i + 1];
+  if (!rc) rc = write_all(f, ends.data(), 8ull * n);
+  if (!rc) rc = write_all(f, idx, 4ull * m);
+  uint32_t zero = 0;
+  if (!rc && (m & 1)) rc = write_all(f, &zero, 4);
+  if (!rc && wt != GG_W_NONE) {
+    if (wt == GG_W_INT32) {
+      rc = write_all(f, w, 4ull * m);
+    } else {
+      std::vector<int32_t> iw(m);
+      for (uint64_t j = 0; j < m; j++) iw[j] = (int32_t)llround(((const float*)w)[j]);
+      rc = write_all(f, iw.data(), 4ull * m);
+    }
+  }
+  if (fclose(f) || rc) return fail(GG_ERR_IO, "write failed: %s", path);
+  return GG_OK;
+}
+
+int gg_host_graph_write_adj(const gg_host_graph* g, const char* path) {
+  if (!g || !path) return fail(GG_ERR_INVALID_ARG, "write_adj: bad arguments");
+  int rc = write_adj_one(g->offsets, g->indices, g->weights, g->weight_type, g->n, g->m, path);
+  if (rc || g->symmetric) return rc;
+  gg_host_graph t;
+  if ((rc = gg_host_graph_transpose(g, &t))) return rc;
+  std::string tp = std::string(path) + "_t";
+  rc = write_adj_one(t.offsets, t.indices, t.weights, t.weight_type, t.n, t.m, tp.c_str());
+  gg_host_graph_free(&t);
+  return rc;
+}
+
+int gg_host_graph_write_gr(const gg_host_graph* g, const char* path) {
+  if (!g || !path) return fail(GG_ERR_INVALID_ARG, "write_gr: bad arguments");
+  int rc = write_gr_one(g->offsets, g->indices, g->weights, g->weight_type, g->n, g->m, path);
+  if (rc || g->symmetric) return rc;
+  gg_host_graph t;
+  if ((rc = gg_host_graph_transpose(g, &t))) return rc;
+  std::string tp = std::string(path) + "_t";
+  rc = write_gr_one(t.offsets, t.indices, t.weights, t.weight_type, t.n, t.m, tp.c_str());
+  gg_host_graph_free(&t);
+  return rc;
+}
+
+static int read_adj(const char* path, int32_t symmetric, int32_t weighted, gg_host_graph* out) {
+  int fd = open(path, O_RDONLY);
+  if (fd < 0) return fail(GG_ERR_IO, "cannot open %s: %s", path, strerror(errno));
+  struct stat st;
+  if (fstat(fd, &st)) {
+    close(fd);
+    return fail(GG_ERR_IO, "cannot stat %s", path);
+  }
+  size_t len = (size_t)st.st_size;
+  std::vector<char> data(len + 1);
+  size_t got = 0;
+  while (got < len) {
+    ssize_t r = read(fd, data.data() + got, len - got);
+    if (r <= 0) break;
+    got += (size_t)r;
+  }
+  close(fd);
+  if (got != len) return fail(GG_ERR_IO, "short read on %s", path);
+  data[len] = 0;
+  char* p = data.data();
+  char* end = p + len;
+  auto skip = [&]() { while (p < end && (*p == ' ' || *p == '\n' || *p == '\r' || *p == '\t')) p++; };
+  skip();
+  const char* hdr = weighted ? "WeightedAdjacencyGraph" : "AdjacencyGraph";
+  size_t hl = strlen(hdr);
+  if ((size_t)(end - p) < hl || strncmp(p, hdr, hl) != 0 || (p + hl < end && !isspace((unsigned char)p[hl])))
+    return fail(GG_ERR_FORMAT, "Bad input file: %s (expected header %s)", path, hdr);
+  p += hl;
+  auto next = [&](long long* x) -> bool {
+    skip();
+    if (p >= end) return false;
+    char* q;
+    errno = 0;
+    *x = strtoll(p, &q, 10);
+    if (q == p || errno) return false;
+    p = q;
+    return true;
+  };
+  long long n, m;
+  if (!next(&n) || !next(&m) || n < 1 || m < 0 || n > 0xffffffffLL || m >= (1LL << 32) - 64)
+    return fail(GG_ERR_FORMAT, "Bad input file (n,m): %s", path);
+  memset(out, 0, sizeof *out);
+  out->n = (uint32_t)n;
+  out->m = (uint64_t)m;
+  out->symmetric = symmetric;
+  out->weight_type = weighted ? GG_W_INT32 : GG_W_NONE;
+  out->offsets = (uint32_t*)malloc(4 * ((size_t)n + 1));
+  out->indices = (uint32_t*)malloc(4 * (size_t)(m ? m : 1));
+  if (weighted) out->weights = malloc(4 * (size_t)(m ? m : 1));
+  if (!out->offsets || !out->indices || (weighted && !out->weights)) {
+    gg_host_graph_free(out);
+    return fail(GG_ERR_OOM, "read: out of host memory");
+  }
+  long long x;
+  for (long long i = 0; i < n; i++) {
+    if (!next(&x) || x < 0 || x > m) {
+      gg_host_graph_free(out);
+      return fail(GG_ERR_FORMAT, "Bad input file (offsets): %s", path);
+    }
+    out->offsets[i] = (uint32_t)x;
+  }
+  out->offsets[n] = (uint32_t)m;
+  for (long long j = 0; j < m; j++) {
+    if (!next(&x) || x < 0 || x >= n) {
+      gg_host_graph_free(out);
+      return fail(GG_ERR_FORMAT, "Bad input file (edges): %s", path);
+    }
+    out->indices[j] = (uint32_t)x;
+  }
+  if (weighted)
+    for (long long j = 0; j < m; j++) {
+      if (!next(&x)) {
+        gg_host_graph_free(out);
+        return fail(GG_ERR_FORMAT, "Bad input file (weights): %s", path);
+      }
+      ((int32_t*)out->weights)[j] = (int32_t)x;
+    }
+  for (long long i = 0; i < n; i++)
+    if (out->offsets[i] > out->offsets[i + 1]) {
+      gg_host_graph_free(out);
+      return fail(GG_ERR_FORMAT, "Bad input file (offsets not monotone): %s", path);
+    }
+  return GG_OK;
+}
+
+static int read_gr(const char* path, int32_t symmetric, int32_t weighted, gg_host_graph* out) {
+  int fd = open(path, O_RDONLY);
+  if (fd < 0) return fail(GG_ERR_IO, "cannot open %s: %s", path, strerror(errno));
+  struct stat st;
+  if (fstat(fd, &st) || st.st_size < 32) {
+    close(fd);
+    return fail(GG_ERR_FORMAT, "Galois file too short: %s", path);
+  }
+  size_t len = (size_t)st.st_size;
+  const char* data = (const char*)mmap(nullptr, len, PROT_READ, MAP_SHARED, fd, 0);
+  close(fd);
+  if (data == (const char*)MAP_FAILED) return fail(GG_ERR_IO, "cannot mmap %s", path);
+  const uint64_t* h = (const uint64_t*)data;
+  int rc = GG_OK;
+  uint64_t n = h[2], m = h[3];
+  bool has_w = h[1] == 4;
+  size_t need = 32 + 8 * n + 4 * (m + (m & 1)) + (has_w ? 4 * m : 0);
+  memset(out, 0, sizeof *out);
+  if (h[0] != 1) rc = fail(GG_ERR_FORMAT, "Error in Galois input file: version (%llx) != 1", (unsigned long long)h[0]);
+  else if (n < 1 || n > 0xffffffffULL || m >= (1ULL << 32) - 64 || len < need)
+    rc = fail(GG_ERR_FORMAT, "Galois file %s: bad n/m or truncated", path);
+  else if (weighted && !has_w)
+    rc = fail(GG_ERR_FORMAT, "Galois file %s has no edge weights", path);
+  if (rc) {
+    munmap((void*)data, len);
+    return rc;
+  }
+  const uint64_t* ends = (const uint64_t*)(data + 32);
+  const uint32_t* dst = (const uint32_t*)(data + 32 + 8 * n);
+  const int32_t* wgt = (const int32_t*)(data + 32 + 8 * n + 4 * (m + (m & 1)));
+  out->n = (uint32_t)n;
+  out->m = m;
+  out->symmetric = symmetric;
+  out->weight_type = weighted ? GG_W_INT32 : GG_W_NONE;
+  out->offsets = (uint32_t*)malloc(4 * (n + 1));
+  out->indices = (uint32_t*)malloc(4 * (m ? m : 1));
+  if (weighted) out->weights = malloc(4 * (m ? m : 1));
+  if (!out->offsets || !out->indices || (weighted && !out->weights)) {
+    munmap((void*)data, len);
+    gg_host_graph_free(out);
+    return fail(GG_ERR_OOM, "read: out of host memory");
+  }
+  out->offsets[0] = 0;
+  for (uint64_t i = 0; i < n; i++) {
+    if (ends[i] > m || (i && ends[i] < ends[i - 1])) {
+      rc = fail(GG_ERR_FORMAT, "Galois file %s: bad offsets", path);
+      break;
+    }
+    out->offsets[i + 1] = (uint32_t)ends[i];
+  }
+  if (!rc && out->offsets[n] != m) rc = fail(GG_ERR_FORMAT, "Galois file %s: offsets end != m", path);
+  if (!rc) {
+    for (uint64_t j = 0; j < m; j++) {
+      if (dst[j] >= n) {
+        rc = fail(GG_ERR_FORMAT, "Galois file %s: edge target out of range", path);
+        break;
+      }
+      out->indices[j] = dst[j];
+    }
+  }
+  if (!rc && weighted) memcpy(out->weights, wgt, 4 * m);
+  munmap((void*)data, len);
+  if (rc) gg_host_graph_free(out);
+  return rc;
+}
+
+int gg_host_graph_read(const char* path, int32_t binary, int32_t symmetric, int32_t weighted,
+                       gg_host_graph* out) {
+  if (!path || !out) return fail(GG_ERR_INVALID_ARG, "read: bad arguments");
+  return binary ? read_gr(path, symmetric, weighted, out) : read_adj(path, symmetric, weighted, out);
+}
+
+// ---------------------------------------------------------------- partitioner
+// partitionByDegree (graphgrind/graph-numa.h:1287-1357) and
+// cscpartitionByDegree (:1208-1256): greedy accumulation of degrees into
+// partition `counter`; close early if the next vertex would overshoot
+// 1.1*average, close once the average is reached (never past P-1 for the
+// second rule).  `deg_next(i)` is degrees[i+1] with degrees[n] == 0.
+static int greedy_by_degree(const uint32_t* deg, uint64_t cnt, uint64_t m, int32_t P, int64_t* sizes) {
+  std::vector<int64_t> edges(P, 0);
+  for (int p = 0; p < P; p++) sizes[p] = 0;
+  const int64_t avg = (int64_t)m / P;
+  int64_t counter = 0;
+  for (uint64_t i = 0; i < cnt; i++) {
+    edges[counter] += deg[i];
+    sizes[counter]++;
+    int64_t nxt = (i + 1 < cnt) ? (int64_t)deg[i + 1] : 0;
+    if (edges[counter] < avg && (double)(nxt + edges[counter]) > 1.1 * (double)avg) counter++;
+    if (counter >= P)
+      return fail(GG_ERR_PARTITION,
+                  "partitionByDegree: partitions exhausted at vertex %llu of %llu (P=%d); the "
+                  "reference indexes past its P-entry arrays here",
+                  (unsigned long long)i, (unsigned long long)cnt, P);
+    if (edges[counter] >= avg && counter < P - 1) counter++;
+  }
+  if (counter + 1 != P)
+    return fail(GG_ERR_PARTITION,
+                "partitionByDegree: assert(counter+1 == numOfNode) fails (counter=%lld, P=%d)",
+                (long long)counter, P);
+  return GG_OK;
+}
+
+// The -o (relabel / VEBO) boundaries: a new partition whenever in-degree
+// rises (graphgrind/graph-numa.h:1180-1193, 1211-1224, 1290-1304).
+static int greedy_relabel(const uint32_t* indeg, uint64_t cnt, int32_t P, int64_t* sizes, bool check) {
+  for (int p = 0; p < P; p++) sizes[p] = 0;
+  int64_t counter = 0;
+  for (uint64_t j = 0; j < cnt; j++) {
+    sizes[counter]++;
+    if (j + 1 < cnt && indeg[j + 1] > indeg[j] && counter < P - 1) counter++;
+  }
+  if (check && counter + 1 != P)
+    return fail(GG_ERR_PARTITION, "relabel partitioning: assert(counter+1 == numOfNode) fails (counter=%lld, P=%d)",
+                (long long)counter, P);
+  return GG_OK;
+}
+
+int gg_partition_sizes(const uint32_t* in_degrees, const uint32_t* out_degrees, uint32_t n, uint64_t m,
+                       int32_t P, int32_t balance, int32_t part_how, int32_t relabel, int64_t* coo_sizes,
+                       int64_t* csc_sizes) {
+  if (!in_degrees || !out_degrees || !coo_sizes || !csc_sizes || P < 1 || n < 1)
+    return fail(GG_ERR_INVALID_ARG, "gg_partition_sizes: bad arguments");
+  const bool use_out = part_how == GG_PART_SOURCE;
+  int rc;
+  // COO partitioner over all n vertices
+  if (balance == GG_BALANCE_VERTEX) {
+    if (relabel) {
+      rc = greedy_relabel(in_degrees, n, P, coo_sizes, false);  // partitionByVertex has no assert
+    } else {
+      int64_t chunk = 0;
+      for (int i = 0; i < P - 1; i++) {
+        coo_sizes[i] = (int64_t)n / P;
+        chunk += coo_sizes[i];
+      }
+      coo_sizes[P - 1] = (int64_t)n - chunk;
+      rc = GG_OK;
+    }
+  } else {
+    rc = relabel ? greedy_relabel(in_degrees, n, P, coo_sizes, true)
+                 : greedy_by_degree(use_out ? out_degrees : in_degrees, n, m, P, coo_sizes);
+  }
+  if (rc) return rc;
+  // compressed CSC view: only vertices with in-degree > 0 (PartitionByDest :1078-1114)
+  std::vector<uint32_t> cin, cout_;
+  cin.reserve(n);
+  cout_.reserve(n);
+  for (uint32_t i = 0; i < n; i++)
+    if (in_degrees[i]) {
+      cin.push_back(in_degrees[i]);
+      cout_.push_back(out_degrees[i]);
+    }
+  const uint64_t cn = cin.size();
+  if (balance == GG_BALANCE_VERTEX) {
+    if (relabel) {
+      rc = greedy_relabel(cin.data(), cn, P, csc_sizes, false);
+    } else {
+      int64_t chunk = 0;
+      for (int i = 0; i < P - 1; i++) {
+        csc_sizes[i] = (int64_t)cn / P;
+        chunk += csc_sizes[i];
+      }
+      csc_sizes[P - 1] = (int64_t)cn - chunk;
+      rc = GG_OK;
+    }
+  } else {
+    if (cn == 0) return fail(GG_ERR_PARTITION, "cscpartitionByDegree: graph has no edges");
+    rc = relabel ? greedy_relabel(cin.data(), cn, P, csc_sizes, true)
+                 : greedy_by_degree(use_out ? cout_.data() : cin.data(), cn, m, P, csc_sizes);
+  }
+  return rc;
+}
+
+// HilbertEdgeSort::xy2d with the reference's grid side, see gg_hilbert.h.
+int64_t gg_hilbert_key(int64_t side_edges, int64_t x, int64_t y) {
+  return gg::hilbert_xy2d(gg::hilbert_side(side_edges), x, y);
+}
+
+}  // extern "C"

@@ -1,0 +1,257 @@
+// Host side of the engine: vertexSubset bookkeeping and the templated
+// edgeMap / vertexMap / vertexFilter drivers that launch the kernels of
+// gg_engine.cuh.  Mirrors graphgrind/ligra-numa.h:91-1082.
+#pragma once
+#include <algorithm>
+
+#include "gg_engine.cuh"
+#include "gg_functors.cuh"
+
+namespace gg {
+
+constexpr uint32_t kGenericThreads = 256;
+
+inline int generic_grid(const gg_graph_s* g, uint64_t work) {
+  uint64_t b = (work + kGenericThreads - 1) / kGenericThreads;
+  uint64_t cap = (uint64_t)g->num_sms * 8;
+  if (b < 1) b = 1;
+  return (int)std::min<uint64_t>(b, cap);
+}
+
+// ------------------------------------------------------------ frontiers
+int frontier_new(gg_graph_s* g, gg_frontier_s** out);
+int frontier_ensure_bits(gg_frontier_s* f, bool zero);
+int frontier_ensure_queue(gg_frontier_s* f);
+int frontier_to_dense(gg_frontier_s* f);
+int frontier_to_sparse(gg_frontier_s* f);
+void frontier_free(gg_frontier_s* f);
+int reset_stats(gg_graph_s* g);
+int read_stats(gg_graph_s* g);  // blocks; checks the device error word
+
+// -------------------------------------------------------------- edgeMap
+// graphgrind/ligra-numa.h:919-1019
+template <class F, bool HW>
+int pull_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f, bool coo) {
+  const bool all = in->bit;
+  PullParams p{};
+  const int orient = g->transposed ? 1 : 0;
+  if (coo) {
+    p.tiles = g->coo_tiles.d_tiles;
+    p.ntiles = g->coo_tiles.count;
+    p.src = g->d_coo_src;
+    p.dloc = g->d_coo_dloc;
+    p.wts = g->d_coo_w;
+    p.off = nullptr;
+  } else {
+    p.tiles = g->csc_tiles[orient].d_tiles;
+    p.ntiles = g->csc_tiles[orient].count;
+    p.src = g->in_idx();
+    p.dloc = nullptr;
+    p.wts = g->in_w();
+    p.off = g->in_off();
+  }
+  p.tile_counter = g->ws.d_stats + 4;
+  p.fr_bits = in->d_bits;
+  p.next_bits = out->d_bits;
+  p.deg_off = g->out_off();
+  // compressed-CSC membership (PartitionByDest, graphgrind/graph-numa.h:1098-1107):
+  // after transpose the pull still walks only vertices with original in-degree > 0
+  p.member_off = (g->transposed && !coo) ? g->d_csc_off : nullptr;
+  p.stats = g->ws.d_stats;
+  p.err = g->ws.d_stats + 3;
+  if (p.ntiles == 0) return GG_OK;
+  constexpr bool kHW = HW;
+  const size_t smem_coo = pull_smem_bytes(true, kHW, 4);
+  const size_t smem_csc = pull_smem_bytes(false, kHW, 4);
+  // one-time per instantiation: opt in to large dynamic shared memory, occupancy
+  static int occ[2][2] = {{-1, -1}, {-1, -1}};
+  auto launch = [&](auto kern, size_t smem, int& o) -> int {
+    if (o < 0) {
+      GG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      GG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, kPullThreads, smem));
+      if (o < 1) o = 1;
+    }
+    const int grid = (int)std::min<uint64_t>((uint64_t)g->num_sms * o, p.ntiles);
+    kern<<<grid, kPullThreads, smem, g->stream>>>(p, f);
+    GG_CUDA(cudaGetLastError());
+    g->kernels++;
+    return GG_OK;
+  };
+  if (coo) {
+    if (all) return launch(k_pull<F, true, kHW, true>, smem_coo, occ[1][1]);
+    return launch(k_pull<F, true, kHW, false>, smem_coo, occ[1][0]);
+  }
+  if (all) return launch(k_pull<F, false, kHW, true>, smem_csc, occ[0][1]);
+  return launch(k_pull<F, false, kHW, false>, smem_csc, occ[0][0]);
+}
+
+template <class F, bool HW>
+int pull_early_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f) {
+  const uint32_t* member = g->transposed ? g->d_csc_off : nullptr;
+  const int grid = generic_grid(g, g->n);
+  if (in->bit)
+    k_pull_early<F, HW, true><<<grid, kGenericThreads, 0, g->stream>>>(
+        g->n, g->in_off(), g->in_idx(), g->in_w(), nullptr, out->d_bits, g->out_off(), member, g->ws.d_stats, f);
+  else
+    k_pull_early<F, HW, false><<<grid, kGenericThreads, 0, g->stream>>>(
+        g->n, g->in_off(), g->in_idx(), g->in_w(), in->d_bits, out->d_bits, g->out_off(), member, g->ws.d_stats, f);
+  GG_CUDA(cudaGetLastError());
+  g->kernels++;
+  return GG_OK;
+}
+
+template <class F, bool HW>
+int push_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f) {
+  const uint32_t k = (uint32_t)in->dm;
+  const uint32_t nb = (k + kScanTile - 1) / kScanTile;
+  Workspace& ws = g->ws;
+  if (nb > ws.bsum_cap) {
+    if (ws.d_bsum) cudaFree(ws.d_bsum);
+    GG_CUDA(cudaMalloc(&ws.d_bsum, sizeof(uint32_t) * (nb + 32)));
+    ws.bsum_cap = nb;
+  }
+  const uint32_t* off = g->out_off();
+  k_scan_sums<<<nb, kScanThreads, 0, g->stream>>>(in->d_queue, k, off, ws.d_bsum);
+  k_scan_blocks<<<1, 1024, 0, g->stream>>>(ws.d_bsum, nb, ws.d_stats + 5);
+  k_scan_write<<<nb, kScanThreads, 0, g->stream>>>(in->d_queue, k, off, ws.d_bsum, ws.d_scan);
+  PushParams p{};
+  p.q = in->d_queue;
+  p.k = k;
+  p.offs = ws.d_scan;
+  p.total = ws.d_stats + 5;
+  p.off = off;
+  p.idx = g->out_idx();
+  p.wts = g->out_w();
+  p.deg_off = off;
+  p.dedup = ws.d_dedup;
+  p.out_q = out->d_queue;
+  p.stats = ws.d_stats;
+  // persistent CTAs: the edge total is read on the device
+  const uint64_t work_ub = std::max<uint64_t>(in->out_edges, 1);
+  const int grid = (int)std::min<uint64_t>((work_ub + kPushEdgesPerCta - 1) / kPushEdgesPerCta + 1,
+                                           (uint64_t)g->num_sms * 8);
+  k_push<F, HW><<<std::max(grid, g->num_sms), kPushThreads, 0, g->stream>>>(p, f);
+  k_clear_dedup<<<g->num_sms, kGenericThreads, 0, g->stream>>>(out->d_queue, ws.d_stats + 2, ws.d_dedup);
+  GG_CUDA(cudaGetLastError());
+  g->kernels += 5;
+  return GG_OK;
+}
+
+template <class F>
+int edge_map(gg_graph_s* g, gg_frontier_s* in, const F& f, int64_t threshold, uint32_t flags, gg_frontier_s** out) {
+  const int64_t m = (int64_t)g->m;
+  if (threshold < 0) threshold = m / 20;    // :932
+  const int64_t dense_threshold = m / 2;    // :934
+  const int64_t fm = (int64_t)in->dm;
+  const int64_t tot = (int64_t)in->out_edges;
+  g->last = gg_edge_map_stats{};
+  g->last.frontier_active = (uint64_t)fm;
+  g->last.frontier_out_edges = (uint64_t)tot;
+  gg_frontier_s* o = nullptr;
+  GG_TRY(frontier_new(g, &o));
+  if (tot == 0) {                           // :947
+    *out = o;
+    return GG_OK;
+  }
+  const bool hw = F::kUsesWeight && g->wtype != GG_W_NONE;
+  int rc = GG_OK;
+  bool dense = fm + tot > threshold;        // :953
+  if (flags & GG_EM_FORCE_SPARSE) dense = false;
+  if ((flags & (GG_EM_FORCE_CSC | GG_EM_FORCE_COO)) && !(flags & GG_EM_FORCE_SPARSE)) dense = true;
+  if (dense) {
+    bool coo = fm + tot > dense_threshold && g->has_coo;   // :957 (!part_ver)
+    if (flags & GG_EM_FORCE_CSC) coo = false;
+    if ((flags & GG_EM_FORCE_COO) && g->has_coo) coo = true;
+    if (!in->bit && !in->has_dense) rc = frontier_to_dense(in);
+    if (!rc) rc = frontier_ensure_bits(o, true);
+    if (!rc) rc = reset_stats(g);
+    if (!rc) {
+      if (!coo && F::kEarlyExit)
+        rc = hw ? pull_early_launch<F, true>(g, in, o, f) : pull_early_launch<F, false>(g, in, o, f);
+      else
+        rc = hw ? pull_launch<F, true>(g, in, o, f, coo) : pull_launch<F, false>(g, in, o, f, coo);
+    }
+    if (!rc) rc = read_stats(g);
+    if (!rc) {
+      o->has_dense = true;
+      o->dm = g->ws.h_stats[0];
+      o->out_edges = g->ws.h_stats[1];
+      g->last.kind = coo ? 3 : 2;
+    }
+  } else {
+    if (!in->has_sparse) rc = frontier_to_sparse(in);
+    if (!rc) rc = frontier_ensure_queue(o);
+    if (!rc) rc = reset_stats(g);
+    if (!rc && in->dm > 0) rc = hw ? push_launch<F, true>(g, in, o, f) : push_launch<F, false>(g, in, o, f);
+    if (!rc) rc = read_stats(g);
+    if (!rc) {
+      o->has_sparse = true;
+      o->dm = g->ws.h_stats[2];
+      o->out_edges = g->ws.h_stats[1];
+      g->last.kind = 1;
+    }
+  }
+  if (rc) {
+    frontier_free(o);
+    return rc;
+  }
+  g->last.output_active = o->dm;
+  g->last.output_out_edges = o->out_edges;
+  *out = o;
+  return GG_OK;
+}
+
+// ------------------------------------------------------------ vertexMap
+// graphgrind/ligra-numa.h:1023-1049
+template <class VF>
+int vertex_map(gg_graph_s* g, gg_frontier_s* f, const VF& vf) {
+  const int grid = generic_grid(g, f->has_dense || f->bit ? g->n : std::max<uint64_t>(f->dm, 1));
+  if (f->bit) {
+    k_vertex_map<VF, 0><<<generic_grid(g, g->n), kGenericThreads, 0, g->stream>>>(g->n, nullptr, nullptr, 0, vf);
+  } else if (f->has_dense) {
+    k_vertex_map<VF, 1><<<grid, kGenericThreads, 0, g->stream>>>(g->n, f->d_bits, nullptr, 0, vf);
+  } else if (f->has_sparse) {
+    if (f->dm == 0) return GG_OK;
+    k_vertex_map<VF, 2><<<grid, kGenericThreads, 0, g->stream>>>(g->n, nullptr, f->d_queue, f->dm, vf);
+  } else {
+    return GG_OK;  // empty
+  }
+  GG_CUDA(cudaGetLastError());
+  g->kernels++;
+  return GG_OK;
+}
+
+// ---------------------------------------------------------- vertexFilter
+// graphgrind/ligra-numa.h:1053-1082: dense output plus (count, out-degree)
+template <class VF>
+int vertex_filter(gg_graph_s* g, gg_frontier_s* f, const VF& vf, gg_frontier_s** out) {
+  gg_frontier_s* o = nullptr;
+  GG_TRY(frontier_new(g, &o));
+  int rc = GG_OK;
+  if (!f->bit && !f->has_dense && f->dm > 0) rc = frontier_to_dense(f);
+  if (!rc) rc = frontier_ensure_bits(o, true);
+  if (!rc) rc = reset_stats(g);
+  if (!rc) {
+    const int grid = generic_grid(g, g->n);
+    if (f->bit)
+      k_vertex_filter<VF, true><<<grid, kGenericThreads, 0, g->stream>>>(g->n, nullptr, o->d_bits, g->out_off(),
+                                                                        g->ws.d_stats, vf);
+    else if (f->has_dense)
+      k_vertex_filter<VF, false><<<grid, kGenericThreads, 0, g->stream>>>(g->n, f->d_bits, o->d_bits,
+                                                                         g->out_off(), g->ws.d_stats, vf);
+    if (cudaGetLastError() != cudaSuccess) rc = fail(GG_ERR_CUDA, "vertex_filter launch failed");
+    g->kernels++;
+  }
+  if (!rc) rc = read_stats(g);
+  if (rc) {
+    frontier_free(o);
+    return rc;
+  }
+  o->has_dense = true;
+  o->dm = g->ws.h_stats[0];
+  o->out_edges = g->ws.h_stats[1];
+  *out = o;
+  return GG_OK;
+}
+
+}  // namespace gg

@@ -1,0 +1,282 @@
+/*
+ * gg.h -- C ABI of the B200 traversal engine (edgeMap / vertexMap / vertexFilter
+ * over a destination-range partitioned, Hilbert-ordered graph).
+ *
+ * The reference (GraphGrind) has no FFI: its interface is header-only C++
+ * templates instantiated by each application's Compute().  Every entry point
+ * below names the reference interface it replaces (file:line inside the
+ * GraphGrind source tree).  Conventions:
+ *   - every function returns an int status: GG_OK (0) or a negative GG_ERR_*;
+ *     the library never aborts; gg_last_error_string() explains the last error
+ *     of the calling thread (the reference abort()s / assert()s instead,
+ *     graphgrind/ligra-numa.h:937-942, graphgrind/graph-numa.h:1253,1353);
+ *   - vertex ids and CSR/CSC offsets are uint32 (m < 2^32);
+ *   - device memory is owned by the library and released by *_destroy;
+ *   - a graph handle is not thread-safe; distinct handles may be used from
+ *     distinct threads.
+ * Functions under "host-only" touch no GPU and work on machines without one.
+ */
+#ifndef GG_H
+#define GG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define GG_OK 0
+#define GG_ERR_INVALID_ARG -1
+#define GG_ERR_CUDA -2
+#define GG_ERR_OOM -3
+#define GG_ERR_PARTITION -4   /* reference partitioner would assert/overflow */
+#define GG_ERR_IO -5
+#define GG_ERR_FORMAT -6
+#define GG_ERR_NO_DEVICE -7
+#define GG_ERR_UNSUPPORTED -8
+#define GG_ERR_TIMEOUT -9     /* a bounded device-side wait gave up */
+#define GG_ERR_SIZE -10       /* n or m beyond the uint32 limits */
+
+/* Human-readable text of the calling thread's last error. */
+const char* gg_last_error_string(void);
+/* Library version string. */
+const char* gg_version(void);
+
+/* ------------------------------------------------------ enums and flags */
+enum gg_weight_type { GG_W_NONE = 0, GG_W_INT32 = 1, GG_W_FLOAT32 = 2 };
+enum gg_balance { GG_BALANCE_EDGE = 0, GG_BALANCE_VERTEX = 1 };     /* -v edge|vertex */
+enum gg_part_how { GG_PART_DEST = 0, GG_PART_SOURCE = 1 };          /* -P dest|source */
+enum gg_order { GG_ORDER_HILBERT = 1, GG_ORDER_CSR = 0 };           /* EDGES_HILBERT */
+
+/* Options of gg_graph_build, mirroring parallel_main's flags
+ * (graphgrind/ligra-numa.h:1097-1130) plus GPU tiling knobs (0 = default). */
+typedef struct gg_build_opts {
+  int32_t num_partitions;   /* -c   (default 384)                           */
+  int32_t balance;          /* -v   gg_balance                              */
+  int32_t part_how;         /* -P   gg_part_how                             */
+  int32_t relabel;          /* -o   partition boundaries at degree rises    */
+  int32_t order;            /* EDGES_HILBERT: gg_order                      */
+  int32_t tile_vertices;    /* GPU: max destinations per CTA tile (<=8192)  */
+  int32_t tile_edges;       /* GPU: target edges per CTA tile               */
+  int32_t build_coo;        /* 1 = build the partitioned COO (default when balance==edge) */
+} gg_build_opts;
+
+typedef struct gg_graph_info {
+  uint32_t n;
+  uint64_t m;
+  int32_t symmetric;
+  int32_t weight_type;
+  int32_t num_partitions;
+  int32_t has_coo;
+  int32_t transposed;
+  int32_t num_csc_tiles;
+  int32_t num_coo_tiles;
+  uint64_t device_bytes;    /* HBM held by the graph */
+} gg_graph_info;
+
+/* ==================================================== host-only: graphs */
+/* A host CSR graph (out-edges).  offsets has n+1 entries. */
+typedef struct gg_host_graph {
+  uint32_t n;
+  uint64_t m;
+  int32_t symmetric;
+  int32_t weight_type;      /* gg_weight_type */
+  uint32_t* offsets;        /* n+1 */
+  uint32_t* indices;        /* m   */
+  void* weights;            /* m x 4 bytes or NULL */
+} gg_host_graph;
+
+/* Seeded generators (replace the absent rMatGraph inputs of the reference
+ * README; no generator exists in the reference).  Self-loops and duplicate
+ * edges are removed; symmetric=1 adds the reverse of every edge first.
+ * RMAT: 2^scale vertices, edge_factor*2^scale sampled edges, (a,b,c,d). */
+int gg_gen_rmat(int32_t scale, int32_t edge_factor, double a, double b, double c,
+                uint64_t seed, int32_t symmetric, gg_host_graph* out);
+/* 2D side x side 4-neighbour grid (symmetric) plus long_range_frac * grid-edges
+ * uniformly random extra undirected edges. */
+int gg_gen_grid(int32_t side, double long_range_frac, uint64_t seed, gg_host_graph* out);
+/* Erdos-Renyi G(n, m): m uniformly random (src,dst) samples. */
+int gg_gen_er(uint32_t n, uint64_t m, uint64_t seed, int32_t symmetric, gg_host_graph* out);
+/* Attach weights: GG_W_INT32 uniform in [lo,hi]; GG_W_FLOAT32 uniform in (0,1].
+ * The weight is a hash of (seed, src, dst), so an edge and its reverse view
+ * in the CSC carry the same weight. */
+int gg_host_graph_add_weights(gg_host_graph* g, int32_t weight_type, uint64_t seed,
+                              int32_t lo, int32_t hi);
+/* Read/write the reference's input formats (graphgrind/IO.h:136-199 PBBS
+ * text, graphgrind/IO.h:365-450 Galois .gr v1).  A directed .gr/.adj also gets
+ * its "<path>_t" transpose file on write, which the reference loads when present. */
+int gg_host_graph_write_adj(const gg_host_graph* g, const char* path);
+int gg_host_graph_write_gr(const gg_host_graph* g, const char* path);
+int gg_host_graph_read(const char* path, int32_t binary, int32_t symmetric,
+                       int32_t weighted, gg_host_graph* out);
+/* CSC (in-edges) of a host graph: in_offsets n+1, in_indices m, in_weights m. */
+int gg_host_graph_transpose(const gg_host_graph* g, gg_host_graph* out);
+void gg_host_graph_free(gg_host_graph* g);
+
+/* Partition sizes exactly as the reference computes them
+ * (partitionByDegree graphgrind/graph-numa.h:1287-1357, partitionByVertex
+ * :1177-1206) for the COO partitions, and (cscpartitionByDegree :1208-1256,
+ * cscpartitionByVertex :1258-1285) for the compressed CSC ranges.  The one
+ * deviation: degrees[n] (read one past the end at :1335 / :1248) is taken as 0.
+ * Returns GG_ERR_PARTITION where the reference asserts (counter+1 != P) or
+ * would index past its P-entry arrays.  sizes has P entries. */
+int gg_partition_sizes(const uint32_t* in_degrees, const uint32_t* out_degrees, uint32_t n,
+                       uint64_t m, int32_t P, int32_t balance, int32_t part_how,
+                       int32_t relabel, int64_t* coo_sizes, int64_t* csc_sizes);
+/* Hilbert key of edge (x=src, y=dst) on the reference's grid, whose side is
+ * roundUpPow2(edges in the partition) (graphgrind/graph-numa.h:353-386, 487). */
+int64_t gg_hilbert_key(int64_t side_edges, int64_t x, int64_t y);
+
+/* ============================================================ device graph */
+typedef struct gg_graph_s* gg_graph_t;
+typedef struct gg_frontier_s* gg_frontier_t;
+
+/* partitioned_graph constructor (graphgrind/graph-numa.h:642-685): uploads the
+ * CSR, builds CSC, the -c destination-range partitions and, for -v edge, the
+ * Hilbert/CSR-sorted partitioned COO, cut into CTA tiles sized to shared memory. */
+int gg_graph_build(const gg_host_graph* g, const gg_build_opts* opts, gg_graph_t* out);
+int gg_graph_destroy(gg_graph_t g);
+int gg_graph_get_info(gg_graph_t g, gg_graph_info* info);
+/* Partition starts (P+1 entries) of the COO partitioner (partitioner::start_of,
+ * graphgrind/partitioner.h:153-165). */
+int gg_graph_partition_starts(gg_graph_t g, int64_t* starts);
+/* partitioned_graph::transpose (graphgrind/graph-numa.h:721-728): swaps the
+ * out/in roles of CSR and CSC for symmetric=0 graphs; the COO partitions are
+ * NOT transposed, as in the reference. */
+int gg_graph_transpose(gg_graph_t g);
+/* Out-degree of every vertex in the current orientation (device pointer). */
+int gg_graph_device_arrays(gg_graph_t g, const uint32_t** out_offsets,
+                           const uint32_t** out_indices, const uint32_t** in_offsets,
+                           const uint32_t** in_indices);
+
+/* ===================================================== vertexSubset API */
+/* partitioned_vertices (graphgrind/ligra-numa.h:91-272). */
+int gg_frontier_single(gg_graph_t g, uint32_t v, gg_frontier_t* out);   /* ::create :103 */
+int gg_frontier_all(gg_graph_t g, gg_frontier_t* out);                  /* ::bits   :169 */
+int gg_frontier_empty(gg_graph_t g, gg_frontier_t* out);                /* ::empty  :119 */
+/* From a host byte mask (1 = active); the frontier is dense with exact stats. */
+int gg_frontier_from_mask(gg_graph_t g, const uint8_t* mask, gg_frontier_t* out);
+/* From a host vertex list (must be duplicate-free); the frontier is sparse. */
+int gg_frontier_from_list(gg_graph_t g, const uint32_t* verts, uint64_t count,
+                          gg_frontier_t* out);
+int gg_frontier_destroy(gg_frontier_t f);                               /* ::del    :210 */
+/* numNonzeros (:268) and num_out_edges (:99). */
+int gg_frontier_stats(gg_frontier_t f, uint64_t* active, uint64_t* out_edges);
+/* Dense byte mask (n bytes) of the members, copied to the host. */
+int gg_frontier_to_mask(gg_frontier_t f, uint8_t* mask);
+/* Force representation: toDense (:228) / toSparse (:246). */
+int gg_frontier_to_dense(gg_frontier_t f);
+int gg_frontier_to_sparse(gg_frontier_t f);
+/* 1 if the frontier currently holds a dense bitmap, 2 if sparse, 3 both, 4 'bit' (all). */
+int gg_frontier_repr(gg_frontier_t f);
+
+/* ================================================== built-in functors */
+/* The functor structs of the app/ sources re-hosted as device functors.  Arguments
+ * point at device vertex arrays allocated with gg_vertex_array_alloc. */
+enum gg_functor_id {
+  GG_F_BFS = 1,            /* app/BFS.C:26-75            args: gg_bfs_args      */
+  GG_F_CC = 2,             /* app/Components.C:127-186   args: gg_cc_args       */
+  GG_F_PR = 3,             /* app/PageRank.C:256-298     args: gg_pr_args       */
+  GG_F_PRDELTA = 4,        /* app/PageRankDelta.C:29-71  args: gg_prdelta_args  */
+  GG_F_SPMV = 5,           /* app/SPMV.C:7-47            args: gg_spmv_args     */
+  GG_F_BF = 6,             /* app/BellmanFord.C:28-92    args: gg_bf_args       */
+  GG_F_BC = 7,             /* app/BC.C:28-71 (BC_F)      args: gg_bc_args       */
+  GG_F_BC_BACK = 8,        /* app/BC.C:73-117 (BC_Back_F) args: gg_bc_args      */
+  GG_F_BP = 9              /* app/BP.C:54-130            args: gg_bp_args       */
+};
+typedef struct { int32_t* parents; int32_t* levels; int32_t round; } gg_bfs_args;
+typedef struct { int32_t* ids; int32_t* prev_ids; } gg_cc_args;
+typedef struct { const float* p_curr; float* p_next; } gg_pr_args;
+typedef struct { const float* delta; float* ngh_sum; } gg_prdelta_args;
+typedef struct { const float* p_curr; float* p_next; } gg_spmv_args;
+typedef struct { int32_t* sp_len; int32_t* visited; } gg_bf_args;
+typedef struct { float* values; uint8_t* visited; } gg_bc_args;
+typedef struct { const float* edge_pot; const float* vert_pot; const float* edge_cur;
+                 float* edge_next; const float* vert_cur; float* vert_next; } gg_bp_args;
+
+/* edgeMap flags */
+#define GG_EM_FORCE_SPARSE 0x1u   /* take the push branch regardless of size   */
+#define GG_EM_FORCE_CSC 0x2u      /* dense branch: pull over CSC                */
+#define GG_EM_FORCE_COO 0x4u      /* dense branch: partitioned COO              */
+#define GG_EM_NO_OUTPUT 0x8u      /* caller discards the output (output.del())  */
+
+/* Per-call statistics of the last edgeMap on a graph handle. */
+typedef struct gg_edge_map_stats {
+  int32_t kind;             /* 0 empty, 1 sparse push, 2 dense CSC pull, 3 dense COO */
+  uint64_t frontier_active;
+  uint64_t frontier_out_edges;
+  uint64_t output_active;
+  uint64_t output_out_edges;
+} gg_edge_map_stats;
+
+/* edgeMap (graphgrind/ligra-numa.h:919-1019): threshold < 0 means m/20;
+ * direction switch m_f + outdeg(F) > threshold -> dense, > m/2 (and
+ * balance==edge) -> COO else CSC pull; otherwise sparse push over CSR. */
+int gg_edge_map(gg_graph_t g, gg_frontier_t in, int32_t functor_id, const void* functor_args,
+                int64_t threshold, uint32_t flags, gg_frontier_t* out);
+int gg_last_edge_map_stats(gg_graph_t g, gg_edge_map_stats* stats);
+
+/* Vertex functors for vertexMap / vertexFilter (graphgrind/ligra-numa.h:1023-1082). */
+enum gg_vertex_functor_id {
+  GG_V_CC_COPY = 101,      /* app/Components.C:189-200  prevIDs[i]=IDs[i]      args gg_cc_args   */
+  GG_V_PR_UPDATE = 102,    /* app/PageRank.C:301-315    p=d*p+(1-d)/n          args gg_pr_vertex_args */
+  GG_V_FILL_F32 = 103,     /* PR/SPMV reset: a[i]=value                        args gg_fill_args */
+  GG_V_FILL_I32 = 104,     /* BF_Vertex_F: a[i]=value                          args gg_fill_args */
+  GG_V_PRDELTA_FIRST = 105,/* app/PageRankDelta.C:73-90 (filter)             args gg_prdelta_vertex_args */
+  GG_V_PRDELTA = 106,      /* app/PageRankDelta.C:92-106 (filter)            args gg_prdelta_vertex_args */
+  GG_V_BC_MARK = 107,      /* app/BC.C:119-128 Visited[i]=1                  args gg_bc_args */
+  GG_V_BC_BACK = 108,      /* app/BC.C:131-143                               args gg_bc_back_vertex_args */
+  GG_V_FILL_U8 = 109       /* a[i]=value (bytes)                              args gg_fill_args */
+};
+typedef struct { float* p_next; float damping; uint32_t n; } gg_pr_vertex_args;
+typedef struct { void* array; double value; } gg_fill_args;
+typedef struct { float* p; float* delta; const float* ngh_sum; float damping; float one_over_n;
+                 float epsilon2; } gg_prdelta_vertex_args;
+typedef struct { uint8_t* visited; float* dependencies; const float* inv_num_paths; } gg_bc_back_vertex_args;
+
+int gg_vertex_map(gg_graph_t g, gg_frontier_t f, int32_t vfunctor_id, const void* args);
+int gg_vertex_filter(gg_graph_t g, gg_frontier_t f, int32_t vfunctor_id, const void* args,
+                     gg_frontier_t* out);
+
+/* Device vertex arrays (mmap_ptr<T>::part_allocate, graphgrind/mm.h:246-324). */
+int gg_vertex_array_alloc(gg_graph_t g, size_t elem_bytes, void** dev_ptr);
+int gg_vertex_array_free(gg_graph_t g, void* dev_ptr);
+int gg_memcpy_h2d(void* dev_dst, const void* host_src, size_t bytes);
+int gg_memcpy_d2h(void* host_dst, const void* dev_src, size_t bytes);
+
+/* ====================================================== applications */
+/* Each runs the Compute() loop of the named app on the device and copies its
+ * result to host arrays of n entries.  Timing (device, ms) of the loop alone
+ * is returned in *ms when ms != NULL, like the reference's "Running : t". */
+typedef struct gg_run_stats {
+  double ms;                /* device time of the Compute loop               */
+  int32_t rounds;           /* edgeMap calls (levels / iterations)           */
+  uint64_t edges_traversed; /* sum of frontier out-degrees (ligra-numa.h:945) */
+  int32_t kernels;          /* kernels launched by the loop                  */
+} gg_run_stats;
+
+/* app/BFS.C:77-101: parents[n] (-1 unreached), levels[n] (-1 unreached). */
+int gg_bfs(gg_graph_t g, uint32_t start, int32_t* parents, int32_t* levels, gg_run_stats* st);
+/* app/Components.C:202-227: ids[n]. */
+int gg_components(gg_graph_t g, int32_t* ids, gg_run_stats* st);
+/* app/PageRank.C:330-378 (bit_all=0) and app/PageRankBit.C (bit_all=1):
+ * ranks[n] in FP32, max_iter iterations (10 in the reference). */
+int gg_pagerank(gg_graph_t g, int32_t max_iter, int32_t bit_all, float* ranks, gg_run_stats* st);
+/* app/PageRankDelta.C:120-174: ranks[n]. */
+int gg_pagerank_delta(gg_graph_t g, float* ranks, gg_run_stats* st);
+/* app/SPMV.C:65-93 with x = 1/n (x_in == NULL) or x_in[n]: y[n] = A^T-weighted sum. */
+int gg_spmv(gg_graph_t g, const float* x_in, float* y, gg_run_stats* st);
+/* app/BellmanFord.C:106-145: dist[n] (1073741823 = unreached). */
+int gg_bellman_ford(gg_graph_t g, uint32_t start, int32_t* dist, gg_run_stats* st);
+/* app/BC.C:156-226 single source: dependencies[n], num_paths[n] (forward counts). */
+int gg_bc(gg_graph_t g, uint32_t start, float* dependencies, float* num_paths, gg_run_stats* st);
+/* app/BP.C:152-212 with defined inputs: 2-state beliefs vert_out[2n] after iters. */
+int gg_bp(gg_graph_t g, int32_t iters, const float* vert_potential, const float* edge_potential,
+          float* vert_out, gg_run_stats* st);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GG_H */

@@ -1,0 +1,65 @@
+/*
+ * gg_oracle.h -- TEST INFRASTRUCTURE ONLY.  A sequential CPU restatement of
+ * GraphGrind's traversal engine and applications, used as the checker for the
+ * GPU library.  Only tests/, __graft_entry__.smoke() and bench.py's CPU
+ * baseline leg may load it; the product never does.
+ *
+ * FP64 throughout for PageRank / PageRankDelta / SPMV / BC (the reference's
+ * PR/PRDelta/SPMV are double, app/PageRank.C:258, and BC's float is widened,
+ * app/BC.C:26); integer apps use int64 like the reference's intT.
+ */
+#ifndef GG_ORACLE_H
+#define GG_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct or_graph {
+  uint32_t n;
+  uint64_t m;
+  int32_t symmetric;
+  int32_t part_vertex;      /* -v vertex: no COO, dense always pulls (ligra-numa.h:957) */
+  const uint32_t* out_off;  /* n+1 */
+  const uint32_t* out_idx;  /* m   */
+  const uint32_t* in_off;   /* n+1 */
+  const uint32_t* in_idx;   /* m   */
+  const double* out_w;      /* m or NULL (weights as read by the app: int or float) */
+  const double* in_w;       /* m or NULL */
+  /* COO edge order for the dense >m/2 branch: m (src,dst) pairs in partition
+   * order, or NULL to use CSC order (dst-major). */
+  const uint32_t* coo_src;
+  const uint32_t* coo_dst;
+  const double* coo_w;
+} or_graph;
+
+typedef struct or_stats {
+  int32_t rounds;           /* edgeMap calls */
+  int64_t edges_traversed;  /* sum of frontier num_out_edges (ligra-numa.h:945) */
+  int32_t kinds[4];         /* edgeMaps per branch: empty, sparse, csc, coo */
+} or_stats;
+
+int or_bfs(const or_graph* g, uint32_t start, int64_t* parents, int32_t* levels, or_stats* st);
+int or_cc(const or_graph* g, int64_t* ids, or_stats* st);
+int or_pagerank(const or_graph* g, int32_t max_iter, int32_t bit_all, double* ranks, or_stats* st);
+int or_pagerank_delta(const or_graph* g, double* ranks, or_stats* st);
+int or_spmv(const or_graph* g, const double* x, double* y, or_stats* st);
+int or_bellman_ford(const or_graph* g, uint32_t start, int64_t* dist, or_stats* st);
+int or_bc(const or_graph* g, uint32_t start, double* dependencies, double* num_paths, or_stats* st);
+int or_bp(const or_graph* g, int32_t iters, const double* vert_pot, const double* edge_pot,
+          double* vert_out, or_stats* st);
+/* PageRank iterated to convergence-free fixed count on every vertex (the
+ * k-column personalised form uses this per column): x_{t+1} = d*A x_t + (1-d)*tele. */
+int or_ppr(const or_graph* g, int32_t iters, double damping, const double* tele, double* x);
+
+/* Partition sizes by the reference rules (same contract as gg_partition_sizes). */
+int or_partition_sizes(const uint32_t* in_deg, const uint32_t* out_deg, uint32_t n, uint64_t m,
+                       int32_t P, int32_t balance, int32_t part_how, int32_t relabel,
+                       int64_t* coo_sizes, int64_t* csc_sizes);
+int64_t or_hilbert_key(int64_t side_edges, int64_t x, int64_t y);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
