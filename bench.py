@@ -1,0 +1,344 @@
+#!/usr/bin/env python3
+"""Throughput of the B200 traversal engine (GTEPS) on RMAT-24.
+
+Workload (one "step"): on RMAT scale 24, edge factor 16, (a,b,c,d) =
+(0.57,0.19,0.19,0.05), seed 2, directed, self-loops and duplicates removed,
+uint32 ids, FP32 edge weights uniform in (0,1], 384 edge-balanced
+destination partitions with Hilbert-ordered COO:
+    BFS from vertex 100  +  PageRank (10 iterations, FP32)  +  SpMV (FP32 weights)
+each run through the library's C ABI (gg_bfs / gg_pagerank / gg_spmv).
+
+  value  = traversed edges of the step / device time of the three Compute
+           loops (CUDA events on the library's stream), graph resident in HBM
+  e2e    = same edges / host wall time of the same C-ABI calls, including the
+           H2D copy of the SpMV input vector from pinned memory and the D2H
+           copies of every result array (BFS parents+levels, ranks, y)
+  roofline = the dense-pull kernel of the PageRank iterations: algorithmic
+           bytes 8m + 16n per launch over its CUDA-event duration
+  cpu_baseline = the reference's own OpenMP build (oracle/_ref) on the host
+           cores, on a bounded RMAT-22 sample of the same workload
+
+Multi-GPU: the path does not shard across GPUs in this build (one GPU per
+graph); --gpus N runs N independent replicas under torchrun and reports the
+aggregate ("scaling": "weak").
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GTEPS"
+UNIT = "GTEPS"
+WORKLOAD = ("RMAT-24 directed (n=2^24, edge factor 16, a/b/c/d=.57/.19/.19/.05, seed 2, dedup, FP32 weights U(0,1]), "
+            "P=384 edge-balanced Hilbert COO; step = BFS from 100 + PageRank 10 iterations + SpMV")
+HBM_FALLBACK_GBS = 6650.0
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: str):
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.proc = None
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", gpu_index, f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception as e:  # no nvidia-smi: report without clocks
+            log("clock sampler unavailable:", e)
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        self.f.close()
+        sm, smax, power, reasons = [], [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+                power.append(float(p[3]))
+            except ValueError:
+                continue
+            for name, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        load = [s for s, w in zip(sm, power) if w > 0.3 * max(power)] or sm
+        return {"sm_mhz": statistics.median(load), "sm_max_mhz": max(smax), "samples": len(sm),
+                "power_w_max": max(power), "reasons": sorted(reasons)}
+
+
+def peak_hbm():
+    try:
+        p = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+# ------------------------------------------------------------- the workload
+def make_graph(gg, scale: int, seed: int, weights: int):
+    hg = gg.HostGraph.rmat(scale, 16, 0.57, 0.19, 0.19, seed=seed, symmetric=False)
+    if weights == gg.W_FLOAT32:
+        hg.add_weights(gg.W_FLOAT32, seed=seed + 100)
+    elif weights == gg.W_INT32:
+        hg.add_weights(gg.W_INT32, seed=seed + 100, lo=1, hi=100)
+    return hg
+
+
+def run_ours(args, rank: int, world: int, local_rank: int, dist):
+    import graphgrind_b200 as gg
+
+    t0 = time.time()
+    hg = make_graph(gg, args.scale, 2, gg.W_FLOAT32)
+    log(f"[rank {rank}] generated RMAT-{args.scale}: n={hg.n} m={hg.m} in {time.time() - t0:.1f}s")
+    t0 = time.time()
+    g = gg.Graph(hg, partitions=args.partitions)
+    g.set_dense_policy(args.dense_policy)
+    info = g.info()
+    log(f"[rank {rank}] device graph built in {time.time() - t0:.1f}s: {info.device_bytes / 2**30:.2f} GiB, "
+        f"{info.num_coo_tiles} COO tiles, {info.num_csc_tiles} CSC tiles")
+    n, m = hg.n, hg.m
+    x = gg.PinnedArray(n, np.float32)
+    x.array[:] = np.random.default_rng(7).random(n, dtype=np.float32)
+    par, lev = gg.PinnedArray(n, np.int32), gg.PinnedArray(n, np.int32)
+    ranks, y = gg.PinnedArray(n, np.float32), gg.PinnedArray(n, np.float32)
+
+    def step():
+        _, _, b = g.bfs(args.start, out=(par.array, lev.array))
+        _, p = g.pagerank(10, out=ranks.array)
+        _, s = g.spmv(x.array, out=y.array)
+        return b, p, s
+
+    for _ in range(args.warmup):
+        step()
+    if dist:
+        dist.barrier()
+    gpu_index = os.environ.get("CUDA_VISIBLE_DEVICES", str(local_rank)).split(",")[local_rank] if \
+        os.environ.get("CUDA_VISIBLE_DEVICES") else str(local_rank)
+    clocks = ClockSampler(gpu_index)
+    g.set_profiling(True)
+    g.profile()  # reset
+    dev_ms, wall_s, edges, launches = 0.0, 0.0, 0, 0
+    per_app = {"bfs": [0, 0.0], "pagerank": [0, 0.0], "spmv": [0, 0.0]}
+    pr_prof = {"launches": 0, "ms": 0.0}
+    pr_kind = None
+    for _ in range(args.steps):
+        w0 = time.perf_counter()
+        b, p, s = step()
+        wall_s += time.perf_counter() - w0
+        for name, r in (("bfs", b), ("pagerank", p), ("spmv", s)):
+            per_app[name][0] += r.edges_traversed
+            per_app[name][1] += r.ms
+            dev_ms += r.ms
+            edges += r.edges_traversed
+            launches += r.kernels
+    prof = g.profile()
+    # PageRank-only profile for the dense-pull roofline (separate, identical calls)
+    for _ in range(2):
+        g.pagerank(10, out=ranks.array)
+    prof_pr = g.profile()
+    g.set_profiling(False)
+    clk = clocks.stop()
+    for k in ("csc_pull", "coo_pull"):
+        if prof_pr[k]["launches"] >= pr_prof["launches"]:
+            pr_kind, pr_prof = k, prof_pr[k]
+    if dist:
+        import torch
+        t = torch.tensor([dev_ms, wall_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_ms, wall_s = float(t[0]), float(t[1])
+        e = torch.tensor([edges, launches], dtype=torch.float64, device="cuda")
+        dist.all_reduce(e, op=dist.ReduceOp.SUM)
+        edges_all, launches_all = float(e[0]), int(e[1])
+    else:
+        edges_all, launches_all = float(edges), launches
+    value = edges_all / (dev_ms / 1e3) / 1e9
+    e2e = edges_all / wall_s / 1e9
+    peak, peak_kind = peak_hbm()
+    pull_ms = pr_prof["ms"] / max(pr_prof["launches"], 1)
+    algo_bytes = 8 * m + 16 * n
+    achieved = algo_bytes / (pull_ms / 1e3) / 1e9 if pull_ms > 0 else None
+    out = {
+        "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(dev_ms / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (PageRank/SpMV), u32 (BFS ids)",
+        "data": "synthetic: seeded RMAT generated on the host (no dataset)",
+        "config": {"workload": WORKLOAD, "n": n, "m": m, "partitions": args.partitions,
+                   "dense_policy": ["reference rule", "csc pull", "coo pull"][args.dense_policy],
+                   "l2": "inputs larger than L2 (graph arrays > 3 GB vs 126 MB L2)",
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "apps": {k: {"edges": int(v[0]), "ms": round(v[1] / args.steps, 4),
+                     "gteps": round(v[0] / (v[1] / 1e3) / 1e9, 4) if v[1] else None} for k, v in per_app.items()},
+        "roofline": {"bound": "hbm", "kernel": f"k_pull ({pr_kind}) in PageRank",
+                     "achieved": round(achieved, 1) if achieved else None, "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4) if achieved else None, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": algo_bytes, "launch_ms": round(pull_ms, 4),
+                     "launches": pr_prof["launches"], "traffic": args.traffic},
+        "kernel_profile": {k: {"launches": v["launches"], "ms": round(v["ms"], 3)} for k, v in prof.items()},
+        "e2e": {"value": round(e2e, 4), "unit": UNIT, "h2d_bytes_per_step": 4 * n + 4,
+                "d2h_bytes_per_step": 16 * n},
+        "gpu_launches": launches_all,
+        "clocks": clk,
+    }
+    return out
+
+
+# ------------------------------------------------------- the reference (CPU)
+def reference_sample(scale: int, partitions: int, rounds: int, workdir: str):
+    """Time the reference's own BFS, PageRank and SPMV (OpenMP build of
+    GraphGrind, oracle/_ref) on an RMAT sample of the workload.  Returns
+    (per-round GTEPS list, info dict)."""
+    import graphgrind_b200 as gg
+    import oracle
+
+    for app in ("BFS", "PR", "SPMV"):
+        if not oracle.ref_available(app):
+            raise RuntimeError(f"reference binary {oracle.ref_binary(app)} not built")
+    hg = make_graph(gg, scale, 5, gg.W_NONE)
+    hw = make_graph(gg, scale, 5, gg.W_INT32)
+    pu, pw = os.path.join(workdir, "g.gr"), os.path.join(workdir, "gw.gr")
+    hg.write_gr(pu)
+    hw.write_gr(pw)
+    og = oracle.Graph.from_host(hg)
+    _, _, bst = og.bfs(100)
+    _, pst = og.pagerank(10)
+    edges = {"BFS": bst.edges_traversed, "PR": pst.edges_traversed, "SPMV": hw.m}
+    times = {}
+    for app, path in (("BFS", pu), ("PR", pu), ("SPMV", pw)):
+        times[app] = oracle.time_ref(app, path, ["-b", "-c", str(partitions), "-r", "100"], rounds=rounds)
+    per_round = [sum(edges.values()) / sum(times[a][r] for a in times) / 1e9 for r in range(rounds)]
+    info = {"n": hg.n, "m": hg.m, "edges_per_step": sum(edges.values()),
+            "seconds_per_step": [round(sum(times[a][r] for a in times), 5) for r in range(rounds)],
+            "apps_s": {a: [round(t, 5) for t in v] for a, v in times.items()}}
+    return per_round, info
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+def run_reference_arm(args):
+    cores = os.cpu_count() or 1
+    sample = f"RMAT-{args.ref_scale} directed, same generator parameters (seed 5), -b -c {args.ref_partitions}"
+    base = {"impl": "reference", "metric": METRIC, "unit": UNIT, "higher_is_better": True, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 (PageRank/SpMV), int64 (BFS ids)", "data": "synthetic: seeded RMAT",
+            "config": {"workload": WORKLOAD, "sample": sample, "parallelism": "host cores (OpenMP)"}}
+    try:
+        with tempfile.TemporaryDirectory() as d:
+            per_round, info = reference_sample(args.ref_scale, args.ref_partitions, args.warmup + args.steps, d)
+    except Exception as e:
+        print(json.dumps({"impl": "reference", "unavailable": f"reference build/run failed: {e}"[:300]}))
+        return
+    timed = per_round[args.warmup:]
+    secs = info["seconds_per_step"][args.warmup:]
+    value = info["edges_per_step"] * len(secs) / sum(secs) / 1e9
+    base.update({"value": round(value, 4), "ms_per_step": round(1e3 * sum(secs) / len(secs), 3),
+                 "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": cores, "kind": "reference",
+                                  "cpu": cpu_model(), "sample": sample + f"; {info['edges_per_step']} edges per step",
+                                  "per_round_gteps": [round(v, 4) for v in timed]},
+                 "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                 "reference_detail": info})
+    print(json.dumps(base))
+
+
+def cpu_baseline_for_ours(args):
+    cores = os.cpu_count() or 1
+    sample = f"RMAT-{args.ref_scale} directed sample (seed 5), reference OpenMP build, -b -c {args.ref_partitions}"
+    try:
+        with tempfile.TemporaryDirectory() as d:
+            per_round, info = reference_sample(args.ref_scale, args.ref_partitions, 3, d)
+        secs = info["seconds_per_step"][1:]
+        value = info["edges_per_step"] * len(secs) / sum(secs) / 1e9
+        return {"value": round(value, 4), "unit": UNIT, "cores": cores, "kind": "reference", "cpu": cpu_model(),
+                "sample": sample + f"; BFS+PageRank(10)+SPMV, {info['edges_per_step']} edges per step, "
+                                   f"mean of 2 rounds after 1 warm-up"}
+    except Exception as e:
+        return {"value": None, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample,
+                "error": str(e)[:200]}
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--scale", type=int, default=24)
+    ap.add_argument("--partitions", type=int, default=384)
+    ap.add_argument("--start", type=int, default=100)
+    ap.add_argument("--dense-policy", type=int, default=0, help="0 reference rule, 1 CSC pull, 2 COO pull")
+    ap.add_argument("--ref-scale", type=int, default=22)
+    ap.add_argument("--ref-partitions", type=int, default=256)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--traffic", type=float, default=None,
+                    help="DRAM bytes per dense-pull launch from an ncu capture (reported as roofline.traffic)")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference_arm(args)
+        return
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(local_rank)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist = tdist
+    out = run_ours(args, rank, world, local_rank, dist)
+    if rank == 0:
+        if world == 1 and not args.no_cpu_baseline:
+            out["cpu_baseline"] = cpu_baseline_for_ours(args)
+        print(json.dumps(out))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -82,6 +82,13 @@ class EdgeMapStats(C.Structure):
                 ("output_out_edges", C.c_uint64)]
 
 
+class Profile(C.Structure):
+    _fields_ = [("launches", C.c_uint64 * 4), ("ms", C.c_double * 4), ("edges", C.c_uint64 * 4)]
+
+
+PROFILE_KINDS = ("push", "csc_pull", "coo_pull", "early_pull")
+
+
 class BfsArgs(C.Structure):
     _fields_ = [("parents", C.c_void_p), ("levels", C.c_void_p), ("round", C.c_int32)]
 
@@ -139,12 +146,17 @@ _sig("gg_frontier_to_sparse", C.c_int, _P)
 _sig("gg_frontier_repr", C.c_int, _P)
 _sig("gg_edge_map", C.c_int, _P, _P, C.c_int32, _P, C.c_int64, C.c_uint32, C.POINTER(_P))
 _sig("gg_last_edge_map_stats", C.c_int, _P, C.POINTER(EdgeMapStats))
+_sig("gg_graph_set_profiling", C.c_int, _P, C.c_int32)
+_sig("gg_graph_get_profile", C.c_int, _P, C.POINTER(Profile))
+_sig("gg_graph_set_dense_policy", C.c_int, _P, C.c_int32)
 _sig("gg_vertex_map", C.c_int, _P, _P, C.c_int32, _P)
 _sig("gg_vertex_filter", C.c_int, _P, _P, C.c_int32, _P, C.POINTER(_P))
 _sig("gg_vertex_array_alloc", C.c_int, _P, C.c_size_t, C.POINTER(_P))
 _sig("gg_vertex_array_free", C.c_int, _P, _P)
 _sig("gg_memcpy_h2d", C.c_int, _P, _P, C.c_size_t)
 _sig("gg_memcpy_d2h", C.c_int, _P, _P, C.c_size_t)
+_sig("gg_host_alloc_pinned", C.c_int, C.c_size_t, C.POINTER(_P))
+_sig("gg_host_free_pinned", C.c_int, _P)
 _sig("gg_bfs", C.c_int, _P, C.c_uint32, _P, _P, C.POINTER(RunStats))
 _sig("gg_components", C.c_int, _P, _P, C.POINTER(RunStats))
 _sig("gg_pagerank", C.c_int, _P, C.c_int32, C.c_int32, _P, C.POINTER(RunStats))
@@ -164,14 +176,24 @@ EXPORTED = [
     "gg_frontier_single", "gg_frontier_all", "gg_frontier_empty", "gg_frontier_from_mask",
     "gg_frontier_from_list", "gg_frontier_destroy", "gg_frontier_stats", "gg_frontier_to_mask",
     "gg_frontier_to_dense", "gg_frontier_to_sparse", "gg_frontier_repr", "gg_edge_map",
-    "gg_last_edge_map_stats", "gg_vertex_map", "gg_vertex_filter", "gg_vertex_array_alloc",
-    "gg_vertex_array_free", "gg_memcpy_h2d", "gg_memcpy_d2h", "gg_bfs", "gg_components",
+    "gg_last_edge_map_stats", "gg_graph_set_profiling", "gg_graph_get_profile",
+    "gg_graph_set_dense_policy", "gg_vertex_map", "gg_vertex_filter", "gg_vertex_array_alloc",
+    "gg_vertex_array_free", "gg_memcpy_h2d", "gg_memcpy_d2h", "gg_host_alloc_pinned", "gg_host_free_pinned", "gg_bfs", "gg_components",
     "gg_pagerank", "gg_pagerank_delta", "gg_spmv", "gg_bellman_ford", "gg_bc", "gg_bp",
 ]
 
 
 def _ptr(a: np.ndarray) -> C.c_void_p:
     return C.c_void_p(a.ctypes.data)
+
+
+def _view(addr: int, count: int, ctype, dtype, owner) -> np.ndarray:
+    """numpy view of library-owned memory that keeps `owner` alive."""
+    if count == 0 or not addr:
+        return np.zeros(0, dtype)
+    buf = (ctype * count).from_address(addr)
+    buf._gg_owner = owner
+    return np.frombuffer(buf, dtype=dtype)
 
 
 # -------------------------------------------------------------- host graph
@@ -205,20 +227,17 @@ class HostGraph:
 
     @property
     def offsets(self) -> np.ndarray:
-        return np.ctypeslib.as_array(self.c.offsets, shape=(self.n + 1,))
+        return _view(C.cast(self.c.offsets, C.c_void_p).value, self.n + 1, C.c_uint32, np.uint32, self)
 
     @property
     def indices(self) -> np.ndarray:
-        if self.m == 0:
-            return np.zeros(0, np.uint32)
-        return np.ctypeslib.as_array(self.c.indices, shape=(self.m,))
+        return _view(C.cast(self.c.indices, C.c_void_p).value, self.m, C.c_uint32, np.uint32, self)
 
     @property
     def weights(self):
         if not self.c.weights or self.m == 0:
             return None
-        buf = (C.c_uint32 * self.m).from_address(self.c.weights)
-        a = np.frombuffer(buf, dtype=np.uint32)
+        a = _view(self.c.weights, self.m, C.c_uint32, np.uint32, self)
         return a.view(np.float32) if self.weight_type == W_FLOAT32 else a.view(np.int32)
 
     def degrees(self) -> np.ndarray:
@@ -299,6 +318,24 @@ def partition_sizes(in_deg, out_deg, m, P, balance=BALANCE_EDGE, part_how=PART_D
 
 def hilbert_key(side_edges: int, x: int, y: int) -> int:
     return int(lib.gg_hilbert_key(side_edges, x, y))
+
+
+class PinnedArray:
+    """A page-locked host buffer viewed as a numpy array (for timed H2D/D2H)."""
+
+    def __init__(self, count: int, dtype):
+        self.dtype = np.dtype(dtype)
+        p = C.c_void_p()
+        check(lib.gg_host_alloc_pinned(max(1, count) * self.dtype.itemsize, C.byref(p)), "gg_host_alloc_pinned")
+        self.ptr = p
+        buf = (C.c_uint8 * (max(1, count) * self.dtype.itemsize)).from_address(p.value)
+        buf._gg_owner = self
+        self.array = np.frombuffer(buf, dtype=self.dtype)[:count]
+
+    def __del__(self):
+        if getattr(self, "ptr", None):
+            lib.gg_host_free_pinned(self.ptr)
+            self.ptr = None
 
 
 # ------------------------------------------------------------ device graph
@@ -411,6 +448,20 @@ class Graph:
     def transpose(self):
         check(lib.gg_graph_transpose(self.h), "gg_graph_transpose")
 
+    def set_profiling(self, enable=True):
+        check(lib.gg_graph_set_profiling(self.h, int(enable)), "gg_graph_set_profiling")
+
+    def profile(self) -> dict:
+        """Per kernel kind: launches, device ms (CUDA events), edges streamed; resets."""
+        p = Profile()
+        check(lib.gg_graph_get_profile(self.h, C.byref(p)), "gg_graph_get_profile")
+        return {k: {"launches": int(p.launches[i]), "ms": float(p.ms[i]), "edges": int(p.edges[i])}
+                for i, k in enumerate(PROFILE_KINDS)}
+
+    def set_dense_policy(self, policy: int):
+        """0: reference rule (COO above m/2), 1: always CSC pull, 2: always COO pull."""
+        check(lib.gg_graph_set_dense_policy(self.h, policy), "gg_graph_set_dense_policy")
+
     # vertexSubset constructors
     def frontier_single(self, v) -> Frontier:
         h = C.c_void_p()
@@ -448,9 +499,8 @@ class Graph:
         return s
 
     # applications
-    def bfs(self, start=100):
-        par = np.empty(self.n, np.int32)
-        lev = np.empty(self.n, np.int32)
+    def bfs(self, start=100, out=None):
+        par, lev = out if out is not None else (np.empty(self.n, np.int32), np.empty(self.n, np.int32))
         st = RunStats()
         check(lib.gg_bfs(self.h, start, _ptr(par), _ptr(lev), C.byref(st)), "gg_bfs")
         return par, lev, _run(st)
@@ -461,8 +511,8 @@ class Graph:
         check(lib.gg_components(self.h, _ptr(ids), C.byref(st)), "gg_components")
         return ids, _run(st)
 
-    def pagerank(self, max_iter=10, bit_all=False):
-        r = np.empty(self.n, np.float32)
+    def pagerank(self, max_iter=10, bit_all=False, out=None):
+        r = out if out is not None else np.empty(self.n, np.float32)
         st = RunStats()
         check(lib.gg_pagerank(self.h, max_iter, int(bit_all), _ptr(r), C.byref(st)), "gg_pagerank")
         return r, _run(st)
@@ -473,8 +523,8 @@ class Graph:
         check(lib.gg_pagerank_delta(self.h, _ptr(r), C.byref(st)), "gg_pagerank_delta")
         return r, _run(st)
 
-    def spmv(self, x=None):
-        y = np.empty(self.n, np.float32)
+    def spmv(self, x=None, out=None):
+        y = out if out is not None else np.empty(self.n, np.float32)
         st = RunStats()
         xp = None
         if x is not None:

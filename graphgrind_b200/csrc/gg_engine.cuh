@@ -116,6 +116,10 @@ struct gg_graph_s {
   bool transposed = false;
   gg::Workspace ws;
   gg_edge_map_stats last{};
+  bool profiling = false;
+  gg_profile prof{};
+  cudaEvent_t prof_ev[2] = {nullptr, nullptr};
+  int dense_policy = 0;
   uint64_t device_bytes = 0;
   int kernels = 0;  // kernels launched since the counter was last reset
   // current orientation views
@@ -173,7 +177,7 @@ __host__ __device__ constexpr size_t pull_smem_bytes(bool coo, bool hw, int vbyt
 // One CTA per tile at a time; CTAs pull tiles from a global ticket counter
 // (tiles are ordered by edge count, largest first).
 template <class F, bool COO, bool HW, bool ALL>
-__global__ void __launch_bounds__(kPullThreads) k_pull(const PullParams p, const F f) {
+__global__ void __launch_bounds__(kPullThreads, 2) k_pull(const PullParams p, const F f) {
   using V = typename F::value_t;
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
@@ -234,9 +238,12 @@ __global__ void __launch_bounds__(kPullThreads) k_pull(const PullParams p, const
     if (!COO && tid == 0) s_off[nv] = __ldg(p.off + v0 + nv);
     __syncthreads();
 
+    uint32_t issued = nchunks < (uint32_t)kPullStages ? nchunks : (uint32_t)kPullStages;
     for (uint32_t c = 0; c < nchunks; ++c) {
       const int st = (int)(c % kPullStages);
-      if (!mbar_wait_bounded(&bars[st], (parity >> st) & 1u)) {
+      // a timed-out wait skips this chunk's edges (the stage may hold stale data)
+      const bool ok = mbar_wait_bounded(&bars[st], (parity >> st) & 1u);
+      if (!ok) {
         atomicOr(p.err, (unsigned long long)DEV_ERR_TIMEOUT);
         s_fail = 1;
       }
@@ -273,7 +280,7 @@ __global__ void __launch_bounds__(kPullThreads) k_pull(const PullParams p, const
       int cur = -1;
       V acc = F::identity();
       uint32_t li = 0;
-      if (!COO && pos0 + kPullK > cs && pos0 < ce) {
+      if (!COO && ok && pos0 + kPullK > cs && pos0 < ce) {
         // last tile-local vertex whose offset is <= max(pos0, cs)
         const uint32_t key = max(pos0, cs);
         uint32_t lo = 0, hi = nv;  // invariant: s_off[lo] <= key < s_off[hi]
@@ -286,7 +293,7 @@ __global__ void __launch_bounds__(kPullThreads) k_pull(const PullParams p, const
 #pragma unroll
       for (int k = 0; k < kPullK; ++k) {
         const uint32_t pos = pos0 + k;
-        if (pos < cs || pos >= ce) continue;
+        if (!ok || pos < cs || pos >= ce) continue;
         const uint32_t s = sv[k];
         uint32_t l;
         if (COO) {
@@ -325,9 +332,21 @@ __global__ void __launch_bounds__(kPullThreads) k_pull(const PullParams p, const
         s_touch[cur] = 1;
       }
       __syncthreads();  // stage st fully consumed
-      if (tid == 0 && c + kPullStages < nchunks && !s_fail) {
-        fence_proxy_async_smem();
-        issue(c + kPullStages, st);
+      if (s_fail) {
+        // drain the copies still in flight (bounded), then leave
+        for (uint32_t cc = c + 1; cc < issued; ++cc) {
+          const int s2 = (int)(cc % kPullStages);
+          mbar_wait_bounded(&bars[s2], (parity >> s2) & 1u);
+          parity ^= 1u << s2;
+        }
+        break;
+      }
+      if (c + kPullStages < nchunks) {
+        if (tid == 0) {
+          fence_proxy_async_smem();
+          issue(c + kPullStages, st);
+        }
+        ++issued;
       }
     }
     if (s_fail) break;

@@ -325,6 +325,8 @@ static void graph_release(gg_graph_s* g) {
   cudaFree(g->ws.d_red);
   if (g->ws.h_stats) cudaFreeHost(g->ws.h_stats);
   if (g->ws.h_red) cudaFreeHost(g->ws.h_red);
+  for (auto& e : g->prof_ev)
+    if (e) cudaEventDestroy(e);
   if (g->stream) cudaStreamDestroy(g->stream);
   delete g;
 }
@@ -491,6 +493,29 @@ int gg_graph_get_info(gg_graph_t g, gg_graph_info* info) {
 int gg_graph_partition_starts(gg_graph_t g, int64_t* starts) {
   if (!g || !starts) return fail(GG_ERR_INVALID_ARG, "gg_graph_partition_starts: bad arguments");
   std::copy(g->coo_starts.begin(), g->coo_starts.end(), starts);
+  return GG_OK;
+}
+
+int gg_graph_set_profiling(gg_graph_t g, int32_t enable) {
+  if (!g) return fail(GG_ERR_INVALID_ARG, "gg_graph_set_profiling: null graph");
+  if (enable && !g->prof_ev[0]) {
+    GG_CUDA(cudaEventCreate(&g->prof_ev[0]));
+    GG_CUDA(cudaEventCreate(&g->prof_ev[1]));
+  }
+  g->profiling = enable != 0;
+  return GG_OK;
+}
+
+int gg_graph_get_profile(gg_graph_t g, gg_profile* out) {
+  if (!g || !out) return fail(GG_ERR_INVALID_ARG, "gg_graph_get_profile: bad arguments");
+  *out = g->prof;
+  g->prof = gg_profile{};
+  return GG_OK;
+}
+
+int gg_graph_set_dense_policy(gg_graph_t g, int32_t policy) {
+  if (!g || policy < 0 || policy > 2) return fail(GG_ERR_INVALID_ARG, "gg_graph_set_dense_policy: bad arguments");
+  g->dense_policy = policy;
   return GG_OK;
 }
 
@@ -674,6 +699,15 @@ int gg_memcpy_h2d(void* d, const void* h, size_t bytes) {
 }
 int gg_memcpy_d2h(void* h, const void* d, size_t bytes) {
   GG_CUDA(cudaMemcpy(h, d, bytes, cudaMemcpyDeviceToHost));
+  return GG_OK;
+}
+int gg_host_alloc_pinned(size_t bytes, void** p) {
+  if (!p || !bytes) return fail(GG_ERR_INVALID_ARG, "gg_host_alloc_pinned: bad arguments");
+  GG_CUDA(cudaMallocHost(p, bytes));
+  return GG_OK;
+}
+int gg_host_free_pinned(void* p) {
+  GG_CUDA(cudaFreeHost(p));
   return GG_OK;
 }
 

@@ -142,6 +142,8 @@ int edge_map(gg_graph_s* g, gg_frontier_s* in, const F& f, int64_t threshold, ui
   const int64_t m = (int64_t)g->m;
   if (threshold < 0) threshold = m / 20;    // :932
   const int64_t dense_threshold = m / 2;    // :934
+  if (in->n != g->n)  // :936-942 (an edgeMap result that was empty() carries 0 rows)
+    return fail(GG_ERR_INVALID_ARG, "edgeMap: Sizes Don't match (numVertices %u and rows %u)", g->n, in->n);
   const int64_t fm = (int64_t)in->dm;
   const int64_t tot = (int64_t)in->out_edges;
   g->last = gg_edge_map_stats{};
@@ -149,7 +151,8 @@ int edge_map(gg_graph_s* g, gg_frontier_s* in, const F& f, int64_t threshold, ui
   g->last.frontier_out_edges = (uint64_t)tot;
   gg_frontier_s* o = nullptr;
   GG_TRY(frontier_new(g, &o));
-  if (tot == 0) {                           // :947
+  if (tot == 0) {                           // :947 partitioned_vertices::empty()
+    o->n = 0;
     *out = o;
     return GG_OK;
   }
@@ -158,18 +161,33 @@ int edge_map(gg_graph_s* g, gg_frontier_s* in, const F& f, int64_t threshold, ui
   bool dense = fm + tot > threshold;        // :953
   if (flags & GG_EM_FORCE_SPARSE) dense = false;
   if ((flags & (GG_EM_FORCE_CSC | GG_EM_FORCE_COO)) && !(flags & GG_EM_FORCE_SPARSE)) dense = true;
+  auto prof_begin = [&]() {
+    if (g->profiling) cudaEventRecord(g->prof_ev[0], g->stream);
+  };
+  auto prof_end = [&](int kind, uint64_t edges) {  // after read_stats (stream synchronised)
+    if (!g->profiling) return;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, g->prof_ev[0], g->prof_ev[1]);
+    g->prof.launches[kind]++;
+    g->prof.ms[kind] += ms;
+    g->prof.edges[kind] += edges;
+  };
   if (dense) {
-    bool coo = fm + tot > dense_threshold && g->has_coo;   // :957 (!part_ver)
+    // :957 (!part_ver); the GPU policy may pin the dense kernel (same results)
+    bool coo = g->has_coo && (g->dense_policy == 2 || (g->dense_policy == 0 && fm + tot > dense_threshold));
     if (flags & GG_EM_FORCE_CSC) coo = false;
     if ((flags & GG_EM_FORCE_COO) && g->has_coo) coo = true;
+    const bool early = !coo && F::kEarlyExit;
     if (!in->bit && !in->has_dense) rc = frontier_to_dense(in);
     if (!rc) rc = frontier_ensure_bits(o, true);
     if (!rc) rc = reset_stats(g);
     if (!rc) {
-      if (!coo && F::kEarlyExit)
+      prof_begin();
+      if (early)
         rc = hw ? pull_early_launch<F, true>(g, in, o, f) : pull_early_launch<F, false>(g, in, o, f);
       else
         rc = hw ? pull_launch<F, true>(g, in, o, f, coo) : pull_launch<F, false>(g, in, o, f, coo);
+      if (g->profiling) cudaEventRecord(g->prof_ev[1], g->stream);
     }
     if (!rc) rc = read_stats(g);
     if (!rc) {
@@ -177,18 +195,24 @@ int edge_map(gg_graph_s* g, gg_frontier_s* in, const F& f, int64_t threshold, ui
       o->dm = g->ws.h_stats[0];
       o->out_edges = g->ws.h_stats[1];
       g->last.kind = coo ? 3 : 2;
+      prof_end(early ? 3 : (coo ? 2 : 1), coo ? g->coo_len : g->m);
     }
   } else {
     if (!in->has_sparse) rc = frontier_to_sparse(in);
     if (!rc) rc = frontier_ensure_queue(o);
     if (!rc) rc = reset_stats(g);
-    if (!rc && in->dm > 0) rc = hw ? push_launch<F, true>(g, in, o, f) : push_launch<F, false>(g, in, o, f);
+    if (!rc && in->dm > 0) {
+      prof_begin();
+      rc = hw ? push_launch<F, true>(g, in, o, f) : push_launch<F, false>(g, in, o, f);
+      if (g->profiling) cudaEventRecord(g->prof_ev[1], g->stream);
+    }
     if (!rc) rc = read_stats(g);
     if (!rc) {
       o->has_sparse = true;
       o->dm = g->ws.h_stats[2];
       o->out_edges = g->ws.h_stats[1];
       g->last.kind = 1;
+      if (in->dm > 0) prof_end(0, g->ws.h_stats[5]);
     }
   }
   if (rc) {

@@ -218,6 +218,22 @@ int gg_edge_map(gg_graph_t g, gg_frontier_t in, int32_t functor_id, const void* 
                 int64_t threshold, uint32_t flags, gg_frontier_t* out);
 int gg_last_edge_map_stats(gg_graph_t g, gg_edge_map_stats* stats);
 
+/* Kernel timing (replaces the reference's per-phase tmlog accumulators,
+ * graphgrind/ligra-numa.h:61-79): when enabled, every edgeMap kernel is
+ * bracketed by CUDA events on the graph's stream.  kind: 0 sparse push,
+ * 1 dense CSC pull, 2 dense COO pull, 3 early-exit pull. */
+typedef struct gg_profile {
+  uint64_t launches[4];
+  double ms[4];
+  uint64_t edges[4];        /* edges streamed by those launches */
+} gg_profile;
+int gg_graph_set_profiling(gg_graph_t g, int32_t enable);
+/* Copies the accumulated profile and resets it. */
+int gg_graph_get_profile(gg_graph_t g, gg_profile* out);
+/* Dense-branch kernel policy: 0 = the reference's rule (COO above m/2 when
+ * the COO exists, else CSC), 1 = always CSC pull, 2 = always COO pull. */
+int gg_graph_set_dense_policy(gg_graph_t g, int32_t policy);
+
 /* Vertex functors for vertexMap / vertexFilter (graphgrind/ligra-numa.h:1023-1082). */
 enum gg_vertex_functor_id {
   GG_V_CC_COPY = 101,      /* app/Components.C:189-200  prevIDs[i]=IDs[i]      args gg_cc_args   */
@@ -245,6 +261,9 @@ int gg_vertex_array_alloc(gg_graph_t g, size_t elem_bytes, void** dev_ptr);
 int gg_vertex_array_free(gg_graph_t g, void* dev_ptr);
 int gg_memcpy_h2d(void* dev_dst, const void* host_src, size_t bytes);
 int gg_memcpy_d2h(void* host_dst, const void* dev_src, size_t bytes);
+/* Page-locked host buffers for the host<->device copies of the app calls. */
+int gg_host_alloc_pinned(size_t bytes, void** host_ptr);
+int gg_host_free_pinned(void* host_ptr);
 
 /* ====================================================== applications */
 /* Each runs the Compute() loop of the named app on the device and copies its

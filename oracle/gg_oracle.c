@@ -95,6 +95,7 @@ typedef struct {
   const or_graph* g;
   int transposed; /* BC backward phase (partitioned_graph::transpose, graph-numa.h:721-728) */
   or_stats* st;
+  int error;      /* set when edgeMap would abort (ligra-numa.h:937-942) */
 } eng_t;
 
 static uint32_t outdeg(const eng_t* e, uint32_t v) {
@@ -111,6 +112,10 @@ static fr_t edge_map(eng_t* e, fr_t* F, const fn_t* f, int64_t threshold) {
   const int64_t dense_threshold = m / 2;            /* :934 */
   const int64_t fm = F->dm;
   const int64_t tot = F->out_edges;
+  if (F->empty) { /* partitioned_vertices::empty() has numVertices 0: "Sizes Don't match" */
+    e->error = 1;
+    return fr_empty();
+  }
   if (e->st) {
     e->st->rounds++;
     e->st->edges_traversed += tot;                  /* :945 */
@@ -261,7 +266,7 @@ static int bfs_update(void* c, uint32_t s, uint32_t d, double w, int64_t pos) {
 int or_bfs(const or_graph* g, uint32_t start, int64_t* parents, int32_t* levels, or_stats* st) {
   /* app/BFS.C:77-101 */
   if (!g || start >= g->n) return -1;
-  eng_t e = {g, 0, st};
+  eng_t e = {g, 0, st, 0};
   for (uint32_t i = 0; i < g->n; i++) {
     parents[i] = -1;
     if (levels) levels[i] = -1;
@@ -340,7 +345,7 @@ static int cc_vertex(void* c, uint32_t i) {
 int or_cc(const or_graph* g, int64_t* ids, or_stats* st) {
   /* app/Components.C:202-227 */
   if (!g) return -1;
-  eng_t e = {g, 0, st};
+  eng_t e = {g, 0, st, 0};
   int64_t* prev = (int64_t*)malloc(sizeof(int64_t) * (g->n ? g->n : 1));
   for (uint32_t i = 0; i < g->n; i++) ids[i] = i;
   cc_ctx c = {ids, prev};
@@ -389,7 +394,7 @@ int or_pagerank(const or_graph* g, int32_t max_iter, int32_t bit_all, double* ra
   /* app/PageRank.C:330-378; bit_all reproduces app/PageRankBit.C:145 */
   if (!g) return -1;
   const uint32_t n = g->n;
-  eng_t e = {g, 0, st};
+  eng_t e = {g, 0, st, 0};
   const double damping = 0.85, eps = 0.0000001;
   double one_over_n = 1 / (double)n;
   double* a = (double*)malloc(sizeof(double) * n);
@@ -406,6 +411,12 @@ int or_pagerank(const or_graph* g, int32_t max_iter, int32_t bit_all, double* ra
   while (count < max_iter) {
     count++;
     fr_t out = edge_map(&e, &F, &f, (int64_t)g->m / 20);
+    if (e.error) {
+      fr_free(&F);
+      free(a);
+      free(b);
+      return -2;
+    }
     vertex_map(n, &F, pr_vertex, &c);
     last = c.p_next;
     double l1 = 0;
@@ -467,7 +478,7 @@ int or_pagerank_delta(const or_graph* g, double* ranks, or_stats* st) {
   /* app/PageRankDelta.C:120-174 */
   if (!g) return -1;
   const uint32_t n = g->n;
-  eng_t e = {g, 0, st};
+  eng_t e = {g, 0, st, 0};
   const double damping = 0.85, eps = 0.0000001, eps2 = 0.01;
   double one_over_n = 1 / (double)n;
   double* delta = (double*)malloc(sizeof(double) * n);
@@ -527,7 +538,7 @@ static void spmv_commit(void* c, double* cache, uint32_t d) { ((spmv_ctx*)c)->y[
 int or_spmv(const or_graph* g, const double* x, double* y, or_stats* st) {
   if (!g) return -1;
   const uint32_t n = g->n;
-  eng_t e = {g, 0, st};
+  eng_t e = {g, 0, st, 0};
   double* xv = (double*)malloc(sizeof(double) * n);
   for (uint32_t j = 0; j < n; j++) {
     xv[j] = x ? x[j] : 1 / (double)n;
@@ -604,7 +615,7 @@ int or_bellman_ford(const or_graph* g, uint32_t start, int64_t* sp, or_stats* st
   /* app/BellmanFord.C:106-145 */
   if (!g || start >= g->n) return -1;
   const uint32_t n = g->n;
-  eng_t e = {g, 0, st};
+  eng_t e = {g, 0, st, 0};
   const int64_t inf = 2147483647 / 2;
   int64_t* visited = (int64_t*)calloc(n, sizeof(int64_t));
   for (uint32_t j = 0; j < n; j++) sp[j] = inf;
@@ -664,7 +675,7 @@ int or_bc(const or_graph* g, uint32_t start, double* dep, double* num_paths, or_
   /* app/BC.C:156-226 */
   if (!g || start >= g->n) return -1;
   const uint32_t n = g->n;
-  eng_t e = {g, 0, st};
+  eng_t e = {g, 0, st, 0};
   double* np = (double*)calloc(n, sizeof(double));
   uint8_t* visited = (uint8_t*)calloc(n, 1);
   np[start] = 1.0;

@@ -1,0 +1,114 @@
+"""Engine-level GPU tests through the C ABI: vertexSubset conversions, the
+edgeMap direction switch, and every edgeMap kernel (sparse push, CSC pull,
+partitioned-COO pull) forced in turn against the oracle."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def sym12(gg, orc):
+    hg = gg.HostGraph.rmat(12, 16, seed=61, symmetric=True)
+    return hg, gg.Graph(hg, partitions=16, tile_vertices=256, tile_edges=2048), orc.Graph.from_host(hg)
+
+
+def test_frontier_conversions(gg, sym12):
+    hg, g, _ = sym12
+    rng = np.random.default_rng(0)
+    mask = (rng.random(hg.n) < 0.1).astype(np.uint8)
+    f = g.frontier_from_mask(mask)
+    deg = hg.degrees().astype(np.int64)
+    assert f.stats() == (int(mask.sum()), int(deg[mask == 1].sum()))
+    f.to_sparse()
+    assert f.repr() & 2
+    np.testing.assert_array_equal(f.mask(), mask)
+    verts = np.nonzero(mask)[0].astype(np.uint32)[::-1].copy()
+    h = g.frontier_from_list(verts)
+    assert h.stats() == f.stats()
+    h.to_dense()
+    np.testing.assert_array_equal(h.mask(), mask)
+    a = g.frontier_all()
+    assert a.stats() == (hg.n, hg.m) and a.repr() == 4
+    s = g.frontier_single(7)
+    assert s.stats() == (1, int(deg[7]))
+
+
+@pytest.mark.parametrize("force", ["none", "sparse", "csc", "coo"])
+def test_bfs_levels_with_forced_kernel(gg, sym12, force):
+    hg, g, og = sym12
+    flags = {"none": 0, "sparse": gg.EM_FORCE_SPARSE, "csc": gg.EM_FORCE_CSC, "coo": gg.EM_FORCE_COO}[force]
+    par = gg.DeviceArray(g, np.int32, -1)
+    lev = gg.DeviceArray(g, np.int32, -1)
+    init_p = np.full(hg.n, -1, np.int32)
+    init_p[3] = 3
+    par.upload(init_p)
+    init_l = np.full(hg.n, -1, np.int32)
+    init_l[3] = 0
+    lev.upload(init_l)
+    F = g.frontier_single(3)
+    rnd = 0
+    kinds = set()
+    while F.stats()[0] > 0:
+        rnd += 1
+        args = gg.BfsArgs(par.ptr, lev.ptr, rnd)
+        F = g.edge_map(F, gg.F_BFS, args, -1, flags)
+        kinds.add(g.last_edge_map_stats().kind)
+    _, olev, _ = og.bfs(3)
+    np.testing.assert_array_equal(lev.download(), olev)
+    expect = {"sparse": {1}, "csc": {2}, "coo": {3}}.get(force)
+    if expect:
+        assert kinds - {0} == expect
+
+
+@pytest.mark.parametrize("force", ["sparse", "csc", "coo"])
+def test_cc_with_forced_kernel(gg, sym12, force):
+    hg, g, og = sym12
+    flags = {"sparse": gg.EM_FORCE_SPARSE, "csc": gg.EM_FORCE_CSC, "coo": gg.EM_FORCE_COO}[force]
+    ids = gg.DeviceArray(g, np.int32, np.arange(hg.n, dtype=np.int32))
+    prev = gg.DeviceArray(g, np.int32, 0)
+    args = gg.CcArgs(ids.ptr, prev.ptr)
+    F = g.frontier_all()
+    rounds = 0
+    while F.stats()[0] > 0 and rounds < 1000:
+        gg.check(gg.lib.gg_vertex_map(g.h, F.h, 101, C.cast(C.byref(args), C.c_void_p)), "vertex_map")
+        F = g.edge_map(F, gg.F_CC, args, -1, flags)
+        rounds += 1
+    np.testing.assert_array_equal(ids.download(), og.cc()[0])
+
+
+def test_direction_switch_follows_reference_thresholds(gg, sym12):
+    """m_f + outdeg(F) > m/20 -> dense; > m/2 -> COO (balance=edge); else push."""
+    hg, g, _ = sym12
+    deg = hg.degrees().astype(np.int64)
+    m = hg.m
+    order = np.argsort(-deg, kind="stable")
+    csum = np.cumsum(deg[order]) + np.arange(1, hg.n + 1)
+    low = order[-1:][deg[order[-1:]] > 0] if deg[order[-1]] > 0 else order[deg[order] > 0][-1:]
+    mid = order[:np.searchsorted(csum, m // 4) + 1]
+    full = np.arange(hg.n)
+    for verts in (low, mid, full):
+        par = gg.DeviceArray(g, np.int32, -1)
+        F = g.frontier_from_list(verts.astype(np.uint32))
+        fm, oe = F.stats()
+        g.edge_map(F, gg.F_BFS, gg.BfsArgs(par.ptr, None, 1))
+        kind = g.last_edge_map_stats().kind
+        want = 1 if fm + oe <= m // 20 else (3 if fm + oe > m // 2 else 2)
+        assert kind == want, (fm, oe, m)
+
+
+def test_empty_result_cannot_be_mapped_again(gg, sym12):
+    """An edgeMap whose frontier has no out-edges returns empty() with 0 rows;
+    mapping it again fails like the reference (ligra-numa.h:937-942)."""
+    hg, g, _ = sym12
+    deg = hg.degrees()
+    iso = int(np.nonzero(deg == 0)[0][0])
+    par = gg.DeviceArray(g, np.int32, -1)
+    F = g.frontier_single(iso)
+    E = g.edge_map(F, gg.F_BFS, gg.BfsArgs(par.ptr, None, 1))
+    assert E.stats() == (0, 0)
+    with pytest.raises(gg.GGError) as e:
+        g.edge_map(E, gg.F_BFS, gg.BfsArgs(par.ptr, None, 2))
+    assert "Sizes Don't match" in str(e.value)

@@ -1,0 +1,168 @@
+"""GPU parity: every application run by the B200 engine (through the C ABI)
+against the oracle on the same inputs.  Integer results bit-exact; FP32
+results within the stated tolerances of the FP64 oracle."""
+import numpy as np
+import pytest
+
+from conftest import (PR_MAX_ABS, PR_REL_L1, golden_flags, golden_names, golden_partitions,
+                      host_graph_from_golden, load_golden, rel_l1)
+
+pytestmark = pytest.mark.gpu
+
+BC_REL_L1 = 1e-4  # FP32 dependency accumulation over many levels vs FP64
+
+
+def build(gg, hg, **kw):
+    return gg.Graph(hg, **kw)
+
+
+def check_bfs(gg_graph, og, start, hg):
+    par, lev, st = gg_graph.bfs(start)
+    _, olev, ost = og.bfs(start)
+    np.testing.assert_array_equal(lev, olev)
+    assert st.rounds == ost.rounds
+    # parents: every reached vertex (but the source) hangs off a valid edge one level up
+    off = hg.offsets.astype(np.int64)
+    idx = hg.indices
+    reached = np.nonzero(lev > 0)[0]
+    for v in reached[:: max(1, len(reached) // 5000)]:
+        p = par[v]
+        assert lev[p] == lev[v] - 1
+        assert v in idx[off[p]:off[p + 1]]
+    assert par[start] == start and np.all(par[lev < 0] == -1)
+
+
+def check_float(a, b, rel=PR_REL_L1, mx=PR_MAX_ABS):
+    assert rel_l1(a, b) <= rel, rel_l1(a, b)
+    assert np.abs(np.asarray(a, np.float64) - b).max() <= mx
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_apps_on_golden_graphs(gg, orc, name):
+    gd = load_golden(name)
+    hg = host_graph_from_golden(gd)
+    fl = golden_flags(gd)
+    part_vertex = "vertex" in fl
+    g = build(gg, hg, partitions=golden_partitions(gd),
+              balance=gg.BALANCE_VERTEX if part_vertex else gg.BALANCE_EDGE)
+    og = orc.Graph.from_host(hg, part_vertex=part_vertex)
+    start = int(gd["start"])
+    if "BFS_levels" in gd:
+        _, lev, _ = g.bfs(start)
+        np.testing.assert_array_equal(lev, gd["BFS_levels"])  # the reference's own levels
+        check_bfs(g, og, start, hg)
+    if "CC_ids" in gd:
+        ids, _ = g.components()
+        np.testing.assert_array_equal(ids, gd["CC_ids"])
+    for app, bit in (("PR", False), ("PRBIT", True)):
+        if f"{app}_ranks" in gd:
+            r, _ = g.pagerank(10, bit)
+            check_float(r, gd[f"{app}_ranks"])
+        if f"{app}_error" in gd:
+            with pytest.raises(gg.GGError) as e:
+                g.pagerank(10, bit)
+            assert "Sizes Don't match" in str(e.value)
+    if "PRD_ranks" in gd:
+        r, _ = g.pagerank_delta()
+        check_float(r, gd["PRD_ranks"])
+    if "BC_num_paths" in gd:
+        dep, npth, _ = g.bc(start)
+        odep, onp, _ = og.bc(start)
+        np.testing.assert_allclose(npth, onp, rtol=1e-6)
+        np.testing.assert_array_equal(np.isnan(dep), np.isnan(odep))
+        fin = np.isfinite(odep)
+        assert rel_l1(dep[fin], odep[fin]) <= BC_REL_L1
+    if "SPMV_y" in gd:
+        y, _ = g.spmv()
+        check_float(y, gd["SPMV_y"], rel=1e-6, mx=1e-6)
+    if "BF_dist" in gd:
+        d, _ = g.bellman_ford(start)
+        np.testing.assert_array_equal(d, gd["BF_dist"])
+
+
+@pytest.fixture(scope="module", params=["sym", "dir"])
+def rmat14(gg, orc, request):
+    sym = request.param == "sym"
+    hg = gg.HostGraph.rmat(14, 16, seed=31, symmetric=sym)
+    return hg, gg.Graph(hg, partitions=64), orc.Graph.from_host(hg)
+
+
+def test_bfs_cc_rmat14(rmat14):
+    hg, g, og = rmat14
+    for start in (0, 100, 12345):
+        check_bfs(g, og, start, hg)
+    ids, _ = g.components()
+    oids, _ = og.cc()
+    np.testing.assert_array_equal(ids, oids)
+
+
+def test_pagerank_family_rmat14(rmat14):
+    hg, g, og = rmat14
+    for bit in (False, True):
+        r, st = g.pagerank(10, bit)
+        o, ost = og.pagerank(10, bit)
+        check_float(r, o)
+        assert st.rounds == ost.rounds
+    r, _ = g.pagerank_delta()
+    o, _ = og.pagerank_delta()
+    check_float(r, o, rel=1e-4, mx=1e-6)
+
+
+def test_bc_rmat14(rmat14):
+    hg, g, og = rmat14
+    dep, npth, _ = g.bc(100)
+    odep, onp, _ = og.bc(100)
+    np.testing.assert_allclose(npth, onp, rtol=1e-5)
+    np.testing.assert_array_equal(np.isnan(dep), np.isnan(odep))
+    fin = np.isfinite(odep)
+    assert rel_l1(dep[fin], odep[fin]) <= BC_REL_L1
+
+
+@pytest.mark.parametrize("sym", [True, False])
+@pytest.mark.parametrize("wt", ["int", "float"])
+def test_weighted_rmat13(gg, orc, sym, wt):
+    hg = gg.HostGraph.rmat(13, 16, seed=41, symmetric=sym)
+    hg.add_weights(gg.W_INT32 if wt == "int" else gg.W_FLOAT32, seed=9, lo=1, hi=100)
+    g = gg.Graph(hg, partitions=32)
+    og = orc.Graph.from_host(hg)
+    x = np.random.default_rng(1).random(hg.n).astype(np.float32)
+    y, _ = g.spmv(x)
+    oy, _ = og.spmv(x.astype(np.float64))
+    check_float(y, oy, rel=1e-6, mx=1e-4 if wt == "int" else 1e-5)
+    if wt == "int":
+        d, _ = g.bellman_ford(100)
+        od, _ = og.bellman_ford(100)
+        np.testing.assert_array_equal(d, od)
+
+
+@pytest.mark.parametrize("order", ["hilbert", "csr"])
+@pytest.mark.parametrize("balance", ["edge", "vertex"])
+def test_build_options(gg, orc, order, balance):
+    hg = gg.HostGraph.rmat(12, 16, seed=51, symmetric=True)
+    g = gg.Graph(hg, partitions=16, order=gg.ORDER_HILBERT if order == "hilbert" else gg.ORDER_CSR,
+                 balance=gg.BALANCE_EDGE if balance == "edge" else gg.BALANCE_VERTEX, tile_vertices=512,
+                 tile_edges=4096)
+    og = orc.Graph.from_host(hg, part_vertex=balance == "vertex")
+    assert bool(g.info().has_coo) == (balance == "edge")
+    r, _ = g.pagerank(10)
+    o, _ = og.pagerank(10)
+    check_float(r, o)
+    ids, _ = g.components()
+    np.testing.assert_array_equal(ids, og.cc()[0])
+
+
+def test_grid_and_er(gg, orc):
+    for hg in (gg.HostGraph.grid(128, 0.001, seed=3), gg.HostGraph.er(1 << 13, 1 << 16, seed=4, symmetric=True)):
+        g = gg.Graph(hg, partitions=16)
+        og = orc.Graph.from_host(hg)
+        check_bfs(g, og, 0, hg)
+        np.testing.assert_array_equal(g.components()[0], og.cc()[0])
+
+
+def test_edgeless_and_tiny(gg, orc):
+    hg = gg.HostGraph.from_csr(np.zeros(5, np.uint32), np.zeros(0, np.uint32), symmetric=True)
+    g = gg.Graph(hg, partitions=1)
+    par, lev, st = g.bfs(2)
+    assert lev.tolist() == [-1, -1, 0, -1] and st.rounds == 1
+    ids, _ = g.components()
+    assert ids.tolist() == [0, 1, 2, 3]
