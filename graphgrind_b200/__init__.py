@@ -11,6 +11,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import weakref
 from dataclasses import dataclass
 
 import numpy as np
@@ -357,13 +358,15 @@ class Frontier:
     def __init__(self, graph: "Graph", handle: C.c_void_p):
         self.graph = graph
         self.h = handle
+        graph._deps.add(self)
 
     def __del__(self):
         self.close()
 
     def close(self):
         if getattr(self, "h", None):
-            lib.gg_frontier_destroy(self.h)
+            if getattr(self.graph, "h", None):
+                lib.gg_frontier_destroy(self.h)
             self.h = None
 
     def stats(self):
@@ -395,6 +398,7 @@ class DeviceArray:
         p = C.c_void_p()
         check(lib.gg_vertex_array_alloc(graph.h, self.dtype.itemsize, C.byref(p)), "gg_vertex_array_alloc")
         self.ptr = p
+        graph._deps.add(self)
         if init is not None:
             self.upload(np.full(graph.n, init, self.dtype) if np.isscalar(init) else init)
 
@@ -407,10 +411,14 @@ class DeviceArray:
         check(lib.gg_memcpy_d2h(_ptr(out), self.ptr, out.nbytes), "gg_memcpy_d2h")
         return out
 
-    def __del__(self):
-        if getattr(self, "ptr", None) and getattr(self.graph, "h", None):
-            lib.gg_vertex_array_free(self.graph.h, self.ptr)
+    def close(self):
+        if getattr(self, "ptr", None):
+            if getattr(self.graph, "h", None):
+                lib.gg_vertex_array_free(self.graph.h, self.ptr)
             self.ptr = None
+
+    def __del__(self):
+        self.close()
 
 
 class Graph:
@@ -419,6 +427,7 @@ class Graph:
     def __init__(self, host: HostGraph, partitions=384, balance=BALANCE_EDGE, part_how=PART_DEST, relabel=False,
                  order=ORDER_HILBERT, tile_vertices=0, tile_edges=0, build_coo=0):
         self.host = host
+        self._deps = weakref.WeakSet()
         o = BuildOpts(partitions, balance, part_how, int(relabel), order, tile_vertices, tile_edges, build_coo)
         h = C.c_void_p()
         check(lib.gg_graph_build(C.byref(host.c), C.byref(o), C.byref(h)), "gg_graph_build")
@@ -428,6 +437,8 @@ class Graph:
 
     def close(self):
         if getattr(self, "h", None):
+            for d in list(getattr(self, "_deps", ())):  # frontiers / arrays first
+                d.close()
             lib.gg_graph_destroy(self.h)
             self.h = None
 

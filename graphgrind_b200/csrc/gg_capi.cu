@@ -494,7 +494,8 @@ extern "C" {
 
 int gg_edge_map(gg_graph_t g, gg_frontier_t in, int32_t fid, const void* args, int64_t threshold, uint32_t flags,
                 gg_frontier_t* out) {
-  if (!g || !in || !out || !args || in->g != g) return fail(GG_ERR_INVALID_ARG, "gg_edge_map: bad arguments");
+  if (!graph_live(g) || !frontier_live(in) || !out || !args || in->g != g)
+    return fail(GG_ERR_INVALID_ARG, "gg_edge_map: bad arguments");
   switch (fid) {
     case GG_F_BFS: {
       const gg_bfs_args* a = (const gg_bfs_args*)args;
@@ -565,7 +566,8 @@ int gg_last_edge_map_stats(gg_graph_t g, gg_edge_map_stats* st) {
 }
 
 int gg_vertex_map(gg_graph_t g, gg_frontier_t f, int32_t vid, const void* args) {
-  if (!g || !f || !args || f->g != g) return fail(GG_ERR_INVALID_ARG, "gg_vertex_map: bad arguments");
+  if (!graph_live(g) || !frontier_live(f) || !args || f->g != g)
+    return fail(GG_ERR_INVALID_ARG, "gg_vertex_map: bad arguments");
   int rc;
   switch (vid) {
     case GG_V_CC_COPY: {
@@ -613,7 +615,8 @@ int gg_vertex_map(gg_graph_t g, gg_frontier_t f, int32_t vid, const void* args) 
 }
 
 int gg_vertex_filter(gg_graph_t g, gg_frontier_t f, int32_t vid, const void* args, gg_frontier_t* out) {
-  if (!g || !f || !args || !out || f->g != g) return fail(GG_ERR_INVALID_ARG, "gg_vertex_filter: bad arguments");
+  if (!graph_live(g) || !frontier_live(f) || !args || !out || f->g != g)
+    return fail(GG_ERR_INVALID_ARG, "gg_vertex_filter: bad arguments");
   const gg_prdelta_vertex_args* a = (const gg_prdelta_vertex_args*)args;
   switch (vid) {
     case GG_V_PRDELTA_FIRST: {

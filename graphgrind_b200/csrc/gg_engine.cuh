@@ -37,6 +37,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <unordered_set>
 #include <vector>
 
 #include "gg_common.h"
@@ -122,6 +123,8 @@ struct gg_graph_s {
   int dense_policy = 0;
   uint64_t device_bytes = 0;
   int kernels = 0;  // kernels launched since the counter was last reset
+  std::unordered_set<gg_frontier_s*> frontiers;  // live frontiers (freed with the graph)
+  std::unordered_set<void*> arrays;             // live vertex arrays
   // current orientation views
   const uint32_t* out_off() const { return transposed ? d_csc_off : d_csr_off; }
   const uint32_t* out_idx() const { return transposed ? d_csc_idx : d_csr_idx; }
@@ -146,6 +149,11 @@ struct gg_frontier_s {
 };
 
 namespace gg {
+
+// Handle registry: C-ABI calls on a destroyed graph or frontier fail with
+// GG_ERR_INVALID_ARG instead of touching freed memory.
+bool graph_live(const gg_graph_s* g);
+bool frontier_live(const gg_frontier_s* f);
 
 // ===================================================== kernel parameters
 struct PullParams {

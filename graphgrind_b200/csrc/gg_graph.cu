@@ -12,13 +12,28 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <mutex>
 #include <numeric>
+#include <unordered_set>
 #include <vector>
 
 #include "gg_hilbert.h"
 #include "gg_runtime.cuh"
 
 namespace gg {
+
+static std::mutex g_reg_mu;
+static std::unordered_set<const gg_graph_s*> g_graphs;
+static std::unordered_set<const gg_frontier_s*> g_frontiers;
+
+bool graph_live(const gg_graph_s* g) {
+  std::lock_guard<std::mutex> lk(g_reg_mu);
+  return g && g_graphs.count(g);
+}
+bool frontier_live(const gg_frontier_s* f) {
+  std::lock_guard<std::mutex> lk(g_reg_mu);
+  return f && g_frontiers.count(f);
+}
 
 template <class T>
 static int dev_alloc(gg_graph_s* g, T** p, size_t count) {
@@ -35,6 +50,11 @@ int frontier_new(gg_graph_s* g, gg_frontier_s** out) {
   if (!f) return fail(GG_ERR_OOM, "frontier: out of host memory");
   f->g = g;
   f->n = g->n;
+  {
+    std::lock_guard<std::mutex> lk(g_reg_mu);
+    g_frontiers.insert(f);
+  }
+  g->frontiers.insert(f);
   *out = f;
   return GG_OK;
 }
@@ -56,6 +76,11 @@ int frontier_ensure_queue(gg_frontier_s* f) {
 void frontier_free(gg_frontier_s* f) {
   if (!f) return;
   gg_graph_s* g = f->g;
+  {
+    std::lock_guard<std::mutex> lk(g_reg_mu);
+    g_frontiers.erase(f);
+  }
+  g->frontiers.erase(f);
   if (f->d_bits) cudaFreeAsync(f->d_bits, g->stream);
   if (f->d_queue) cudaFreeAsync(f->d_queue, g->stream);
   delete f;
@@ -305,6 +330,16 @@ static int build_coo(gg_graph_s* g, const uint32_t* h_in_off) {
 
 static void graph_release(gg_graph_s* g) {
   if (!g) return;
+  {
+    std::lock_guard<std::mutex> lk(g_reg_mu);
+    g_graphs.erase(g);
+  }
+  // frontiers and vertex arrays still alive die with their graph
+  const std::vector<gg_frontier_s*> fl(g->frontiers.begin(), g->frontiers.end());
+  for (gg_frontier_s* f : fl) frontier_free(f);
+  if (g->stream) cudaStreamSynchronize(g->stream);
+  for (void* a : g->arrays) cudaFree(a);
+  g->arrays.clear();
   cudaFree(g->d_csr_off);
   cudaFree(g->d_csr_idx);
   cudaFree(g->d_csr_w);
@@ -464,12 +499,16 @@ int gg_graph_build(const gg_host_graph* hg, const gg_build_opts* opts, gg_graph_
     set_error("%s", keep.c_str());
     return rc;
   }
+  {
+    std::lock_guard<std::mutex> lk(g_reg_mu);
+    g_graphs.insert(g);
+  }
   *out = g;
   return GG_OK;
 }
 
 int gg_graph_destroy(gg_graph_t g) {
-  if (!g) return fail(GG_ERR_INVALID_ARG, "gg_graph_destroy: null graph");
+  if (!graph_live(g)) return fail(GG_ERR_INVALID_ARG, "gg_graph_destroy: not a live graph");
   cudaStreamSynchronize(g->stream);
   graph_release(g);
   return GG_OK;
@@ -626,7 +665,7 @@ int gg_frontier_from_list(gg_graph_t g, const uint32_t* verts, uint64_t count, g
 }
 
 int gg_frontier_destroy(gg_frontier_t f) {
-  if (!f) return fail(GG_ERR_INVALID_ARG, "gg_frontier_destroy: null frontier");
+  if (!frontier_live(f)) return fail(GG_ERR_INVALID_ARG, "gg_frontier_destroy: not a live frontier");
   frontier_free(f);
   return GG_OK;
 }
@@ -685,10 +724,12 @@ int gg_frontier_repr(gg_frontier_t f) {
 int gg_vertex_array_alloc(gg_graph_t g, size_t elem_bytes, void** dev_ptr) {
   if (!g || !dev_ptr || !elem_bytes) return fail(GG_ERR_INVALID_ARG, "gg_vertex_array_alloc: bad arguments");
   GG_CUDA(cudaMalloc(dev_ptr, elem_bytes * ((size_t)g->n + 4)));
+  g->arrays.insert(*dev_ptr);
   return GG_OK;
 }
 int gg_vertex_array_free(gg_graph_t g, void* p) {
-  if (!g) return fail(GG_ERR_INVALID_ARG, "gg_vertex_array_free: null graph");
+  if (!graph_live(g)) return fail(GG_ERR_INVALID_ARG, "gg_vertex_array_free: not a live graph");
+  if (!g->arrays.erase(p)) return fail(GG_ERR_INVALID_ARG, "gg_vertex_array_free: not an array of this graph");
   cudaStreamSynchronize(g->stream);
   GG_CUDA(cudaFree(p));
   return GG_OK;

@@ -650,7 +650,6 @@ int gg_partition_sizes(const uint32_t* in_degrees, const uint32_t* out_degrees, 
       rc = GG_OK;
     }
   } else {
-    if (cn == 0) return fail(GG_ERR_PARTITION, "cscpartitionByDegree: graph has no edges");
     rc = relabel ? greedy_relabel(cin.data(), cn, P, csc_sizes, true)
                  : greedy_by_degree(use_out ? cout_.data() : cin.data(), cn, m, P, csc_sizes);
   }

@@ -845,7 +845,7 @@ int or_partition_sizes(const uint32_t* in_deg, const uint32_t* out_deg, uint32_t
     if (relabel) or_relabel(ci, cn, P, csc, 0);
     else or_even(cn, P, csc);
   } else {
-    rc = cn == 0 ? -4 : relabel ? or_relabel(ci, cn, P, csc, 1) : or_greedy(part_how ? co : ci, cn, m, P, csc);
+    rc = relabel ? or_relabel(ci, cn, P, csc, 1) : or_greedy(part_how ? co : ci, cn, m, P, csc);
   }
   free(ci);
   free(co);

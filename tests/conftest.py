@@ -42,6 +42,21 @@ def golden_partitions(gd):
     return int(fl[fl.index("-c") + 1]) if "-c" in fl else 384
 
 
+def ok_partitions(hg, preferred):
+    """Largest P <= preferred that the reference partitioner accepts for hg
+    (partitionByDegree asserts for some (graph, P) pairs)."""
+    import graphgrind_b200 as gg
+    outd = hg.degrees()
+    ind = hg.transpose().degrees() if not hg.symmetric else outd
+    for P in range(preferred, 0, -1):
+        try:
+            gg.partition_sizes(ind, outd, hg.m, P)
+            return P
+        except gg.GGError:
+            continue
+    raise AssertionError("no partition count accepted")
+
+
 def rel_l1(a, b):
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)

@@ -6,13 +6,15 @@ import ctypes as C
 import numpy as np
 import pytest
 
+from conftest import ok_partitions
+
 pytestmark = pytest.mark.gpu
 
 
 @pytest.fixture(scope="module")
 def sym12(gg, orc):
     hg = gg.HostGraph.rmat(12, 16, seed=61, symmetric=True)
-    return hg, gg.Graph(hg, partitions=16, tile_vertices=256, tile_edges=2048), orc.Graph.from_host(hg)
+    return hg, gg.Graph(hg, partitions=ok_partitions(hg, 16), tile_vertices=256, tile_edges=2048), orc.Graph.from_host(hg)
 
 
 def test_frontier_conversions(gg, sym12):

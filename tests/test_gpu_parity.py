@@ -4,7 +4,7 @@ results within the stated tolerances of the FP64 oracle."""
 import numpy as np
 import pytest
 
-from conftest import (PR_MAX_ABS, PR_REL_L1, golden_flags, golden_names, golden_partitions,
+from conftest import (PR_MAX_ABS, PR_REL_L1, golden_flags, golden_names, golden_partitions, ok_partitions,
                       host_graph_from_golden, load_golden, rel_l1)
 
 pytestmark = pytest.mark.gpu
@@ -84,7 +84,7 @@ def test_apps_on_golden_graphs(gg, orc, name):
 def rmat14(gg, orc, request):
     sym = request.param == "sym"
     hg = gg.HostGraph.rmat(14, 16, seed=31, symmetric=sym)
-    return hg, gg.Graph(hg, partitions=64), orc.Graph.from_host(hg)
+    return hg, gg.Graph(hg, partitions=ok_partitions(hg, 64)), orc.Graph.from_host(hg)
 
 
 def test_bfs_cc_rmat14(rmat14):
@@ -123,12 +123,16 @@ def test_bc_rmat14(rmat14):
 def test_weighted_rmat13(gg, orc, sym, wt):
     hg = gg.HostGraph.rmat(13, 16, seed=41, symmetric=sym)
     hg.add_weights(gg.W_INT32 if wt == "int" else gg.W_FLOAT32, seed=9, lo=1, hi=100)
-    g = gg.Graph(hg, partitions=32)
+    g = gg.Graph(hg, partitions=ok_partitions(hg, 32))
     og = orc.Graph.from_host(hg)
     x = np.random.default_rng(1).random(hg.n).astype(np.float32)
     y, _ = g.spmv(x)
     oy, _ = og.spmv(x.astype(np.float64))
-    check_float(y, oy, rel=1e-6, mx=1e-4 if wt == "int" else 1e-5)
+    # FP32 sums of up to thousands of terms: bound the relative error (y reaches ~1e5)
+    assert rel_l1(y, oy) <= 1e-6
+    nz = oy != 0
+    assert np.max(np.abs(y[nz] - oy[nz]) / np.abs(oy[nz])) <= 1e-5
+    assert np.all(y[~nz] == 0)
     if wt == "int":
         d, _ = g.bellman_ford(100)
         od, _ = og.bellman_ford(100)
@@ -139,7 +143,7 @@ def test_weighted_rmat13(gg, orc, sym, wt):
 @pytest.mark.parametrize("balance", ["edge", "vertex"])
 def test_build_options(gg, orc, order, balance):
     hg = gg.HostGraph.rmat(12, 16, seed=51, symmetric=True)
-    g = gg.Graph(hg, partitions=16, order=gg.ORDER_HILBERT if order == "hilbert" else gg.ORDER_CSR,
+    g = gg.Graph(hg, partitions=ok_partitions(hg, 16), order=gg.ORDER_HILBERT if order == "hilbert" else gg.ORDER_CSR,
                  balance=gg.BALANCE_EDGE if balance == "edge" else gg.BALANCE_VERTEX, tile_vertices=512,
                  tile_edges=4096)
     og = orc.Graph.from_host(hg, part_vertex=balance == "vertex")
@@ -153,7 +157,7 @@ def test_build_options(gg, orc, order, balance):
 
 def test_grid_and_er(gg, orc):
     for hg in (gg.HostGraph.grid(128, 0.001, seed=3), gg.HostGraph.er(1 << 13, 1 << 16, seed=4, symmetric=True)):
-        g = gg.Graph(hg, partitions=16)
+        g = gg.Graph(hg, partitions=ok_partitions(hg, 16))
         og = orc.Graph.from_host(hg)
         check_bfs(g, og, 0, hg)
         np.testing.assert_array_equal(g.components()[0], og.cc()[0])
