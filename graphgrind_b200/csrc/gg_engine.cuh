@@ -81,6 +81,19 @@ struct TileSet {
   std::vector<uint4> host;
 };
 
+// Row structure of a CSC (or, transposed, CSR) edge stream for the
+// segmented pull: bit j of `head` is set iff edge j is the first in-edge of
+// its destination; blk[b] = number of heads in edges [0, 256 b); rows[r] =
+// the vertex of the r-th non-empty row (the compressed CSC vertex list of
+// the reference, PartitionByDest, graphgrind/graph-numa.h:1098-1107).
+constexpr int kSegBlock = 256;  // edges per warp block
+struct SegIndex {
+  uint32_t* d_head = nullptr;
+  uint32_t* d_blk = nullptr;
+  uint32_t* d_rows = nullptr;
+  uint64_t nrows = 0;
+};
+
 struct Workspace {
   unsigned long long* d_stats = nullptr;  // [0] count [1] outdeg [2] queue len [3] err [4] tile ctr [5] total edges
   unsigned long long* h_stats = nullptr;  // pinned mirror
@@ -109,6 +122,8 @@ struct gg_graph_s {
   uint32_t *d_csc_off = nullptr, *d_csc_idx = nullptr, *d_csc_w = nullptr;
   std::vector<uint32_t> h_csr_off, h_csc_off;  // host copies of the offsets
   gg::TileSet csc_tiles[2];  // [0]: pull over CSC (in-edges); [1]: transposed (pull over CSR)
+  gg::SegIndex seg[2];       // row structure of the pulled stream, same indexing
+  uint64_t m_pad = 0;        // edge arrays hold m_pad entries (zero padded)
   gg::TileSet coo_tiles;
   bool has_coo = false;
   uint32_t *d_coo_src = nullptr, *d_coo_w = nullptr;
@@ -285,8 +300,11 @@ __global__ void __launch_bounds__(kPullThreads, 2) k_pull(const PullParams p, co
         dv[0] = a.x & 0xffff; dv[1] = a.x >> 16; dv[2] = a.y & 0xffff; dv[3] = a.y >> 16;
         dv[4] = a.z & 0xffff; dv[5] = a.z >> 16; dv[6] = a.w & 0xffff; dv[7] = a.w >> 16;
       }
-      int cur = -1;
-      V acc = F::identity();
+      // The slots are processed in phases so that each thread keeps all of
+      // its frontier-bit loads, then all of its gathers, in flight at once.
+      // phase 1: tile-local destination and validity of every slot
+      uint32_t lv[kPullK];
+      bool vld[kPullK];
       uint32_t li = 0;
       if (!COO && ok && pos0 + kPullK > cs && pos0 < ce) {
         // last tile-local vertex whose offset is <= max(pos0, cs)
@@ -301,28 +319,44 @@ __global__ void __launch_bounds__(kPullThreads, 2) k_pull(const PullParams p, co
 #pragma unroll
       for (int k = 0; k < kPullK; ++k) {
         const uint32_t pos = pos0 + k;
-        if (!ok || pos < cs || pos >= ce) continue;
-        const uint32_t s = sv[k];
-        uint32_t l;
+        bool v = ok && pos >= cs && pos < ce;
+        uint32_t l = 0;
         if (COO) {
-          if (s == kPad) continue;
+          v = v && sv[k] != kPad;
           l = dv[k];
-        } else {
+        } else if (v) {
           while (s_off[li + 1] <= pos) ++li;
           l = li;
         }
-        if (!s_cond[l]) continue;
-        if (!ALL && !test_bit(p.fr_bits, s)) continue;
-        const V val = f.gather(s, wv[k]);
-        if ((int)l != cur) {
+        lv[k] = l;
+        vld[k] = v && s_cond[l];
+      }
+      // phase 2: frontier membership of the sources (independent loads)
+      if (!ALL) {
+#pragma unroll
+        for (int k = 0; k < kPullK; ++k)
+          if (vld[k]) vld[k] = test_bit(p.fr_bits, sv[k]);
+      }
+      // phase 3: contributions (independent gathers)
+      V val[kPullK];
+#pragma unroll
+      for (int k = 0; k < kPullK; ++k) val[k] = vld[k] ? f.gather(sv[k], wv[k]) : F::identity();
+      // phase 4: run accumulation into the tile's shared-memory accumulators
+      int cur = -1;
+      V acc = F::identity();
+#pragma unroll
+      for (int k = 0; k < kPullK; ++k) {
+        if (!vld[k]) continue;
+        const int l = (int)lv[k];
+        if (l != cur) {
           if (cur >= 0) {
             F::atomic_combine(&s_acc[cur], acc);
             s_touch[cur] = 1;
           }
-          cur = (int)l;
-          acc = val;
+          cur = l;
+          acc = val[k];
         } else {
-          acc = F::combine(acc, val);
+          acc = F::combine(acc, val[k]);
         }
       }
       // final run: warp-aggregate when the whole warp ends on one destination
@@ -392,6 +426,254 @@ __global__ void __launch_bounds__(kPullThreads, 2) k_pull(const PullParams p, co
     }
     if (a) atomicAdd(p.stats + 0, a);
     if (b) atomicAdd(p.stats + 1, b);
+  }
+}
+
+// ------------------------------------------------ segmented CSC pull
+// The CTA owns a destination tile (accumulators in shared memory, one
+// commit per destination, no global atomics).  Inside the tile each warp
+// streams its own 256-edge blocks through a private 3-stage bulk-copy ring
+// (no CTA-wide barrier per block); lane l takes 8 consecutive edges.
+// Destinations come from the head-bit stream: a warp prefix count of head
+// bits plus the block's head count gives every edge's row ordinal, and the
+// compressed row list gives the vertex.  Contributions reduce in registers
+// along rows; only rows that cross a lane boundary touch shared memory.
+constexpr int kSegWarps = 8;
+constexpr int kSegThreads = kSegWarps * 32;
+constexpr int kSegStages = 3;
+
+struct SegParams {
+  const uint4* tiles;
+  uint32_t ntiles;
+  unsigned long long* tile_counter;
+  const uint32_t* src;      // in-neighbour ids, padded to whole 256-edge blocks
+  const uint32_t* wts;      // weights, same padding, or null
+  const uint32_t* head;     // head bits
+  const uint32_t* blk;      // heads before each 256-edge block
+  const uint32_t* rows;     // vertex of every non-empty row
+  const uint32_t* fr_bits;
+  uint32_t* next_bits;
+  const uint32_t* deg_off;
+  const uint32_t* member_off;
+  unsigned long long* stats;
+  unsigned long long* err;
+};
+
+__host__ __device__ constexpr size_t seg_stage_bytes(bool hw) {
+  return (size_t)kSegBlock * 4 + 32 + (hw ? (size_t)kSegBlock * 4 : 0);
+}
+__host__ __device__ constexpr size_t seg_smem_bytes(bool hw, int vbytes) {
+  return 256 + (size_t)kSegWarps * kSegStages * seg_stage_bytes(hw) + (size_t)kMaxTileVertices * vbytes +
+         (size_t)kMaxTileVertices * 2;
+}
+
+template <class F, bool HW, bool ALL>
+__global__ void __launch_bounds__(kSegThreads, 3) k_pull_seg(const SegParams p, const F f) {
+  using V = typename F::value_t;
+  extern __shared__ __align__(128) unsigned char smem[];
+  constexpr uint32_t SB = (uint32_t)seg_stage_bytes(HW);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem);  // [warp][stage]
+  unsigned char* stages = smem + 256;
+  V* s_acc = reinterpret_cast<V*>(stages + (size_t)kSegWarps * kSegStages * SB);
+  uint8_t* s_touch = reinterpret_cast<uint8_t*>(s_acc + kMaxTileVertices);
+  uint8_t* s_cond = s_touch + kMaxTileVertices;
+  __shared__ uint32_t s_tile;
+  __shared__ unsigned long long s_red[2][kSegWarps];
+  __shared__ int s_fail;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  uint64_t* wbar = bars + warp * kSegStages;
+  unsigned char* wst = stages + (size_t)warp * kSegStages * SB;
+  if (lane == 0)
+    for (int s = 0; s < kSegStages; ++s) mbar_init(&wbar[s], 1);
+  if (tid == 0) s_fail = 0;
+  fence_mbar_init();
+  __syncthreads();
+  uint32_t parity = 0;
+  unsigned long long my_cnt = 0, my_deg = 0;
+
+  for (;;) {
+    if (tid == 0) s_tile = (uint32_t)atomicAdd(p.tile_counter, 1ull);
+    __syncthreads();
+    const uint32_t t = s_tile;
+    if (t >= p.ntiles || s_fail) break;
+    const uint4 td = p.tiles[t];
+    const uint32_t v0 = td.x, nv = td.y, e0 = td.z, ne = td.w;
+    for (uint32_t i = tid; i < nv; i += kSegThreads) {
+      const uint32_t v = v0 + i;
+      s_acc[i] = F::identity();
+      s_touch[i] = 0;
+      bool c = F::kCondTrue ? true : f.cond(v);
+      if (p.member_off) c = c && (__ldg(p.member_off + v + 1) > __ldg(p.member_off + v));
+      s_cond[i] = c ? 1 : 0;
+    }
+    __syncthreads();
+    const bool need_cond = !F::kCondTrue || p.member_off != nullptr;
+    const uint32_t e1 = e0 + ne;
+    const uint32_t b_first = e0 / kSegBlock;
+    const uint32_t nb = (e1 - 1) / kSegBlock - b_first + 1;
+    const uint32_t nbw = (uint32_t)warp < nb ? (nb - (uint32_t)warp + kSegWarps - 1) / kSegWarps : 0;
+    auto issue = [&](uint32_t i, int st) {
+      const uint32_t b = b_first + (uint32_t)warp + i * kSegWarps;
+      unsigned char* d = wst + st * SB;
+      mbar_arrive_expect_tx(&wbar[st], SB);
+      bulk_g2s(d, p.src + (size_t)b * kSegBlock, kSegBlock * 4, &wbar[st]);
+      bulk_g2s(d + kSegBlock * 4, p.head + (size_t)b * (kSegBlock / 32), 32, &wbar[st]);
+      if (HW) bulk_g2s(d + kSegBlock * 4 + 32, p.wts + (size_t)b * kSegBlock, kSegBlock * 4, &wbar[st]);
+    };
+    if (lane == 0)
+      for (uint32_t i = 0; i < nbw && i < (uint32_t)kSegStages; ++i) issue(i, (int)i);
+    uint32_t issued = nbw < (uint32_t)kSegStages ? nbw : (uint32_t)kSegStages;
+    bool fail = false;
+    for (uint32_t i = 0; i < nbw; ++i) {
+      const int st = (int)(i % kSegStages);
+      const uint32_t b = b_first + (uint32_t)warp + i * kSegWarps;
+      const uint32_t hb = __ldg(p.blk + b);  // heads before this block
+      // warp-uniform outcome: the lanes leave the loop together
+      const bool ok = __all_sync(0xffffffffu, mbar_wait_bounded(&wbar[st], (parity >> st) & 1u));
+      parity ^= 1u << st;
+      if (!ok) {
+        if (lane == 0) atomicOr(p.err, (unsigned long long)DEV_ERR_TIMEOUT);
+        s_fail = 1;
+        fail = true;
+        for (uint32_t cc = i + 1; cc < issued; ++cc) {  // drain (bounded)
+          const int s2 = (int)(cc % kSegStages);
+          mbar_wait_bounded(&wbar[s2], (parity >> s2) & 1u);
+          parity ^= 1u << s2;
+        }
+        break;
+      }
+      const unsigned char* d = wst + st * SB;
+      const uint32_t* ssrc = reinterpret_cast<const uint32_t*>(d) + lane * 8;
+      uint32_t sv[8], wv[8];
+      {
+        const uint4 a = reinterpret_cast<const uint4*>(ssrc)[0];
+        const uint4 c = reinterpret_cast<const uint4*>(ssrc)[1];
+        sv[0] = a.x; sv[1] = a.y; sv[2] = a.z; sv[3] = a.w;
+        sv[4] = c.x; sv[5] = c.y; sv[6] = c.z; sv[7] = c.w;
+      }
+      if (HW) {
+        const uint32_t* sw = reinterpret_cast<const uint32_t*>(d + kSegBlock * 4 + 32) + lane * 8;
+        const uint4 a = reinterpret_cast<const uint4*>(sw)[0];
+        const uint4 c = reinterpret_cast<const uint4*>(sw)[1];
+        wv[0] = a.x; wv[1] = a.y; wv[2] = a.z; wv[3] = a.w;
+        wv[4] = c.x; wv[5] = c.y; wv[6] = c.z; wv[7] = c.w;
+      } else {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) wv[k] = 1u;
+      }
+      const uint32_t hw32 = reinterpret_cast<const uint32_t*>(d + kSegBlock * 4)[lane >> 2];
+      const uint32_t bits = (hw32 >> ((lane & 3) * 8)) & 0xffu;
+      // heads strictly before this lane's first edge
+      const uint32_t cnt = __popc(bits);
+      uint32_t incl = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      const uint32_t before = hb + incl - cnt;
+      __syncwarp();
+      if (lane == 0 && i + kSegStages < nbw) {  // refill this stage: the warp has read it
+        fence_proxy_async_smem();
+        issue(i + kSegStages, st);
+      }
+      if (i + kSegStages < nbw) ++issued;
+      const uint32_t pos0 = b * kSegBlock + (uint32_t)lane * 8;
+      // destinations: row ordinal of slot k = before + heads in slots [0, k] - 1
+      uint32_t lv[8];
+      bool vld[8];
+      uint32_t cur_ord = 0xffffffffu, cur_l = 0;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const uint32_t pos = pos0 + k;
+        const bool in = pos >= e0 && pos < e1;
+        const uint32_t ord = before + __popc(bits & ((2u << k) - 1u)) - 1u;
+        if (in && ord != cur_ord) {
+          cur_ord = ord;
+          cur_l = __ldg(p.rows + ord) - v0;
+        }
+        lv[k] = cur_l;
+        vld[k] = in;
+      }
+      if (need_cond) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) vld[k] = vld[k] && s_cond[lv[k]];
+      }
+      if (!ALL) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+          if (vld[k]) vld[k] = test_bit(p.fr_bits, sv[k]);
+      }
+      V val[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) val[k] = vld[k] ? f.gather(sv[k], wv[k]) : F::identity();
+      int cur = -1;
+      V acc = F::identity();
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        if (!vld[k]) continue;
+        const int l = (int)lv[k];
+        if (l != cur) {
+          if (cur >= 0) {
+            F::atomic_combine(&s_acc[cur], acc);
+            s_touch[cur] = 1;
+          }
+          cur = l;
+          acc = val[k];
+        } else {
+          acc = F::combine(acc, val[k]);
+        }
+      }
+      const int c0 = __shfl_sync(0xffffffffu, cur, 0);
+      if (__all_sync(0xffffffffu, cur == c0) && c0 >= 0) {  // whole warp on one row (hubs)
+        V r = acc;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) r = F::combine(r, __shfl_xor_sync(0xffffffffu, r, o));
+        if (lane == 0) {
+          F::atomic_combine(&s_acc[c0], r);
+          s_touch[c0] = 1;
+        }
+      } else if (cur >= 0) {
+        F::atomic_combine(&s_acc[cur], acc);
+        s_touch[cur] = 1;
+      }
+    }
+    (void)fail;
+    __syncthreads();
+    if (s_fail) break;
+    const uint32_t base0 = v0 & ~31u;
+    for (uint32_t bb = base0 + (uint32_t)warp * 32u; bb < v0 + nv; bb += kSegThreads) {
+      const uint32_t v = bb + (uint32_t)lane;
+      bool act = false;
+      if (v >= v0 && v < v0 + nv) {
+        const uint32_t l = v - v0;
+        if (s_touch[l] && s_cond[l]) act = f.commit(v, s_acc[l]);
+      }
+      const uint32_t word = __ballot_sync(0xffffffffu, act);
+      if (act) my_deg += __ldg(p.deg_off + v + 1) - __ldg(p.deg_off + v);
+      if (lane == 0 && word) {
+        atomicOr(p.next_bits + (bb >> 5), word);
+        my_cnt += __popc(word);
+      }
+    }
+    __syncthreads();
+  }
+  my_deg = warp_sum(my_deg);
+  my_cnt = warp_sum(my_cnt);
+  if (lane == 0) {
+    s_red[0][warp] = my_cnt;
+    s_red[1][warp] = my_deg;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    unsigned long long a = 0, b2 = 0;
+    for (int w = 0; w < kSegWarps; ++w) {
+      a += s_red[0][w];
+      b2 += s_red[1][w];
+    }
+    if (a) atomicAdd(p.stats + 0, a);
+    if (b2) atomicAdd(p.stats + 1, b2);
   }
 }
 

@@ -33,6 +33,7 @@ struct SumF32 {
 // Also records the level (edgeMap round) of every newly reached vertex.
 struct BfsF : MinU32 {
   static constexpr bool kEarlyExit = true;
+  static constexpr bool kCondTrue = false;
   static constexpr bool kUsesWeight = false;
   int32_t* parents;
   int32_t* levels;
@@ -58,6 +59,7 @@ struct BfsF : MinU32 {
 // Push = updateAtomic (:152-157): writeMin(IDs[d], IDs[s]) && orig==prevIDs[d].
 struct CcF : MinI32 {
   static constexpr bool kEarlyExit = false;
+  static constexpr bool kCondTrue = true;
   static constexpr bool kUsesWeight = false;
   int32_t* ids;
   int32_t* prev;
@@ -84,6 +86,7 @@ struct CcF : MinI32 {
 // Also PageRankDelta's PR_F (app/PageRankDelta.C:29-71) with contrib = Delta/outdeg.
 struct PrF : SumF32 {
   static constexpr bool kEarlyExit = false;
+  static constexpr bool kCondTrue = true;
   static constexpr bool kUsesWeight = false;
   const float* contrib;
   float* acc_out;
@@ -103,6 +106,7 @@ struct PrF : SumF32 {
 // the reference's int edge lengths, or FP32 when the graph carries FP32 weights.
 struct SpmvF : SumF32 {
   static constexpr bool kEarlyExit = false;
+  static constexpr bool kCondTrue = true;
   static constexpr bool kUsesWeight = true;
   const float* x;
   float* y;
@@ -125,6 +129,7 @@ struct SpmvF : SumF32 {
 // Push = writeMin(SP[d], SP[s]+w) && CAS(Visited[d], 0, 1).
 struct BfF : MinI32 {
   static constexpr bool kEarlyExit = false;
+  static constexpr bool kCondTrue = true;
   static constexpr bool kUsesWeight = true;
   int32_t* sp;
   int32_t* visited;
@@ -152,6 +157,7 @@ struct BfF : MinI32 {
 // output iff value[d] was 0 before (first path reaching d).
 struct BcF : SumF32 {
   static constexpr bool kEarlyExit = false;
+  static constexpr bool kCondTrue = false;
   static constexpr bool kUsesWeight = false;
   float* values;
   const uint8_t* visited;

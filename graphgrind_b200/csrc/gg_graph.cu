@@ -173,6 +173,33 @@ static void make_tiles(const uint32_t* off, uint32_t vbeg, uint32_t vend, uint32
   }
 }
 
+// Head bits, per-block head counts and the compressed row list of the edge
+// stream described by host offsets `off` (n+1 entries), see SegIndex.
+static int build_seg(gg_graph_s* g, const uint32_t* off, SegIndex& si) {
+  const uint32_t n = g->n;
+  const uint64_t nwords = g->m_pad / 32;
+  const uint64_t nblk = g->m_pad / kSegBlock;
+  std::vector<uint32_t> head(nwords, 0), blk(nblk + 1, 0), rows;
+  rows.reserve(n);
+  for (uint32_t v = 0; v < n; ++v) {
+    if (off[v + 1] == off[v]) continue;
+    const uint32_t e = off[v];
+    head[e >> 5] |= 1u << (e & 31);
+    blk[e / kSegBlock + 1]++;
+    rows.push_back(v);
+  }
+  for (uint64_t b = 0; b < nblk; ++b) blk[b + 1] += blk[b];
+  si.nrows = rows.size();
+  rows.resize(rows.size() + 8, 0);
+  GG_TRY(dev_alloc(g, &si.d_head, nwords));
+  GG_TRY(dev_alloc(g, &si.d_blk, nblk + 1));
+  GG_TRY(dev_alloc(g, &si.d_rows, rows.size()));
+  GG_CUDA(cudaMemcpy(si.d_head, head.data(), 4 * nwords, cudaMemcpyHostToDevice));
+  GG_CUDA(cudaMemcpy(si.d_blk, blk.data(), 4 * (nblk + 1), cudaMemcpyHostToDevice));
+  GG_CUDA(cudaMemcpy(si.d_rows, rows.data(), 4 * rows.size(), cudaMemcpyHostToDevice));
+  return GG_OK;
+}
+
 static int upload_tiles(gg_graph_s* g, TileSet& ts, std::vector<uint4>& tiles) {
   std::stable_sort(tiles.begin(), tiles.end(), [](const uint4& a, const uint4& b) { return a.w > b.w; });
   ts.host = tiles;
@@ -349,6 +376,11 @@ static void graph_release(gg_graph_s* g) {
     cudaFree(g->d_csc_w);
   }
   for (auto& t : g->csc_tiles) cudaFree(t.d_tiles);
+  for (auto& s : g->seg) {
+    cudaFree(s.d_head);
+    cudaFree(s.d_blk);
+    cudaFree(s.d_rows);
+  }
   cudaFree(g->coo_tiles.d_tiles);
   cudaFree(g->d_coo_src);
   cudaFree(g->d_coo_dloc);
@@ -420,9 +452,13 @@ static int graph_build(const gg_host_graph* hg, const gg_build_opts* opts_in, gg
     if (count) GG_CUDA(cudaMemcpy(*d, h, sizeof(uint32_t) * count, cudaMemcpyHostToDevice));
     return GG_OK;
   };
+  // edge arrays padded (with zeros) to whole 256-edge blocks plus one block,
+  // so that the segmented pull may copy any block that holds a tile edge
+  g->m_pad = (m + kSegBlock - 1) / kSegBlock * kSegBlock + kSegBlock;
+  const size_t epad = (size_t)(g->m_pad - m);
   rc = up(&g->d_csr_off, hg->offsets, (size_t)n + 1, 4);
-  if (!rc) rc = up(&g->d_csr_idx, hg->indices, m, 16);
-  if (!rc && g->wtype != GG_W_NONE) rc = up(&g->d_csr_w, hg->weights, m, 16);
+  if (!rc) rc = up(&g->d_csr_idx, hg->indices, m, epad);
+  if (!rc && g->wtype != GG_W_NONE) rc = up(&g->d_csr_w, hg->weights, m, epad);
   if (!rc) {
     if (g->symmetric) {
       g->d_csc_off = g->d_csr_off;
@@ -430,9 +466,16 @@ static int graph_build(const gg_host_graph* hg, const gg_build_opts* opts_in, gg
       g->d_csc_w = g->d_csr_w;
     } else {
       rc = up(&g->d_csc_off, in->offsets, (size_t)n + 1, 4);
-      if (!rc) rc = up(&g->d_csc_idx, in->indices, m, 16);
-      if (!rc && g->wtype != GG_W_NONE) rc = up(&g->d_csc_w, in->weights, m, 16);
+      if (!rc) rc = up(&g->d_csc_idx, in->indices, m, epad);
+      if (!rc && g->wtype != GG_W_NONE) rc = up(&g->d_csc_w, in->weights, m, epad);
     }
+  }
+  // row structure of the pulled streams: CSC, and CSR for the transposed pull
+  if (!rc) rc = build_seg(g, in->offsets, g->seg[0]);
+  if (!rc && !g->symmetric) rc = build_seg(g, hg->offsets, g->seg[1]);
+  else if (!rc) {
+    g->seg[1] = g->seg[0];
+    g->seg[1].d_head = g->seg[1].d_blk = g->seg[1].d_rows = nullptr;  // shared; never used
   }
   // CTA tiles for the CSC pull, both orientations
   if (!rc) {

@@ -81,8 +81,40 @@ int pull_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f
     if (all) return launch(k_pull<F, true, kHW, true>, smem_coo, occ[1][1]);
     return launch(k_pull<F, true, kHW, false>, smem_coo, occ[1][0]);
   }
-  if (all) return launch(k_pull<F, false, kHW, true>, smem_csc, occ[0][1]);
-  return launch(k_pull<F, false, kHW, false>, smem_csc, occ[0][0]);
+  (void)smem_csc;
+  // CSC: the segmented pull over head bits
+  SegParams s{};
+  const SegIndex& si = g->seg[orient];
+  s.tiles = p.tiles;
+  s.ntiles = p.ntiles;
+  s.tile_counter = p.tile_counter;
+  s.src = p.src;
+  s.wts = p.wts;
+  s.head = si.d_head;
+  s.blk = si.d_blk;
+  s.rows = si.d_rows;
+  s.fr_bits = p.fr_bits;
+  s.next_bits = p.next_bits;
+  s.deg_off = p.deg_off;
+  s.member_off = p.member_off;
+  s.stats = p.stats;
+  s.err = p.err;
+  const size_t smem_seg = seg_smem_bytes(kHW, 4);
+  static int occ_seg[2] = {-1, -1};
+  auto launch_seg = [&](auto kern, int& o) -> int {
+    if (o < 0) {
+      GG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_seg));
+      GG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, kSegThreads, smem_seg));
+      if (o < 1) o = 1;
+    }
+    const int grid = (int)std::min<uint64_t>((uint64_t)g->num_sms * o, s.ntiles);
+    kern<<<grid, kSegThreads, smem_seg, g->stream>>>(s, f);
+    GG_CUDA(cudaGetLastError());
+    g->kernels++;
+    return GG_OK;
+  };
+  if (all) return launch_seg(k_pull_seg<F, kHW, true>, occ_seg[1]);
+  return launch_seg(k_pull_seg<F, kHW, false>, occ_seg[0]);
 }
 
 template <class F, bool HW>
