@@ -134,6 +134,7 @@ _sig("gg_graph_destroy", C.c_int, _P)
 _sig("gg_graph_get_info", C.c_int, _P, C.POINTER(GraphInfo))
 _sig("gg_graph_partition_starts", C.c_int, _P, _i64p)
 _sig("gg_graph_transpose", C.c_int, _P)
+_sig("gg_graph_device_arrays", C.c_int, _P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), C.POINTER(_P))
 _sig("gg_frontier_single", C.c_int, _P, C.c_uint32, C.POINTER(_P))
 _sig("gg_frontier_all", C.c_int, _P, C.POINTER(_P))
 _sig("gg_frontier_empty", C.c_int, _P, C.POINTER(_P))
@@ -166,6 +167,7 @@ _sig("gg_spmv", C.c_int, _P, _P, _P, C.POINTER(RunStats))
 _sig("gg_bellman_ford", C.c_int, _P, C.c_uint32, _P, C.POINTER(RunStats))
 _sig("gg_bc", C.c_int, _P, C.c_uint32, _P, _P, C.POINTER(RunStats))
 _sig("gg_bp", C.c_int, _P, C.c_int32, _P, _P, _P, C.POINTER(RunStats))
+_sig("gg_bfs_push_step_noalloc", C.c_int, _P, _P, C.c_uint32, _P, C.c_uint32, _P, _P, C.c_int32, _P, _P, _P)
 
 # Every symbol declared in include/gg.h (checked by the tests).
 EXPORTED = [
@@ -181,6 +183,7 @@ EXPORTED = [
     "gg_graph_set_dense_policy", "gg_vertex_map", "gg_vertex_filter", "gg_vertex_array_alloc",
     "gg_vertex_array_free", "gg_memcpy_h2d", "gg_memcpy_d2h", "gg_host_alloc_pinned", "gg_host_free_pinned", "gg_bfs", "gg_components",
     "gg_pagerank", "gg_pagerank_delta", "gg_spmv", "gg_bellman_ford", "gg_bc", "gg_bp",
+    "gg_bfs_push_step_noalloc",
 ]
 
 

@@ -265,6 +265,33 @@ int gg_memcpy_d2h(void* host_dst, const void* dev_src, size_t bytes);
 int gg_host_alloc_pinned(size_t bytes, void** host_ptr);
 int gg_host_free_pinned(void* host_ptr);
 
+/* =========================================== push step without allocation */
+/* No counterpart in the reference.  One BFS level on the sparse-push path
+ * (the same kernels as gg_edge_map's push branch with GG_F_BFS) for callers
+ * that must not let the library allocate device memory: programs that own
+ * all device memory and give the library fixed buffers, and latency-critical
+ * loops where cudaMalloc/cudaFree would add allocator latency or an implicit
+ * device synchronisation.  Its temporaries live in one static device array of
+ * GG_NOALLOC_SCRATCH_BYTES that every GPU using the library holds until exit.
+ *   out_offsets/out_indices: device CSR of the graph (n+1 / m entries)
+ *   frontier[frontier_len]:  device queue of the current level (no duplicates)
+ *   parents/levels[n]:       device BFS state (-1 = unvisited); levels may be NULL
+ *   next_frontier[n]:        device output queue (caller-allocated, n entries)
+ *   next_counts[2]:          device output: {output size, its out-degree sum}
+ *   stream:                  a cudaStream_t (NULL = legacy default stream)
+ * Sizes above GG_NOALLOC_MAX_VERTICES / GG_NOALLOC_MAX_FRONTIER return
+ * GG_ERR_SIZE.  The call is asynchronous on `stream`.  All calls share the
+ * array: calls that overlap on the GPU race, so issue them in sequence.  The
+ * first call on each device looks up the array's device address; make it
+ * before any stream capture. */
+#define GG_NOALLOC_MAX_VERTICES (1u << 24)
+#define GG_NOALLOC_MAX_FRONTIER (1u << 19)
+#define GG_NOALLOC_SCRATCH_BYTES ((4u << 20) + (64u << 10))
+int gg_bfs_push_step_noalloc(const uint32_t* out_offsets, const uint32_t* out_indices, uint32_t n,
+                             const uint32_t* frontier, uint32_t frontier_len, int32_t* parents,
+                             int32_t* levels, int32_t round, uint32_t* next_frontier,
+                             uint64_t* next_counts, void* stream);
+
 /* ====================================================== applications */
 /* Each runs the Compute() loop of the named app on the device and copies its
  * result to host arrays of n entries.  Timing (device, ms) of the loop alone
