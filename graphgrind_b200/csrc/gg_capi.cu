@@ -102,9 +102,12 @@ __device__ __forceinline__ void block_add_double(double v, double* out) {
 //   vertexMap(F, PR_Vertex_F)            p_next[i] = d*p_next[i] + (1-d)/n, i in F
 //   p_curr[j] = |p_curr[j] - p_next[j]|  for every j, L1 = sum
 //   vertexMap(F, PR_Vertex_Reset)        p_curr[i] = 0, i in F
-// plus the next iteration's contrib[j] = p_next[j]/outdeg(j).
+// plus the next iteration's contrib[j] = p_next[j]/outdeg(j).  When the next
+// frontier's bitmap is given, sources outside it get -1 (contributions are
+// > 0), so the next pull reads membership from the gathered value itself.
 __global__ void k_pr_epilogue(uint32_t n, int all, const uint32_t* fbits, float* p_curr, float* p_next,
-                              const uint32_t* off, float damping, float added, float* contrib, double* l1) {
+                              const uint32_t* off, float damping, float added, float* contrib, double* l1,
+                              const uint32_t* next_bits) {
   double acc = 0;
   for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x) {
     const bool in = all || test_bit(fbits, (uint32_t)j);
@@ -117,7 +120,8 @@ __global__ void k_pr_epilogue(uint32_t n, int all, const uint32_t* fbits, float*
     acc += diff;
     p_curr[j] = in ? 0.0f : diff;
     const uint32_t d = off[j + 1] - off[j];
-    contrib[j] = d ? pn / (float)d : 0.0f;
+    const bool next_in = !next_bits || test_bit(next_bits, (uint32_t)j);
+    contrib[j] = d ? (next_in ? pn / (float)d : -1.0f) : 0.0f;
   }
   block_add_double(acc, l1);
 }
@@ -260,20 +264,25 @@ static int run_pagerank(gg_graph_s* g, int max_iter, int bit_all, float* ranks, 
   int count = 0;
   uint64_t trav = 0;
   float* last = p_next;
+  bool masked = false;  // contrib marks the frontier (sources outside hold -1)
   while (count < max_iter) {
     ++count;
-    PrF f;
+    PrPosF f;  // frontier sources have p > 0
     f.contrib = contrib.p;
     f.acc_out = p_next;
+    f.frontier_in_values = masked;
     trav += F.f->out_edges;
     gg_frontier_s* out = nullptr;
     GG_TRY(edge_map(g, F.f, f, (int64_t)g->m / 20, 0, &out));
     FrontierHold O;
     O.f = out;
     if (!F.f->bit && !F.f->has_dense) GG_TRY(frontier_to_dense(F.f));
+    // the output becomes the next frontier: mark it in the next contributions
+    masked = !bit_all && out->n == n && out->has_dense;
     GG_CUDA(cudaMemsetAsync(g->ws.d_red, 0, sizeof(double), g->stream));
     k_pr_epilogue<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(
-        n, F.f->bit ? 1 : 0, F.f->d_bits, p_curr, p_next, g->out_off(), damping, added, contrib.p, g->ws.d_red);
+        n, F.f->bit ? 1 : 0, F.f->d_bits, p_curr, p_next, g->out_off(), damping, added, contrib.p, g->ws.d_red,
+        masked ? out->d_bits : nullptr);
     GG_CUDA(cudaGetLastError());
     g->kernels++;
     last = p_next;

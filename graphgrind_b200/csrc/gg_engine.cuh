@@ -185,16 +185,18 @@ struct PullParams {
   const uint32_t* member_off;  // original in-offsets: compressed-CSC membership, or null
   unsigned long long* stats;   // [0] count [1] out-degree sum
   unsigned long long* err;
+  uint32_t tv;                 // widest tile of the tile set
 };
 
-__host__ __device__ constexpr size_t pull_smem_bytes(bool coo, bool hw, int vbytes) {
+// tv: the widest tile of the tile set (its accumulators and flags are sized by it)
+__host__ __device__ constexpr size_t pull_smem_bytes(bool coo, bool hw, int vbytes, uint32_t tv = kMaxTileVertices) {
   return 128                                                       // mbarriers
          + (size_t)kPullStages * kPullSlots * 4                     // src
          + (hw ? (size_t)kPullStages * kPullSlots * 4 : 0)          // weights
          + (coo ? (size_t)kPullStages * kPullSlots * 2 : 0)         // dloc
-         + (size_t)kMaxTileVertices * vbytes                         // accumulators
-         + (coo ? 0 : (size_t)(kMaxTileVertices + 4) * 4)           // tile offsets
-         + (size_t)kMaxTileVertices * 2;                             // touched + cond flags
+         + (size_t)((tv + 3) & ~3u) * vbytes                         // accumulators
+         + (coo ? 0 : (size_t)(tv + 4) * 4)                         // tile offsets
+         + (size_t)((tv + 3) & ~3u) * 2;                             // touched + cond flags
 }
 
 // One CTA per tile at a time; CTAs pull tiles from a global ticket counter
@@ -203,14 +205,15 @@ template <class F, bool COO, bool HW, bool ALL>
 __global__ void __launch_bounds__(kPullThreads, 2) k_pull(const PullParams p, const F f) {
   using V = typename F::value_t;
   extern __shared__ __align__(128) unsigned char smem[];
+  const uint32_t tv4 = (p.tv + 3) & ~3u;
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
   uint32_t* s_src = reinterpret_cast<uint32_t*>(smem + 128);
   uint32_t* s_w = s_src + kPullStages * kPullSlots;
   uint16_t* s_dl = reinterpret_cast<uint16_t*>(s_w + (HW ? kPullStages * kPullSlots : 0));
   V* s_acc = reinterpret_cast<V*>(s_dl + (COO ? kPullStages * kPullSlots : 0));
-  uint32_t* s_off = reinterpret_cast<uint32_t*>(s_acc + kMaxTileVertices);
-  uint8_t* s_touch = reinterpret_cast<uint8_t*>(s_off + (COO ? 0 : kMaxTileVertices + 4));
-  uint8_t* s_cond = s_touch + kMaxTileVertices;
+  uint32_t* s_off = reinterpret_cast<uint32_t*>(s_acc + tv4);
+  uint8_t* s_touch = reinterpret_cast<uint8_t*>(s_off + (COO ? 0 : p.tv + 4));
+  uint8_t* s_cond = s_touch + tv4;
   __shared__ uint32_t s_tile;
   __shared__ unsigned long long s_red[2][kPullThreads / 32];
   __shared__ int s_fail;
@@ -329,7 +332,7 @@ __global__ void __launch_bounds__(kPullThreads, 2) k_pull(const PullParams p, co
           l = li;
         }
         lv[k] = l;
-        vld[k] = v && s_cond[l];
+        vld[k] = v && (F::kCondTrue || s_cond[l]);
       }
       // phase 2: frontier membership of the sources (independent loads)
       if (!ALL) {
@@ -340,7 +343,11 @@ __global__ void __launch_bounds__(kPullThreads, 2) k_pull(const PullParams p, co
       // phase 3: contributions (independent gathers)
       V val[kPullK];
 #pragma unroll
-      for (int k = 0; k < kPullK; ++k) val[k] = vld[k] ? f.gather(sv[k], wv[k]) : F::identity();
+      for (int k = 0; k < kPullK; ++k) {
+        val[k] = vld[k] ? f.gather(sv[k], wv[k]) : F::identity();
+        // positive functors mark sources outside the frontier with a negative value
+        if (F::kPositive) vld[k] = vld[k] && !(val[k] < F::identity());
+      }
       // phase 4: run accumulation into the tile's shared-memory accumulators
       int cur = -1;
       V acc = F::identity();
@@ -351,7 +358,7 @@ __global__ void __launch_bounds__(kPullThreads, 2) k_pull(const PullParams p, co
         if (l != cur) {
           if (cur >= 0) {
             F::atomic_combine(&s_acc[cur], acc);
-            s_touch[cur] = 1;
+            if (!F::kPositive) s_touch[cur] = 1;
           }
           cur = l;
           acc = val[k];
@@ -367,11 +374,11 @@ __global__ void __launch_bounds__(kPullThreads, 2) k_pull(const PullParams p, co
         for (int o = 16; o > 0; o >>= 1) r = F::combine(r, __shfl_xor_sync(0xffffffffu, r, o));
         if (lane == 0) {
           F::atomic_combine(&s_acc[c0], r);
-          s_touch[c0] = 1;
+          if (!F::kPositive) s_touch[c0] = 1;
         }
       } else if (cur >= 0) {
         F::atomic_combine(&s_acc[cur], acc);
-        s_touch[cur] = 1;
+        if (!F::kPositive) s_touch[cur] = 1;
       }
       __syncthreads();  // stage st fully consumed
       if (s_fail) {
@@ -399,7 +406,8 @@ __global__ void __launch_bounds__(kPullThreads, 2) k_pull(const PullParams p, co
       bool act = false;
       if (v >= v0 && v < v0 + nv) {
         const uint32_t l = v - v0;
-        if (s_touch[l] && s_cond[l]) act = f.commit(v, s_acc[l]);
+        const bool touched = F::kPositive ? (s_acc[l] != F::identity()) : (s_touch[l] != 0);
+        if (touched && s_cond[l]) act = f.commit(v, s_acc[l]);
       }
       const uint32_t word = __ballot_sync(0xffffffffu, act);
       if (act) my_deg += __ldg(p.deg_off + v + 1) - __ldg(p.deg_off + v);
@@ -607,7 +615,10 @@ __global__ void __launch_bounds__(kSegThreads, 3) k_pull_seg(const SegParams p, 
       }
       V val[8];
 #pragma unroll
-      for (int k = 0; k < 8; ++k) val[k] = vld[k] ? f.gather(sv[k], wv[k]) : F::identity();
+      for (int k = 0; k < 8; ++k) {
+        val[k] = vld[k] ? f.gather(sv[k], wv[k]) : F::identity();
+        if (F::kPositive) vld[k] = vld[k] && !(val[k] < F::identity());
+      }
       int cur = -1;
       V acc = F::identity();
 #pragma unroll
@@ -617,7 +628,7 @@ __global__ void __launch_bounds__(kSegThreads, 3) k_pull_seg(const SegParams p, 
         if (l != cur) {
           if (cur >= 0) {
             F::atomic_combine(&s_acc[cur], acc);
-            s_touch[cur] = 1;
+            if (!F::kPositive) s_touch[cur] = 1;
           }
           cur = l;
           acc = val[k];
@@ -632,11 +643,11 @@ __global__ void __launch_bounds__(kSegThreads, 3) k_pull_seg(const SegParams p, 
         for (int o = 16; o > 0; o >>= 1) r = F::combine(r, __shfl_xor_sync(0xffffffffu, r, o));
         if (lane == 0) {
           F::atomic_combine(&s_acc[c0], r);
-          s_touch[c0] = 1;
+          if (!F::kPositive) s_touch[c0] = 1;
         }
       } else if (cur >= 0) {
         F::atomic_combine(&s_acc[cur], acc);
-        s_touch[cur] = 1;
+        if (!F::kPositive) s_touch[cur] = 1;
       }
     }
     (void)fail;
@@ -648,7 +659,8 @@ __global__ void __launch_bounds__(kSegThreads, 3) k_pull_seg(const SegParams p, 
       bool act = false;
       if (v >= v0 && v < v0 + nv) {
         const uint32_t l = v - v0;
-        if (s_touch[l] && s_cond[l]) act = f.commit(v, s_acc[l]);
+        const bool touched = F::kPositive ? (s_acc[l] != F::identity()) : (s_touch[l] != 0);
+        if (touched && s_cond[l]) act = f.commit(v, s_acc[l]);
       }
       const uint32_t word = __ballot_sync(0xffffffffu, act);
       if (act) my_deg += __ldg(p.deg_off + v + 1) - __ldg(p.deg_off + v);

@@ -10,18 +10,21 @@ namespace gg {
 
 struct MinI32 {
   using value_t = int32_t;
+  bool frontier_in_values = false;  // gathered values already mark frontier membership
   __device__ static value_t identity() { return 0x7fffffff; }
   __device__ static value_t combine(value_t a, value_t b) { return a < b ? a : b; }
   __device__ static void atomic_combine(value_t* s, value_t v) { atomicMin(s, v); }
 };
 struct MinU32 {
   using value_t = uint32_t;
+  bool frontier_in_values = false;  // gathered values already mark frontier membership
   __device__ static value_t identity() { return 0xffffffffu; }
   __device__ static value_t combine(value_t a, value_t b) { return a < b ? a : b; }
   __device__ static void atomic_combine(value_t* s, value_t v) { atomicMin(s, v); }
 };
 struct SumF32 {
   using value_t = float;
+  bool frontier_in_values = false;  // gathered values already mark frontier membership
   __device__ static value_t identity() { return 0.0f; }
   __device__ static value_t combine(value_t a, value_t b) { return a + b; }
   __device__ static void atomic_combine(value_t* s, value_t v) { atomicAdd(s, v); }
@@ -32,6 +35,7 @@ struct SumF32 {
 // order-dependent in the reference too); updateAtomic = CAS(-1 -> s).
 // Also records the level (edgeMap round) of every newly reached vertex.
 struct BfsF : MinU32 {
+  static constexpr bool kPositive = false;
   static constexpr bool kEarlyExit = true;
   static constexpr bool kCondTrue = false;
   static constexpr bool kUsesWeight = false;
@@ -58,6 +62,7 @@ struct BfsF : MinU32 {
 // min over prevIDs[s]; output iff the label drops and IDs[d]==prevIDs[d].
 // Push = updateAtomic (:152-157): writeMin(IDs[d], IDs[s]) && orig==prevIDs[d].
 struct CcF : MinI32 {
+  static constexpr bool kPositive = false;
   static constexpr bool kEarlyExit = false;
   static constexpr bool kCondTrue = true;
   static constexpr bool kUsesWeight = false;
@@ -84,9 +89,14 @@ struct CcF : MinI32 {
 // division is done once per source (contrib[s] = p_curr[s]/outdeg(s)) by the
 // iteration's vertex pass; the per-edge value is the same FP32 quotient.
 // Also PageRankDelta's PR_F (app/PageRankDelta.C:29-71) with contrib = Delta/outdeg.
-struct PrF : SumF32 {
+// POS: every contribution is > 0 (PageRank: frontier sources have p > 0), so
+// a destination was updated iff its accumulator differs from 0 and the pull
+// needs no separate "touched" flag.  PageRankDelta's Delta can be 0 or < 0.
+template <bool POS>
+struct PrT : SumF32 {
   static constexpr bool kEarlyExit = false;
   static constexpr bool kCondTrue = true;
+  static constexpr bool kPositive = POS;
   static constexpr bool kUsesWeight = false;
   const float* contrib;
   float* acc_out;
@@ -101,10 +111,13 @@ struct PrF : SumF32 {
     return true;
   }
 };
+using PrF = PrT<false>;
+using PrPosF = PrT<true>;
 
 // SPMV_F, app/SPMV.C:7-47: p_next[d] += p_curr[s] * edgeLen.  Weights are
 // the reference's int edge lengths, or FP32 when the graph carries FP32 weights.
 struct SpmvF : SumF32 {
+  static constexpr bool kPositive = false;
   static constexpr bool kEarlyExit = false;
   static constexpr bool kCondTrue = true;
   static constexpr bool kUsesWeight = true;
@@ -128,6 +141,7 @@ struct SpmvF : SumF32 {
 // frontier in-neighbours; output iff it lowers SP[d] and Visited[d] was 0.
 // Push = writeMin(SP[d], SP[s]+w) && CAS(Visited[d], 0, 1).
 struct BfF : MinI32 {
+  static constexpr bool kPositive = false;
   static constexpr bool kEarlyExit = false;
   static constexpr bool kCondTrue = true;
   static constexpr bool kUsesWeight = true;
@@ -156,6 +170,7 @@ struct BfF : MinI32 {
 // BC_F / BC_Back_F, app/BC.C:28-117: value[d] += value[s] for unvisited d;
 // output iff value[d] was 0 before (first path reaching d).
 struct BcF : SumF32 {
+  static constexpr bool kPositive = false;
   static constexpr bool kEarlyExit = false;
   static constexpr bool kCondTrue = false;
   static constexpr bool kUsesWeight = false;

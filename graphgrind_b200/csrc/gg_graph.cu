@@ -238,6 +238,20 @@ __global__ void k_coo_keys(const uint32_t* src, const uint32_t* dst, uint64_t m,
   }
 }
 
+// Second-level order inside a tile: positions keep their 256-edge window of
+// the Hilbert order, and inside a window edges go by destination, so that a
+// thread's 8 consecutive edges form destination runs while the window keeps
+// the Hilbert locality of its sources.  key = window << 12 | local destination.
+constexpr int kCooWindow = 256;
+__global__ void k_coo_window_keys(const uint4* seg, uint32_t ntiles, const uint32_t* perm, const uint32_t* dst,
+                                  uint32_t* keys) {
+  for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const uint4 s = seg[t];  // {v0, nv, e0 (CSC), ne}
+    for (uint32_t i = threadIdx.x; i < s.w; i += blockDim.x)
+      keys[s.z + i] = ((i / kCooWindow) << 12) | (dst[perm[s.z + i]] - s.x);
+  }
+}
+
 // scatter sorted tile segments into their padded COO slots
 __global__ void k_coo_scatter(const uint4* seg, const uint32_t* pad_start, uint32_t ntiles, const uint32_t* perm,
                               const uint32_t* src, const uint32_t* dst, const uint32_t* w, uint32_t* coo_src,
@@ -339,7 +353,23 @@ static int build_coo(gg_graph_s* g, const uint32_t* h_in_off) {
     GG_BUILD(cudaMalloc(&d_temp, temp_bytes));
     GG_BUILD(cub::DeviceSegmentedRadixSort::SortPairs(d_temp, temp_bytes, d_keys, d_keys_out, d_vals, d_perm, (int)m,
                                                       (int)segs.size(), d_seg_begin, d_seg_begin + 1));
-    k_coo_scatter<<<grid, 256>>>(d_segs, d_pad, (uint32_t)segs.size(), d_perm, g->d_csc_idx, d_dst, g->d_csc_w,
+    // destination order inside 256-edge windows (the u64 key buffers are reused as u32)
+    uint32_t* k32 = reinterpret_cast<uint32_t*>(d_keys);
+    uint32_t* k32_out = reinterpret_cast<uint32_t*>(d_keys_out);
+    k_coo_window_keys<<<grid, 256>>>(d_segs, (uint32_t)segs.size(), d_perm, d_dst, k32);
+    GG_BUILD(cudaGetLastError());
+    size_t temp2 = 0;
+    GG_BUILD(cub::DeviceSegmentedRadixSort::SortPairs(nullptr, temp2, k32, k32_out, d_perm, d_vals, (int)m,
+                                                      (int)segs.size(), d_seg_begin, d_seg_begin + 1));
+    if (temp2 > temp_bytes) {
+      cudaFree(d_temp);
+      d_temp = nullptr;
+      GG_BUILD(cudaMalloc(&d_temp, temp2));
+      temp_bytes = temp2;
+    }
+    GG_BUILD(cub::DeviceSegmentedRadixSort::SortPairs(d_temp, temp2, k32, k32_out, d_perm, d_vals, (int)m,
+                                                      (int)segs.size(), d_seg_begin, d_seg_begin + 1));
+    k_coo_scatter<<<grid, 256>>>(d_segs, d_pad, (uint32_t)segs.size(), d_vals, g->d_csc_idx, d_dst, g->d_csc_w,
                                  g->d_coo_src, g->d_coo_dloc, g->d_coo_w);
     GG_BUILD(cudaGetLastError());
   }

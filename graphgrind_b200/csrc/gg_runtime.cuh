@@ -32,7 +32,8 @@ int read_stats(gg_graph_s* g);  // blocks; checks the device error word
 // graphgrind/ligra-numa.h:919-1019
 template <class F, bool HW>
 int pull_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f, bool coo) {
-  const bool all = in->bit;
+  // a positive functor whose gathered values already mark the frontier needs no bitmap
+  const bool all = in->bit || (F::kPositive && f.frontier_in_values);
   PullParams p{};
   const int orient = g->transposed ? 1 : 0;
   if (coo) {
@@ -61,17 +62,22 @@ int pull_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f
   p.err = g->ws.d_stats + 3;
   if (p.ntiles == 0) return GG_OK;
   constexpr bool kHW = HW;
-  const size_t smem_coo = pull_smem_bytes(true, kHW, 4);
+  p.tv = (uint32_t)g->opts.tile_vertices;
+  const size_t smem_coo = pull_smem_bytes(true, kHW, 4, p.tv);
   const size_t smem_csc = pull_smem_bytes(false, kHW, 4);
-  // one-time per instantiation: opt in to large dynamic shared memory, occupancy
+  // opt in once to the largest dynamic shared memory (widest tiles); the
+  // occupancy follows the tile width of this graph
   static int occ[2][2] = {{-1, -1}, {-1, -1}};
   auto launch = [&](auto kern, size_t smem, int& o) -> int {
     if (o < 0) {
-      GG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      GG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, kPullThreads, smem));
-      if (o < 1) o = 1;
+      GG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)pull_smem_bytes(true, kHW, 4, kMaxTileVertices)));
+      o = 0;
     }
-    const int grid = (int)std::min<uint64_t>((uint64_t)g->num_sms * o, p.ntiles);
+    int blocks = 1;
+    GG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kern, kPullThreads, smem));
+    if (blocks < 1) blocks = 1;
+    const int grid = (int)std::min<uint64_t>((uint64_t)g->num_sms * blocks, p.ntiles);
     kern<<<grid, kPullThreads, smem, g->stream>>>(p, f);
     GG_CUDA(cudaGetLastError());
     g->kernels++;
