@@ -151,6 +151,9 @@ _sig("gg_last_edge_map_stats", C.c_int, _P, C.POINTER(EdgeMapStats))
 _sig("gg_graph_set_profiling", C.c_int, _P, C.c_int32)
 _sig("gg_graph_get_profile", C.c_int, _P, C.POINTER(Profile))
 _sig("gg_graph_set_dense_policy", C.c_int, _P, C.c_int32)
+_sig("gg_graph_set_tuning", C.c_int, _P, C.c_int32, C.c_int64)
+_sig("gg_graph_get_tuning", C.c_int, _P, C.c_int32, C.POINTER(C.c_int64))
+TUNE_DENSE_POLICY, TUNE_COO_KERNEL = 1, 2
 _sig("gg_vertex_map", C.c_int, _P, _P, C.c_int32, _P)
 _sig("gg_vertex_filter", C.c_int, _P, _P, C.c_int32, _P, C.POINTER(_P))
 _sig("gg_vertex_array_alloc", C.c_int, _P, C.c_size_t, C.POINTER(_P))
@@ -180,7 +183,7 @@ EXPORTED = [
     "gg_frontier_from_list", "gg_frontier_destroy", "gg_frontier_stats", "gg_frontier_to_mask",
     "gg_frontier_to_dense", "gg_frontier_to_sparse", "gg_frontier_repr", "gg_edge_map",
     "gg_last_edge_map_stats", "gg_graph_set_profiling", "gg_graph_get_profile",
-    "gg_graph_set_dense_policy", "gg_vertex_map", "gg_vertex_filter", "gg_vertex_array_alloc",
+    "gg_graph_set_dense_policy", "gg_graph_set_tuning", "gg_graph_get_tuning", "gg_vertex_map", "gg_vertex_filter", "gg_vertex_array_alloc",
     "gg_vertex_array_free", "gg_memcpy_h2d", "gg_memcpy_d2h", "gg_host_alloc_pinned", "gg_host_free_pinned", "gg_bfs", "gg_components",
     "gg_pagerank", "gg_pagerank_delta", "gg_spmv", "gg_bellman_ford", "gg_bc", "gg_bp",
     "gg_bfs_push_step_noalloc",
@@ -475,6 +478,14 @@ class Graph:
     def set_dense_policy(self, policy: int):
         """0: reference rule (COO above m/2), 1: always CSC pull, 2: always COO pull."""
         check(lib.gg_graph_set_dense_policy(self.h, policy), "gg_graph_set_dense_policy")
+
+    def set_tuning(self, key: int, value: int):
+        check(lib.gg_graph_set_tuning(self.h, key, value), "gg_graph_set_tuning")
+
+    def get_tuning(self, key: int) -> int:
+        v = C.c_int64()
+        check(lib.gg_graph_get_tuning(self.h, key, C.byref(v)), "gg_graph_get_tuning")
+        return int(v.value)
 
     # vertexSubset constructors
     def frontier_single(self, v) -> Frontier:

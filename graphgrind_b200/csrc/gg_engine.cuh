@@ -136,6 +136,7 @@ struct gg_graph_s {
   gg_profile prof{};
   cudaEvent_t prof_ev[2] = {nullptr, nullptr};
   int dense_policy = 0;
+  int coo_kernel = 1;  // 0 CTA ring (k_pull), 1 per-warp direct loads (fastest measured), 2/3 per-warp bulk-copy rings
   uint64_t device_bytes = 0;
   int kernels = 0;  // kernels launched since the counter was last reset
   std::unordered_set<gg_frontier_s*> frontiers;  // live frontiers (freed with the graph)
@@ -434,6 +435,224 @@ __global__ void __launch_bounds__(kPullThreads, 2) k_pull(const PullParams p, co
     }
     if (a) atomicAdd(p.stats + 0, a);
     if (b) atomicAdd(p.stats + 1, b);
+  }
+}
+
+// ------------------------------------------ per-warp partitioned-COO pull
+// Same tile ownership as k_pull (shared-memory accumulators, one commit per
+// destination), but every warp streams its own 256-edge blocks of the tile:
+// STAGES > 0 through a private bulk-copy ring in shared memory, STAGES == 0
+// with direct 16-byte loads (no staging; all of L1 left to the source
+// gathers).  No CTA-wide barrier per block.
+constexpr int kCooWarps = 8;
+constexpr int kCooThreads = kCooWarps * 32;
+
+__host__ __device__ constexpr size_t coo_w_stage_bytes(bool hw) {
+  return (size_t)kSegBlock * 4 + (size_t)kSegBlock * 2 + (hw ? (size_t)kSegBlock * 4 : 0);
+}
+__host__ __device__ constexpr size_t coo_w_smem_bytes(bool hw, int stages, int vbytes, uint32_t tv) {
+  return 256 + (size_t)kCooWarps * stages * coo_w_stage_bytes(hw) + (size_t)((tv + 3) & ~3u) * (vbytes + 2);
+}
+
+template <class F, bool HW, bool ALL, int STAGES>
+__global__ void __launch_bounds__(kCooThreads, 4) k_pull_coo_w(const PullParams p, const F f) {
+  using V = typename F::value_t;
+  extern __shared__ __align__(128) unsigned char smem[];
+  constexpr uint32_t SB = (uint32_t)coo_w_stage_bytes(HW);
+  const uint32_t tv4 = (p.tv + 3) & ~3u;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
+  unsigned char* stages = smem + 256;
+  V* s_acc = reinterpret_cast<V*>(stages + (size_t)kCooWarps * STAGES * SB);
+  uint8_t* s_touch = reinterpret_cast<uint8_t*>(s_acc + tv4);
+  uint8_t* s_cond = s_touch + tv4;
+  __shared__ uint32_t s_tile;
+  __shared__ unsigned long long s_red[2][kCooWarps];
+  __shared__ int s_fail;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  uint64_t* wbar = bars + warp * (STAGES > 0 ? STAGES : 1);
+  unsigned char* wst = stages + (size_t)warp * STAGES * SB;
+  if (STAGES > 0 && lane == 0)
+    for (int s = 0; s < STAGES; ++s) mbar_init(&wbar[s], 1);
+  if (tid == 0) s_fail = 0;
+  if (STAGES > 0) fence_mbar_init();
+  __syncthreads();
+  uint32_t parity = 0;
+  unsigned long long my_cnt = 0, my_deg = 0;
+
+  for (;;) {
+    if (tid == 0) s_tile = (uint32_t)atomicAdd(p.tile_counter, 1ull);
+    __syncthreads();
+    const uint32_t t = s_tile;
+    if (t >= p.ntiles || s_fail) break;
+    const uint4 td = p.tiles[t];
+    const uint32_t v0 = td.x, nv = td.y, e0 = td.z, ne = td.w;  // e0, ne multiples of 8
+    for (uint32_t i = tid; i < nv; i += kCooThreads) {
+      s_acc[i] = F::identity();
+      if (!F::kPositive) s_touch[i] = 0;
+      s_cond[i] = (F::kCondTrue || f.cond(v0 + i)) ? 1 : 0;
+    }
+    __syncthreads();
+    const uint32_t nb = (ne + kSegBlock - 1) / kSegBlock;
+    const uint32_t nbw = (uint32_t)warp < nb ? (nb - (uint32_t)warp + kCooWarps - 1) / kCooWarps : 0;
+    auto blk_len = [&](uint32_t j) { return min((uint32_t)kSegBlock, ne - j * kSegBlock); };
+    auto issue = [&](uint32_t i, int st) {
+      const uint32_t j = (uint32_t)warp + i * kCooWarps;
+      const uint32_t b0 = e0 + j * kSegBlock, nel = blk_len(j);
+      unsigned char* d = wst + st * SB;
+      mbar_arrive_expect_tx(&wbar[st], nel * (HW ? 10u : 6u));
+      bulk_g2s(d, p.src + b0, nel * 4, &wbar[st]);
+      bulk_g2s(d + kSegBlock * 4, p.dloc + b0, nel * 2, &wbar[st]);
+      if (HW) bulk_g2s(d + kSegBlock * 6, p.wts + b0, nel * 4, &wbar[st]);
+    };
+    uint32_t issued = 0;
+    if constexpr (STAGES > 0) {
+      if (lane == 0)
+        for (uint32_t i = 0; i < nbw && i < (uint32_t)STAGES; ++i) issue(i, (int)i);
+      issued = nbw < (uint32_t)STAGES ? nbw : (uint32_t)STAGES;
+    }
+    for (uint32_t i = 0; i < nbw; ++i) {
+      const uint32_t j = (uint32_t)warp + i * kCooWarps;
+      const uint32_t nel = blk_len(j);
+      const bool in = (uint32_t)lane * 8 < nel;  // 8-slot groups are wholly in or out
+      uint32_t sv[8], wv[8];
+      uint16_t dv[8];
+      if constexpr (STAGES > 0) {
+        const int st = (int)(i % STAGES);
+        const bool ok = __all_sync(0xffffffffu, mbar_wait_bounded(&wbar[st], (parity >> st) & 1u));
+        parity ^= 1u << st;
+        if (!ok) {
+          if (lane == 0) atomicOr(p.err, (unsigned long long)DEV_ERR_TIMEOUT);
+          s_fail = 1;
+          for (uint32_t cc = i + 1; cc < issued; ++cc) {
+            const int s2 = (int)(cc % STAGES);
+            mbar_wait_bounded(&wbar[s2], (parity >> s2) & 1u);
+            parity ^= 1u << s2;
+          }
+          break;
+        }
+        const unsigned char* d = wst + st * SB;
+        if (in) {
+          const uint4 a = reinterpret_cast<const uint4*>(d)[lane * 2];
+          const uint4 c = reinterpret_cast<const uint4*>(d)[lane * 2 + 1];
+          sv[0] = a.x; sv[1] = a.y; sv[2] = a.z; sv[3] = a.w;
+          sv[4] = c.x; sv[5] = c.y; sv[6] = c.z; sv[7] = c.w;
+          const uint4 q = reinterpret_cast<const uint4*>(d + kSegBlock * 4)[lane];
+          dv[0] = q.x & 0xffff; dv[1] = q.x >> 16; dv[2] = q.y & 0xffff; dv[3] = q.y >> 16;
+          dv[4] = q.z & 0xffff; dv[5] = q.z >> 16; dv[6] = q.w & 0xffff; dv[7] = q.w >> 16;
+          if (HW) {
+            const uint4 u = reinterpret_cast<const uint4*>(d + kSegBlock * 6)[lane * 2];
+            const uint4 v = reinterpret_cast<const uint4*>(d + kSegBlock * 6)[lane * 2 + 1];
+            wv[0] = u.x; wv[1] = u.y; wv[2] = u.z; wv[3] = u.w;
+            wv[4] = v.x; wv[5] = v.y; wv[6] = v.z; wv[7] = v.w;
+          }
+        }
+        __syncwarp();
+        if (lane == 0 && i + STAGES < nbw) {
+          fence_proxy_async_smem();
+          issue(i + STAGES, st);
+        }
+        if (i + STAGES < nbw) ++issued;
+      } else if (in) {
+        const size_t b0 = (size_t)e0 + (size_t)j * kSegBlock + (size_t)lane * 8;
+        const uint4 a = __ldg(reinterpret_cast<const uint4*>(p.src + b0));
+        const uint4 c = __ldg(reinterpret_cast<const uint4*>(p.src + b0) + 1);
+        sv[0] = a.x; sv[1] = a.y; sv[2] = a.z; sv[3] = a.w;
+        sv[4] = c.x; sv[5] = c.y; sv[6] = c.z; sv[7] = c.w;
+        const uint4 q = __ldg(reinterpret_cast<const uint4*>(p.dloc + b0));
+        dv[0] = q.x & 0xffff; dv[1] = q.x >> 16; dv[2] = q.y & 0xffff; dv[3] = q.y >> 16;
+        dv[4] = q.z & 0xffff; dv[5] = q.z >> 16; dv[6] = q.w & 0xffff; dv[7] = q.w >> 16;
+        if (HW) {
+          const uint4 u = __ldg(reinterpret_cast<const uint4*>(p.wts + b0));
+          const uint4 v = __ldg(reinterpret_cast<const uint4*>(p.wts + b0) + 1);
+          wv[0] = u.x; wv[1] = u.y; wv[2] = u.z; wv[3] = u.w;
+          wv[4] = v.x; wv[5] = v.y; wv[6] = v.z; wv[7] = v.w;
+        }
+      }
+      if (!HW) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) wv[k] = 1u;
+      }
+      bool vld[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) vld[k] = in && sv[k] != kPad && (F::kCondTrue || s_cond[dv[k]]);
+      if (!ALL) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+          if (vld[k]) vld[k] = test_bit(p.fr_bits, sv[k]);
+      }
+      V val[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        val[k] = vld[k] ? f.gather(sv[k], wv[k]) : F::identity();
+        if (F::kPositive) vld[k] = vld[k] && !(val[k] < F::identity());
+      }
+      int cur = -1;
+      V acc = F::identity();
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        if (!vld[k]) continue;
+        const int l = (int)dv[k];
+        if (l != cur) {
+          if (cur >= 0) {
+            F::atomic_combine(&s_acc[cur], acc);
+            if (!F::kPositive) s_touch[cur] = 1;
+          }
+          cur = l;
+          acc = val[k];
+        } else {
+          acc = F::combine(acc, val[k]);
+        }
+      }
+      const int c0 = __shfl_sync(0xffffffffu, cur, 0);
+      if (__all_sync(0xffffffffu, cur == c0) && c0 >= 0) {
+        V r = acc;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) r = F::combine(r, __shfl_xor_sync(0xffffffffu, r, o));
+        if (lane == 0) {
+          F::atomic_combine(&s_acc[c0], r);
+          if (!F::kPositive) s_touch[c0] = 1;
+        }
+      } else if (cur >= 0) {
+        F::atomic_combine(&s_acc[cur], acc);
+        if (!F::kPositive) s_touch[cur] = 1;
+      }
+    }
+    __syncthreads();
+    if (s_fail) break;
+    const uint32_t base0 = v0 & ~31u;
+    for (uint32_t bb = base0 + (uint32_t)warp * 32u; bb < v0 + nv; bb += kCooThreads) {
+      const uint32_t v = bb + (uint32_t)lane;
+      bool act = false;
+      if (v >= v0 && v < v0 + nv) {
+        const uint32_t l = v - v0;
+        const bool touched = F::kPositive ? (s_acc[l] != F::identity()) : (s_touch[l] != 0);
+        if (touched && s_cond[l]) act = f.commit(v, s_acc[l]);
+      }
+      const uint32_t word = __ballot_sync(0xffffffffu, act);
+      if (act) my_deg += __ldg(p.deg_off + v + 1) - __ldg(p.deg_off + v);
+      if (lane == 0 && word) {
+        atomicOr(p.next_bits + (bb >> 5), word);
+        my_cnt += __popc(word);
+      }
+    }
+    __syncthreads();
+  }
+  my_deg = warp_sum(my_deg);
+  my_cnt = warp_sum(my_cnt);
+  if (lane == 0) {
+    s_red[0][warp] = my_cnt;
+    s_red[1][warp] = my_deg;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    unsigned long long a = 0, b2 = 0;
+    for (int w = 0; w < kCooWarps; ++w) {
+      a += s_red[0][w];
+      b2 += s_red[1][w];
+    }
+    if (a) atomicAdd(p.stats + 0, a);
+    if (b2) atomicAdd(p.stats + 1, b2);
   }
 }
 

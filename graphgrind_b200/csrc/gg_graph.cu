@@ -631,6 +631,34 @@ int gg_graph_set_dense_policy(gg_graph_t g, int32_t policy) {
   return GG_OK;
 }
 
+int gg_graph_set_tuning(gg_graph_t g, int32_t key, int64_t value) {
+  if (!graph_live(g)) return fail(GG_ERR_INVALID_ARG, "gg_graph_set_tuning: not a live graph");
+  switch (key) {
+    case GG_TUNE_DENSE_POLICY:
+      return gg_graph_set_dense_policy(g, (int32_t)value);
+    case GG_TUNE_COO_KERNEL:
+      if (value < 0 || value > 3) return fail(GG_ERR_INVALID_ARG, "COO kernel must be 0..3");
+      g->coo_kernel = (int)value;
+      return GG_OK;
+    default:
+      return fail(GG_ERR_INVALID_ARG, "unknown tuning key %d", key);
+  }
+}
+
+int gg_graph_get_tuning(gg_graph_t g, int32_t key, int64_t* value) {
+  if (!graph_live(g) || !value) return fail(GG_ERR_INVALID_ARG, "gg_graph_get_tuning: bad arguments");
+  switch (key) {
+    case GG_TUNE_DENSE_POLICY:
+      *value = g->dense_policy;
+      return GG_OK;
+    case GG_TUNE_COO_KERNEL:
+      *value = g->coo_kernel;
+      return GG_OK;
+    default:
+      return fail(GG_ERR_INVALID_ARG, "unknown tuning key %d", key);
+  }
+}
+
 int gg_graph_transpose(gg_graph_t g) {
   if (!g) return fail(GG_ERR_INVALID_ARG, "gg_graph_transpose: null graph");
   if (!g->symmetric) g->transposed = !g->transposed;  // graphgrind/graph-numa.h:598-611

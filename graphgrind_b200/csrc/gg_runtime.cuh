@@ -83,6 +83,36 @@ int pull_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f
     g->kernels++;
     return GG_OK;
   };
+  if (coo && g->coo_kernel > 0) {  // per-warp COO pull: 0, 2 or 3 staging stages
+    static bool opted[2][4] = {};
+    auto launch_w = [&](auto kern, int stages, bool& done) -> int {
+      const size_t smem = coo_w_smem_bytes(kHW, stages, 4, p.tv);
+      if (!done) {
+        GG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)coo_w_smem_bytes(kHW, stages, 4, kMaxTileVertices)));
+        done = true;
+      }
+      int blocks = 1;
+      GG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kern, kCooThreads, smem));
+      if (blocks < 1) blocks = 1;
+      const int grid = (int)std::min<uint64_t>((uint64_t)g->num_sms * blocks, p.ntiles);
+      kern<<<grid, kCooThreads, smem, g->stream>>>(p, f);
+      GG_CUDA(cudaGetLastError());
+      g->kernels++;
+      return GG_OK;
+    };
+    switch (g->coo_kernel) {
+      case 1:
+        return all ? launch_w(k_pull_coo_w<F, kHW, true, 0>, 0, opted[1][1])
+                   : launch_w(k_pull_coo_w<F, kHW, false, 0>, 0, opted[0][1]);
+      case 2:
+        return all ? launch_w(k_pull_coo_w<F, kHW, true, 2>, 2, opted[1][2])
+                   : launch_w(k_pull_coo_w<F, kHW, false, 2>, 2, opted[0][2]);
+      default:
+        return all ? launch_w(k_pull_coo_w<F, kHW, true, 3>, 3, opted[1][3])
+                   : launch_w(k_pull_coo_w<F, kHW, false, 3>, 3, opted[0][3]);
+    }
+  }
   if (coo) {
     if (all) return launch(k_pull<F, true, kHW, true>, smem_coo, occ[1][1]);
     return launch(k_pull<F, true, kHW, false>, smem_coo, occ[1][0]);
@@ -211,8 +241,13 @@ int edge_map(gg_graph_s* g, gg_frontier_s* in, const F& f, int64_t threshold, ui
     g->prof.edges[kind] += edges;
   };
   if (dense) {
-    // :957 (!part_ver); the GPU policy may pin the dense kernel (same results)
-    bool coo = g->has_coo && (g->dense_policy == 2 || (g->dense_policy == 0 && fm + tot > dense_threshold));
+    // :957 (!part_ver).  The GPU policy may pin the dense kernel, which keeps the
+    // results only while the graph is not transposed: the reference never
+    // transposes its COO partitions (graphgrind/graph-numa.h:721-728), so after
+    // transpose() the COO and CSC kernels compute different maps and the
+    // reference's rule is followed exactly.
+    const bool ref_rule = g->dense_policy == 0 || g->transposed;
+    bool coo = g->has_coo && (ref_rule ? fm + tot > dense_threshold : g->dense_policy == 2);
     if (flags & GG_EM_FORCE_CSC) coo = false;
     if ((flags & GG_EM_FORCE_COO) && g->has_coo) coo = true;
     const bool early = !coo && F::kEarlyExit;

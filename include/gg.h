@@ -233,6 +233,14 @@ int gg_graph_get_profile(gg_graph_t g, gg_profile* out);
 /* Dense-branch kernel policy: 0 = the reference's rule (COO above m/2 when
  * the COO exists, else CSC), 1 = always CSC pull, 2 = always COO pull. */
 int gg_graph_set_dense_policy(gg_graph_t g, int32_t policy);
+/* Engine tuning knobs (all keep edgeMap's results; they pick kernels):
+ *   GG_TUNE_DENSE_POLICY  as gg_graph_set_dense_policy
+ *   GG_TUNE_COO_KERNEL    0 CTA-wide bulk-copy ring, 1 per-warp direct loads,
+ *                         2/3 per-warp bulk-copy ring with 2/3 stages */
+#define GG_TUNE_DENSE_POLICY 1
+#define GG_TUNE_COO_KERNEL 2
+int gg_graph_set_tuning(gg_graph_t g, int32_t key, int64_t value);
+int gg_graph_get_tuning(gg_graph_t g, int32_t key, int64_t* value);
 
 /* Vertex functors for vertexMap / vertexFilter (graphgrind/ligra-numa.h:1023-1082). */
 enum gg_vertex_functor_id {

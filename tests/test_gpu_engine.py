@@ -114,3 +114,26 @@ def test_empty_result_cannot_be_mapped_again(gg, sym12):
     with pytest.raises(gg.GGError) as e:
         g.edge_map(E, gg.F_BFS, gg.BfsArgs(par.ptr, None, 2))
     assert "Sizes Don't match" in str(e.value)
+
+
+@pytest.mark.parametrize("coo_kernel", [0, 1, 2, 3])
+def test_apps_with_each_coo_kernel(gg, orc, coo_kernel):
+    """Every COO pull variant (CTA ring, per-warp direct, per-warp 2/3-stage
+    rings) gives the oracle's results when all dense steps use the COO."""
+    from conftest import PR_MAX_ABS, PR_REL_L1, rel_l1
+    hg = gg.HostGraph.rmat(12, 16, seed=81, symmetric=False).add_weights(gg.W_INT32, seed=2, lo=1, hi=100)
+    g = gg.Graph(hg, partitions=ok_partitions(hg, 16), tile_vertices=1024)
+    g.set_dense_policy(2)
+    g.set_tuning(gg.TUNE_COO_KERNEL, coo_kernel)
+    assert g.get_tuning(gg.TUNE_COO_KERNEL) == coo_kernel
+    og = orc.Graph.from_host(hg)
+    r, _ = g.pagerank(10)
+    o, _ = og.pagerank(10)
+    assert rel_l1(r, o) <= PR_REL_L1 and np.abs(r - o).max() <= PR_MAX_ABS
+    np.testing.assert_array_equal(g.components()[0], og.cc()[0])
+    np.testing.assert_array_equal(g.bfs(7)[1], og.bfs(7)[1])
+    np.testing.assert_array_equal(g.bellman_ford(7)[0], og.bellman_ford(7)[0])
+    dep, npth, _ = g.bc(7)
+    odep, onp, _ = og.bc(7)
+    fin = np.isfinite(odep)
+    assert rel_l1(dep[fin], odep[fin]) <= 1e-4
