@@ -171,6 +171,7 @@ _sig("gg_bellman_ford", C.c_int, _P, C.c_uint32, _P, C.POINTER(RunStats))
 _sig("gg_bc", C.c_int, _P, C.c_uint32, _P, _P, C.POINTER(RunStats))
 _sig("gg_bp", C.c_int, _P, C.c_int32, _P, _P, _P, C.POINTER(RunStats))
 _sig("gg_bfs_push_step_noalloc", C.c_int, _P, _P, C.c_uint32, _P, C.c_uint32, _P, _P, C.c_int32, _P, _P, _P)
+_sig("gg_ppr_k", C.c_int, _P, C.c_int32, C.c_int32, C.c_float, _P, _P, _P, C.POINTER(RunStats))
 
 # Every symbol declared in include/gg.h (checked by the tests).
 EXPORTED = [
@@ -186,7 +187,7 @@ EXPORTED = [
     "gg_graph_set_dense_policy", "gg_graph_set_tuning", "gg_graph_get_tuning", "gg_vertex_map", "gg_vertex_filter", "gg_vertex_array_alloc",
     "gg_vertex_array_free", "gg_memcpy_h2d", "gg_memcpy_d2h", "gg_host_alloc_pinned", "gg_host_free_pinned", "gg_bfs", "gg_components",
     "gg_pagerank", "gg_pagerank_delta", "gg_spmv", "gg_bellman_ford", "gg_bc", "gg_bp",
-    "gg_bfs_push_step_noalloc",
+    "gg_bfs_push_step_noalloc", "gg_ppr_k",
 ]
 
 
@@ -563,6 +564,21 @@ class Graph:
         st = RunStats()
         check(lib.gg_bellman_ford(self.h, start, _ptr(d), C.byref(st)), "gg_bellman_ford")
         return d, _run(st)
+
+    def ppr_k(self, k=64, iters=20, damping=0.85, tele=None, seeds=None, out=None):
+        """k-column personalised PageRank; returns (X[n, k] float32, Run)."""
+        y = out if out is not None else np.empty((self.n, k), np.float32)
+        tp = sp = None
+        if tele is not None:
+            tele = np.ascontiguousarray(tele, np.float32).reshape(self.n, k)
+            tp = _ptr(tele)
+        else:
+            seeds = np.ascontiguousarray(seeds, np.uint32)
+            assert len(seeds) == k
+            sp = _ptr(seeds)
+        st = RunStats()
+        check(lib.gg_ppr_k(self.h, k, iters, damping, tp, sp, _ptr(y), C.byref(st)), "gg_ppr_k")
+        return y, _run(st)
 
     def bc(self, start=100):
         dep = np.empty(self.n, np.float32)

@@ -330,6 +330,18 @@ int gg_bc(gg_graph_t g, uint32_t start, float* dependencies, float* num_paths, g
 int gg_bp(gg_graph_t g, int32_t iters, const float* vert_potential, const float* edge_potential,
           float* vert_out, gg_run_stats* st);
 
+/* ============================================================ batching */
+/* k-column personalised PageRank, the batched form of PR_F/PR_Vertex_F
+ * (app/PageRank.C:256-315) with every vertex active (app/PageRankBit.C:145)
+ * and a teleport matrix in place of the uniform 1/n:
+ *   X_0 = T,  X_{t+1} = damping * A X_t + (1 - damping) * T,  A[v,u] = 1/outdeg(u)
+ * k = 32 or 64 runs all columns in one SpMM-shaped pull per iteration (each
+ * edge moves a whole k-column row); k = 1 runs the scalar engine pull.
+ * tele: host n x k row-major ([v][j]), or NULL with seeds[k] (one-hot columns).
+ * out: host n x k row-major result X_iters. */
+int gg_ppr_k(gg_graph_t g, int32_t k, int32_t iters, float damping, const float* tele,
+             const uint32_t* seeds, float* out, gg_run_stats* st);
+
 #ifdef __cplusplus
 }
 #endif
