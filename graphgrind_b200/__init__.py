@@ -172,6 +172,8 @@ _sig("gg_bc", C.c_int, _P, C.c_uint32, _P, _P, C.POINTER(RunStats))
 _sig("gg_bp", C.c_int, _P, C.c_int32, _P, _P, _P, C.POINTER(RunStats))
 _sig("gg_bfs_push_step_noalloc", C.c_int, _P, _P, C.c_uint32, _P, C.c_uint32, _P, _P, C.c_int32, _P, _P, _P)
 _sig("gg_ppr_k", C.c_int, _P, C.c_int32, C.c_int32, C.c_float, _P, _P, _P, C.POINTER(RunStats))
+_sig("gg_msbfs", C.c_int, _P, C.c_int32, _P, _P, C.POINTER(RunStats))
+_sig("gg_msbc", C.c_int, _P, C.c_int32, _P, _P, _P, C.POINTER(RunStats))
 
 # Every symbol declared in include/gg.h (checked by the tests).
 EXPORTED = [
@@ -187,7 +189,7 @@ EXPORTED = [
     "gg_graph_set_dense_policy", "gg_graph_set_tuning", "gg_graph_get_tuning", "gg_vertex_map", "gg_vertex_filter", "gg_vertex_array_alloc",
     "gg_vertex_array_free", "gg_memcpy_h2d", "gg_memcpy_d2h", "gg_host_alloc_pinned", "gg_host_free_pinned", "gg_bfs", "gg_components",
     "gg_pagerank", "gg_pagerank_delta", "gg_spmv", "gg_bellman_ford", "gg_bc", "gg_bp",
-    "gg_bfs_push_step_noalloc", "gg_ppr_k",
+    "gg_bfs_push_step_noalloc", "gg_ppr_k", "gg_msbfs", "gg_msbc",
 ]
 
 
@@ -579,6 +581,24 @@ class Graph:
         st = RunStats()
         check(lib.gg_ppr_k(self.h, k, iters, damping, tp, sp, _ptr(y), C.byref(st)), "gg_ppr_k")
         return y, _run(st)
+
+    def msbfs(self, sources, out=None):
+        """Levels from up to 64 sources in one traversal: (levels[n, k] int32, Run)."""
+        src = np.ascontiguousarray(sources, np.uint32)
+        lev = out if out is not None else np.empty((self.n, len(src)), np.int32)
+        st = RunStats()
+        check(lib.gg_msbfs(self.h, len(src), _ptr(src), _ptr(lev), C.byref(st)), "gg_msbfs")
+        return lev, _run(st)
+
+    def msbc(self, sources, dep_out=None, paths_out=None):
+        """BC contributions of up to 64 sources: (dependencies[n, k], num_paths[n, k], Run)."""
+        src = np.ascontiguousarray(sources, np.uint32)
+        k = len(src)
+        dep = dep_out if dep_out is not None else np.empty((self.n, k), np.float32)
+        npth = paths_out if paths_out is not None else np.empty((self.n, k), np.float32)
+        st = RunStats()
+        check(lib.gg_msbc(self.h, k, _ptr(src), _ptr(dep), _ptr(npth), C.byref(st)), "gg_msbc")
+        return dep, npth, _run(st)
 
     def bc(self, start=100):
         dep = np.empty(self.n, np.float32)

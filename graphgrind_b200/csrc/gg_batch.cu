@@ -253,6 +253,391 @@ static int run_ppr_k(gg_graph_s* g, int32_t k, int32_t iters, float damping, con
   return GG_OK;
 }
 
+
+// ------------------------------------------------------------------ multi-source
+// k <= 64 sources share one level-synchronous traversal.  Per vertex, bit j of
+// a 64-bit mask says "reached from sources[j]"; per (vertex, source) values
+// (levels, path counts, dependencies) are n x 64 row-major.
+//
+// Row pull over a segmented edge stream (CSC for the forward levels, CSR for
+// the backward dependency pass): for each row x and edge (x, y) of the row,
+//   b = filter(x) & edge_mask(y)
+//   out[x] |= b                        (the next frontier's masks, forward)
+//   vals[x][j] += vals[y][j] for j in b  (path counts or dependencies)
+// filter(x) = ~seen[x] forward and the level-r mask backward.  One warp per
+// 256-edge block; lane l owns columns 2l, 2l+1.  (x, j) pairs written and
+// (y, j) pairs read are disjoint in both passes (unreached vs frontier,
+// level r vs level r+1), so the pass updates vals in place.
+struct MsPull {
+  const uint32_t* idx;
+  const uint32_t* head;
+  const uint32_t* blk;
+  const uint32_t* rows;
+  uint64_t nblocks, m;
+  const uint64_t* row_mask;
+  uint64_t row_xor, kmask;
+  const uint64_t* edge_mask;
+  float* vals;
+  uint64_t* out;
+};
+
+template <bool VALS, bool OUT>
+__global__ void __launch_bounds__(256) k_ms_pull(MsPull p) {
+  __shared__ uint64_t s_filt[8][kSegBlock + 1];
+  __shared__ uint32_t s_row[8][kSegBlock + 1];
+  __shared__ uint64_t s_em[VALS ? 8 : 1][kSegBlock];
+  __shared__ uint16_t s_rel[VALS ? 8 : 1][kSegBlock];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t lanemask_le = 0xffffffffu >> (31 - lane);
+  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  for (uint64_t b = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp; b < p.nblocks; b += warps) {
+    const uint64_t e0 = b * kSegBlock;
+    // rows touching the block: slot 0 continues from the previous block, one slot per head
+    const uint32_t h0 = __ldg(p.blk + b), nr = __ldg(p.blk + b + 1) - h0 + 1;
+    for (uint32_t i = lane; i < nr; i += 32) {
+      uint64_t f = 0;
+      uint32_t x = 0;
+      if (i > 0 || h0 > 0) {
+        x = __ldg(p.rows + h0 - 1 + i);
+        f = (__ldg(p.row_mask + x) ^ p.row_xor) & p.kmask;
+      }
+      s_row[warp][i] = x;
+      s_filt[warp][i] = f;
+    }
+    __syncwarp();
+    const uint64_t nb = e0 + kSegBlock;
+    const bool ends_block = nb >= p.m || (__ldg(p.head + (nb >> 5)) & 1u);
+    // mask phase: lane l takes edge 32 i + l of the block
+    uint32_t running = 0, act[8];
+    uint64_t carry = 0;
+    uint32_t hw = __ldg(p.head + b * 8);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const uint32_t hw_next = i < 7 ? __ldg(p.head + b * 8 + i + 1) : 0u;
+      const uint64_t e = e0 + 32 * i + lane;
+      const uint32_t rel = running + __popc(hw & lanemask_le);
+      const uint64_t f = s_filt[warp][rel];
+      const uint32_t y = e < p.m ? __ldg(p.idx + e) : 0u;
+      uint64_t x = (e < p.m && f) ? (__ldg(p.edge_mask + y) & f) : 0ull;
+      if (VALS) {
+        s_em[warp][32 * i + lane] = x;
+        s_rel[warp][32 * i + lane] = (uint16_t)rel;
+        act[i] = __ballot_sync(0xffffffffu, x != 0);
+      }
+      if (OUT) {
+        // segmented inclusive OR over the lanes of each row
+        const uint32_t hb = hw & lanemask_le;
+        const int seg0 = hb ? 31 - __clz(hb) : 0;
+        if (lane == 0 && !(hw & 1u)) x |= carry;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+          const uint64_t t = __shfl_up_sync(0xffffffffu, x, d);
+          if (lane >= seg0 + d) x |= t;
+        }
+        const bool ends = lane < 31 ? ((hw >> (lane + 1)) & 1u) : (i < 7 ? (hw_next & 1u) : ends_block);
+        if ((ends || (lane == 31 && i == 7)) && x) {
+          const uint32_t row = s_row[warp][rel];
+          if (rel > 0 && ends)
+            p.out[row] = x;
+          else
+            atomicOr(reinterpret_cast<unsigned long long*>(p.out + row), (unsigned long long)x);
+        }
+        const uint64_t x31 = __shfl_sync(0xffffffffu, x, 31);
+        carry = (i < 7 && !(hw_next & 1u)) ? x31 : 0ull;
+      }
+      running += __popc(hw);
+      hw = hw_next;
+    }
+    if (VALS) {
+      __syncwarp();
+      // column phase over the active edges in edge order; lane l owns columns 2l, 2l+1
+      uint32_t cur = 0xffffffffu;
+      uint64_t rm = 0;
+      float a0 = 0.f, a1 = 0.f;
+      auto flush = [&]() {
+        if (cur == 0xffffffffu || rm == 0) return;
+        const bool complete = cur > 0 && (cur < nr - 1 || ends_block);
+        const uint32_t mb = (uint32_t)(rm >> (2 * lane)) & 3u;
+        float* dst = p.vals + (uint64_t)s_row[warp][cur] * 64 + 2 * lane;
+        if (complete) {
+          if (mb & 1u) dst[0] += a0;
+          if (mb & 2u) dst[1] += a1;
+        } else {
+          if (mb & 1u) atomicAdd(dst, a0);
+          if (mb & 2u) atomicAdd(dst + 1, a1);
+        }
+      };
+      int i = 0;
+      uint32_t bits = act[0];
+      while (true) {
+        // next batch of up to 8 active edges
+        uint32_t el[8];
+        int cnt = 0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          while (bits == 0 && i < 7) bits = act[++i];
+          el[q] = 0xffffffffu;
+          if (bits) {
+            el[q] = 32 * i + __ffs(bits) - 1;
+            bits &= bits - 1;
+            ++cnt;
+          }
+        }
+        if (cnt == 0) break;
+        float2 v[8];
+        uint64_t em[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          v[q] = make_float2(0.f, 0.f);
+          em[q] = 0;
+          if (el[q] != 0xffffffffu) {
+            em[q] = s_em[warp][el[q]];
+            if ((uint32_t)(em[q] >> (2 * lane)) & 3u)
+              v[q] = __ldg(reinterpret_cast<const float2*>(p.vals + (uint64_t)__ldg(p.idx + e0 + el[q]) * 64) + lane);
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          if (el[q] == 0xffffffffu) break;
+          const uint32_t rel = s_rel[warp][el[q]];
+          if (rel != cur) {
+            flush();
+            cur = rel;
+            rm = 0;
+            a0 = a1 = 0.f;
+          }
+          rm |= em[q];
+          const uint32_t mb = (uint32_t)(em[q] >> (2 * lane)) & 3u;
+          if (mb & 1u) a0 += v[q].x;
+          if (mb & 2u) a1 += v[q].y;
+        }
+      }
+      flush();
+    }
+    __syncwarp();
+  }
+}
+
+// Sources: seen = visit = bit j at sources[j], level 0, one path.
+__global__ void k_ms_seed(const uint32_t* src, uint32_t k, uint64_t* seen, uint64_t* visit, int32_t* lvl,
+                          float* sigma) {
+  const uint32_t j = threadIdx.x;
+  if (j >= k) return;
+  const uint32_t s = src[j];
+  atomicOr(reinterpret_cast<unsigned long long*>(seen + s), 1ull << j);
+  atomicOr(reinterpret_cast<unsigned long long*>(visit + s), 1ull << j);
+  lvl[(uint64_t)s * 64 + j] = 0;
+  if (sigma) sigma[(uint64_t)s * 64 + j] = 1.f;
+}
+
+// After a forward level r: the new frontier masks become visit, join seen and
+// set the level of each new (vertex, source) pair; stats[0] += vertices in the
+// frontier, stats[1] += sum of out-degree x sources over it.
+__global__ void k_ms_fwd_vertex(uint32_t n, int32_t r, uint64_t* seen, uint64_t* visit, uint64_t* next, int32_t* lvl,
+                                const uint32_t* out_off, unsigned long long* stats) {
+  unsigned long long cnt = 0, trav = 0;
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t nm = next[v];
+    visit[v] = nm;
+    if (nm) {
+      next[v] = 0;
+      seen[v] |= nm;
+      ++cnt;
+      trav += (unsigned long long)(out_off[v + 1] - out_off[v]) * __popcll(nm);
+      while (nm) {
+        const int j = __ffsll((long long)nm) - 1;
+        nm &= nm - 1;
+        lvl[v * 64 + j] = r;
+      }
+    }
+  }
+  cnt = warp_sum(cnt);
+  trav = warp_sum(trav);
+  if ((threadIdx.x & 31) == 0 && (cnt | trav)) {
+    atomicAdd(stats, cnt);
+    atomicAdd(stats + 1, trav);
+  }
+}
+
+// Backward level r: mask[v] = sources with level r at v, and dep[v][j] =
+// 1/paths[v][j] there (BC_Back_Vertex_F, app/BC.C:140-154).  One warp per vertex.
+__global__ void k_ms_level_mask(uint32_t n, int32_t r, const int32_t* lvl, uint64_t* mask, const float* sigma,
+                                float* dep) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t w0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t v = w0; v < n; v += nw) {
+    const int32_t l0 = lvl[v * 64 + lane], l1 = lvl[v * 64 + 32 + lane];
+    const uint32_t lo = __ballot_sync(0xffffffffu, l0 == r), hi = __ballot_sync(0xffffffffu, l1 == r);
+    if (lane == 0) mask[v] = (uint64_t)lo | ((uint64_t)hi << 32);
+    if (l0 == r) dep[v * 64 + lane] = 1.f / sigma[v * 64 + lane];
+    if (l1 == r) dep[v * 64 + 32 + lane] = 1.f / sigma[v * 64 + 32 + lane];
+  }
+}
+
+// (dep - 1/paths) / (1/paths), app/BC.C:220-222, into n x k outputs; NaN where unreached.
+__global__ void k_ms_bc_final(uint32_t n, uint32_t k, const float* dep, const float* sigma, float* dep_out,
+                              float* sigma_out) {
+  const uint64_t total = (uint64_t)n * k;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t v = i / k, j = i % k;
+    const float inv = 1.0f / sigma[v * 64 + j];
+    dep_out[i] = (dep[v * 64 + j] - inv) / inv;
+    if (sigma_out) sigma_out[i] = sigma[v * 64 + j];
+  }
+}
+
+__global__ void k_ms_levels_out(uint32_t n, uint32_t k, const int32_t* lvl, int32_t* out) {
+  const uint64_t total = (uint64_t)n * k;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = lvl[(i / k) * 64 + i % k];
+}
+
+// Device allocations released (stream-ordered) when the holder leaves scope.
+struct DevAllocs {
+  cudaStream_t st;
+  std::vector<void*> ptrs;
+  explicit DevAllocs(cudaStream_t s) : st(s) {}
+  template <class T>
+  int get(T** p, uint64_t count) {
+    *p = nullptr;
+    GG_CUDA(cudaMallocAsync((void**)p, sizeof(T) * count + 64, st));
+    ptrs.push_back(*p);
+    return GG_OK;
+  }
+  ~DevAllocs() {
+    for (void* q : ptrs) cudaFreeAsync(q, st);
+  }
+};
+
+static int ms_pull(gg_graph_s* g, bool vals, bool out, bool forward, const uint64_t* row_mask, uint64_t row_xor,
+                   uint64_t kmask, const uint64_t* edge_mask, float* v, uint64_t* o) {
+  if (g->m == 0) return GG_OK;
+  MsPull p{};
+  // forward pulls in-edges, backward pulls out-edges of the current orientation
+  const bool in_edges = forward;
+  const int seg = g->symmetric ? 0 : ((in_edges != g->transposed) ? 0 : 1);
+  const SegIndex& si = g->seg[seg];
+  p.idx = in_edges ? g->in_idx() : g->out_idx();
+  p.head = si.d_head;
+  p.blk = si.d_blk;
+  p.rows = si.d_rows;
+  p.nblocks = (g->m + kSegBlock - 1) / kSegBlock;
+  p.m = g->m;
+  p.row_mask = row_mask;
+  p.row_xor = row_xor;
+  p.kmask = kmask;
+  p.edge_mask = edge_mask;
+  p.vals = v;
+  p.out = o;
+  const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((p.nblocks + 7) / 8, (uint64_t)g->num_sms * 8));
+  if (vals && out)
+    k_ms_pull<true, true><<<grid, 256, 0, g->stream>>>(p);
+  else if (vals)
+    k_ms_pull<true, false><<<grid, 256, 0, g->stream>>>(p);
+  else
+    k_ms_pull<false, true><<<grid, 256, 0, g->stream>>>(p);
+  g->kernels++;
+  return GG_OK;
+}
+
+static int run_ms(gg_graph_s* g, int32_t k, const uint32_t* sources, bool bc, int32_t* levels_out, float* dep_out,
+                  float* np_out, gg_run_stats* st) {
+  const uint32_t n = g->n;
+  const uint64_t n64 = (uint64_t)n * 64;
+  const uint64_t kmask = k == 64 ? ~0ull : ((1ull << k) - 1);
+  DevAllocs mem(g->stream);
+  uint64_t *seen, *visit, *next, *mask_a, *mask_b;
+  int32_t* lvl;
+  float *sigma = nullptr, *dep = nullptr;
+  uint32_t* d_src;
+  unsigned long long* d_stats;
+  GG_TRY(mem.get(&seen, n));
+  GG_TRY(mem.get(&visit, n));
+  GG_TRY(mem.get(&next, n));
+  GG_TRY(mem.get(&lvl, n64));
+  GG_TRY(mem.get(&d_src, 64));
+  GG_TRY(mem.get(&d_stats, 2));
+  if (bc) {
+    GG_TRY(mem.get(&sigma, n64));
+    GG_TRY(mem.get(&dep, n64));
+  }
+  unsigned long long* h_stats = reinterpret_cast<unsigned long long*>(g->ws.h_red);
+  g->kernels = 0;
+  EventTimer tm(g->stream);
+  GG_CUDA(cudaMemcpyAsync(d_src, sources, 4 * k, cudaMemcpyHostToDevice, g->stream));
+  GG_CUDA(cudaMemsetAsync(seen, 0, 8 * (uint64_t)n, g->stream));
+  GG_CUDA(cudaMemsetAsync(visit, 0, 8 * (uint64_t)n, g->stream));
+  GG_CUDA(cudaMemsetAsync(next, 0, 8 * (uint64_t)n, g->stream));
+  GG_CUDA(cudaMemsetAsync(lvl, 0xff, 4 * n64, g->stream));
+  if (bc) GG_CUDA(cudaMemsetAsync(sigma, 0, 4 * n64, g->stream));
+  k_ms_seed<<<1, 64, 0, g->stream>>>(d_src, (uint32_t)k, seen, visit, lvl, sigma);
+  g->kernels++;
+  uint64_t trav = 0;
+  for (int32_t j = 0; j < k; ++j) trav += g->h_out_off()[sources[j] + 1] - g->h_out_off()[sources[j]];
+  std::vector<uint64_t> level_trav{trav};
+  int32_t L = 0;
+  const int vgrid = generic_grid(g, n);
+  for (int32_t r = 1;; ++r) {
+    GG_TRY(ms_pull(g, bc, true, true, seen, ~0ull, kmask, visit, sigma, next));
+    GG_CUDA(cudaMemsetAsync(d_stats, 0, 16, g->stream));
+    k_ms_fwd_vertex<<<vgrid, kGenericThreads, 0, g->stream>>>(n, r, seen, visit, next, lvl, g->out_off(), d_stats);
+    g->kernels++;
+    GG_CUDA(cudaMemcpyAsync(h_stats, d_stats, 16, cudaMemcpyDeviceToHost, g->stream));
+    GG_CUDA(cudaStreamSynchronize(g->stream));
+    if (h_stats[0] == 0) break;
+    L = r;
+    level_trav.push_back(h_stats[1]);
+    trav += h_stats[1];
+  }
+  if (bc) {
+    GG_TRY(mem.get(&mask_a, n));
+    GG_TRY(mem.get(&mask_b, n));
+    GG_CUDA(cudaMemsetAsync(dep, 0, 4 * n64, g->stream));
+    const int wgrid = generic_grid(g, (uint64_t)n * 32);
+    uint64_t *cur = mask_a, *prev = mask_b;
+    for (int32_t r = L; r >= 0; --r) {
+      k_ms_level_mask<<<wgrid, kGenericThreads, 0, g->stream>>>(n, r, lvl, cur, sigma, dep);
+      g->kernels++;
+      if (r < L) {
+        GG_TRY(ms_pull(g, true, false, false, cur, 0, kmask, prev, dep, nullptr));
+        trav += level_trav[r + 1];
+      }
+      std::swap(cur, prev);
+    }
+  }
+  DevBuf<float> dout, sout;
+  DevBuf<int32_t> lout;
+  const uint64_t nk = (uint64_t)n * k;
+  if (bc) {
+    GG_TRY(dout.alloc(g, nk));
+    if (np_out) GG_TRY(sout.alloc(g, nk));
+    k_ms_bc_final<<<generic_grid(g, nk), kGenericThreads, 0, g->stream>>>(n, (uint32_t)k, dep, sigma, dout.p,
+                                                                          np_out ? sout.p : nullptr);
+    g->kernels++;
+  } else if (levels_out) {
+    GG_TRY(lout.alloc(g, nk));
+    k_ms_levels_out<<<generic_grid(g, nk), kGenericThreads, 0, g->stream>>>(n, (uint32_t)k, lvl, lout.p);
+    g->kernels++;
+  }
+  GG_CUDA(cudaGetLastError());
+  const double ms = tm.stop();
+  if (bc) {
+    GG_CUDA(cudaMemcpyAsync(dep_out, dout.p, 4 * nk, cudaMemcpyDeviceToHost, g->stream));
+    if (np_out) GG_CUDA(cudaMemcpyAsync(np_out, sout.p, 4 * nk, cudaMemcpyDeviceToHost, g->stream));
+  } else if (levels_out) {
+    GG_CUDA(cudaMemcpyAsync(levels_out, lout.p, 4 * nk, cudaMemcpyDeviceToHost, g->stream));
+  }
+  GG_CUDA(cudaStreamSynchronize(g->stream));
+  if (st) {
+    st->ms = ms;
+    st->rounds = L + 1;
+    st->edges_traversed = trav;
+    st->kernels = g->kernels;
+  }
+  return GG_OK;
+}
+
 }  // namespace gg
 
 using namespace gg;
@@ -266,4 +651,23 @@ extern "C" int gg_ppr_k(gg_graph_t g, int32_t k, int32_t iters, float damping, c
     for (int32_t j = 0; j < k; ++j)
       if (seeds[j] >= g->n) return fail(GG_ERR_INVALID_ARG, "gg_ppr_k: seed %u out of range", seeds[j]);
   return run_ppr_k(g, k, iters, damping, tele, seeds, out, st);
+}
+
+static int check_sources(gg_graph_t g, int32_t k, const uint32_t* sources, const char* who) {
+  if (!graph_live(g) || k < 1 || k > 64 || !sources) return fail(GG_ERR_INVALID_ARG, "%s: 1 <= k <= 64 sources", who);
+  for (int32_t j = 0; j < k; ++j)
+    if (sources[j] >= g->n) return fail(GG_ERR_INVALID_ARG, "%s: source %u out of range", who, sources[j]);
+  return GG_OK;
+}
+
+extern "C" int gg_msbfs(gg_graph_t g, int32_t k, const uint32_t* sources, int32_t* levels, gg_run_stats* st) {
+  GG_TRY(check_sources(g, k, sources, "gg_msbfs"));
+  return run_ms(g, k, sources, false, levels, nullptr, nullptr, st);
+}
+
+extern "C" int gg_msbc(gg_graph_t g, int32_t k, const uint32_t* sources, float* dependencies, float* num_paths,
+                       gg_run_stats* st) {
+  GG_TRY(check_sources(g, k, sources, "gg_msbc"));
+  if (!dependencies) return fail(GG_ERR_INVALID_ARG, "gg_msbc: null dependencies");
+  return run_ms(g, k, sources, true, nullptr, dependencies, num_paths, st);
 }

@@ -9,27 +9,6 @@
 namespace gg {
 
 // ------------------------------------------------------------- helpers
-struct EventTimer {
-  cudaEvent_t a = nullptr, b = nullptr;
-  cudaStream_t s;
-  explicit EventTimer(cudaStream_t st) : s(st) {
-    cudaEventCreate(&a);
-    cudaEventCreate(&b);
-    cudaEventRecord(a, s);
-  }
-  double stop() {
-    cudaEventRecord(b, s);
-    cudaEventSynchronize(b);
-    float ms = 0;
-    cudaEventElapsedTime(&ms, a, b);
-    return ms;
-  }
-  ~EventTimer() {
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
-  }
-};
-
 template <class T>
 __global__ void k_fill(T* a, uint64_t n, T v) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
@@ -49,20 +28,6 @@ static int set_one(gg_graph_s* g, T* a, uint32_t i, T v) {
   GG_CUDA(cudaMemcpyAsync(a + i, &v, sizeof(T), cudaMemcpyHostToDevice, g->stream));
   return GG_OK;
 }
-
-template <class T>
-struct DevBuf {
-  T* p = nullptr;
-  gg_graph_s* g = nullptr;
-  int alloc(gg_graph_s* gg_, uint64_t n) {
-    g = gg_;
-    GG_CUDA(cudaMallocAsync((void**)&p, sizeof(T) * (n + 4), g->stream));
-    return GG_OK;
-  }
-  ~DevBuf() {
-    if (p) cudaFreeAsync(p, g->stream);
-  }
-};
 
 struct FrontierHold {
   gg_frontier_s* f = nullptr;

@@ -11,6 +11,43 @@ namespace gg {
 
 constexpr uint32_t kGenericThreads = 256;
 
+// Device time between construction and stop() on one stream.
+struct EventTimer {
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaStream_t s;
+  explicit EventTimer(cudaStream_t st) : s(st) {
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, s);
+  }
+  double stop() {
+    cudaEventRecord(b, s);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms;
+  }
+  ~EventTimer() {
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  }
+};
+
+// A stream-ordered device allocation released when the holder leaves scope.
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  gg_graph_s* g = nullptr;
+  int alloc(gg_graph_s* gg_, uint64_t n) {
+    g = gg_;
+    GG_CUDA(cudaMallocAsync((void**)&p, sizeof(T) * (n + 4), g->stream));
+    return GG_OK;
+  }
+  ~DevBuf() {
+    if (p) cudaFreeAsync(p, g->stream);
+  }
+};
+
 inline int generic_grid(const gg_graph_s* g, uint64_t work) {
   uint64_t b = (work + kGenericThreads - 1) / kGenericThreads;
   uint64_t cap = (uint64_t)g->num_sms * 8;

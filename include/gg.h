@@ -342,6 +342,26 @@ int gg_bp(gg_graph_t g, int32_t iters, const float* vert_potential, const float*
 int gg_ppr_k(gg_graph_t g, int32_t k, int32_t iters, float damping, const float* tele,
              const uint32_t* seeds, float* out, gg_run_stats* st);
 
+/* Multi-source BFS: k <= 64 sources in one level-synchronous traversal, with
+ * a 64-bit mask per vertex (bit j: reached from sources[j]) moved along every
+ * edge once per level.  levels: host n x k row-major ([v][j]); levels[v][j] is
+ * gg_bfs's level of v from sources[j] (app/BFS.C:77-101), -1 if unreached.
+ * Duplicate sources are allowed.  st->edges_traversed sums the per-source
+ * counts of gg_bfs. */
+int gg_msbfs(gg_graph_t g, int32_t k, const uint32_t* sources, int32_t* levels, gg_run_stats* st);
+
+/* Multi-source betweenness contributions (app/BC.C:156-226 for each of k <= 64
+ * sources): dependencies and num_paths are host n x k row-major (num_paths may
+ * be NULL).  num_paths = forward path counts (0 where unreached);
+ * dependencies = (dep - 1/paths) * paths with dep = 1/paths + the successors'
+ * dep, NaN where unreached.  The backward pass follows the out-edges of the
+ * current orientation on every level, which is app/BC.C's result on symmetric
+ * graphs; on directed graphs app/BC.C also pulls some levels through the
+ * untransposed COO (graphgrind/ligra-numa.h:957-966 after GA.transpose()),
+ * which gg_bc reproduces and this call does not. */
+int gg_msbc(gg_graph_t g, int32_t k, const uint32_t* sources, float* dependencies, float* num_paths,
+            gg_run_stats* st);
+
 #ifdef __cplusplus
 }
 #endif

@@ -57,6 +57,7 @@ for name, args in {
     "or_spmv": [C.POINTER(OrGraph), _P, _P, C.POINTER(OrStats)],
     "or_bellman_ford": [C.POINTER(OrGraph), C.c_uint32, _P, C.POINTER(OrStats)],
     "or_bc": [C.POINTER(OrGraph), C.c_uint32, _P, _P, C.POINTER(OrStats)],
+    "or_bc_brandes": [C.POINTER(OrGraph), C.c_uint32, _P, _P],
     "or_bp": [C.POINTER(OrGraph), C.c_int32, _P, _P, _P, C.POINTER(OrStats)],
     "or_ppr": [C.POINTER(OrGraph), C.c_int32, C.c_double, _P, _P],
     "or_partition_sizes": [_P, _P, C.c_uint32, C.c_uint64, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, _P],
@@ -160,6 +161,12 @@ class Graph:
         st = self._st()
         assert _lib.or_bc(C.byref(self.c), start, _p(dep), _p(np_), C.byref(st)) == 0
         return dep, np_, st
+
+    def bc_brandes(self, start):
+        dep = np.empty(self.n, np.float64)
+        np_ = np.empty(self.n, np.float64)
+        assert _lib.or_bc_brandes(C.byref(self.c), start, _p(dep), _p(np_)) == 0
+        return dep, np_
 
     def bp(self, iters, vert_pot, edge_pot):
         out = np.empty(2 * self.n, np.float64)

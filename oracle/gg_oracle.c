@@ -722,6 +722,53 @@ int or_bc(const or_graph* g, uint32_t start, double* dep, double* num_paths, or_
   return 0;
 }
 
+int or_bc_brandes(const or_graph* g, uint32_t start, double* dep, double* num_paths) {
+  if (!g || start >= g->n) return -1;
+  const uint32_t n = g->n;
+  int32_t* lev = (int32_t*)malloc(sizeof(int32_t) * n);
+  uint32_t* order = (uint32_t*)malloc(sizeof(uint32_t) * n);
+  double* np = (double*)calloc(n, sizeof(double));
+  for (uint32_t v = 0; v < n; v++) lev[v] = -1;
+  lev[start] = 0;
+  np[start] = 1.0;
+  order[0] = start;
+  uint64_t head = 0, tail = 1;
+  while (head < tail) { /* queue BFS: vertices leave in level order */
+    const uint32_t v = order[head++];
+    for (uint32_t e = g->out_off[v]; e < g->out_off[v + 1]; e++) {
+      const uint32_t u = g->out_idx[e];
+      if (lev[u] < 0) {
+        lev[u] = lev[v] + 1;
+        order[tail++] = u;
+      }
+    }
+  }
+  for (uint64_t i = 1; i < tail; i++) { /* path counts from in-edges of the previous level */
+    const uint32_t u = order[i];
+    double s = 0;
+    for (uint32_t e = g->in_off[u]; e < g->in_off[u + 1]; e++)
+      if (lev[g->in_idx[e]] == lev[u] - 1) s += np[g->in_idx[e]];
+    np[u] = s;
+  }
+  if (num_paths) memcpy(num_paths, np, sizeof(double) * n);
+  for (uint32_t v = 0; v < n; v++) dep[v] = 0.0;
+  for (uint64_t i = tail; i-- > 0;) { /* successors first */
+    const uint32_t v = order[i];
+    double s = 0;
+    for (uint32_t e = g->out_off[v]; e < g->out_off[v + 1]; e++)
+      if (lev[g->out_idx[e]] == lev[v] + 1) s += dep[g->out_idx[e]];
+    dep[v] = s + 1.0 / np[v];
+  }
+  for (uint32_t v = 0; v < n; v++) {
+    const double inv = 1.0 / np[v]; /* inf where unreached, giving NaN below */
+    dep[v] = (dep[v] - inv) / inv;
+  }
+  free(lev);
+  free(order);
+  free(np);
+  return 0;
+}
+
 /* ======================================================================= BP */
 /* Two-state belief propagation in the form the GPU library defines
  * (app/BP.C:54-149 leaves vertex/edge potentials uninitialised and resets

@@ -47,6 +47,12 @@ int or_pagerank_delta(const or_graph* g, double* ranks, or_stats* st);
 int or_spmv(const or_graph* g, const double* x, double* y, or_stats* st);
 int or_bellman_ford(const or_graph* g, uint32_t start, int64_t* dist, or_stats* st);
 int or_bc(const or_graph* g, uint32_t start, double* dependencies, double* num_paths, or_stats* st);
+/* The value app/BC.C:156-226 computes when every backward edgeMap follows the
+ * transposed edges (always so on symmetric graphs): levels by BFS, path
+ * counts summed over in-edges from the previous level, dependencies summed
+ * over out-edges to the next level, dependencies = (dep - 1/paths) * paths
+ * with dep = 1/paths + sum of successors' dep, NaN where unreached. */
+int or_bc_brandes(const or_graph* g, uint32_t start, double* dependencies, double* num_paths);
 int or_bp(const or_graph* g, int32_t iters, const double* vert_pot, const double* edge_pot,
           double* vert_out, or_stats* st);
 /* PageRank iterated to convergence-free fixed count on every vertex (the

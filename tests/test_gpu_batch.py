@@ -35,3 +35,61 @@ def test_ppr_k_dense_teleport(gg, orc):
     for j in range(32):
         o = og.ppr(7, 0.8, tele[:, j].astype(np.float64))
         assert rel_l1(x[:, j], o) <= 1e-5
+
+
+@pytest.fixture(scope="module", params=["sym", "dir"])
+def rmat12(gg, orc, request):
+    hg = gg.HostGraph.rmat(12, 16, seed=93, symmetric=request.param == "sym")
+    return hg, gg.Graph(hg, partitions=ok_partitions(hg, 32)), orc.Graph.from_host(hg)
+
+
+@pytest.mark.parametrize("k", [64, 5])
+def test_msbfs_levels_bit_exact(rmat12, k):
+    hg, g, og = rmat12
+    src = np.random.default_rng(k).integers(0, hg.n, k).astype(np.uint32)
+    src[-1] = src[0]  # duplicate sources are allowed
+    lev, run = g.msbfs(src)
+    assert lev.shape == (hg.n, k)
+    trav = 0
+    for j, s in enumerate(src):
+        _, olev, ost = og.bfs(int(s))
+        np.testing.assert_array_equal(lev[:, j], olev, err_msg=f"source {s}")
+        trav += ost.edges_traversed
+    assert run.edges_traversed == trav
+
+
+def test_msbfs_transposed(gg, orc):
+    hg = gg.HostGraph.rmat(11, 8, seed=94, symmetric=False)
+    g = gg.Graph(hg, partitions=ok_partitions(hg, 16))
+    g.transpose()
+    og = orc.Graph.from_host(hg.transpose())
+    src = np.arange(0, 640, 10, dtype=np.uint32)
+    lev, _ = g.msbfs(src)
+    for j, s in enumerate(src):
+        np.testing.assert_array_equal(lev[:, j], og.bfs(int(s))[1])
+
+
+@pytest.mark.parametrize("k", [64, 7])
+def test_msbc_matches_brandes(rmat12, k):
+    hg, g, og = rmat12
+    src = np.random.default_rng(100 + k).integers(0, hg.n, k).astype(np.uint32)
+    dep, npth, _ = g.msbc(src)
+    for j, s in enumerate(src):
+        odep, onp = og.bc_brandes(int(s))
+        np.testing.assert_allclose(npth[:, j], onp, rtol=1e-6)
+        np.testing.assert_array_equal(np.isnan(dep[:, j]), np.isnan(odep))
+        fin = np.isfinite(odep)
+        assert rel_l1(dep[fin, j], odep[fin]) <= 1e-4, s
+
+
+def test_msbc_equals_single_source_on_symmetric(gg, orc):
+    hg = gg.HostGraph.rmat(11, 16, seed=95, symmetric=True)
+    g = gg.Graph(hg, partitions=ok_partitions(hg, 16))
+    src = np.array([0, 3, 100, 2047], np.uint32)
+    dep, npth, _ = g.msbc(src)
+    for j, s in enumerate(src):
+        d1, n1, _ = g.bc(int(s))
+        np.testing.assert_allclose(npth[:, j], n1, rtol=1e-6)
+        fin = np.isfinite(d1)
+        np.testing.assert_array_equal(np.isnan(dep[:, j]), np.isnan(d1))
+        assert rel_l1(dep[fin, j], d1[fin]) <= 1e-5
