@@ -174,6 +174,10 @@ _sig("gg_bfs_push_step_noalloc", C.c_int, _P, _P, C.c_uint32, _P, C.c_uint32, _P
 _sig("gg_ppr_k", C.c_int, _P, C.c_int32, C.c_int32, C.c_float, _P, _P, _P, C.POINTER(RunStats))
 _sig("gg_msbfs", C.c_int, _P, C.c_int32, _P, _P, C.POINTER(RunStats))
 _sig("gg_msbc", C.c_int, _P, C.c_int32, _P, _P, _P, C.POINTER(RunStats))
+_sig("gg_batch_create", C.c_int, C.c_int32, _P, C.POINTER(_P))
+_sig("gg_batch_destroy", C.c_int, _P)
+_sig("gg_batch_info", C.c_int, _P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), _P)
+_sig("gg_batch_bfs", C.c_int, _P, _P, _P, C.POINTER(RunStats))
 
 # Every symbol declared in include/gg.h (checked by the tests).
 EXPORTED = [
@@ -190,6 +194,7 @@ EXPORTED = [
     "gg_vertex_array_free", "gg_memcpy_h2d", "gg_memcpy_d2h", "gg_host_alloc_pinned", "gg_host_free_pinned", "gg_bfs", "gg_components",
     "gg_pagerank", "gg_pagerank_delta", "gg_spmv", "gg_bellman_ford", "gg_bc", "gg_bp",
     "gg_bfs_push_step_noalloc", "gg_ppr_k", "gg_msbfs", "gg_msbc",
+    "gg_batch_create", "gg_batch_destroy", "gg_batch_info", "gg_batch_bfs",
 ]
 
 
@@ -610,3 +615,44 @@ class Graph:
 
 def version() -> str:
     return lib.gg_version().decode()
+
+
+class GraphBatch:
+    """Many independent graphs in one device arena (gg_batch_*)."""
+
+    def __init__(self, host_graphs):
+        arr = (HostGraphC * len(host_graphs))(*[hg.c for hg in host_graphs])
+        self._hosts = list(host_graphs)
+        h = _P()
+        check(lib.gg_batch_create(len(host_graphs), arr, C.byref(h)), "gg_batch_create")
+        self.h = h
+        self.count = len(host_graphs)
+        tn, tm = C.c_uint64(), C.c_uint64()
+        self.firsts = np.empty(self.count, np.uint64)
+        check(lib.gg_batch_info(self.h, C.byref(tn), C.byref(tm), _ptr(self.firsts)), "gg_batch_info")
+        self.total_vertices, self.total_edges = tn.value, tm.value
+
+    def bfs(self, sources, out=None):
+        """Levels of every graph from its source: (flat levels[total_vertices], Run)."""
+        src = np.ascontiguousarray(sources, np.uint32)
+        assert len(src) == self.count
+        lev = out if out is not None else np.empty(self.total_vertices, np.int32)
+        st = RunStats()
+        check(lib.gg_batch_bfs(self.h, _ptr(src), _ptr(lev), C.byref(st)), "gg_batch_bfs")
+        return lev, _run(st)
+
+    def split(self, flat):
+        """Per-graph views of a flat per-vertex array."""
+        ends = list(self.firsts[1:]) + [self.total_vertices]
+        return [flat[int(a):int(b)] for a, b in zip(self.firsts, ends)]
+
+    def close(self):
+        if self.h:
+            check(lib.gg_batch_destroy(self.h), "gg_batch_destroy")
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

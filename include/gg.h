@@ -362,6 +362,26 @@ int gg_msbfs(gg_graph_t g, int32_t k, const uint32_t* sources, int32_t* levels, 
 int gg_msbc(gg_graph_t g, int32_t k, const uint32_t* sources, float* dependencies, float* num_paths,
             gg_run_stats* st);
 
+/* ======================================================== many graphs */
+/* No single counterpart in the reference (one graph per process there).  A
+ * batch of independent graphs of uneven size held in one device arena, for
+ * running one traversal over all of them in a single persistent launch. */
+typedef struct gg_graph_batch_s* gg_graph_batch_t;
+/* Uploads `count` host graphs (out-edge CSR each; weights ignored). */
+int gg_batch_create(int32_t count, const gg_host_graph* graphs, gg_graph_batch_t* out);
+int gg_batch_destroy(gg_graph_batch_t b);
+/* Sum of vertices and edges over the batch; firsts[count] (may be NULL)
+ * receives each graph's first slot in the level output. */
+int gg_batch_info(gg_graph_batch_t b, uint64_t* total_vertices, uint64_t* total_edges, uint64_t* firsts);
+/* BFS from sources[i] in graph i for every graph (app/BFS.C:77-101 levels),
+ * in one persistent launch whose CTAs take graphs, largest first, from a
+ * device work queue and traverse each inside the CTA.  levels: host array of
+ * total_vertices int32 (may be NULL), graph i's at firsts[i], -1 unreached.
+ * The sequence source upload -> traversal -> level download is a CUDA graph
+ * captured at gg_batch_create and replayed by every call; st->ms is its
+ * device time, st->edges_traversed the sum over graphs of gg_bfs's count. */
+int gg_batch_bfs(gg_graph_batch_t b, const uint32_t* sources, int32_t* levels, gg_run_stats* st);
+
 #ifdef __cplusplus
 }
 #endif

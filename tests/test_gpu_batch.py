@@ -93,3 +93,42 @@ def test_msbc_equals_single_source_on_symmetric(gg, orc):
         fin = np.isfinite(d1)
         np.testing.assert_array_equal(np.isnan(dep[:, j]), np.isnan(d1))
         assert rel_l1(dep[fin, j], d1[fin]) <= 1e-5
+
+
+def _batch_graphs(gg, count, seed):
+    rng = np.random.default_rng(seed)
+    hgs = []
+    for i in range(count):
+        kind = i % 5
+        if kind == 3:
+            hgs.append(gg.HostGraph.grid(int(rng.integers(4, 40)), 0.01, seed=int(i)))
+        elif kind == 4:
+            hgs.append(gg.HostGraph.er(int(rng.integers(1, 300)), int(rng.integers(0, 900)), seed=int(i)))
+        else:
+            hgs.append(gg.HostGraph.rmat(int(rng.integers(4, 13)), int(rng.integers(2, 33)), seed=1000 + i,
+                                         symmetric=bool(kind % 2)))
+    return hgs
+
+
+def test_batch_bfs_matches_oracle(gg, orc):
+    hgs = _batch_graphs(gg, 60, 7)
+    b = gg.GraphBatch(hgs)
+    rng = np.random.default_rng(3)
+    for rep in range(2):  # the second call replays the captured launch with new sources
+        src = np.array([0 if rep == 0 else int(rng.integers(0, h.n)) for h in hgs], np.uint32)
+        lev, run = b.bfs(src)
+        trav = 0
+        for h, s, lv in zip(hgs, src, b.split(lev)):
+            _, olev, ost = orc.Graph.from_host(h).bfs(int(s))
+            np.testing.assert_array_equal(lv, olev)
+            trav += ost.edges_traversed
+        assert run.edges_traversed == trav
+    b.close()
+
+
+def test_batch_rejects_bad_source(gg):
+    hgs = [gg.HostGraph.rmat(5, 4, seed=1), gg.HostGraph.rmat(6, 4, seed=2)]
+    b = gg.GraphBatch(hgs)
+    with pytest.raises(gg.GGError):
+        b.bfs(np.array([0, 64], np.uint32))
+    b.close()

@@ -148,3 +148,6 @@ def test_device_calls_fail_cleanly_without_gpu(gg):
     with pytest.raises(gg.GGError) as e:
         gg.Graph(g, partitions=2)
     assert "NO_DEVICE" in str(e.value)
+    with pytest.raises(gg.GGError) as e:
+        gg.GraphBatch([g, g])
+    assert "NO_DEVICE" in str(e.value)
