@@ -178,6 +178,10 @@ _sig("gg_batch_create", C.c_int, C.c_int32, _P, C.POINTER(_P))
 _sig("gg_batch_destroy", C.c_int, _P)
 _sig("gg_batch_info", C.c_int, _P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), _P)
 _sig("gg_batch_bfs", C.c_int, _P, _P, _P, C.POINTER(RunStats))
+_sig("gg_pagerank_weighted_create", C.c_int, _P, C.c_int32, C.c_float, C.c_int32, C.c_int32, C.POINTER(_P))
+_sig("gg_pagerank_weighted_destroy", C.c_int, _P)
+_sig("gg_pagerank_weighted_fwd", C.c_int, _P, _P, _P, _P, _P, C.POINTER(RunStats))
+_sig("gg_pagerank_weighted_bwd", C.c_int, _P, _P, _P, _P, _P, C.POINTER(RunStats))
 
 # Every symbol declared in include/gg.h (checked by the tests).
 EXPORTED = [
@@ -195,6 +199,8 @@ EXPORTED = [
     "gg_pagerank", "gg_pagerank_delta", "gg_spmv", "gg_bellman_ford", "gg_bc", "gg_bp",
     "gg_bfs_push_step_noalloc", "gg_ppr_k", "gg_msbfs", "gg_msbc",
     "gg_batch_create", "gg_batch_destroy", "gg_batch_info", "gg_batch_bfs",
+    "gg_pagerank_weighted_create", "gg_pagerank_weighted_destroy", "gg_pagerank_weighted_fwd",
+    "gg_pagerank_weighted_bwd",
 ]
 
 
@@ -649,6 +655,50 @@ class GraphBatch:
     def close(self):
         if self.h:
             check(lib.gg_batch_destroy(self.h), "gg_batch_destroy")
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class WeightedPageRank:
+    """Weighted PageRank with its adjoint (gg_pagerank_weighted_*): forward
+    keeps checkpoints every `checkpoint_every` steps, backward returns
+    (dL/dweights, dL/dtele, dL/dx0) for dL/dx of the last forward."""
+
+    def __init__(self, graph, iters=30, damping=0.85, checkpoint_every=5, normalize=False):
+        h = _P()
+        check(lib.gg_pagerank_weighted_create(graph.h, iters, damping, checkpoint_every, int(normalize), C.byref(h)),
+              "gg_pagerank_weighted_create")
+        self.h, self.graph, self.n, self.m = h, graph, graph.n, graph.m
+        graph._deps.add(self)
+
+    def forward(self, weights, tele, x0=None):
+        w = np.ascontiguousarray(weights, np.float32)
+        t = np.ascontiguousarray(tele, np.float32)
+        x0a = None if x0 is None else np.ascontiguousarray(x0, np.float32)
+        x = np.empty(self.n, np.float32)
+        st = RunStats()
+        check(lib.gg_pagerank_weighted_fwd(self.h, _ptr(w), _ptr(t), None if x0a is None else _ptr(x0a), _ptr(x),
+                                           C.byref(st)), "gg_pagerank_weighted_fwd")
+        return x, _run(st)
+
+    def backward(self, grad_x):
+        g = np.ascontiguousarray(grad_x, np.float32)
+        gw = np.empty(self.m, np.float32)
+        gt = np.empty(self.n, np.float32)
+        g0 = np.empty(self.n, np.float32)
+        st = RunStats()
+        check(lib.gg_pagerank_weighted_bwd(self.h, _ptr(g), _ptr(gw), _ptr(gt), _ptr(g0), C.byref(st)),
+              "gg_pagerank_weighted_bwd")
+        return gw, gt, g0, _run(st)
+
+    def close(self):
+        if self.h:
+            check(lib.gg_pagerank_weighted_destroy(self.h), "gg_pagerank_weighted_destroy")
             self.h = None
 
     def __del__(self):

@@ -382,6 +382,31 @@ int gg_batch_info(gg_graph_batch_t b, uint64_t* total_vertices, uint64_t* total_
  * device time, st->edges_traversed the sum over graphs of gg_bfs's count. */
 int gg_batch_bfs(gg_graph_batch_t b, const uint32_t* sources, int32_t* levels, gg_run_stats* st);
 
+/* ==================================================== differentiation */
+/* No counterpart in the reference.  Weighted PageRank
+ *   a_e = w_e, or w_e / (sum of w over u's out-edges) when normalize != 0
+ *   x_{t+1}[v] = damping * sum_{e = u->v} a_e x_t[u] + (1 - damping) * tele[v]
+ * for t < iters from x_0 (x0, or 1/n when x0 == NULL): PR_F / PR_Vertex_F
+ * (app/PageRank.C:28-100) with a_e in place of 1/outdeg(u) (a_e = 1/outdeg(u),
+ * tele = 1/n gives PageRankBit), and SPMV_F (app/SPMV.C:7-47) at iters = 1,
+ * damping = 1.  Its adjoint is the transposed traversal (a pull over the
+ * out-edges where the forward pulls the in-edges).  A context holds the
+ * forward's checkpoints (x_t every checkpoint_every steps) for the backward,
+ * which recomputes each segment from its checkpoint and reverses through it.
+ * weights / grad_weights: host, m entries in the graph's out-edge order
+ * (gg_host_graph offsets/indices of the current orientation); tele, x0, x_out,
+ * grad_x, grad_tele, grad_x0: host, n entries (grad_* may be NULL). */
+typedef struct gg_wpr_s* gg_wpr_t;
+int gg_pagerank_weighted_create(gg_graph_t g, int32_t iters, float damping, int32_t checkpoint_every,
+                                int32_t normalize, gg_wpr_t* out);
+int gg_pagerank_weighted_destroy(gg_wpr_t ctx);
+/* x_out = x_iters; keeps the checkpoints in ctx. */
+int gg_pagerank_weighted_fwd(gg_wpr_t ctx, const float* weights, const float* tele, const float* x0, float* x_out,
+                             gg_run_stats* st);
+/* Given grad_x = dL/dx_iters of the last forward: dL/dweights, dL/dtele, dL/dx0. */
+int gg_pagerank_weighted_bwd(gg_wpr_t ctx, const float* grad_x, float* grad_weights, float* grad_tele,
+                             float* grad_x0, gg_run_stats* st);
+
 #ifdef __cplusplus
 }
 #endif

@@ -60,6 +60,8 @@ for name, args in {
     "or_bc_brandes": [C.POINTER(OrGraph), C.c_uint32, _P, _P],
     "or_bp": [C.POINTER(OrGraph), C.c_int32, _P, _P, _P, C.POINTER(OrStats)],
     "or_ppr": [C.POINTER(OrGraph), C.c_int32, C.c_double, _P, _P],
+    "or_wpr_forward": [C.POINTER(OrGraph), _P, _P, _P, C.c_int32, C.c_double, C.c_int32, _P],
+    "or_wpr_backward": [C.POINTER(OrGraph), _P, _P, _P, C.c_int32, C.c_double, C.c_int32, _P, _P, _P, _P],
     "or_partition_sizes": [_P, _P, C.c_uint32, C.c_uint64, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, _P],
     "or_hilbert_key": [C.c_int64, C.c_int64, C.c_int64],
 }.items():
@@ -174,6 +176,28 @@ class Graph:
         ep = np.ascontiguousarray(edge_pot, np.float64)
         assert _lib.or_bp(C.byref(self.c), iters, _p(vp), _p(ep), _p(out), None) == 0
         return out
+
+    def wpr_forward(self, w, tele, iters, damping, normalize=False, x0=None):
+        """Weighted PageRank x_iters (FP64); w in out-edge order."""
+        w = np.ascontiguousarray(w, np.float64)
+        t = np.ascontiguousarray(tele, np.float64)
+        x0a = None if x0 is None else np.ascontiguousarray(x0, np.float64)  # kept alive across the call
+        out = np.empty(self.n, np.float64)
+        assert _lib.or_wpr_forward(C.byref(self.c), _p(w), _p(t), _p(x0a), iters, damping, int(normalize), _p(out)) == 0
+        return out
+
+    def wpr_backward(self, w, tele, iters, damping, grad_x, normalize=False, x0=None):
+        """(dL/dw, dL/dtele, dL/dx0) of weighted PageRank for dL/dx_iters = grad_x (FP64)."""
+        w = np.ascontiguousarray(w, np.float64)
+        t = np.ascontiguousarray(tele, np.float64)
+        gx = np.ascontiguousarray(grad_x, np.float64)
+        x0a = None if x0 is None else np.ascontiguousarray(x0, np.float64)
+        gw = np.empty(len(w), np.float64)
+        gt = np.empty(self.n, np.float64)
+        g0 = np.empty(self.n, np.float64)
+        assert _lib.or_wpr_backward(C.byref(self.c), _p(w), _p(t), None if x0a is None else _p(x0a), iters, damping,
+                                    int(normalize), _p(gx), _p(gw), _p(gt), _p(g0)) == 0
+        return gw, gt, g0
 
     def ppr(self, iters, damping, tele):
         x = np.empty(self.n, np.float64)

@@ -827,6 +827,89 @@ int or_ppr(const or_graph* g, int32_t iters, double damping, const double* tele,
   return 0;
 }
 
+/* ======================================================= weighted PageRank */
+static double* wpr_coeffs(const or_graph* g, const double* w, int32_t normalize) {
+  double* a = (double*)malloc(sizeof(double) * (g->m ? g->m : 1));
+  for (uint32_t u = 0; u < g->n; u++) {
+    double s = 0;
+    for (uint32_t e = g->out_off[u]; e < g->out_off[u + 1]; e++) s += w[e];
+    for (uint32_t e = g->out_off[u]; e < g->out_off[u + 1]; e++) a[e] = normalize ? w[e] / s : w[e];
+  }
+  return a;
+}
+
+/* x_{t+1} from x_t over out-edges (the same sums as a pull over in-edges). */
+static void wpr_step(const or_graph* g, const double* a, const double* tele, double damping, const double* x,
+                     double* y) {
+  for (uint32_t v = 0; v < g->n; v++) y[v] = 0;
+  for (uint32_t u = 0; u < g->n; u++)
+    for (uint32_t e = g->out_off[u]; e < g->out_off[u + 1]; e++) y[g->out_idx[e]] += a[e] * x[u];
+  for (uint32_t v = 0; v < g->n; v++) y[v] = damping * y[v] + (1 - damping) * tele[v];
+}
+
+static double* wpr_states(const or_graph* g, const double* a, const double* tele, const double* x0, int32_t iters,
+                          double damping) {
+  const uint32_t n = g->n;
+  double* xs = (double*)malloc(sizeof(double) * n * (iters + 1));
+  for (uint32_t v = 0; v < n; v++) xs[v] = x0 ? x0[v] : 1.0 / n;
+  for (int32_t t = 0; t < iters; t++) wpr_step(g, a, tele, damping, xs + (size_t)t * n, xs + (size_t)(t + 1) * n);
+  return xs;
+}
+
+int or_wpr_forward(const or_graph* g, const double* w, const double* tele, const double* x0, int32_t iters,
+                   double damping, int32_t normalize, double* x_out) {
+  if (!g || iters < 0) return -1;
+  double* a = wpr_coeffs(g, w, normalize);
+  double* xs = wpr_states(g, a, tele, x0, iters, damping);
+  memcpy(x_out, xs + (size_t)iters * g->n, sizeof(double) * g->n);
+  free(xs);
+  free(a);
+  return 0;
+}
+
+int or_wpr_backward(const or_graph* g, const double* w, const double* tele, const double* x0, int32_t iters,
+                    double damping, int32_t normalize, const double* grad_x, double* grad_w, double* grad_tele,
+                    double* grad_x0) {
+  if (!g || iters < 0) return -1;
+  const uint32_t n = g->n;
+  double* a = wpr_coeffs(g, w, normalize);
+  double* xs = wpr_states(g, a, tele, x0, iters, damping);
+  double* lam = (double*)malloc(sizeof(double) * n);
+  double* nl = (double*)malloc(sizeof(double) * n);
+  double* ga = (double*)calloc(g->m ? g->m : 1, sizeof(double));
+  memcpy(lam, grad_x, sizeof(double) * n);
+  for (uint32_t v = 0; v < n; v++) grad_tele[v] = 0;
+  for (int32_t t = iters - 1; t >= 0; t--) {
+    const double* x = xs + (size_t)t * n;
+    for (uint32_t v = 0; v < n; v++) grad_tele[v] += (1 - damping) * lam[v];
+    for (uint32_t u = 0; u < n; u++) {
+      double s = 0;
+      for (uint32_t e = g->out_off[u]; e < g->out_off[u + 1]; e++) {
+        const uint32_t v = g->out_idx[e];
+        ga[e] += damping * lam[v] * x[u];
+        s += a[e] * lam[v];
+      }
+      nl[u] = damping * s;
+    }
+    memcpy(lam, nl, sizeof(double) * n);
+  }
+  if (grad_x0) memcpy(grad_x0, lam, sizeof(double) * n);
+  for (uint32_t u = 0; u < n; u++) { /* chain rule through the normalisation */
+    double W = 0, r = 0;
+    for (uint32_t e = g->out_off[u]; e < g->out_off[u + 1]; e++) {
+      W += w[e];
+      r += ga[e] * a[e];
+    }
+    for (uint32_t e = g->out_off[u]; e < g->out_off[u + 1]; e++) grad_w[e] = normalize ? (ga[e] - r) / W : ga[e];
+  }
+  free(a);
+  free(xs);
+  free(lam);
+  free(nl);
+  free(ga);
+  return 0;
+}
+
 /* ============================================================== partitioner */
 /* graphgrind/graph-numa.h:1287-1357 (partitionByDegree), :1208-1256
  * (cscpartitionByDegree); degrees[cnt] read as 0. */

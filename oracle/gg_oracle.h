@@ -59,6 +59,20 @@ int or_bp(const or_graph* g, int32_t iters, const double* vert_pot, const double
  * k-column personalised form uses this per column): x_{t+1} = d*A x_t + (1-d)*tele. */
 int or_ppr(const or_graph* g, int32_t iters, double damping, const double* tele, double* x);
 
+/* Weighted PageRank and its adjoint (no reference counterpart; the weighted
+ * form of PR_F / PR_Vertex_F, app/PageRank.C:28-100, with the edge weight in
+ * place of 1/outdeg, and SPMV_F, app/SPMV.C:7-47, at iters = 1, damping = 1):
+ *   a_e = w_e (or w_e / sum of w over the source's out-edges when normalize)
+ *   x_{t+1}[v] = damping * sum_{e = u->v} a_e x_t[u] + (1 - damping) * tele[v]
+ * weights in out-edge (CSR) order; x0 NULL means 1/n.  The backward takes
+ * dL/dx_iters and returns dL/dw (CSR order), dL/dtele and dL/dx0 (NULL to
+ * skip), by reverse iteration over the transposed edges with every x_t kept. */
+int or_wpr_forward(const or_graph* g, const double* w, const double* tele, const double* x0, int32_t iters,
+                   double damping, int32_t normalize, double* x_out);
+int or_wpr_backward(const or_graph* g, const double* w, const double* tele, const double* x0, int32_t iters,
+                    double damping, int32_t normalize, const double* grad_x, double* grad_w, double* grad_tele,
+                    double* grad_x0);
+
 /* Partition sizes by the reference rules (same contract as gg_partition_sizes). */
 int or_partition_sizes(const uint32_t* in_deg, const uint32_t* out_deg, uint32_t n, uint64_t m,
                        int32_t P, int32_t balance, int32_t part_how, int32_t relabel,
