@@ -593,6 +593,15 @@ class Graph:
         check(lib.gg_ppr_k(self.h, k, iters, damping, tp, sp, _ptr(y), C.byref(st)), "gg_ppr_k")
         return y, _run(st)
 
+    def bp(self, iters, vert_pot, edge_pot):
+        """Belief propagation products after `iters` iterations: (prod[n, 2], Run)."""
+        vp = np.ascontiguousarray(vert_pot, np.float32).reshape(self.n, 2)
+        ep = np.ascontiguousarray(edge_pot, np.float32).reshape(self.m, 2, 2)
+        out = np.empty((self.n, 2), np.float32)
+        st = RunStats()
+        check(lib.gg_bp(self.h, iters, _ptr(vp), _ptr(ep), _ptr(out), C.byref(st)), "gg_bp")
+        return out, _run(st)
+
     def msbfs(self, sources, out=None):
         """Levels from up to 64 sources in one traversal: (levels[n, k] int32, Run)."""
         src = np.ascontiguousarray(sources, np.uint32)

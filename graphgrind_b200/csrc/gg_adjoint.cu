@@ -18,7 +18,7 @@
 #include <unordered_set>
 #include <vector>
 
-#include "gg_runtime.cuh"
+#include "gg_segreduce.cuh"
 
 struct gg_wpr_s {
   gg_graph_s* g = nullptr;
@@ -44,74 +44,27 @@ static bool wpr_live(const gg_wpr_s* w) {
   return w && g_wprs.count(w) && graph_live(w->g);
 }
 
-// Edge stream with its head-bit row structure (in-edges or out-edges).
-struct SegSum {
-  const uint32_t* idx;
-  const uint32_t* head;
-  const uint32_t* blk;
-  const uint32_t* rows;
-  uint64_t nblocks, m;
+// Sums into S: rows inside a block are stored, rows split across blocks added.
+struct SumInto {
+  using T = float;
+  static constexpr bool kNeedsIdx = true;
   float* S;
+  __device__ static T identity() { return 0.f; }
+  __device__ static T combine(T a, T b) { return a + b; }
+  __device__ void flush(uint32_t row, T v, bool complete) const {
+    if (complete)
+      S[row] = v;
+    else
+      atomicAdd(S + row, v);
+  }
 };
 
-// S[row] += sum over the row's edges e (other end y) of op.val(e, y, row).
-// One warp per 256-edge block, lane l takes edge 32 i + l; a segmented
-// shuffle scan sums each row's lanes, rows inside the block are stored and
-// rows crossing a block boundary are added atomically (S starts at zero).
-template <class Op>
-__global__ void __launch_bounds__(256) k_seg_sum(SegSum p, Op op) {
-  __shared__ uint32_t s_row[8][kSegBlock + 1];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const uint32_t lanemask_le = 0xffffffffu >> (31 - lane);
-  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
-  for (uint64_t b = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp; b < p.nblocks; b += warps) {
-    const uint64_t e0 = b * kSegBlock;
-    const uint32_t h0 = __ldg(p.blk + b), nr = __ldg(p.blk + b + 1) - h0 + 1;
-    for (uint32_t i = lane; i < nr; i += 32) s_row[warp][i] = (i > 0 || h0 > 0) ? __ldg(p.rows + h0 - 1 + i) : 0u;
-    __syncwarp();
-    const uint64_t nb = e0 + kSegBlock;
-    const bool ends_block = nb >= p.m || (__ldg(p.head + (nb >> 5)) & 1u);
-    uint32_t running = 0;
-    float carry = 0.f;
-    uint32_t hw = __ldg(p.head + b * 8);
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const uint32_t hw_next = i < 7 ? __ldg(p.head + b * 8 + i + 1) : 0u;
-      const uint64_t e = e0 + 32 * i + lane;
-      const uint32_t rel = running + __popc(hw & lanemask_le);
-      float v = 0.f;
-      if (e < p.m) v = op.val(e, __ldg(p.idx + e), s_row[warp][rel]);
-      const uint32_t hb = hw & lanemask_le;
-      const int seg0 = hb ? 31 - __clz(hb) : 0;
-      if (lane == 0 && !(hw & 1u)) v += carry;
-#pragma unroll
-      for (int d = 1; d < 32; d <<= 1) {
-        const float t = __shfl_up_sync(0xffffffffu, v, d);
-        if (lane >= seg0 + d) v += t;
-      }
-      const bool ends = lane < 31 ? ((hw >> (lane + 1)) & 1u) : (i < 7 ? (hw_next & 1u) : ends_block);
-      if (ends || (lane == 31 && i == 7)) {
-        const uint32_t row = s_row[warp][rel];
-        if (rel > 0 && ends)
-          p.S[row] = v;
-        else if (rel > 0 || h0 > 0)
-          atomicAdd(p.S + row, v);
-      }
-      const float v31 = __shfl_sync(0xffffffffu, v, 31);
-      carry = (i < 7 && !(hw_next & 1u)) ? v31 : 0.f;
-      running += __popc(hw);
-      hw = hw_next;
-    }
-    __syncwarp();
-  }
-}
-
-struct OpFwd {  // a_e x[u] over in-edges
+struct OpFwd : SumInto {  // a_e x[u] over in-edges
   const float* a;
   const float* x;
   __device__ float val(uint64_t e, uint32_t y, uint32_t) const { return __ldg(a + e) * __ldg(x + y); }
 };
-struct OpBwd {  // a_e lambda[v] over out-edges; dL/da_e += d lambda[v] x_t[u]
+struct OpBwd : SumInto {  // a_e lambda[v] over out-edges; dL/da_e += d lambda[v] x_t[u]
   const float* a;
   const float* lam;
   const float* x;
@@ -123,11 +76,11 @@ struct OpBwd {  // a_e lambda[v] over out-edges; dL/da_e += d lambda[v] x_t[u]
     return __ldg(a + e) * l;
   }
 };
-struct OpW {  // sum of out-edge weights
+struct OpW : SumInto {  // sum of out-edge weights
   const float* w;
   __device__ float val(uint64_t e, uint32_t, uint32_t) const { return __ldg(w + e); }
 };
-struct OpNormBack {  // sum of dL/da_e * a_e over out-edges
+struct OpNormBack : SumInto {  // sum of dL/da_e * a_e over out-edges
   const float* ga;
   const float* a;
   __device__ float val(uint64_t e, uint32_t, uint32_t) const { return __ldg(ga + e) * __ldg(a + e); }
@@ -136,15 +89,8 @@ struct OpNormBack {  // sum of dL/da_e * a_e over out-edges
 template <class Op>
 static int seg_sum(gg_graph_s* g, bool in_edges, float* S, Op op) {
   GG_CUDA(cudaMemsetAsync(S, 0, 4ull * g->n, g->stream));
-  if (g->m == 0) return GG_OK;
-  const int seg = g->symmetric ? 0 : ((in_edges != g->transposed) ? 0 : 1);
-  const SegIndex& si = g->seg[seg];
-  SegSum p{in_edges ? g->in_idx() : g->out_idx(), si.d_head, si.d_blk, si.d_rows,
-           (g->m + kSegBlock - 1) / kSegBlock, g->m, S};
-  const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((p.nblocks + 7) / 8, (uint64_t)g->num_sms * 8));
-  k_seg_sum<Op><<<grid, 256, 0, g->stream>>>(p, op);
-  g->kernels++;
-  return GG_OK;
+  op.S = S;
+  return seg_reduce(g, in_edges, op);
 }
 
 __global__ void k_wpr_row_of(uint64_t m, uint32_t n, const uint32_t* off, uint32_t* row_of) {
@@ -217,7 +163,7 @@ __global__ void k_wpr_fill(uint32_t n, float v, float* x) {
 
 static int wpr_step(gg_wpr_s* c, const float* x, float* y) {
   gg_graph_s* g = c->g;
-  GG_TRY(seg_sum(g, true, c->S, OpFwd{c->a_csc, x}));
+  GG_TRY(seg_sum(g, true, c->S, OpFwd{{}, c->a_csc, x}));
   k_wpr_fwd_vertex<<<generic_grid(g, c->n), kGenericThreads, 0, g->stream>>>(c->n, c->S, c->tele, c->damping, y);
   g->kernels++;
   return GG_OK;
@@ -284,7 +230,7 @@ static int wpr_forward(gg_wpr_s* c, const float* w, const float* tele, const flo
     g->kernels++;
   }
   if (m) {
-    if (c->normalize) GG_TRY(seg_sum(g, false, c->wsum, OpW{c->w}));
+    if (c->normalize) GG_TRY(seg_sum(g, false, c->wsum, OpW{{}, c->w}));
     k_wpr_coeffs<<<generic_grid(g, m), kGenericThreads, 0, g->stream>>>(m, c->w, c->normalize ? c->wsum : nullptr,
                                                                         c->row_of, c->perm, c->a_csr, c->a_csc);
     g->kernels++;
@@ -333,7 +279,7 @@ static int wpr_backward(gg_wpr_s* c, const float* grad_x, float* grad_w, float* 
     }
     for (int32_t t = t1 - 1; t >= t0; --t) {
       const float* xt = c->seg + (uint64_t)n * (t - t0);
-      GG_TRY(seg_sum(g, false, c->S, OpBwd{c->a_csr, c->lam, xt, c->ga, c->damping}));
+      GG_TRY(seg_sum(g, false, c->S, OpBwd{{}, c->a_csr, c->lam, xt, c->ga, c->damping}));
       k_wpr_bwd_vertex<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(n, c->S, c->lam, c->damping, c->lam2,
                                                                               c->gt);
       g->kernels++;
@@ -343,7 +289,7 @@ static int wpr_backward(gg_wpr_s* c, const float* grad_x, float* grad_w, float* 
   float* gw = c->ga;
   if (m && c->normalize) {
     // dL/dw_e = (dL/da_e - sum_{e' of u} dL/da_e' a_e') / W_u
-    GG_TRY(seg_sum(g, false, c->S, OpNormBack{c->ga, c->a_csr}));
+    GG_TRY(seg_sum(g, false, c->S, OpNormBack{{}, c->ga, c->a_csr}));
     k_wpr_norm_back<<<generic_grid(g, m), kGenericThreads, 0, g->stream>>>(m, c->ga, c->S, c->wsum, c->row_of,
                                                                            c->gw);
     g->kernels++;

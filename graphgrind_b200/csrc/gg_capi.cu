@@ -633,8 +633,5 @@ int gg_bc(gg_graph_t g, uint32_t start, float* dep, float* np, gg_run_stats* st)
   if (!g || start >= g->n) return fail(GG_ERR_INVALID_ARG, "gg_bc: bad arguments");
   return run_bc(g, start, dep, np, st);
 }
-int gg_bp(gg_graph_t, int32_t, const float*, const float*, float*, gg_run_stats*) {
-  return fail(GG_ERR_UNSUPPORTED, "gg_bp: not built yet");
-}
 
 }  // extern "C"

@@ -326,7 +326,13 @@ int gg_spmv(gg_graph_t g, const float* x_in, float* y, gg_run_stats* st);
 int gg_bellman_ford(gg_graph_t g, uint32_t start, int32_t* dist, gg_run_stats* st);
 /* app/BC.C:156-226 single source: dependencies[n], num_paths[n] (forward counts). */
 int gg_bc(gg_graph_t g, uint32_t start, float* dependencies, float* num_paths, gg_run_stats* st);
-/* app/BP.C:152-212 with defined inputs: 2-state beliefs vert_out[2n] after iters. */
+/* app/BP.C:152-212 with defined inputs (the reference leaves them
+ * uninitialised): vert_potential[2n], edge_potential[4m] with edge e's 2x2
+ * potential (i, k) at 4e + 2i + k, e = the edge's in-edge slot of the current
+ * orientation (CSC position); per iteration, products reset to 1,
+ *   belief_e[i] = sum_k vert_potential[d][k] edge_potential[e][i][k] prod[d][k]
+ *   prod_next[d][i] = product of belief_e[i] over d's in-edges.
+ * vert_out[2n] = the products after iters iterations. */
 int gg_bp(gg_graph_t g, int32_t iters, const float* vert_potential, const float* edge_potential,
           float* vert_out, gg_run_stats* st);
 

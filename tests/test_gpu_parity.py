@@ -170,3 +170,26 @@ def test_edgeless_and_tiny(gg, orc):
     assert lev.tolist() == [-1, -1, 0, -1] and st.rounds == 1
     ids, _ = g.components()
     assert ids.tolist() == [0, 1, 2, 3]
+
+
+@pytest.mark.parametrize("sym", [True, False])
+def test_bp_matches_oracle(gg, orc, sym):
+    hg = gg.HostGraph.rmat(11, 8, seed=51, symmetric=sym)
+    g = gg.Graph(hg, partitions=ok_partitions(hg, 16))
+    og = orc.Graph.from_host(hg)
+    rng = np.random.default_rng(5)
+    vp = rng.uniform(0.9, 1.1, (hg.n, 2)).astype(np.float32)
+    ep = rng.uniform(0.45, 0.55, (hg.m, 2, 2)).astype(np.float32)
+    for iters in (0, 1, 2, 3):
+        out, run = g.bp(iters, vp, ep)
+        ref = og.bp(iters, vp.astype(np.float64).ravel(), ep.astype(np.float64).ravel()).reshape(hg.n, 2)
+        assert run.rounds == iters
+        # unnormalised products leave FP32's range on hubs: compare inside it,
+        # and require overflow / underflow where FP64 is far outside
+        inside = (ref > 1e-30) & (ref < 1e30)
+        assert inside.mean() > 0.5
+        # a product over d in-edges of beliefs built from the previous products
+        # multiplies their relative error by about d each iteration
+        np.testing.assert_allclose(out[inside], ref[inside], rtol=2e-5 if iters < 2 else 1e-2)
+        assert np.all(np.isinf(out[ref > 1e40]))
+        assert np.all(out[ref < 1e-50] == 0)
