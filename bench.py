@@ -17,6 +17,14 @@ each run through the library's C ABI (gg_bfs / gg_pagerank / gg_spmv).
            bytes 8m + 16n per launch over its CUDA-event duration
   cpu_baseline = the reference's own OpenMP build (oracle/_ref) on the host
            cores, on a bounded RMAT-22 sample of the same workload
+  batched  = (N=1, outside the timed step) the batched and differentiated
+           forms against the plain form on the same GPU: k=64 personalised
+           PageRank (RMAT-22 seed 5, 20 iterations) vs 64 single-column runs;
+           64-source BFS and BC vs 64 single-source runs; 1,024 RMAT graphs
+           (scales 10-16, edge factor 8-32, seeds 1000-2023, BFS from 0) in one
+           persistent launch vs plain per-graph BFS on a sample; weighted
+           PageRank adjoint (RMAT-22 seed 6, 30 iterations, checkpoints every 5)
+           backward vs forward time
 
 Multi-GPU: the path does not shard across GPUs in this build (one GPU per
 graph); --gpus N runs N independent replicas under torchrun and reports the
@@ -65,8 +73,12 @@ class ClockSampler:
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", gpu_index, f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
+            # the timed region starts once samples are flowing
+            t0 = time.time()
+            while time.time() - t0 < 5 and os.path.getsize(self.path) == 0:
+                time.sleep(0.02)
         except Exception as e:  # no nvidia-smi: report without clocks
             log("clock sampler unavailable:", e)
 
@@ -215,6 +227,102 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
     return out
 
 
+# ------------------------------------------------ batched and adjoint forms
+def _best(f, reps):
+    return min(f() for _ in range(reps))
+
+
+def run_batched(gg):
+    """Batched / differentiated forms vs the plain form, each on its own graph."""
+    out = {}
+    rng = np.random.default_rng(11)
+    t0 = time.time()
+    hg = gg.HostGraph.rmat(22, 16, 0.57, 0.19, 0.19, seed=5, symmetric=False)
+    g = gg.Graph(hg, partitions=96)
+    m = hg.m
+    seeds = rng.integers(0, hg.n, 64).astype(np.uint32)
+    o64 = np.empty((hg.n, 64), np.float32)
+    o1 = np.empty((hg.n, 1), np.float32)
+    g.ppr_k(64, 20, 0.85, seeds=seeds, out=o64)
+    k64 = _best(lambda: g.ppr_k(64, 20, 0.85, seeds=seeds, out=o64)[1].ms, 3)
+    plain, diffs = 0.0, []
+    g.ppr_k(1, 20, 0.85, seeds=seeds[:1], out=o1)
+    for j in range(64):
+        plain += g.ppr_k(1, 20, 0.85, seeds=seeds[j:j + 1], out=o1)[1].ms
+        if j < 4:
+            diffs.append(float(np.abs(o64[:, j] - o1[:, 0]).sum() / np.abs(o1[:, 0]).sum()))
+    out["ppr_k64"] = {"workload": f"RMAT-22 seed 5 directed (m={m}), 64 one-hot teleports, 20 iterations",
+                      "batched_ms": round(k64, 3), "batched_gteps": round(64 * 20 * m / k64 / 1e6, 2),
+                      "plain_64x_ms": round(plain, 3), "plain_gteps": round(64 * 20 * m / plain / 1e6, 2),
+                      "speedup": round(plain / k64, 2), "max_rel_l1_vs_plain_cols0_3": max(diffs)}
+    src = rng.integers(0, hg.n, 64).astype(np.uint32)
+    lev = np.empty((hg.n, 64), np.int32)
+    g.msbfs(src, out=lev)
+    r = g.msbfs(src, out=lev)[1]
+    ms_bfs = _best(lambda: g.msbfs(src, out=lev)[1].ms, 3)
+    plain = sum(g.bfs(int(s))[2].ms for s in src)
+    out["msbfs_k64"] = {"workload": "RMAT-22 seed 5 directed, 64 uniform sources", "batched_ms": round(ms_bfs, 3),
+                        "batched_gteps": round(r.edges_traversed / ms_bfs / 1e6, 2), "plain_64x_ms": round(plain, 3),
+                        "speedup": round(plain / ms_bfs, 2)}
+    dep, npth = np.empty((hg.n, 64), np.float32), np.empty((hg.n, 64), np.float32)
+    rb = g.msbc(src, dep_out=dep, paths_out=npth)[2]
+    ms_bc = _best(lambda: g.msbc(src, dep_out=dep, paths_out=npth)[2].ms, 2)
+    plain = sum(g.bc(int(s))[2].ms for s in src)
+    out["msbc_k64"] = {"workload": "RMAT-22 seed 5 directed, 64 uniform sources", "batched_ms": round(ms_bc, 3),
+                       "batched_gteps": round(rb.edges_traversed / ms_bc / 1e6, 2), "plain_64x_ms": round(plain, 3),
+                       "speedup": round(plain / ms_bc, 2)}
+    g.close()
+    # 1,024 independent graphs in one persistent launch
+    count = 1024
+    scales, efs = rng.integers(10, 17, count), rng.integers(8, 33, count)
+    hgs = [gg.HostGraph.rmat(int(sc), int(ef), 0.57, 0.19, 0.19, seed=1000 + i, symmetric=False)
+           for i, (sc, ef) in enumerate(zip(scales, efs))]
+    b = gg.GraphBatch(hgs)
+    zeros = np.zeros(count, np.uint32)
+    levs = np.empty(b.total_vertices, np.int32)
+    rr = b.bfs(zeros, out=levs)[1]
+    many = _best(lambda: b.bfs(zeros, out=levs)[1].ms, 5)
+    sample = rng.choice(count, 32, replace=False)
+    p_ms, p_edges = 0.0, 0
+    for i in sample:
+        gi = gg.Graph(hgs[i], partitions=1)
+        gi.bfs(0)
+        r1 = gi.bfs(0)[2]
+        p_ms += r1.ms
+        p_edges += r1.edges_traversed
+        gi.close()
+    b.close()
+    plain_gteps = p_edges / p_ms / 1e6
+    out["many_graphs_bfs"] = {
+        "workload": f"{count} RMAT graphs, scales U{{10..16}}, edge factor U{{8..32}}, seeds 1000-{999 + count}, "
+                    f"directed, BFS from 0; {b.total_vertices} vertices, {b.total_edges} edges",
+        "batched_ms": round(many, 3), "batched_gteps": round(rr.edges_traversed / many / 1e6, 2),
+        "includes": "source upload, persistent traversal, level download (one CUDA-graph replay)",
+        "plain_gteps_sample32": round(plain_gteps, 3),
+        "speedup_vs_plain_gteps": round(rr.edges_traversed / many / 1e6 / plain_gteps, 2)}
+    # weighted PageRank adjoint
+    hw = gg.HostGraph.rmat(22, 16, 0.57, 0.19, 0.19, seed=6, symmetric=False)
+    gw = gg.Graph(hw, partitions=96)
+    w = rng.uniform(0, 1, hw.m).astype(np.float32)
+    w[w == 0] = 0.5
+    tele = np.full(hw.n, 1.0 / hw.n, np.float32)
+    c = rng.standard_normal(hw.n).astype(np.float32)
+    wpr = gg.WeightedPageRank(gw, 30, 0.85, 5, True)
+    wpr.forward(w, tele)
+    wpr.backward(c)
+    fwd = _best(lambda: wpr.forward(w, tele)[1].ms, 3)
+    bwd = _best(lambda: wpr.backward(c)[3].ms, 3)
+    wpr.close()
+    gw.close()
+    out["adjoint_weighted_pagerank"] = {
+        "workload": f"RMAT-22 seed 6 directed (m={hw.m}), weights U(0,1] normalised per source inside the function, "
+                    "damping 0.85, 30 iterations, loss weights N(0,1), checkpoints every 5",
+        "forward_ms": round(fwd, 3), "backward_ms": round(bwd, 3), "backward_over_forward": round(bwd / fwd, 3),
+        "forward_gteps": round(30 * hw.m / fwd / 1e6, 2)}
+    out["seconds"] = round(time.time() - t0, 1)
+    return out
+
+
 # ------------------------------------------------------- the reference (CPU)
 def reference_sample(scale: int, partitions: int, rounds: int, workdir: str):
     """Time the reference's own BFS, PageRank and SPMV (OpenMP build of
@@ -299,7 +407,7 @@ def cpu_baseline_for_ours(args):
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--scale", type=int, default=24)
@@ -309,6 +417,7 @@ def main():
     ap.add_argument("--ref-scale", type=int, default=22)
     ap.add_argument("--ref-partitions", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched / adjoint comparisons")
     ap.add_argument("--traffic", type=float, default=None,
                     help="DRAM bytes per dense-pull launch from an ncu capture (reported as roofline.traffic)")
     args = ap.parse_args()
@@ -334,6 +443,12 @@ def main():
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline_for_ours(args)
+        if world == 1 and not args.no_batched:
+            import graphgrind_b200 as gg
+            try:
+                out["batched"] = run_batched(gg)
+            except Exception as e:  # reported, the headline line still prints
+                out["batched"] = {"error": str(e)[:300]}
         print(json.dumps(out))
     if dist:
         dist.barrier()

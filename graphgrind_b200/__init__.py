@@ -17,7 +17,8 @@ from dataclasses import dataclass
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libgg.so")
+# GG_LIBRARY names another build of the same C ABI (for side-by-side builds)
+LIB_PATH = os.environ.get("GG_LIBRARY") or os.path.join(_HERE, "libgg.so")
 
 if not os.path.exists(LIB_PATH):
     raise ImportError(
@@ -62,7 +63,7 @@ class HostGraphC(C.Structure):
 class BuildOpts(C.Structure):
     _fields_ = [("num_partitions", C.c_int32), ("balance", C.c_int32), ("part_how", C.c_int32),
                 ("relabel", C.c_int32), ("order", C.c_int32), ("tile_vertices", C.c_int32),
-                ("tile_edges", C.c_int32), ("build_coo", C.c_int32)]
+                ("tile_edges", C.c_int32), ("build_coo", C.c_int32), ("coo_window", C.c_int32)]
 
 
 class GraphInfo(C.Structure):
@@ -445,10 +446,11 @@ class Graph:
     """partitioned_graph on the device (gg_graph_build)."""
 
     def __init__(self, host: HostGraph, partitions=384, balance=BALANCE_EDGE, part_how=PART_DEST, relabel=False,
-                 order=ORDER_HILBERT, tile_vertices=0, tile_edges=0, build_coo=0):
+                 order=ORDER_HILBERT, tile_vertices=0, tile_edges=0, build_coo=0, coo_window=0):
         self.host = host
         self._deps = weakref.WeakSet()
-        o = BuildOpts(partitions, balance, part_how, int(relabel), order, tile_vertices, tile_edges, build_coo)
+        o = BuildOpts(partitions, balance, part_how, int(relabel), order, tile_vertices, tile_edges, build_coo,
+                      coo_window)
         h = C.c_void_p()
         check(lib.gg_graph_build(C.byref(host.c), C.byref(o), C.byref(h)), "gg_graph_build")
         self.h = h

@@ -454,8 +454,13 @@ __host__ __device__ constexpr size_t coo_w_smem_bytes(bool hw, int stages, int v
   return 256 + (size_t)kCooWarps * stages * coo_w_stage_bytes(hw) + (size_t)((tv + 3) & ~3u) * (vbytes + 2);
 }
 
-template <class F, bool HW, bool ALL, int STAGES>
-__global__ void __launch_bounds__(kCooThreads, 4) k_pull_coo_w(const PullParams p, const F f) {
+#ifndef GG_COO_MIN_BLOCKS
+#define GG_COO_MIN_BLOCKS 4  // resident CTAs per SM the register allocation must allow
+#endif
+template <class F, bool HW, bool ALL, int STAGES, bool CONTIG = false, bool PF = false>
+__global__ void __launch_bounds__(kCooThreads, GG_COO_MIN_BLOCKS) k_pull_coo_w(const PullParams p, const F f) {
+  static_assert(!CONTIG || STAGES == 0, "lane-contiguous edges use direct loads");
+  static_assert(!PF || (STAGES == 0 && !CONTIG), "register prefetch applies to direct loads");
   using V = typename F::value_t;
   extern __shared__ __align__(128) unsigned char smem[];
   constexpr uint32_t SB = (uint32_t)coo_w_stage_bytes(HW);
@@ -511,6 +516,25 @@ __global__ void __launch_bounds__(kCooThreads, 4) k_pull_coo_w(const PullParams 
         for (uint32_t i = 0; i < nbw && i < (uint32_t)STAGES; ++i) issue(i, (int)i);
       issued = nbw < (uint32_t)STAGES ? nbw : (uint32_t)STAGES;
     }
+    // PF: the next block's edge stream is loaded into registers while the
+    // current block's gathers are in flight
+    uint4 pa = make_uint4(0, 0, 0, 0), pc = pa, pq = pa, pu = pa, pw = pa;
+    auto pload = [&](uint32_t i2) {
+      const uint32_t j2 = (uint32_t)warp + i2 * kCooWarps;
+      if ((uint32_t)lane * 8 < blk_len(j2)) {
+        const size_t b = (size_t)e0 + (size_t)j2 * kSegBlock + (size_t)lane * 8;
+        pa = __ldg(reinterpret_cast<const uint4*>(p.src + b));
+        pc = __ldg(reinterpret_cast<const uint4*>(p.src + b) + 1);
+        pq = __ldg(reinterpret_cast<const uint4*>(p.dloc + b));
+        if (HW) {
+          pu = __ldg(reinterpret_cast<const uint4*>(p.wts + b));
+          pw = __ldg(reinterpret_cast<const uint4*>(p.wts + b) + 1);
+        }
+      }
+    };
+    if constexpr (PF) {
+      if (nbw > 0) pload(0);
+    }
     for (uint32_t i = 0; i < nbw; ++i) {
       const uint32_t j = (uint32_t)warp + i * kCooWarps;
       const uint32_t nel = blk_len(j);
@@ -553,6 +577,30 @@ __global__ void __launch_bounds__(kCooThreads, 4) k_pull_coo_w(const PullParams 
           issue(i + STAGES, st);
         }
         if (i + STAGES < nbw) ++issued;
+      } else if (CONTIG) {
+        // lane l takes edges 32 k + l of the block: each gather instruction
+        // covers 32 consecutive (source-ordered) edges
+        const size_t b0 = (size_t)e0 + (size_t)j * kSegBlock + (size_t)lane;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const bool ink = (uint32_t)(32 * k + lane) < nel;
+          sv[k] = ink ? __ldg(p.src + b0 + 32 * k) : kPad;
+          dv[k] = ink ? __ldg(p.dloc + b0 + 32 * k) : (uint16_t)0;
+          if (HW) wv[k] = ink ? __ldg(p.wts + b0 + 32 * k) : 0u;
+        }
+      } else if (PF) {
+        const uint4 a = pa, c = pc, q = pq, u = pu, w = pw;
+        if (i + 1 < nbw) pload(i + 1);
+        if (in) {
+          sv[0] = a.x; sv[1] = a.y; sv[2] = a.z; sv[3] = a.w;
+          sv[4] = c.x; sv[5] = c.y; sv[6] = c.z; sv[7] = c.w;
+          dv[0] = q.x & 0xffff; dv[1] = q.x >> 16; dv[2] = q.y & 0xffff; dv[3] = q.y >> 16;
+          dv[4] = q.z & 0xffff; dv[5] = q.z >> 16; dv[6] = q.w & 0xffff; dv[7] = q.w >> 16;
+          if (HW) {
+            wv[0] = u.x; wv[1] = u.y; wv[2] = u.z; wv[3] = u.w;
+            wv[4] = w.x; wv[5] = w.y; wv[6] = w.z; wv[7] = w.w;
+          }
+        }
       } else if (in) {
         const size_t b0 = (size_t)e0 + (size_t)j * kSegBlock + (size_t)lane * 8;
         const uint4 a = __ldg(reinterpret_cast<const uint4*>(p.src + b0));
@@ -575,7 +623,7 @@ __global__ void __launch_bounds__(kCooThreads, 4) k_pull_coo_w(const PullParams 
       }
       bool vld[8];
 #pragma unroll
-      for (int k = 0; k < 8; ++k) vld[k] = in && sv[k] != kPad && (F::kCondTrue || s_cond[dv[k]]);
+      for (int k = 0; k < 8; ++k) vld[k] = (CONTIG || in) && sv[k] != kPad && (F::kCondTrue || s_cond[dv[k]]);
       if (!ALL) {
 #pragma unroll
         for (int k = 0; k < 8; ++k)
@@ -586,6 +634,17 @@ __global__ void __launch_bounds__(kCooThreads, 4) k_pull_coo_w(const PullParams 
       for (int k = 0; k < 8; ++k) {
         val[k] = vld[k] ? f.gather(sv[k], wv[k]) : F::identity();
         if (F::kPositive) vld[k] = vld[k] && !(val[k] < F::identity());
+      }
+      if constexpr (CONTIG) {
+        // destinations of consecutive source-ordered edges are scattered:
+        // one shared-memory accumulation per edge
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          if (!vld[k]) continue;
+          F::atomic_combine(&s_acc[dv[k]], val[k]);
+          if (!F::kPositive) s_touch[dv[k]] = 1;
+        }
+        continue;
       }
       int cur = -1;
       V acc = F::identity();

@@ -252,6 +252,18 @@ __global__ void k_coo_window_keys(const uint4* seg, uint32_t ntiles, const uint3
   }
 }
 
+// Alternative second-level order: windows of W edges of the Hilbert order,
+// sources ascending inside a window, so that 32 consecutive edges gather from
+// few cache lines.  key = window << 32 | source.
+__global__ void k_coo_window_src_keys(const uint4* seg, uint32_t ntiles, const uint32_t* perm, const uint32_t* src,
+                                      uint32_t window, uint64_t* keys) {
+  for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const uint4 s = seg[t];  // {v0, nv, e0 (CSC), ne}
+    for (uint32_t i = threadIdx.x; i < s.w; i += blockDim.x)
+      keys[s.z + i] = ((uint64_t)(i / window) << 32) | src[perm[s.z + i]];
+  }
+}
+
 // scatter sorted tile segments into their padded COO slots
 __global__ void k_coo_scatter(const uint4* seg, const uint32_t* pad_start, uint32_t ntiles, const uint32_t* perm,
                               const uint32_t* src, const uint32_t* dst, const uint32_t* w, uint32_t* coo_src,
@@ -353,22 +365,40 @@ static int build_coo(gg_graph_s* g, const uint32_t* h_in_off) {
     GG_BUILD(cudaMalloc(&d_temp, temp_bytes));
     GG_BUILD(cub::DeviceSegmentedRadixSort::SortPairs(d_temp, temp_bytes, d_keys, d_keys_out, d_vals, d_perm, (int)m,
                                                       (int)segs.size(), d_seg_begin, d_seg_begin + 1));
-    // destination order inside 256-edge windows (the u64 key buffers are reused as u32)
-    uint32_t* k32 = reinterpret_cast<uint32_t*>(d_keys);
-    uint32_t* k32_out = reinterpret_cast<uint32_t*>(d_keys_out);
-    k_coo_window_keys<<<grid, 256>>>(d_segs, (uint32_t)segs.size(), d_perm, d_dst, k32);
-    GG_BUILD(cudaGetLastError());
-    size_t temp2 = 0;
-    GG_BUILD(cub::DeviceSegmentedRadixSort::SortPairs(nullptr, temp2, k32, k32_out, d_perm, d_vals, (int)m,
-                                                      (int)segs.size(), d_seg_begin, d_seg_begin + 1));
-    if (temp2 > temp_bytes) {
-      cudaFree(d_temp);
-      d_temp = nullptr;
-      GG_BUILD(cudaMalloc(&d_temp, temp2));
-      temp_bytes = temp2;
+    if (g->opts.coo_window > 0) {
+      // source order inside windows of coo_window edges (64-bit keys)
+      k_coo_window_src_keys<<<grid, 256>>>(d_segs, (uint32_t)segs.size(), d_perm, g->d_csc_idx,
+                                           (uint32_t)g->opts.coo_window, d_keys);
+      GG_BUILD(cudaGetLastError());
+      size_t temp2 = 0;
+      GG_BUILD(cub::DeviceSegmentedRadixSort::SortPairs(nullptr, temp2, d_keys, d_keys_out, d_perm, d_vals, (int)m,
+                                                        (int)segs.size(), d_seg_begin, d_seg_begin + 1));
+      if (temp2 > temp_bytes) {
+        cudaFree(d_temp);
+        d_temp = nullptr;
+        GG_BUILD(cudaMalloc(&d_temp, temp2));
+        temp_bytes = temp2;
+      }
+      GG_BUILD(cub::DeviceSegmentedRadixSort::SortPairs(d_temp, temp2, d_keys, d_keys_out, d_perm, d_vals, (int)m,
+                                                        (int)segs.size(), d_seg_begin, d_seg_begin + 1));
+    } else {
+      // destination order inside 256-edge windows (the u64 key buffers are reused as u32)
+      uint32_t* k32 = reinterpret_cast<uint32_t*>(d_keys);
+      uint32_t* k32_out = reinterpret_cast<uint32_t*>(d_keys_out);
+      k_coo_window_keys<<<grid, 256>>>(d_segs, (uint32_t)segs.size(), d_perm, d_dst, k32);
+      GG_BUILD(cudaGetLastError());
+      size_t temp2 = 0;
+      GG_BUILD(cub::DeviceSegmentedRadixSort::SortPairs(nullptr, temp2, k32, k32_out, d_perm, d_vals, (int)m,
+                                                        (int)segs.size(), d_seg_begin, d_seg_begin + 1));
+      if (temp2 > temp_bytes) {
+        cudaFree(d_temp);
+        d_temp = nullptr;
+        GG_BUILD(cudaMalloc(&d_temp, temp2));
+        temp_bytes = temp2;
+      }
+      GG_BUILD(cub::DeviceSegmentedRadixSort::SortPairs(d_temp, temp2, k32, k32_out, d_perm, d_vals, (int)m,
+                                                        (int)segs.size(), d_seg_begin, d_seg_begin + 1));
     }
-    GG_BUILD(cub::DeviceSegmentedRadixSort::SortPairs(d_temp, temp2, k32, k32_out, d_perm, d_vals, (int)m,
-                                                      (int)segs.size(), d_seg_begin, d_seg_begin + 1));
     k_coo_scatter<<<grid, 256>>>(d_segs, d_pad, (uint32_t)segs.size(), d_vals, g->d_csc_idx, d_dst, g->d_csc_w,
                                  g->d_coo_src, g->d_coo_dloc, g->d_coo_w);
     GG_BUILD(cudaGetLastError());
@@ -382,6 +412,7 @@ static int build_coo(gg_graph_s* g, const uint32_t* h_in_off) {
     tiles[t] = make_uint4(segs[t].x, segs[t].y, pad_start[t], (segs[t].w + 7u) & ~7u);
   GG_TRY(upload_tiles(g, g->coo_tiles, tiles));
   g->has_coo = true;
+  if (g->opts.coo_window > 0) g->coo_kernel = 4;  // the lane-contiguous pull matches source-ordered windows
   return GG_OK;
 }
 
@@ -436,6 +467,8 @@ static int graph_build(const gg_host_graph* hg, const gg_build_opts* opts_in, gg
   if (o.num_partitions <= 0) o.num_partitions = 384;
   if (o.tile_vertices <= 0 || o.tile_vertices > kMaxTileVertices) o.tile_vertices = kMaxTileVertices;
   if (o.tile_edges <= 0) o.tile_edges = 1 << 16;
+  if (o.coo_window < 0) o.coo_window = 0;
+  if (o.coo_window > 0) o.coo_window = (o.coo_window + kSegBlock - 1) / kSegBlock * kSegBlock;
   if (o.order != GG_ORDER_CSR) o.order = GG_ORDER_HILBERT;
   if (o.part_how == GG_PART_SOURCE)
     return fail(GG_ERR_UNSUPPORTED, "-P source partitioning is not supported by this build");
@@ -637,7 +670,7 @@ int gg_graph_set_tuning(gg_graph_t g, int32_t key, int64_t value) {
     case GG_TUNE_DENSE_POLICY:
       return gg_graph_set_dense_policy(g, (int32_t)value);
     case GG_TUNE_COO_KERNEL:
-      if (value < 0 || value > 3) return fail(GG_ERR_INVALID_ARG, "COO kernel must be 0..3");
+      if (value < 0 || value > 5) return fail(GG_ERR_INVALID_ARG, "COO kernel must be 0..5");
       g->coo_kernel = (int)value;
       return GG_OK;
     default:

@@ -122,6 +122,7 @@ int pull_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f
   };
   if (coo && g->coo_kernel > 0) {  // per-warp COO pull: 0, 2 or 3 staging stages
     static bool opted[2][4] = {};
+    static bool opted_pf[2] = {};
     auto launch_w = [&](auto kern, int stages, bool& done) -> int {
       const size_t smem = coo_w_smem_bytes(kHW, stages, 4, p.tv);
       if (!done) {
@@ -139,6 +140,12 @@ int pull_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f
       return GG_OK;
     };
     switch (g->coo_kernel) {
+      case 5:
+        return all ? launch_w(k_pull_coo_w<F, kHW, true, 0, false, true>, 0, opted_pf[1])
+                   : launch_w(k_pull_coo_w<F, kHW, false, 0, false, true>, 0, opted_pf[0]);
+      case 4:
+        return all ? launch_w(k_pull_coo_w<F, kHW, true, 0, true>, 0, opted[1][0])
+                   : launch_w(k_pull_coo_w<F, kHW, false, 0, true>, 0, opted[0][0]);
       case 1:
         return all ? launch_w(k_pull_coo_w<F, kHW, true, 0>, 0, opted[1][1])
                    : launch_w(k_pull_coo_w<F, kHW, false, 0>, 0, opted[0][1]);

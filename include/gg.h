@@ -61,6 +61,11 @@ typedef struct gg_build_opts {
   int32_t tile_vertices;    /* GPU: max destinations per CTA tile (<=8192)  */
   int32_t tile_edges;       /* GPU: target edges per CTA tile               */
   int32_t build_coo;        /* 1 = build the partitioned COO (default when balance==edge) */
+  int32_t coo_window;       /* GPU: order inside a COO tile after the Hilbert sort:
+                               0 = destination order inside 256-edge windows;
+                               W > 0 = source order inside windows of W edges
+                               (rounded up to a multiple of 256), which lets a
+                               warp's 32 gathers share cache lines          */
 } gg_build_opts;
 
 typedef struct gg_graph_info {
@@ -236,7 +241,12 @@ int gg_graph_set_dense_policy(gg_graph_t g, int32_t policy);
 /* Engine tuning knobs (all keep edgeMap's results; they pick kernels):
  *   GG_TUNE_DENSE_POLICY  as gg_graph_set_dense_policy
  *   GG_TUNE_COO_KERNEL    0 CTA-wide bulk-copy ring, 1 per-warp direct loads,
- *                         2/3 per-warp bulk-copy ring with 2/3 stages */
+ *                         2/3 per-warp bulk-copy ring with 2/3 stages,
+ *                         4 per-warp direct loads with lane-contiguous edges
+ *                         and one shared-memory accumulation per edge (the
+ *                         default for graphs built with coo_window > 0),
+ *                         5 per-warp direct loads with the next block's edge
+ *                         stream prefetched into registers */
 #define GG_TUNE_DENSE_POLICY 1
 #define GG_TUNE_COO_KERNEL 2
 int gg_graph_set_tuning(gg_graph_t g, int32_t key, int64_t value);

@@ -116,13 +116,16 @@ def test_empty_result_cannot_be_mapped_again(gg, sym12):
     assert "Sizes Don't match" in str(e.value)
 
 
-@pytest.mark.parametrize("coo_kernel", [0, 1, 2, 3])
-def test_apps_with_each_coo_kernel(gg, orc, coo_kernel):
+@pytest.mark.parametrize("coo_window", [0, 1024, 100000])
+@pytest.mark.parametrize("coo_kernel", [0, 1, 2, 3, 4, 5])
+def test_apps_with_each_coo_kernel(gg, orc, coo_kernel, coo_window):
     """Every COO pull variant (CTA ring, per-warp direct, per-warp 2/3-stage
-    rings) gives the oracle's results when all dense steps use the COO."""
+    rings, lane-contiguous) on every window order gives the oracle's results
+    when all dense steps use the COO."""
     from conftest import PR_MAX_ABS, PR_REL_L1, rel_l1
     hg = gg.HostGraph.rmat(12, 16, seed=81, symmetric=False).add_weights(gg.W_INT32, seed=2, lo=1, hi=100)
-    g = gg.Graph(hg, partitions=ok_partitions(hg, 16), tile_vertices=1024)
+    g = gg.Graph(hg, partitions=ok_partitions(hg, 16), tile_vertices=1024, coo_window=coo_window)
+    assert g.get_tuning(gg.TUNE_COO_KERNEL) == (4 if coo_window else 1)
     g.set_dense_policy(2)
     g.set_tuning(gg.TUNE_COO_KERNEL, coo_kernel)
     assert g.get_tuning(gg.TUNE_COO_KERNEL) == coo_kernel
