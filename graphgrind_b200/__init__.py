@@ -66,6 +66,15 @@ class BuildOpts(C.Structure):
                 ("tile_edges", C.c_int32), ("build_coo", C.c_int32), ("coo_window", C.c_int32)]
 
 
+class TuneTrial(C.Structure):
+    _fields_ = [("dense_policy", C.c_int32), ("coo_kernel", C.c_int32), ("sparse_div", C.c_int32),
+                ("partitions", C.c_int32), ("tile_vertices", C.c_int32), ("tile_edges", C.c_int32),
+                ("coo_window", C.c_int32), ("pad", C.c_int32), ("ms", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
+
+
 class GraphInfo(C.Structure):
     _fields_ = [("n", C.c_uint32), ("m", C.c_uint64), ("symmetric", C.c_int32),
                 ("weight_type", C.c_int32), ("num_partitions", C.c_int32), ("has_coo", C.c_int32),
@@ -154,7 +163,8 @@ _sig("gg_graph_get_profile", C.c_int, _P, C.POINTER(Profile))
 _sig("gg_graph_set_dense_policy", C.c_int, _P, C.c_int32)
 _sig("gg_graph_set_tuning", C.c_int, _P, C.c_int32, C.c_int64)
 _sig("gg_graph_get_tuning", C.c_int, _P, C.c_int32, C.POINTER(C.c_int64))
-TUNE_DENSE_POLICY, TUNE_COO_KERNEL = 1, 2
+TUNE_DENSE_POLICY, TUNE_COO_KERNEL, TUNE_SPARSE_DIV = 1, 2, 3
+APP_BFS, APP_COMPONENTS, APP_PAGERANK, APP_PAGERANK_DELTA, APP_SPMV, APP_BELLMAN_FORD, APP_BC = range(1, 8)
 _sig("gg_vertex_map", C.c_int, _P, _P, C.c_int32, _P)
 _sig("gg_vertex_filter", C.c_int, _P, _P, C.c_int32, _P, C.POINTER(_P))
 _sig("gg_vertex_array_alloc", C.c_int, _P, C.c_size_t, C.POINTER(_P))
@@ -179,6 +189,9 @@ _sig("gg_batch_create", C.c_int, C.c_int32, _P, C.POINTER(_P))
 _sig("gg_batch_destroy", C.c_int, _P)
 _sig("gg_batch_info", C.c_int, _P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), _P)
 _sig("gg_batch_bfs", C.c_int, _P, _P, _P, C.POINTER(RunStats))
+_sig("gg_autotune", C.c_int, _P, C.c_int32, C.c_uint32, _P, C.c_int32, C.POINTER(C.c_int32))
+_sig("gg_autotune_build", C.c_int, _P, C.c_int32, C.c_uint32, _P, C.c_int32, _P, _P)
+_sig("gg_autotune_ppr_k", C.c_int, _P, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double))
 _sig("gg_pagerank_weighted_create", C.c_int, _P, C.c_int32, C.c_float, C.c_int32, C.c_int32, C.POINTER(_P))
 _sig("gg_pagerank_weighted_destroy", C.c_int, _P)
 _sig("gg_pagerank_weighted_fwd", C.c_int, _P, _P, _P, _P, _P, C.POINTER(RunStats))
@@ -201,7 +214,7 @@ EXPORTED = [
     "gg_bfs_push_step_noalloc", "gg_ppr_k", "gg_msbfs", "gg_msbc",
     "gg_batch_create", "gg_batch_destroy", "gg_batch_info", "gg_batch_bfs",
     "gg_pagerank_weighted_create", "gg_pagerank_weighted_destroy", "gg_pagerank_weighted_fwd",
-    "gg_pagerank_weighted_bwd",
+    "gg_pagerank_weighted_bwd", "gg_autotune", "gg_autotune_build", "gg_autotune_ppr_k",
 ]
 
 
@@ -604,6 +617,20 @@ class Graph:
         check(lib.gg_bp(self.h, iters, _ptr(vp), _ptr(ep), _ptr(out), C.byref(st)), "gg_bp")
         return out, _run(st)
 
+    def autotune(self, app=APP_PAGERANK, start=0):
+        """Time `app` under every runtime knob combination; the fastest stays
+        set on the graph.  Returns the trials (dicts), fastest first."""
+        trials = (TuneTrial * 64)()
+        nt = C.c_int32()
+        check(lib.gg_autotune(self.h, app, start, trials, 64, C.byref(nt)), "gg_autotune")
+        return [trials[i].as_dict() for i in range(min(nt.value, 64))]
+
+    def autotune_ppr_k(self, iters=5):
+        """(k, column-edges/s) of the fastest gg_ppr_k column count on this graph."""
+        k, rate = C.c_int32(), C.c_double()
+        check(lib.gg_autotune_ppr_k(self.h, iters, C.byref(k), C.byref(rate)), "gg_autotune_ppr_k")
+        return k.value, rate.value
+
     def msbfs(self, sources, out=None):
         """Levels from up to 64 sources in one traversal: (levels[n, k] int32, Run)."""
         src = np.ascontiguousarray(sources, np.uint32)
@@ -717,3 +744,21 @@ class WeightedPageRank:
             self.close()
         except Exception:
             pass
+
+
+def autotune_build(host, app=APP_PAGERANK, start=0, candidates=()):
+    """Build `host` under each candidate (dicts of Graph keyword options),
+    autotune each, and return (best options dict, best trial dict)."""
+    names = ("partitions", "balance", "part_how", "relabel", "order", "tile_vertices", "tile_edges", "build_coo",
+             "coo_window")
+    defaults = dict(partitions=384, balance=BALANCE_EDGE, part_how=PART_DEST, relabel=0, order=ORDER_HILBERT,
+                    tile_vertices=0, tile_edges=0, build_coo=0, coo_window=0)
+    cands = (BuildOpts * len(candidates))()
+    for i, c in enumerate(candidates):
+        d = dict(defaults, **c)
+        cands[i] = BuildOpts(*[int(d[k]) for k in names])
+    best = BuildOpts()
+    trial = TuneTrial()
+    check(lib.gg_autotune_build(C.byref(host.c), app, start, cands, len(candidates), C.byref(best), C.byref(trial)),
+          "gg_autotune_build")
+    return {k: getattr(best, f) for k, f in zip(names, [f for f, _ in BuildOpts._fields_])}, trial.as_dict()

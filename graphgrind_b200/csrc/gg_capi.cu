@@ -163,7 +163,7 @@ static int run_bfs(gg_graph_s* g, uint32_t start, int32_t* parents, int32_t* lev
     f.round = round;
     trav += F.f->out_edges;
     gg_frontier_s* out = nullptr;
-    GG_TRY(edge_map(g, F.f, f, (int64_t)g->m / 20, 0, &out));
+    GG_TRY(edge_map(g, F.f, f, app_threshold(g), 0, &out));
     F.reset(out);
   }
   const double ms = tm.stop();
@@ -194,7 +194,7 @@ static int run_cc(gg_graph_s* g, int32_t* ids_out, gg_run_stats* st) {
     f.prev = prev.p;
     trav += F.f->out_edges;
     gg_frontier_s* out = nullptr;
-    GG_TRY(edge_map(g, F.f, f, (int64_t)g->m / 20, 0, &out));
+    GG_TRY(edge_map(g, F.f, f, app_threshold(g), 0, &out));
     F.reset(out);
     ++rounds;
   }
@@ -238,7 +238,7 @@ static int run_pagerank(gg_graph_s* g, int max_iter, int bit_all, float* ranks, 
     f.frontier_in_values = masked;
     trav += F.f->out_edges;
     gg_frontier_s* out = nullptr;
-    GG_TRY(edge_map(g, F.f, f, (int64_t)g->m / 20, 0, &out));
+    GG_TRY(edge_map(g, F.f, f, app_threshold(g), 0, &out));
     FrontierHold O;
     O.f = out;
     if (!F.f->bit && !F.f->has_dense) GG_TRY(frontier_to_dense(F.f));
@@ -296,7 +296,7 @@ static int run_pagerank_delta(gg_graph_s* g, float* ranks, gg_run_stats* st) {
     f.acc_out = ngh.p;
     trav += F.f->out_edges;
     gg_frontier_s* out = nullptr;
-    GG_TRY(edge_map(g, F.f, f, (int64_t)g->m / 20, 0, &out));
+    GG_TRY(edge_map(g, F.f, f, app_threshold(g), 0, &out));
     frontier_free(out);
     gg_frontier_s* active = nullptr;
     if (round == 1) {
@@ -342,7 +342,7 @@ static int run_spmv(gg_graph_s* g, const float* x_in, float* y_out, gg_run_stats
   f.y = y.p;
   f.float_w = g->wtype == GG_W_FLOAT32;
   gg_frontier_s* out = nullptr;
-  GG_TRY(edge_map(g, F.f, f, (int64_t)g->m / 20, 0, &out));
+  GG_TRY(edge_map(g, F.f, f, app_threshold(g), 0, &out));
   frontier_free(out);
   const double ms = tm.stop();
   GG_TRY(to_host(g, y_out, y.p, n));
@@ -376,7 +376,7 @@ static int run_bf(gg_graph_s* g, uint32_t start, int32_t* dist, gg_run_stats* st
     f.visited = vis.p;
     trav += F.f->out_edges;
     gg_frontier_s* out = nullptr;
-    GG_TRY(edge_map(g, F.f, f, (int64_t)g->m / 20, 0, &out));
+    GG_TRY(edge_map(g, F.f, f, app_threshold(g), 0, &out));
     VFill<int32_t> vf{vis.p, 0};
     GG_TRY(vertex_map(g, out, vf));
     F.reset(out);
@@ -422,7 +422,7 @@ static int run_bc(gg_graph_s* g, uint32_t start, float* dep_out, float* np_out, 
     f.visited = vis.p;
     trav += F->out_edges;
     gg_frontier_s* out = nullptr;
-    GG_TRY(edge_map(g, F, f, (int64_t)g->m / 20, 0, &out));
+    GG_TRY(edge_map(g, F, f, app_threshold(g), 0, &out));
     VBcMark vm{vis.p};
     GG_TRY(vertex_map(g, out, vm));
     levels.push_back(out);
@@ -444,7 +444,7 @@ static int run_bc(gg_graph_s* g, uint32_t start, float* dep_out, float* np_out, 
     f.visited = vis.p;
     trav += F->out_edges;
     gg_frontier_s* out = nullptr;
-    rc = edge_map(g, F, f, (int64_t)g->m / 20, 0, &out);
+    rc = edge_map(g, F, f, app_threshold(g), 0, &out);
     if (rc) break;
     frontier_free(out);
     F = levels[r];

@@ -15,6 +15,12 @@ const char* last_error();
 // Return `code` after recording a formatted message.
 int fail(int code, const char* fmt, ...);
 
+#define GG_TRY_HOST(expr)         \
+  do {                            \
+    int r__ = (expr);             \
+    if (r__ != GG_OK) return r__; \
+  } while (0)
+
 inline uint64_t mix64(uint64_t z) {
   // SplitMix64 output function (Steele, Lea & Flood, OOPSLA 2014).
   z += 0x9e3779b97f4a7c15ULL;

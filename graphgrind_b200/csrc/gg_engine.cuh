@@ -136,6 +136,7 @@ struct gg_graph_s {
   gg_profile prof{};
   cudaEvent_t prof_ev[2] = {nullptr, nullptr};
   int dense_policy = 0;
+  int sparse_div = 20;  // the apps' edgeMap threshold is m / sparse_div (app/*.C pass m/20)
   int coo_kernel = 1;  // 0 CTA ring (k_pull), 1 per-warp direct loads (fastest measured), 2/3 per-warp bulk-copy rings
   uint64_t device_bytes = 0;
   int kernels = 0;  // kernels launched since the counter was last reset

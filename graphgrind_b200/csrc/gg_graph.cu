@@ -673,6 +673,10 @@ int gg_graph_set_tuning(gg_graph_t g, int32_t key, int64_t value) {
       if (value < 0 || value > 5) return fail(GG_ERR_INVALID_ARG, "COO kernel must be 0..5");
       g->coo_kernel = (int)value;
       return GG_OK;
+    case GG_TUNE_SPARSE_DIV:
+      if (value < 1 || value > (1 << 20)) return fail(GG_ERR_INVALID_ARG, "threshold divisor must be 1..2^20");
+      g->sparse_div = (int)value;
+      return GG_OK;
     default:
       return fail(GG_ERR_INVALID_ARG, "unknown tuning key %d", key);
   }
@@ -686,6 +690,9 @@ int gg_graph_get_tuning(gg_graph_t g, int32_t key, int64_t* value) {
       return GG_OK;
     case GG_TUNE_COO_KERNEL:
       *value = g->coo_kernel;
+      return GG_OK;
+    case GG_TUNE_SPARSE_DIV:
+      *value = g->sparse_div;
       return GG_OK;
     default:
       return fail(GG_ERR_INVALID_ARG, "unknown tuning key %d", key);

@@ -48,6 +48,9 @@ struct DevBuf {
   }
 };
 
+// edgeMap threshold of the application loops: m/20 in app/*.C, m/sparse_div when tuned.
+inline int64_t app_threshold(const gg_graph_s* g) { return (int64_t)g->m / g->sparse_div; }
+
 inline int generic_grid(const gg_graph_s* g, uint64_t work) {
   uint64_t b = (work + kGenericThreads - 1) / kGenericThreads;
   uint64_t cap = (uint64_t)g->num_sms * 8;

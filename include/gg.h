@@ -246,9 +246,12 @@ int gg_graph_set_dense_policy(gg_graph_t g, int32_t policy);
  *                         and one shared-memory accumulation per edge (the
  *                         default for graphs built with coo_window > 0),
  *                         5 per-warp direct loads with the next block's edge
- *                         stream prefetched into registers */
+ *                         stream prefetched into registers
+ *   GG_TUNE_SPARSE_DIV    the application loops (gg_bfs ... gg_bc) call edgeMap
+ *                         with threshold m / value (20 in the reference apps) */
 #define GG_TUNE_DENSE_POLICY 1
 #define GG_TUNE_COO_KERNEL 2
+#define GG_TUNE_SPARSE_DIV 3
 int gg_graph_set_tuning(gg_graph_t g, int32_t key, int64_t value);
 int gg_graph_get_tuning(gg_graph_t g, int32_t key, int64_t* value);
 
@@ -422,6 +425,45 @@ int gg_pagerank_weighted_fwd(gg_wpr_t ctx, const float* weights, const float* te
 /* Given grad_x = dL/dx_iters of the last forward: dL/dweights, dL/dtele, dL/dx0. */
 int gg_pagerank_weighted_bwd(gg_wpr_t ctx, const float* grad_x, float* grad_weights, float* grad_tele,
                              float* grad_x0, gg_run_stats* st);
+
+/* ========================================================= autotuner */
+/* No counterpart in the reference (its knobs are command-line flags).  The
+ * tuner times an application and keeps the fastest knobs; no knob changes
+ * results beyond the summation order of FP32 sums. */
+enum gg_tune_app {
+  GG_APP_BFS = 1,            /* gg_bfs from `start`                 */
+  GG_APP_COMPONENTS = 2,     /* gg_components                       */
+  GG_APP_PAGERANK = 3,       /* gg_pagerank, 10 iterations          */
+  GG_APP_PAGERANK_DELTA = 4, /* gg_pagerank_delta                   */
+  GG_APP_SPMV = 5,           /* gg_spmv with x = 1/n                */
+  GG_APP_BELLMAN_FORD = 6,   /* gg_bellman_ford from `start`        */
+  GG_APP_BC = 7              /* gg_bc from `start`                  */
+};
+typedef struct gg_tune_trial {
+  int32_t dense_policy;   /* GG_TUNE_DENSE_POLICY                       */
+  int32_t coo_kernel;     /* GG_TUNE_COO_KERNEL                         */
+  int32_t sparse_div;     /* GG_TUNE_SPARSE_DIV                         */
+  int32_t partitions;     /* build knobs of gg_autotune_build (else 0)  */
+  int32_t tile_vertices;
+  int32_t tile_edges;
+  int32_t coo_window;
+  int32_t pad;
+  double ms;              /* best of 3 device times of the application  */
+} gg_tune_trial;
+/* Runtime search on a built graph: every combination of dense policy, COO
+ * kernel (where a COO exists) and threshold divisor {20, 10, 40}; the fastest
+ * is left set on g.  trials[max_trials] (may be NULL) receives the trials,
+ * fastest first; *n_trials the number run. */
+int gg_autotune(gg_graph_t g, int32_t app, uint32_t start, gg_tune_trial* trials, int32_t max_trials,
+                int32_t* n_trials);
+/* Build-time search: builds hg under each candidate option set (candidates
+ * the reference partitioner rejects are skipped), runs gg_autotune on each
+ * and returns the fastest options in *best_opts and its trial in *best. */
+int gg_autotune_build(const gg_host_graph* hg, int32_t app, uint32_t start, const gg_build_opts* candidates,
+                      int32_t n_candidates, gg_build_opts* best_opts, gg_tune_trial* best);
+/* Column count for gg_ppr_k on g: the k in {1, 32, 64} with the most
+ * column-edges per second over `iters` iterations. */
+int gg_autotune_ppr_k(gg_graph_t g, int32_t iters, int32_t* best_k, double* column_edges_per_s);
 
 #ifdef __cplusplus
 }
