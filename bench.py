@@ -53,6 +53,9 @@ UNIT = "GTEPS"
 WORKLOAD = ("RMAT-24 directed (n=2^24, edge factor 16, a/b/c/d=.57/.19/.19/.05, seed 2, dedup, FP32 weights U(0,1]), "
             "P=384 edge-balanced Hilbert COO; step = BFS from 100 + PageRank 10 iterations + SpMV")
 HBM_FALLBACK_GBS = 6650.0
+# DRAM bytes per PageRank-pull launch of the default workload, from one ncu
+# capture (profiles/dram_k_pull_coo_w_pagerank_rmat24.md)
+TRAFFIC_RMAT24_PR_PULL = 2175428096
 
 
 def log(*a):
@@ -201,6 +204,10 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
     peak, peak_kind = peak_hbm()
     pull_ms = pr_prof["ms"] / max(pr_prof["launches"], 1)
     algo_bytes = 8 * m + 16 * n
+    traffic, traffic_src = args.traffic, "--traffic" if args.traffic else None
+    if traffic is None and args.scale == 24 and args.partitions == 384 and args.dense_policy == 0:
+        traffic = TRAFFIC_RMAT24_PR_PULL
+        traffic_src = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/dram_k_pull_coo_w_pagerank_rmat24.md"
     achieved = algo_bytes / (pull_ms / 1e3) / 1e9 if pull_ms > 0 else None
     out = {
         "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -217,7 +224,8 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
                      "achieved": round(achieved, 1) if achieved else None, "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4) if achieved else None, "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": algo_bytes, "launch_ms": round(pull_ms, 4),
-                     "launches": pr_prof["launches"], "traffic": args.traffic},
+                     "launches": pr_prof["launches"], "traffic": traffic,
+                     "traffic_source": traffic_src},
         "kernel_profile": {k: {"launches": v["launches"], "ms": round(v["ms"], 3)} for k, v in prof.items()},
         "e2e": {"value": round(e2e, 4), "unit": UNIT, "h2d_bytes_per_step": 4 * n + 4,
                 "d2h_bytes_per_step": 16 * n},
