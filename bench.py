@@ -204,6 +204,10 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
     peak, peak_kind = peak_hbm()
     pull_ms = pr_prof["ms"] / max(pr_prof["launches"], 1)
     algo_bytes = 8 * m + 16 * n
+    coo_names = {0: "k_pull (CTA ring)", 1: "k_pull_coo_w", 2: "k_pull_coo_w (2-stage ring)",
+                 3: "k_pull_coo_w (3-stage ring)", 4: "k_pull_coo_w (lane-contiguous)", 5: "k_pull_coo_w (prefetch)"}
+    kernel_name = coo_names.get(g.get_tuning(gg.TUNE_COO_KERNEL), "k_pull_coo_w") if pr_kind == "coo_pull" \
+        else "k_pull_seg"
     traffic, traffic_src = args.traffic, "--traffic" if args.traffic else None
     if traffic is None and args.scale == 24 and args.partitions == 384 and args.dense_policy == 0:
         traffic = TRAFFIC_RMAT24_PR_PULL
@@ -220,7 +224,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "apps": {k: {"edges": int(v[0]), "ms": round(v[1] / args.steps, 4),
                      "gteps": round(v[0] / (v[1] / 1e3) / 1e9, 4) if v[1] else None} for k, v in per_app.items()},
-        "roofline": {"bound": "hbm", "kernel": f"k_pull ({pr_kind}) in PageRank",
+        "roofline": {"bound": "hbm", "kernel": f"{kernel_name} (PageRank dense pull)",
                      "achieved": round(achieved, 1) if achieved else None, "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4) if achieved else None, "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": algo_bytes, "launch_ms": round(pull_ms, 4),

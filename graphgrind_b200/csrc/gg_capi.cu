@@ -70,23 +70,49 @@ __device__ __forceinline__ void block_add_double(double v, double* out) {
 // plus the next iteration's contrib[j] = p_next[j]/outdeg(j).  When the next
 // frontier's bitmap is given, sources outside it get -1 (contributions are
 // > 0), so the next pull reads membership from the gathered value itself.
+__device__ __forceinline__ float pr_vertex(bool in, float pc, float& pn, uint32_t d, bool next_in, float damping,
+                                           float added, float& contrib, float& pc_out) {
+  if (in) pn = damping * pn + added;
+  const float diff = fabsf(pc - pn);
+  pc_out = in ? 0.0f : diff;
+  contrib = d ? (next_in ? pn / (float)d : -1.0f) : 0.0f;
+  return diff;
+}
+
+// PageRank round epilogue, four vertices per thread with 16-byte accesses:
+// for frontier members p_next = damping * p_next + (1-damping)/n (PR_Vertex_F,
+// app/PageRank.C:84-100), L1 += |p_curr - p_next|, p_curr reset, and the next
+// iteration's contributions p_next/outdeg (-1 for sources outside the next
+// frontier when the frontier is carried in the values).
 __global__ void k_pr_epilogue(uint32_t n, int all, const uint32_t* fbits, float* p_curr, float* p_next,
                               const uint32_t* off, float damping, float added, float* contrib, double* l1,
                               const uint32_t* next_bits) {
   double acc = 0;
-  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x) {
-    const bool in = all || test_bit(fbits, (uint32_t)j);
-    float pn = p_next[j];
-    if (in) {
-      pn = damping * pn + added;
-      p_next[j] = pn;
-    }
-    const float diff = fabsf(p_curr[j] - pn);
-    acc += diff;
-    p_curr[j] = in ? 0.0f : diff;
-    const uint32_t d = off[j + 1] - off[j];
-    const bool next_in = !next_bits || test_bit(next_bits, (uint32_t)j);
-    contrib[j] = d ? (next_in ? pn / (float)d : -1.0f) : 0.0f;
+  const uint64_t n4 = n / 4;
+  for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t j = 4 * q;
+    const float4 pc = reinterpret_cast<const float4*>(p_curr)[q];
+    float4 pn = reinterpret_cast<const float4*>(p_next)[q];
+    const uint32_t o0 = off[j], o1 = off[j + 1], o2 = off[j + 2], o3 = off[j + 3], o4 = off[j + 4];
+    const uint32_t fw = all ? 0xfu : (fbits[j >> 5] >> (j & 31)) & 0xfu;
+    const uint32_t nw = next_bits ? (next_bits[j >> 5] >> (j & 31)) & 0xfu : 0xfu;
+    float4 c, po;
+    acc += pr_vertex(fw & 1u, pc.x, pn.x, o1 - o0, nw & 1u, damping, added, c.x, po.x);
+    acc += pr_vertex(fw & 2u, pc.y, pn.y, o2 - o1, nw & 2u, damping, added, c.y, po.y);
+    acc += pr_vertex(fw & 4u, pc.z, pn.z, o3 - o2, nw & 4u, damping, added, c.z, po.z);
+    acc += pr_vertex(fw & 8u, pc.w, pn.w, o4 - o3, nw & 8u, damping, added, c.w, po.w);
+    reinterpret_cast<float4*>(p_next)[q] = pn;
+    reinterpret_cast<float4*>(p_curr)[q] = po;
+    reinterpret_cast<float4*>(contrib)[q] = c;
+  }
+  for (uint64_t j = 4 * n4 + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+       j += (uint64_t)gridDim.x * blockDim.x) {
+    float pn = p_next[j], c, po;
+    acc += pr_vertex(all || test_bit(fbits, (uint32_t)j), p_curr[j], pn, off[j + 1] - off[j],
+                     !next_bits || test_bit(next_bits, (uint32_t)j), damping, added, c, po);
+    p_next[j] = pn;
+    p_curr[j] = po;
+    contrib[j] = c;
   }
   block_add_double(acc, l1);
 }
