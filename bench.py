@@ -56,6 +56,7 @@ HBM_FALLBACK_GBS = 6650.0
 # DRAM bytes per PageRank-pull launch of the default workload, from one ncu
 # capture (profiles/dram_k_pull_coo_w_pagerank_rmat24.md)
 TRAFFIC_RMAT24_PR_PULL = 2175428096
+TRAFFIC_TILE_EDGES = 1 << 16
 
 
 def log(*a):
@@ -139,7 +140,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
     hg = make_graph(gg, args.scale, 2, gg.W_FLOAT32)
     log(f"[rank {rank}] generated RMAT-{args.scale}: n={hg.n} m={hg.m} in {time.time() - t0:.1f}s")
     t0 = time.time()
-    g = gg.Graph(hg, partitions=args.partitions)
+    g = gg.Graph(hg, partitions=args.partitions, tile_edges=args.tile_edges)
     g.set_dense_policy(args.dense_policy)
     info = g.info()
     log(f"[rank {rank}] device graph built in {time.time() - t0:.1f}s: {info.device_bytes / 2**30:.2f} GiB, "
@@ -150,9 +151,30 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
     par, lev = gg.PinnedArray(n, np.int32), gg.PinnedArray(n, np.int32)
     ranks, y = gg.PinnedArray(n, np.float32), gg.PinnedArray(n, np.float32)
 
+    # runtime knobs per application, chosen by the library's autotuner on this graph
+    knobs = {}
+    tune_s = 0.0
+    if not args.no_autotune:
+        t0 = time.time()
+        for name, app in (("bfs", gg.APP_BFS), ("pagerank", gg.APP_PAGERANK), ("spmv", gg.APP_SPMV)):
+            best = g.autotune(app, start=args.start)[0]
+            knobs[name] = {k: best[k] for k in ("dense_policy", "coo_kernel", "sparse_div")}
+        tune_s = time.time() - t0
+        log(f"[rank {rank}] autotuned in {tune_s:.1f}s: {knobs}")
+
+    def use(name):
+        if name in knobs:
+            kb = knobs[name]
+            g.set_tuning(gg.TUNE_DENSE_POLICY, kb["dense_policy"])
+            g.set_tuning(gg.TUNE_COO_KERNEL, kb["coo_kernel"])
+            g.set_tuning(gg.TUNE_SPARSE_DIV, kb["sparse_div"])
+
     def step():
+        use("bfs")
         _, _, b = g.bfs(args.start, out=(par.array, lev.array))
+        use("pagerank")
         _, p = g.pagerank(10, out=ranks.array)
+        use("spmv")
         _, s = g.spmv(x.array, out=y.array)
         return b, p, s
 
@@ -181,6 +203,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
             launches += r.kernels
     prof = g.profile()
     # PageRank-only profile for the dense-pull roofline (separate, identical calls)
+    use("pagerank")
     for _ in range(2):
         g.pagerank(10, out=ranks.array)
     prof_pr = g.profile()
@@ -209,7 +232,8 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
     kernel_name = coo_names.get(g.get_tuning(gg.TUNE_COO_KERNEL), "k_pull_coo_w") if pr_kind == "coo_pull" \
         else "k_pull_seg"
     traffic, traffic_src = args.traffic, "--traffic" if args.traffic else None
-    if traffic is None and args.scale == 24 and args.partitions == 384 and args.dense_policy == 0:
+    if traffic is None and args.scale == 24 and args.partitions == 384 and args.dense_policy == 0 and \
+            args.tile_edges == TRAFFIC_TILE_EDGES and kernel_name == "k_pull_coo_w":
         traffic = TRAFFIC_RMAT24_PR_PULL
         traffic_src = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/dram_k_pull_coo_w_pagerank_rmat24.md"
     achieved = algo_bytes / (pull_ms / 1e3) / 1e9 if pull_ms > 0 else None
@@ -220,6 +244,8 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
         "data": "synthetic: seeded RMAT generated on the host (no dataset)",
         "config": {"workload": WORKLOAD, "n": n, "m": m, "partitions": args.partitions,
                    "dense_policy": ["reference rule", "csc pull", "coo pull"][args.dense_policy],
+                   "tile_edges": args.tile_edges,
+                   "autotuned_knobs": knobs or None, "autotune_seconds": round(tune_s, 2),
                    "l2": "inputs larger than L2 (graph arrays > 3 GB vs 126 MB L2)",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "apps": {k: {"edges": int(v[0]), "ms": round(v[1] / args.steps, 4),
@@ -430,6 +456,9 @@ def main():
     ap.add_argument("--ref-partitions", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched / adjoint comparisons")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the library's default runtime knobs")
+    ap.add_argument("--tile-edges", type=int, default=1 << 17,
+                    help="target edges per CTA tile (gg_autotune_build's choice for this workload)")
     ap.add_argument("--traffic", type=float, default=None,
                     help="DRAM bytes per dense-pull launch from an ncu capture (reported as roofline.traffic)")
     args = ap.parse_args()

