@@ -181,7 +181,20 @@ static int run_bfs(gg_graph_s* g, uint32_t start, int32_t* parents, int32_t* lev
   GG_TRY(gg_frontier_single(g, start, &F.f));
   int32_t round = 0;
   uint64_t trav = 0;
+  const int64_t thr = app_threshold(g);
   while (F.f->dm > 0) {
+    if (g->device_loop && (int64_t)(F.f->dm + F.f->out_edges) <= thr && F.f->out_edges > 0) {
+      // sparse levels run on the device until the frontier empties or turns dense
+      int32_t levels_run = 0;
+      uint64_t t = 0;
+      gg_frontier_s* cur = F.release();
+      const int rc = bfs_device_levels(g, &cur, par.p, lev.p, round + 1, (uint64_t)thr, &levels_run, &t);
+      F.f = cur;
+      if (rc) return rc;
+      round += levels_run;
+      trav += t;
+      continue;
+    }
     ++round;
     BfsF f;
     f.parents = par.p;
@@ -189,7 +202,7 @@ static int run_bfs(gg_graph_s* g, uint32_t start, int32_t* parents, int32_t* lev
     f.round = round;
     trav += F.f->out_edges;
     gg_frontier_s* out = nullptr;
-    GG_TRY(edge_map(g, F.f, f, app_threshold(g), 0, &out));
+    GG_TRY(edge_map(g, F.f, f, thr, 0, &out));
     F.reset(out);
   }
   const double ms = tm.stop();

@@ -103,6 +103,7 @@ struct Workspace {
   uint32_t bsum_cap = 0;
   double* d_red = nullptr;                // reduction scratch (double)
   double* h_red = nullptr;                // pinned
+  unsigned long long* d_loop = nullptr;   // state of the device-driven level loop (16 words)
 };
 
 }  // namespace gg
@@ -137,6 +138,7 @@ struct gg_graph_s {
   cudaEvent_t prof_ev[2] = {nullptr, nullptr};
   int dense_policy = 0;
   int sparse_div = 20;  // the apps' edgeMap threshold is m / sparse_div (app/*.C pass m/20)
+  int device_loop = 1;  // BFS runs consecutive sparse levels in one cooperative launch
   int coo_kernel = 1;  // 0 CTA ring (k_pull), 1 per-warp direct loads (fastest measured), 2/3 per-warp bulk-copy rings
   uint64_t device_bytes = 0;
   int kernels = 0;  // kernels launched since the counter was last reset

@@ -451,6 +451,7 @@ static void graph_release(gg_graph_s* g) {
   cudaFree(g->ws.d_scan);
   cudaFree(g->ws.d_bsum);
   cudaFree(g->ws.d_red);
+  cudaFree(g->ws.d_loop);
   if (g->ws.h_stats) cudaFreeHost(g->ws.h_stats);
   if (g->ws.h_red) cudaFreeHost(g->ws.h_red);
   for (auto& e : g->prof_ev)
@@ -567,6 +568,7 @@ static int graph_build(const gg_host_graph* hg, const gg_build_opts* opts_in, gg
   GG_CUDA(cudaMemset(g->ws.d_dedup, 0, sizeof(uint32_t) * ((size_t)g->words() + 4)));
   GG_TRY(dev_alloc(g, &g->ws.d_scan, (size_t)n + 4));
   GG_TRY(dev_alloc(g, &g->ws.d_red, 64));
+  GG_TRY(dev_alloc(g, &g->ws.d_loop, 16));
   GG_CUDA(cudaMallocHost((void**)&g->ws.h_red, 64 * sizeof(double)));
   // keep stream-ordered allocations (frontiers) cached in the pool
   cudaMemPool_t pool;
@@ -677,6 +679,10 @@ int gg_graph_set_tuning(gg_graph_t g, int32_t key, int64_t value) {
       if (value < 1 || value > (1 << 20)) return fail(GG_ERR_INVALID_ARG, "threshold divisor must be 1..2^20");
       g->sparse_div = (int)value;
       return GG_OK;
+    case GG_TUNE_DEVICE_LOOP:
+      if (value != 0 && value != 1) return fail(GG_ERR_INVALID_ARG, "device loop switch must be 0 or 1");
+      g->device_loop = (int)value;
+      return GG_OK;
     default:
       return fail(GG_ERR_INVALID_ARG, "unknown tuning key %d", key);
   }
@@ -693,6 +699,9 @@ int gg_graph_get_tuning(gg_graph_t g, int32_t key, int64_t* value) {
       return GG_OK;
     case GG_TUNE_SPARSE_DIV:
       *value = g->sparse_div;
+      return GG_OK;
+    case GG_TUNE_DEVICE_LOOP:
+      *value = g->device_loop;
       return GG_OK;
     default:
       return fail(GG_ERR_INVALID_ARG, "unknown tuning key %d", key);

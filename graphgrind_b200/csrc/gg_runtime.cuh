@@ -65,6 +65,8 @@ int frontier_ensure_queue(gg_frontier_s* f);
 int frontier_to_dense(gg_frontier_s* f);
 int frontier_to_sparse(gg_frontier_s* f);
 void frontier_free(gg_frontier_s* f);
+int bfs_device_levels(gg_graph_s* g, gg_frontier_s** F, int32_t* parents, int32_t* levels, int32_t round0,
+                      uint64_t threshold, int32_t* rounds, uint64_t* trav);
 int reset_stats(gg_graph_s* g);
 int read_stats(gg_graph_s* g);  // blocks; checks the device error word
 

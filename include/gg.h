@@ -248,10 +248,14 @@ int gg_graph_set_dense_policy(gg_graph_t g, int32_t policy);
  *                         5 per-warp direct loads with the next block's edge
  *                         stream prefetched into registers
  *   GG_TUNE_SPARSE_DIV    the application loops (gg_bfs ... gg_bc) call edgeMap
- *                         with threshold m / value (20 in the reference apps) */
+ *                         with threshold m / value (20 in the reference apps)
+ *   GG_TUNE_DEVICE_LOOP   1 (default): gg_bfs runs consecutive sparse levels in
+ *                         one cooperative launch that applies the direction
+ *                         rule on the device; 0: one host round trip per level */
 #define GG_TUNE_DENSE_POLICY 1
 #define GG_TUNE_COO_KERNEL 2
 #define GG_TUNE_SPARSE_DIV 3
+#define GG_TUNE_DEVICE_LOOP 4
 int gg_graph_set_tuning(gg_graph_t g, int32_t key, int64_t value);
 int gg_graph_get_tuning(gg_graph_t g, int32_t key, int64_t* value);
 

@@ -140,3 +140,40 @@ def test_apps_with_each_coo_kernel(gg, orc, coo_kernel, coo_window):
     odep, onp, _ = og.bc(7)
     fin = np.isfinite(odep)
     assert rel_l1(dep[fin], odep[fin]) <= 1e-4
+
+
+@pytest.mark.parametrize("graph", ["grid", "rmat_sym", "rmat_dir", "rmat_dir_t"])
+def test_bfs_device_loop_matches_host_loop(gg, orc, graph):
+    """BFS with consecutive sparse levels in one cooperative launch gives the
+    per-level host loop's levels, level count and traversed edges (and the
+    oracle's), for every push/pull threshold."""
+    if graph == "grid":
+        hg = gg.HostGraph.grid(96, 0.002, seed=5)
+    else:
+        hg = gg.HostGraph.rmat(12, 8, seed=17, symmetric=graph == "rmat_sym")
+    g = gg.Graph(hg, partitions=ok_partitions(hg, 16))
+    oh = hg
+    if graph == "rmat_dir_t":
+        g.transpose()
+        oh = hg.transpose()
+    og = orc.Graph.from_host(oh)
+    assert g.get_tuning(gg.TUNE_DEVICE_LOOP) == 1
+    for div in (20, 2, 1000):
+        g.set_tuning(gg.TUNE_SPARSE_DIV, div)
+        for start in (0, 77):
+            g.set_tuning(gg.TUNE_DEVICE_LOOP, 1)
+            par, lev, run = g.bfs(start)
+            g.set_tuning(gg.TUNE_DEVICE_LOOP, 0)
+            par0, lev0, run0 = g.bfs(start)
+            np.testing.assert_array_equal(lev, lev0)
+            assert run.rounds == run0.rounds and run.edges_traversed == run0.edges_traversed
+            if graph != "rmat_dir_t":
+                # after transpose() the dense COO levels keep the reference's
+                # untransposed COO, which a fresh graph of the transpose does not
+                _, olev, ost = og.bfs(start)
+                np.testing.assert_array_equal(lev, olev)
+                assert run.rounds == ost.rounds and run.edges_traversed == ost.edges_traversed
+            reached = lev >= 0
+            # every reached vertex other than the source has a parent one level up
+            p = par[reached & (lev > 0)]
+            assert np.all(lev[p] == lev[reached & (lev > 0)] - 1)
