@@ -207,6 +207,11 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
     for _ in range(2):
         g.pagerank(10, out=ranks.array)
     prof_pr = g.profile()
+    # SpMV-only profile for its own roofline line
+    use("spmv")
+    for _ in range(2):
+        g.spmv(x.array, out=y.array)
+    prof_sp = g.profile()
     g.set_profiling(False)
     clk = clocks.stop()
     for k in ("csc_pull", "coo_pull"):
@@ -231,6 +236,16 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
                  3: "k_pull_coo_w (3-stage ring)", 4: "k_pull_coo_w (lane-contiguous)", 5: "k_pull_coo_w (prefetch)"}
     kernel_name = coo_names.get(g.get_tuning(gg.TUNE_COO_KERNEL), "k_pull_coo_w") if pr_kind == "coo_pull" \
         else "k_pull_seg"
+    # per-application dense-pull rooflines (SURVEY 8d bytes): PageRank 8m+16n, SpMV 12m+12n
+    roofline_by_app = {}
+    for app, pf, bytes_ in (("pagerank", prof_pr, 8 * m + 16 * n), ("spmv", prof_sp, 12 * m + 12 * n)):
+        kind = max(("coo_pull", "csc_pull"), key=lambda k: pf[k]["launches"])
+        if pf[kind]["launches"]:
+            lm = pf[kind]["ms"] / pf[kind]["launches"]
+            ach = bytes_ / (lm / 1e3) / 1e9
+            roofline_by_app[app] = {"kernel": kind, "launch_ms": round(lm, 4), "algorithmic_bytes": bytes_,
+                                    "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                                    "frac": round(ach / peak, 4)}
     traffic, traffic_src = args.traffic, "--traffic" if args.traffic else None
     if traffic is None and args.scale == 24 and args.partitions == 384 and args.dense_policy == 0 and \
             args.tile_edges == TRAFFIC_TILE_EDGES and kernel_name == "k_pull_coo_w":
@@ -256,6 +271,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
                      "algorithmic_bytes_per_launch": algo_bytes, "launch_ms": round(pull_ms, 4),
                      "launches": pr_prof["launches"], "traffic": traffic,
                      "traffic_source": traffic_src},
+        "roofline_by_app": roofline_by_app,
         "kernel_profile": {k: {"launches": v["launches"], "ms": round(v["ms"], 3)} for k, v in prof.items()},
         "e2e": {"value": round(e2e, 4), "unit": UNIT, "h2d_bytes_per_step": 4 * n + 4,
                 "d2h_bytes_per_step": 16 * n},

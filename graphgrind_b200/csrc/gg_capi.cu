@@ -382,7 +382,7 @@ static int run_spmv(gg_graph_s* g, const float* x_in, float* y_out, gg_run_stats
   f.y = y.p;
   f.float_w = g->wtype == GG_W_FLOAT32;
   gg_frontier_s* out = nullptr;
-  GG_TRY(edge_map(g, F.f, f, app_threshold(g), 0, &out));
+  GG_TRY(edge_map(g, F.f, f, app_threshold(g), GG_EM_NO_OUTPUT, &out));  // output.del()
   frontier_free(out);
   const double ms = tm.stop();
   GG_TRY(to_host(g, y_out, y.p, n));

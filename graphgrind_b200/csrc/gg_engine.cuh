@@ -460,8 +460,12 @@ __host__ __device__ constexpr size_t coo_w_smem_bytes(bool hw, int stages, int v
 #ifndef GG_COO_MIN_BLOCKS
 #define GG_COO_MIN_BLOCKS 4  // resident CTAs per SM the register allocation must allow
 #endif
-template <class F, bool HW, bool ALL, int STAGES, bool CONTIG = false, bool PF = false>
+// NOOUT: the caller discards edgeMap's output (GG_EM_NO_OUTPUT) and F's
+// commit of the identity is a no-op (sums): no touched flags, no next-frontier
+// bits, no stats; destinations with a non-identity sum are committed.
+template <class F, bool HW, bool ALL, int STAGES, bool CONTIG = false, bool PF = false, bool NOOUT = false>
 __global__ void __launch_bounds__(kCooThreads, GG_COO_MIN_BLOCKS) k_pull_coo_w(const PullParams p, const F f) {
+  static_assert(!NOOUT || F::kIdentityCommitNoop, "discarding the output needs a no-op identity commit");
   static_assert(!CONTIG || STAGES == 0, "lane-contiguous edges use direct loads");
   static_assert(!PF || (STAGES == 0 && !CONTIG), "register prefetch applies to direct loads");
   using V = typename F::value_t;
@@ -497,7 +501,7 @@ __global__ void __launch_bounds__(kCooThreads, GG_COO_MIN_BLOCKS) k_pull_coo_w(c
     const uint32_t v0 = td.x, nv = td.y, e0 = td.z, ne = td.w;  // e0, ne multiples of 8
     for (uint32_t i = tid; i < nv; i += kCooThreads) {
       s_acc[i] = F::identity();
-      if (!F::kPositive) s_touch[i] = 0;
+      if (!F::kPositive && !NOOUT) s_touch[i] = 0;
       s_cond[i] = (F::kCondTrue || f.cond(v0 + i)) ? 1 : 0;
     }
     __syncthreads();
@@ -645,7 +649,7 @@ __global__ void __launch_bounds__(kCooThreads, GG_COO_MIN_BLOCKS) k_pull_coo_w(c
         for (int k = 0; k < 8; ++k) {
           if (!vld[k]) continue;
           F::atomic_combine(&s_acc[dv[k]], val[k]);
-          if (!F::kPositive) s_touch[dv[k]] = 1;
+          if (!F::kPositive && !NOOUT) s_touch[dv[k]] = 1;
         }
         continue;
       }
@@ -658,7 +662,7 @@ __global__ void __launch_bounds__(kCooThreads, GG_COO_MIN_BLOCKS) k_pull_coo_w(c
         if (l != cur) {
           if (cur >= 0) {
             F::atomic_combine(&s_acc[cur], acc);
-            if (!F::kPositive) s_touch[cur] = 1;
+            if (!F::kPositive && !NOOUT) s_touch[cur] = 1;
           }
           cur = l;
           acc = val[k];
@@ -673,15 +677,21 @@ __global__ void __launch_bounds__(kCooThreads, GG_COO_MIN_BLOCKS) k_pull_coo_w(c
         for (int o = 16; o > 0; o >>= 1) r = F::combine(r, __shfl_xor_sync(0xffffffffu, r, o));
         if (lane == 0) {
           F::atomic_combine(&s_acc[c0], r);
-          if (!F::kPositive) s_touch[c0] = 1;
+          if (!F::kPositive && !NOOUT) s_touch[c0] = 1;
         }
       } else if (cur >= 0) {
         F::atomic_combine(&s_acc[cur], acc);
-        if (!F::kPositive) s_touch[cur] = 1;
+        if (!F::kPositive && !NOOUT) s_touch[cur] = 1;
       }
     }
     __syncthreads();
     if (s_fail) break;
+    if constexpr (NOOUT) {
+      for (uint32_t l = tid; l < nv; l += kCooThreads)
+        if (s_acc[l] != F::identity() && s_cond[l]) f.commit(v0 + l, s_acc[l]);
+      __syncthreads();
+      continue;
+    }
     const uint32_t base0 = v0 & ~31u;
     for (uint32_t bb = base0 + (uint32_t)warp * 32u; bb < v0 + nv; bb += kCooThreads) {
       const uint32_t v = bb + (uint32_t)lane;

@@ -10,6 +10,7 @@ namespace gg {
 
 struct MinI32 {
   using value_t = int32_t;
+  static constexpr bool kIdentityCommitNoop = false;
   bool frontier_in_values = false;  // gathered values already mark frontier membership
   __device__ static value_t identity() { return 0x7fffffff; }
   __device__ static value_t combine(value_t a, value_t b) { return a < b ? a : b; }
@@ -17,6 +18,7 @@ struct MinI32 {
 };
 struct MinU32 {
   using value_t = uint32_t;
+  static constexpr bool kIdentityCommitNoop = false;
   bool frontier_in_values = false;  // gathered values already mark frontier membership
   __device__ static value_t identity() { return 0xffffffffu; }
   __device__ static value_t combine(value_t a, value_t b) { return a < b ? a : b; }
@@ -24,6 +26,7 @@ struct MinU32 {
 };
 struct SumF32 {
   using value_t = float;
+  static constexpr bool kIdentityCommitNoop = false;  // set by functors whose commit is "+= acc" alone
   bool frontier_in_values = false;  // gathered values already mark frontier membership
   __device__ static value_t identity() { return 0.0f; }
   __device__ static value_t combine(value_t a, value_t b) { return a + b; }
@@ -117,6 +120,7 @@ using PrPosF = PrT<true>;
 // SPMV_F, app/SPMV.C:7-47: p_next[d] += p_curr[s] * edgeLen.  Weights are
 // the reference's int edge lengths, or FP32 when the graph carries FP32 weights.
 struct SpmvF : SumF32 {
+  static constexpr bool kIdentityCommitNoop = true;  // commit is y[d] += acc
   static constexpr bool kPositive = false;
   static constexpr bool kEarlyExit = false;
   static constexpr bool kCondTrue = true;

@@ -73,7 +73,7 @@ int read_stats(gg_graph_s* g);  // blocks; checks the device error word
 // -------------------------------------------------------------- edgeMap
 // graphgrind/ligra-numa.h:919-1019
 template <class F, bool HW>
-int pull_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f, bool coo) {
+int pull_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f, bool coo, bool no_out = false) {
   // a positive functor whose gathered values already mark the frontier needs no bitmap
   const bool all = in->bit || (F::kPositive && f.frontier_in_values);
   PullParams p{};
@@ -128,6 +128,7 @@ int pull_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f
   if (coo && g->coo_kernel > 0) {  // per-warp COO pull: 0, 2 or 3 staging stages
     static bool opted[2][4] = {};
     static bool opted_pf[2] = {};
+    static bool opted_no[2] = {};
     auto launch_w = [&](auto kern, int stages, bool& done) -> int {
       const size_t smem = coo_w_smem_bytes(kHW, stages, 4, p.tv);
       if (!done) {
@@ -144,6 +145,11 @@ int pull_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f
       g->kernels++;
       return GG_OK;
     };
+    if constexpr (F::kIdentityCommitNoop) {
+      if (no_out && g->coo_kernel == 1)
+        return all ? launch_w(k_pull_coo_w<F, kHW, true, 0, false, false, true>, 0, opted_no[1])
+                   : launch_w(k_pull_coo_w<F, kHW, false, 0, false, false, true>, 0, opted_no[0]);
+    }
     switch (g->coo_kernel) {
       case 5:
         return all ? launch_w(k_pull_coo_w<F, kHW, true, 0, false, true>, 0, opted_pf[1])
@@ -300,6 +306,9 @@ int edge_map(gg_graph_s* g, gg_frontier_s* in, const F& f, int64_t threshold, ui
     if (flags & GG_EM_FORCE_CSC) coo = false;
     if ((flags & GG_EM_FORCE_COO) && g->has_coo) coo = true;
     const bool early = !coo && F::kEarlyExit;
+    // GG_EM_NO_OUTPUT: the caller discards the output, which the COO pull of a
+    // sum functor then does not build
+    const bool no_out = (flags & GG_EM_NO_OUTPUT) && coo && F::kIdentityCommitNoop;
     if (!in->bit && !in->has_dense) rc = frontier_to_dense(in);
     if (!rc) rc = frontier_ensure_bits(o, true);
     if (!rc) rc = reset_stats(g);
@@ -308,11 +317,16 @@ int edge_map(gg_graph_s* g, gg_frontier_s* in, const F& f, int64_t threshold, ui
       if (early)
         rc = hw ? pull_early_launch<F, true>(g, in, o, f) : pull_early_launch<F, false>(g, in, o, f);
       else
-        rc = hw ? pull_launch<F, true>(g, in, o, f, coo) : pull_launch<F, false>(g, in, o, f, coo);
+        rc = hw ? pull_launch<F, true>(g, in, o, f, coo, no_out) : pull_launch<F, false>(g, in, o, f, coo, no_out);
       if (g->profiling) cudaEventRecord(g->prof_ev[1], g->stream);
     }
     if (!rc) rc = read_stats(g);
-    if (!rc) {
+    if (!rc && no_out) {  // an output nobody reads: empty
+      o->dm = 0;
+      o->out_edges = 0;
+      g->last.kind = 3;
+      prof_end(2, g->coo_len);
+    } else if (!rc) {
       o->has_dense = true;
       o->dm = g->ws.h_stats[0];
       o->out_edges = g->ws.h_stats[1];

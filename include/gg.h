@@ -205,7 +205,9 @@ typedef struct { const float* edge_pot; const float* vert_pot; const float* edge
 #define GG_EM_FORCE_SPARSE 0x1u   /* take the push branch regardless of size   */
 #define GG_EM_FORCE_CSC 0x2u      /* dense branch: pull over CSC                */
 #define GG_EM_FORCE_COO 0x4u      /* dense branch: partitioned COO              */
-#define GG_EM_NO_OUTPUT 0x8u      /* caller discards the output (output.del())  */
+#define GG_EM_NO_OUTPUT 0x8u      /* caller discards the output (output.del()):
+                                     a dense COO pull of a sum functor (GG_F_SPMV)
+                                     then skips building it and *out is empty  */
 
 /* Per-call statistics of the last edgeMap on a graph handle. */
 typedef struct gg_edge_map_stats {

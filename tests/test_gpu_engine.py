@@ -177,3 +177,21 @@ def test_bfs_device_loop_matches_host_loop(gg, orc, graph):
             # every reached vertex other than the source has a parent one level up
             p = par[reached & (lev > 0)]
             assert np.all(lev[p] == lev[reached & (lev > 0)] - 1)
+
+
+@pytest.mark.parametrize("force", ["coo", "csc", "sparse"])
+def test_spmv_edge_map_without_output(gg, sym12, force):
+    """GG_EM_NO_OUTPUT keeps the SPMV sums; the dense COO pull then returns an
+    empty output instead of building it."""
+    hg, g, _ = sym12
+    flags = {"sparse": gg.EM_FORCE_SPARSE, "csc": gg.EM_FORCE_CSC, "coo": gg.EM_FORCE_COO}[force]
+    x = gg.DeviceArray(g, np.float32, np.random.default_rng(1).random(hg.n, dtype=np.float32))
+    y0 = gg.DeviceArray(g, np.float32, 0)
+    y1 = gg.DeviceArray(g, np.float32, 0)
+    F = g.frontier_all()
+    out0 = g.edge_map(F, gg.F_SPMV, gg.PairArgs(x.ptr, y0.ptr), -1, flags)
+    out1 = g.edge_map(F, gg.F_SPMV, gg.PairArgs(x.ptr, y1.ptr), -1, flags | gg.EM_NO_OUTPUT)
+    # the order of shared-memory accumulations varies from run to run
+    np.testing.assert_allclose(y0.download(), y1.download(), rtol=2e-6)
+    if force == "coo":
+        assert out1.stats()[0] == 0 and out0.stats()[0] > 0
