@@ -242,13 +242,12 @@ __global__ void k_coo_keys(const uint32_t* src, const uint32_t* dst, uint64_t m,
 // the Hilbert order, and inside a window edges go by destination, so that a
 // thread's 8 consecutive edges form destination runs while the window keeps
 // the Hilbert locality of its sources.  key = window << 12 | local destination.
-constexpr int kCooWindow = 256;
 __global__ void k_coo_window_keys(const uint4* seg, uint32_t ntiles, const uint32_t* perm, const uint32_t* dst,
-                                  uint32_t* keys) {
+                                  uint32_t window, uint32_t* keys) {
   for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const uint4 s = seg[t];  // {v0, nv, e0 (CSC), ne}
     for (uint32_t i = threadIdx.x; i < s.w; i += blockDim.x)
-      keys[s.z + i] = ((i / kCooWindow) << 12) | (dst[perm[s.z + i]] - s.x);
+      keys[s.z + i] = ((i / window) << 12) | (dst[perm[s.z + i]] - s.x);
   }
 }
 
@@ -385,7 +384,8 @@ static int build_coo(gg_graph_s* g, const uint32_t* h_in_off) {
       // destination order inside 256-edge windows (the u64 key buffers are reused as u32)
       uint32_t* k32 = reinterpret_cast<uint32_t*>(d_keys);
       uint32_t* k32_out = reinterpret_cast<uint32_t*>(d_keys_out);
-      k_coo_window_keys<<<grid, 256>>>(d_segs, (uint32_t)segs.size(), d_perm, d_dst, k32);
+      k_coo_window_keys<<<grid, 256>>>(d_segs, (uint32_t)segs.size(), d_perm, d_dst,
+                                       (uint32_t)g->opts.coo_dst_window, k32);
       GG_BUILD(cudaGetLastError());
       size_t temp2 = 0;
       GG_BUILD(cub::DeviceSegmentedRadixSort::SortPairs(nullptr, temp2, k32, k32_out, d_perm, d_vals, (int)m,
@@ -470,6 +470,8 @@ static int graph_build(const gg_host_graph* hg, const gg_build_opts* opts_in, gg
   if (o.tile_edges <= 0) o.tile_edges = 1 << 16;
   if (o.coo_window < 0) o.coo_window = 0;
   if (o.coo_window > 0) o.coo_window = (o.coo_window + kSegBlock - 1) / kSegBlock * kSegBlock;
+  if (o.coo_dst_window <= 0) o.coo_dst_window = kSegBlock;
+  o.coo_dst_window = std::min((o.coo_dst_window + kSegBlock - 1) / kSegBlock * kSegBlock, 1 << 16);
   if (o.order != GG_ORDER_CSR) o.order = GG_ORDER_HILBERT;
   if (o.part_how == GG_PART_SOURCE)
     return fail(GG_ERR_UNSUPPORTED, "-P source partitioning is not supported by this build");

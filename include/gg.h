@@ -66,6 +66,8 @@ typedef struct gg_build_opts {
                                W > 0 = source order inside windows of W edges
                                (rounded up to a multiple of 256), which lets a
                                warp's 32 gathers share cache lines          */
+  int32_t coo_dst_window;   /* GPU: edges per destination-ordered window when
+                               coo_window == 0 (multiple of 256; 0 = 256)    */
 } gg_build_opts;
 
 typedef struct gg_graph_info {
