@@ -283,12 +283,27 @@ struct MsPull {
   uint64_t* out;
 };
 
+#ifndef GG_MS_MIN_BLOCKS
+#define GG_MS_MIN_BLOCKS 3  // resident CTAs per SM the register allocation must allow (3: fastest measured)
+#endif
+// Dynamic shared memory per CTA (8 warps): row filters and rows of the block,
+// and for VALS the active edges' masks, sources and row slots.
+template <bool VALS>
+constexpr size_t ms_pull_smem() {
+  return 8 * (kSegBlock + 1) * (8 + 4) + (VALS ? 8 * kSegBlock * (8 + 4 + 2) : 0);
+}
+
 template <bool VALS, bool OUT>
-__global__ void __launch_bounds__(256) k_ms_pull(MsPull p) {
-  __shared__ uint64_t s_filt[8][kSegBlock + 1];
-  __shared__ uint32_t s_row[8][kSegBlock + 1];
-  __shared__ uint64_t s_em[VALS ? 8 : 1][kSegBlock];
-  __shared__ uint16_t s_rel[VALS ? 8 : 1][kSegBlock];
+__global__ void __launch_bounds__(256, GG_MS_MIN_BLOCKS) k_ms_pull(MsPull p) {
+  extern __shared__ __align__(16) unsigned char ms_smem[];
+  auto s_filt = reinterpret_cast<uint64_t(*)[kSegBlock + 1]>(ms_smem);
+  auto s_em = reinterpret_cast<uint64_t(*)[kSegBlock]>(ms_smem + 8 * (kSegBlock + 1) * 8);
+  auto s_row = reinterpret_cast<uint32_t(*)[kSegBlock + 1]>(ms_smem + 8 * (kSegBlock + 1) * 8 +
+                                                            (VALS ? 8 * kSegBlock * 8 : 0));
+  auto s_src = reinterpret_cast<uint32_t(*)[kSegBlock]>(reinterpret_cast<unsigned char*>(s_row) +
+                                                        8 * (kSegBlock + 1) * 4);
+  auto s_rel = reinterpret_cast<uint16_t(*)[kSegBlock]>(reinterpret_cast<unsigned char*>(s_src) +
+                                                        (VALS ? 8 * kSegBlock * 4 : 0));
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t lanemask_le = 0xffffffffu >> (31 - lane);
   const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
@@ -323,6 +338,7 @@ __global__ void __launch_bounds__(256) k_ms_pull(MsPull p) {
       uint64_t x = (e < p.m && f) ? (__ldg(p.edge_mask + y) & f) : 0ull;
       if (VALS) {
         s_em[warp][32 * i + lane] = x;
+        s_src[warp][32 * i + lane] = y;
         s_rel[warp][32 * i + lane] = (uint16_t)rel;
         act[i] = __ballot_sync(0xffffffffu, x != 0);
       }
@@ -395,7 +411,7 @@ __global__ void __launch_bounds__(256) k_ms_pull(MsPull p) {
           if (el[q] != 0xffffffffu) {
             em[q] = s_em[warp][el[q]];
             if ((uint32_t)(em[q] >> (2 * lane)) & 3u)
-              v[q] = __ldg(reinterpret_cast<const float2*>(p.vals + (uint64_t)__ldg(p.idx + e0 + el[q]) * 64) + lane);
+              v[q] = __ldg(reinterpret_cast<const float2*>(p.vals + (uint64_t)s_src[warp][el[q]] * 64) + lane);
           }
         }
 #pragma unroll
@@ -533,12 +549,20 @@ static int ms_pull(gg_graph_s* g, bool vals, bool out, bool forward, const uint6
   p.vals = v;
   p.out = o;
   const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((p.nblocks + 7) / 8, (uint64_t)g->num_sms * 8));
+  static bool opted = false;
+  if (!opted) {
+    GG_CUDA(cudaFuncSetAttribute(k_ms_pull<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)ms_pull_smem<true>()));
+    GG_CUDA(cudaFuncSetAttribute(k_ms_pull<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)ms_pull_smem<true>()));
+    opted = true;
+  }
   if (vals && out)
-    k_ms_pull<true, true><<<grid, 256, 0, g->stream>>>(p);
+    k_ms_pull<true, true><<<grid, 256, ms_pull_smem<true>(), g->stream>>>(p);
   else if (vals)
-    k_ms_pull<true, false><<<grid, 256, 0, g->stream>>>(p);
+    k_ms_pull<true, false><<<grid, 256, ms_pull_smem<true>(), g->stream>>>(p);
   else
-    k_ms_pull<false, true><<<grid, 256, 0, g->stream>>>(p);
+    k_ms_pull<false, true><<<grid, 256, ms_pull_smem<false>(), g->stream>>>(p);
   g->kernels++;
   return GG_OK;
 }
