@@ -183,6 +183,7 @@ _sig("gg_bellman_ford", C.c_int, _P, C.c_uint32, _P, C.POINTER(RunStats))
 _sig("gg_bc", C.c_int, _P, C.c_uint32, _P, _P, C.POINTER(RunStats))
 _sig("gg_bp", C.c_int, _P, C.c_int32, _P, _P, _P, C.POINTER(RunStats))
 _sig("gg_bfs_push_step_noalloc", C.c_int, _P, _P, C.c_uint32, _P, C.c_uint32, _P, _P, C.c_int32, _P, _P, _P)
+_sig("gg_pagerank_converge", C.c_int, _P, C.c_int32, C.c_double, _P, C.POINTER(RunStats))
 _sig("gg_ppr_k", C.c_int, _P, C.c_int32, C.c_int32, C.c_float, _P, _P, _P, C.POINTER(RunStats))
 _sig("gg_msbfs", C.c_int, _P, C.c_int32, _P, _P, C.POINTER(RunStats))
 _sig("gg_msbc", C.c_int, _P, C.c_int32, _P, _P, _P, C.POINTER(RunStats))
@@ -212,7 +213,7 @@ EXPORTED = [
     "gg_graph_set_dense_policy", "gg_graph_set_tuning", "gg_graph_get_tuning", "gg_vertex_map", "gg_vertex_filter", "gg_vertex_array_alloc",
     "gg_vertex_array_free", "gg_memcpy_h2d", "gg_memcpy_d2h", "gg_host_alloc_pinned", "gg_host_free_pinned", "gg_bfs", "gg_components",
     "gg_pagerank", "gg_pagerank_delta", "gg_spmv", "gg_bellman_ford", "gg_bc", "gg_bp",
-    "gg_bfs_push_step_noalloc", "gg_ppr_k", "gg_msbfs", "gg_msbc",
+    "gg_bfs_push_step_noalloc", "gg_ppr_k", "gg_pagerank_converge", "gg_msbfs", "gg_msbc",
     "gg_batch_create", "gg_batch_destroy", "gg_batch_info", "gg_batch_bfs",
     "gg_pagerank_weighted_create", "gg_pagerank_weighted_destroy", "gg_pagerank_weighted_fwd",
     "gg_pagerank_weighted_bwd", "gg_autotune", "gg_autotune_build", "gg_autotune_ppr_k",
@@ -593,6 +594,13 @@ class Graph:
         st = RunStats()
         check(lib.gg_bellman_ford(self.h, start, _ptr(d), C.byref(st)), "gg_bellman_ford")
         return d, _run(st)
+
+    def pagerank_converge(self, max_iter=100, eps=1e-7, out=None):
+        """app/PageRankConverage.C: (ranks, Run)."""
+        r = out if out is not None else np.empty(self.n, np.float32)
+        st = RunStats()
+        check(lib.gg_pagerank_converge(self.h, max_iter, eps, _ptr(r), C.byref(st)), "gg_pagerank_converge")
+        return r, _run(st)
 
     def ppr_k(self, k=64, iters=20, damping=0.85, tele=None, seeds=None, out=None):
         """k-column personalised PageRank; returns (X[n, k] float32, Run)."""

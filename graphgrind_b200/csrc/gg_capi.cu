@@ -304,6 +304,94 @@ static int run_pagerank(gg_graph_s* g, int max_iter, int bit_all, float* ranks, 
   return GG_OK;
 }
 
+// PageRankConverage (app/PageRankConverage.C:243-310) kernels.  Sums are
+// accumulated in FP64 like the reference's sum()/normdiff().
+// Next contributions: add_factor = (0.85 / outdeg) * p (sinks are never gathered).
+__global__ void k_prc_contrib(uint32_t n, const float* p, const uint32_t* off, float* contrib) {
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t d = off[j + 1] - off[j];
+    contrib[j] = d ? (0.85f / (float)d) * p[j] : 0.0f;
+  }
+}
+__global__ void k_prc_sum(uint32_t n, const float* a, double* out) {
+  double acc = 0;
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x)
+    acc += a[j];
+  block_add_double(acc, out);
+}
+// p_next += (1 - sum)/n (PR_Vertex_Csum), L1 = sum |p_curr - p_next| (normdiff), and the new sum.
+__global__ void k_prc_fix(uint32_t n, const float* p_curr, float* p_next, const double* red, double* l1,
+                          double* sum2) {
+  const float c = (float)((1.0 - red[0]) / (double)n);
+  double a = 0, b = 0;
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x) {
+    const float pn = p_next[j] + c;
+    p_next[j] = pn;
+    a += fabsf(p_curr[j] - pn);
+    b += pn;
+  }
+  block_add_double(a, l1);
+  __syncthreads();
+  block_add_double(b, sum2);
+}
+// p_next /= sum (PR_Vertex_norm), p_curr = 0 (PR_Vertex_Reset), next contributions from p_next.
+__global__ void k_prc_norm(uint32_t n, float* p_curr, float* p_next, const double* sum2, const uint32_t* off,
+                           float* contrib) {
+  const float inv = (float)(1.0 / sum2[0]);
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x) {
+    const float pn = p_next[j] * inv;
+    p_next[j] = pn;
+    p_curr[j] = 0.0f;
+    const uint32_t d = off[j + 1] - off[j];
+    contrib[j] = d ? (0.85f / (float)d) * pn : 0.0f;
+  }
+}
+
+static int run_pagerank_converge(gg_graph_s* g, int32_t max_iter, double eps, float* ranks, gg_run_stats* st) {
+  const uint32_t n = g->n;
+  g->kernels = 0;
+  DevBuf<float> a, b, contrib;
+  GG_TRY(a.alloc(g, n));
+  GG_TRY(b.alloc(g, n));
+  GG_TRY(contrib.alloc(g, n));
+  double* red = g->ws.d_red;  // [0] sum after the edgeMap, [1] L1, [2] sum after the correction
+  EventTimer tm(g->stream);
+  float* p_curr = a.p;
+  float* p_next = b.p;
+  const int grid = generic_grid(g, n);
+  GG_TRY(fill<float>(g, p_curr, n, (float)(1 / (double)n)));
+  GG_TRY(fill<float>(g, p_next, n, 0.0f));
+  k_prc_contrib<<<grid, kGenericThreads, 0, g->stream>>>(n, p_curr, g->out_off(), contrib.p);
+  g->kernels++;
+  FrontierHold F;
+  GG_TRY(gg_frontier_all(g, &F.f));  // partitioned_vertices::bits
+  int count = 0;
+  double L1 = 2;
+  while (count < max_iter && L1 > eps) {
+    PrPosF f;
+    f.contrib = contrib.p;
+    f.acc_out = p_next;
+    gg_frontier_s* out = nullptr;
+    GG_TRY(edge_map(g, F.f, f, app_threshold(g), GG_EM_NO_OUTPUT, &out));  // output.del()
+    frontier_free(out);
+    GG_CUDA(cudaMemsetAsync(red, 0, 3 * sizeof(double), g->stream));
+    k_prc_sum<<<grid, kGenericThreads, 0, g->stream>>>(n, p_next, red);
+    k_prc_fix<<<grid, kGenericThreads, 0, g->stream>>>(n, p_curr, p_next, red, red + 1, red + 2);
+    k_prc_norm<<<grid, kGenericThreads, 0, g->stream>>>(n, p_curr, p_next, red + 2, g->out_off(), contrib.p);
+    GG_CUDA(cudaGetLastError());
+    g->kernels += 3;
+    GG_CUDA(cudaMemcpyAsync(g->ws.h_red, red, 3 * sizeof(double), cudaMemcpyDeviceToHost, g->stream));
+    GG_CUDA(cudaStreamSynchronize(g->stream));
+    L1 = g->ws.h_red[1];
+    ++count;
+    std::swap(p_curr, p_next);
+  }
+  const double ms = tm.stop();
+  GG_TRY(to_host(g, ranks, p_curr, n));
+  fill_stats(st, ms, count, (uint64_t)count * g->m, g->kernels);
+  return GG_OK;
+}
+
 // app/PageRankDelta.C:120-174
 static int run_pagerank_delta(gg_graph_s* g, float* ranks, gg_run_stats* st) {
   const uint32_t n = g->n;
@@ -660,6 +748,10 @@ int gg_pagerank(gg_graph_t g, int32_t max_iter, int32_t bit_all, float* ranks, g
 int gg_pagerank_delta(gg_graph_t g, float* ranks, gg_run_stats* st) {
   if (!g) return fail(GG_ERR_INVALID_ARG, "gg_pagerank_delta: null graph");
   return run_pagerank_delta(g, ranks, st);
+}
+int gg_pagerank_converge(gg_graph_t g, int32_t max_iter, double eps, float* ranks, gg_run_stats* st) {
+  if (!graph_live(g) || max_iter < 0 || !ranks) return fail(GG_ERR_INVALID_ARG, "gg_pagerank_converge: bad arguments");
+  return run_pagerank_converge(g, max_iter, eps, ranks, st);
 }
 int gg_spmv(gg_graph_t g, const float* x, float* y, gg_run_stats* st) {
   if (!g) return fail(GG_ERR_INVALID_ARG, "gg_spmv: null graph");

@@ -97,6 +97,7 @@ struct CcF : MinI32 {
 // needs no separate "touched" flag.  PageRankDelta's Delta can be 0 or < 0.
 template <bool POS>
 struct PrT : SumF32 {
+  static constexpr bool kIdentityCommitNoop = true;  // commit is acc_out[d] += acc
   static constexpr bool kEarlyExit = false;
   static constexpr bool kCondTrue = true;
   static constexpr bool kPositive = POS;

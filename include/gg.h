@@ -339,6 +339,11 @@ int gg_components(gg_graph_t g, int32_t* ids, gg_run_stats* st);
 /* app/PageRank.C:330-378 (bit_all=0) and app/PageRankBit.C (bit_all=1):
  * ranks[n] in FP32, max_iter iterations (10 in the reference). */
 int gg_pagerank(gg_graph_t g, int32_t max_iter, int32_t bit_all, float* ranks, gg_run_stats* st);
+/* app/PageRankConverage.C:243-310: PageRank whose dangling mass is spread
+ * evenly and whose ranks are renormalised every iteration, until the L1
+ * change is at most eps or max_iter iterations ran (100 and 1e-7 in the
+ * reference).  ranks[n]; st->rounds = iterations. */
+int gg_pagerank_converge(gg_graph_t g, int32_t max_iter, double eps, float* ranks, gg_run_stats* st);
 /* app/PageRankDelta.C:120-174: ranks[n]. */
 int gg_pagerank_delta(gg_graph_t g, float* ranks, gg_run_stats* st);
 /* app/SPMV.C:65-93 with x = 1/n (x_in == NULL) or x_in[n]: y[n] = A^T-weighted sum. */

@@ -60,6 +60,7 @@ for name, args in {
     "or_bc_brandes": [C.POINTER(OrGraph), C.c_uint32, _P, _P],
     "or_bp": [C.POINTER(OrGraph), C.c_int32, _P, _P, _P, C.POINTER(OrStats)],
     "or_ppr": [C.POINTER(OrGraph), C.c_int32, C.c_double, _P, _P],
+    "or_pagerank_converge": [C.POINTER(OrGraph), C.c_int32, C.c_double, _P, C.POINTER(C.c_int32), _P],
     "or_wpr_forward": [C.POINTER(OrGraph), _P, _P, _P, C.c_int32, C.c_double, C.c_int32, _P],
     "or_wpr_backward": [C.POINTER(OrGraph), _P, _P, _P, C.c_int32, C.c_double, C.c_int32, _P, _P, _P, _P],
     "or_partition_sizes": [_P, _P, C.c_uint32, C.c_uint64, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, _P],
@@ -176,6 +177,14 @@ class Graph:
         ep = np.ascontiguousarray(edge_pot, np.float64)
         assert _lib.or_bp(C.byref(self.c), iters, _p(vp), _p(ep), _p(out), None) == 0
         return out
+
+    def pagerank_converge(self, max_iter=100, eps=1e-7):
+        """(ranks, iterations, per-iteration L1 changes) of app/PageRankConverage.C (FP64)."""
+        ranks = np.empty(self.n, np.float64)
+        l1 = np.zeros(max(max_iter, 1), np.float64)
+        it = C.c_int32()
+        assert _lib.or_pagerank_converge(C.byref(self.c), max_iter, eps, _p(ranks), C.byref(it), _p(l1)) == 0
+        return ranks, it.value, l1[:it.value]
 
     def wpr_forward(self, w, tele, iters, damping, normalize=False, x0=None):
         """Weighted PageRank x_iters (FP64); w in out-edge order."""

@@ -827,6 +827,55 @@ int or_ppr(const or_graph* g, int32_t iters, double damping, const double* tele,
   return 0;
 }
 
+/* ================================================ PageRankConverage */
+int or_pagerank_converge(const or_graph* g, int32_t max_iter, double eps, double* ranks, int32_t* iters,
+                         double* l1) {
+  if (!g || max_iter < 0) return -1;
+  const uint32_t n = g->n;
+  double* pc = (double*)malloc(sizeof(double) * n);
+  double* pn = (double*)malloc(sizeof(double) * n);
+  double* add = (double*)malloc(sizeof(double) * n);
+  for (uint32_t j = 0; j < n; j++) {
+    pc[j] = 1 / (double)n;
+    pn[j] = 0;
+  }
+  int32_t count = 0;
+  double L1 = 2;
+  while (count < max_iter && L1 > eps) {
+    for (uint32_t j = 0; j < n; j++) { /* edge_factor * p_curr; sinks are never gathered */
+      const uint32_t d = g->out_off[j + 1] - g->out_off[j];
+      add[j] = d ? 0.85 / d * pc[j] : 0.0;
+    }
+    for (uint32_t d = 0; d < n; d++)
+      for (uint32_t e = g->in_off[d]; e < g->in_off[d + 1]; e++) pn[d] += add[g->in_idx[e]];
+    double s = 0;
+    for (uint32_t j = 0; j < n; j++) s += pn[j];
+    const double c = (1 - s) / n; /* PR_Vertex_Csum with sum(..., scale=1) */
+    L1 = 0;
+    double s2 = 0;
+    for (uint32_t j = 0; j < n; j++) {
+      pn[j] += c;
+      L1 += fabs(pc[j] - pn[j]);
+    }
+    for (uint32_t j = 0; j < n; j++) s2 += pn[j];
+    if (l1) l1[count] = L1;
+    for (uint32_t j = 0; j < n; j++) {
+      pn[j] /= s2; /* PR_Vertex_norm */
+      pc[j] = 0;   /* PR_Vertex_Reset */
+    }
+    count++;
+    double* t = pc;
+    pc = pn;
+    pn = t;
+  }
+  memcpy(ranks, pc, sizeof(double) * n);
+  if (iters) *iters = count;
+  free(pc);
+  free(pn);
+  free(add);
+  return 0;
+}
+
 /* ======================================================= weighted PageRank */
 static double* wpr_coeffs(const or_graph* g, const double* w, int32_t normalize) {
   double* a = (double*)malloc(sizeof(double) * (g->m ? g->m : 1));

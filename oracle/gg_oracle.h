@@ -59,6 +59,13 @@ int or_bp(const or_graph* g, int32_t iters, const double* vert_pot, const double
  * k-column personalised form uses this per column): x_{t+1} = d*A x_t + (1-d)*tele. */
 int or_ppr(const or_graph* g, int32_t iters, double damping, const double* tele, double* x);
 
+/* app/PageRankConverage.C:243-310: PageRank with the dangling mass spread
+ * evenly and the ranks renormalised every iteration, until the L1 change
+ * drops to eps or max_iter iterations ran.  ranks[n]; *iters = iterations;
+ * l1[max_iter] (may be NULL) = each iteration's L1 change. */
+int or_pagerank_converge(const or_graph* g, int32_t max_iter, double eps, double* ranks, int32_t* iters,
+                         double* l1);
+
 /* Weighted PageRank and its adjoint (no reference counterpart; the weighted
  * form of PR_F / PR_Vertex_F, app/PageRank.C:28-100, with the edge weight in
  * place of 1/outdeg, and SPMV_F, app/SPMV.C:7-47, at iters = 1, damping = 1):

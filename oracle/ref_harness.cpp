@@ -182,6 +182,47 @@ static void replay(G& GA, long) {  // app/PageRank.C:330-378, app/PageRankBit.C:
   p_curr.del();
   p_next.del();
 }
+#elif defined(GG_APP_PRC)
+template <class G>
+static void replay(G& GA, long) {  // app/PageRankConverage.C:243-310
+  typedef typename G::vertex_type vertex;
+  const partitioner& part = GA.get_partitioner();
+  graph<vertex>& WG = GA.get_partition();
+  const intT n = GA.n, m = GA.m;
+  const double epsilon = 0.0000001;
+  double one_over_n = 1 / (double)n;
+  mmap_ptr<double> p_curr, p_next, edge_factor, add_factor;
+  p_curr.part_allocate(part);
+  p_next.part_allocate(part);
+  edge_factor.part_allocate(part);
+  add_factor.part_allocate(part);
+  map_vertexL(part, [&](intT j) { p_curr[j] = one_over_n; });
+  map_vertexL(part, [&](intT j) { p_next[j] = 0; });
+  map_vertexL(part, [&](intT j) { edge_factor[j] = (double)0.85 / (WG.V[j].getOutDegree()); });
+  int count = 0;
+  double L1_norm = 2;
+  std::vector<double> l1s;
+  partitioned_vertices F = partitioned_vertices::bits(part, n, m);
+  while (count < MaxIter && L1_norm > epsilon) {
+    map_vertexL(part, [&](intT j) { add_factor[j] = (double)edge_factor[j] * p_curr[j]; });
+    partitioned_vertices out = edgeMap(GA, F, PR_F<vertex>(p_curr, p_next, WG.V, add_factor), m / 20);
+    vertexMap(part, F, PR_Vertex_Csum(p_next, sum(part, p_next, n, 1), n));
+    L1_norm = normdiff(part, p_curr, p_next, n);
+    l1s.push_back(L1_norm);
+    vertexMap(part, F, PR_Vertex_norm(p_next, sum(part, p_next, n, 0), n));
+    vertexMap(part, F, PR_Vertex_Reset(p_curr));
+    count++;
+    swap(p_curr, p_next);
+    out.del();
+  }
+  F.del();
+  put_f64("ranks", p_curr.get(), n);
+  put_f64("l1", l1s.data(), l1s.size());
+  p_curr.del();
+  p_next.del();
+  edge_factor.del();
+  add_factor.del();
+}
 #elif defined(GG_APP_PRD)
 template <class G>
 static void replay(G& GA, long) {  // app/PageRankDelta.C:120-174

@@ -24,7 +24,7 @@ import oracle  # noqa: E402
 
 OUT = os.path.dirname(os.path.abspath(__file__))
 UNWEIGHTED = {"BFS": ["levels", "trace"], "CC": ["ids"], "PR": ["ranks", "trace"], "PRBIT": ["ranks", "trace"],
-              "PRD": ["ranks", "trace"], "BC": ["dependencies", "num_paths"]}
+              "PRD": ["ranks", "trace"], "PRC": ["ranks", "l1"], "BC": ["dependencies", "num_paths"]}
 WEIGHTED = {"SPMV": ["y"], "BF": ["dist"]}
 
 

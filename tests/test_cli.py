@@ -25,8 +25,8 @@ def test_cli_rejects_bad_flags_like_the_reference(tmp_path):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("app", ["BFS", "BC", "Components", "PageRank", "PageRankBit", "PageRankDelta", "SPMV",
-                                 "BellmanFord", "BP"])
+@pytest.mark.parametrize("app", ["BFS", "BC", "Components", "PageRank", "PageRankBit", "PageRankDelta",
+                                 "PageRankConverage", "SPMV", "BellmanFord", "BP"])
 def test_cli_runs_every_app(gg, tmp_path, app):
     hg = gg.HostGraph.rmat(10, 8, seed=3, symmetric=True)
     weighted = app in ("BellmanFord", "SPMV")

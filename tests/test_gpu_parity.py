@@ -72,6 +72,13 @@ def test_apps_on_golden_graphs(gg, orc, name):
         np.testing.assert_array_equal(np.isnan(dep), np.isnan(odep))
         fin = np.isfinite(odep)
         assert rel_l1(dep[fin], odep[fin]) <= BC_REL_L1
+    if "PRC_ranks" in gd:  # app/PageRankConverage.C, the reference's own output
+        r, run = g.pagerank_converge()
+        check_float(r, gd["PRC_ranks"])
+        # FP32 L1 changes below ~1e-6 sit at the values' rounding resolution, so
+        # the FP32 loop may stop a little earlier or later than the FP64 one; it
+        # must not stop while the reference's change is still above that
+        assert 100 >= run.rounds >= int((gd["PRC_l1"] > 1e-5).sum())
     if "SPMV_y" in gd:
         y, _ = g.spmv()
         check_float(y, gd["SPMV_y"], rel=1e-6, mx=1e-6)
@@ -193,3 +200,16 @@ def test_bp_matches_oracle(gg, orc, sym):
         np.testing.assert_allclose(out[inside], ref[inside], rtol=2e-5 if iters < 2 else 1e-2)
         assert np.all(np.isinf(out[ref > 1e40]))
         assert np.all(out[ref < 1e-50] == 0)
+
+
+@pytest.mark.parametrize("sym", [True, False])
+def test_pagerank_converge_rmat14(gg, orc, sym):
+    hg = gg.HostGraph.rmat(14, 16, seed=44, symmetric=sym)
+    g = gg.Graph(hg, partitions=ok_partitions(hg, 64))
+    og = orc.Graph.from_host(hg)
+    for max_iter in (1, 5, 100):
+        r, run = g.pagerank_converge(max_iter)
+        o, oit, l1 = og.pagerank_converge(max_iter)
+        check_float(r, o)
+        assert abs(float(r.sum()) - 1.0) <= 1e-5  # renormalised every iteration
+        assert max_iter >= run.rounds >= int((l1 > 1e-5).sum())

@@ -42,6 +42,12 @@ def test_oracle_matches_reference(orc, name):
         r, _ = og.pagerank_delta()
         assert rel_l1(r, gd["PRD_ranks"]) < 1e-12
         checked += 1
+    if "PRC_ranks" in gd:  # app/PageRankConverage.C: same iterations, same L1 trajectory
+        r, it, l1 = og.pagerank_converge()
+        assert it == len(gd["PRC_l1"])
+        np.testing.assert_allclose(l1, gd["PRC_l1"], rtol=1e-10, atol=1e-13)  # sums of tiny differences
+        assert rel_l1(r, gd["PRC_ranks"]) < 1e-12
+        checked += 1
     if "BC_num_paths" in gd:
         dep, npth, _ = og.bc(start)
         np.testing.assert_allclose(npth, gd["BC_num_paths"], rtol=1e-6)
