@@ -137,6 +137,7 @@ _sig("gg_host_graph_write_gr", C.c_int, C.POINTER(HostGraphC), C.c_char_p)
 _sig("gg_host_graph_read", C.c_int, C.c_char_p, C.c_int32, C.c_int32, C.c_int32, C.POINTER(HostGraphC))
 _sig("gg_host_graph_transpose", C.c_int, C.POINTER(HostGraphC), C.POINTER(HostGraphC))
 _sig("gg_host_graph_free", None, C.POINTER(HostGraphC))
+_sig("gg_vebo", C.c_int, C.POINTER(HostGraphC), C.c_int32, _P, _P, C.POINTER(HostGraphC))
 _sig("gg_partition_sizes", C.c_int, _u32p, _u32p, C.c_uint32, C.c_uint64, C.c_int32, C.c_int32, C.c_int32,
      C.c_int32, _i64p, _i64p)
 _sig("gg_hilbert_key", C.c_int64, C.c_int64, C.c_int64, C.c_int64)
@@ -213,7 +214,7 @@ EXPORTED = [
     "gg_graph_set_dense_policy", "gg_graph_set_tuning", "gg_graph_get_tuning", "gg_vertex_map", "gg_vertex_filter", "gg_vertex_array_alloc",
     "gg_vertex_array_free", "gg_memcpy_h2d", "gg_memcpy_d2h", "gg_host_alloc_pinned", "gg_host_free_pinned", "gg_bfs", "gg_components",
     "gg_pagerank", "gg_pagerank_delta", "gg_spmv", "gg_bellman_ford", "gg_bc", "gg_bp",
-    "gg_bfs_push_step_noalloc", "gg_ppr_k", "gg_pagerank_converge", "gg_msbfs", "gg_msbc",
+    "gg_bfs_push_step_noalloc", "gg_ppr_k", "gg_pagerank_converge", "gg_vebo", "gg_msbfs", "gg_msbc",
     "gg_batch_create", "gg_batch_destroy", "gg_batch_info", "gg_batch_bfs",
     "gg_pagerank_weighted_create", "gg_pagerank_weighted_destroy", "gg_pagerank_weighted_fwd",
     "gg_pagerank_weighted_bwd", "gg_autotune", "gg_autotune_build", "gg_autotune_ppr_k",
@@ -339,6 +340,14 @@ class HostGraph:
         t = HostGraphC()
         check(lib.gg_host_graph_transpose(C.byref(self.c), C.byref(t)), "gg_host_graph_transpose")
         return HostGraph(t)
+
+    def vebo(self, partitions=384):
+        """VEBO reordering: (relabelled HostGraph, new_of_old[n], vertices per partition[P])."""
+        t = HostGraphC()
+        new_of_old = np.empty(self.n, np.uint32)
+        sizes = np.empty(partitions, np.int64)
+        check(lib.gg_vebo(C.byref(self.c), partitions, _ptr(new_of_old), _ptr(sizes), C.byref(t)), "gg_vebo")
+        return HostGraph(t), new_of_old, sizes
 
 
 def partition_sizes(in_deg, out_deg, m, P, balance=BALANCE_EDGE, part_how=PART_DEST, relabel=False):

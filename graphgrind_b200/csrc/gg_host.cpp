@@ -602,6 +602,141 @@ static int greedy_relabel(const uint32_t* indeg, uint64_t cnt, int32_t P, int64_
   return GG_OK;
 }
 
+// VEBO vertex reordering (graphtools/VEBO.C:56-395): vertices sorted by
+// in-degree, highest first (ties by id, LargePairSort), are dealt degree
+// group by degree group to the partition with the fewest edges so far (the
+// first such partition; when the spread of edge counts exceeds the degree, a
+// batch of (remaining / P) vertices goes at once), zero-degree vertices then
+// even out the vertex counts (:225-262), and each partition's vertices take
+// consecutive new ids in the order they were dealt (:276-300).  The output
+// graph has, at new id i, the out-edges of the old vertex dealt to i, with
+// neighbours renamed and kept in their old order (:330-343).  The in-degree of
+// a symmetric graph is its degree (the reference leaves it unset).
+int gg_vebo(const gg_host_graph* g, int32_t partitions, uint32_t* new_of_old, int64_t* part_sizes,
+            gg_host_graph* out) {
+  if (!g || !out || !g->offsets || (g->m && !g->indices) || partitions < 1 || g->n == 0)
+    return fail(GG_ERR_INVALID_ARG, "gg_vebo: bad arguments");
+  const int64_t n = g->n, P = partitions;
+  const uint64_t m = g->m;
+  std::vector<int64_t> indeg(n, 0);
+  if (g->symmetric) {
+    for (int64_t v = 0; v < n; v++) indeg[v] = g->offsets[v + 1] - g->offsets[v];
+  } else {
+    for (uint64_t e = 0; e < m; e++) indeg[g->indices[e]]++;
+  }
+  std::vector<std::pair<int64_t, int64_t>> check(n);
+  for (int64_t i = 0; i < n; i++) check[i] = {i, indeg[i]};
+  std::sort(check.begin(), check.end(), [](const std::pair<int64_t, int64_t>& a, const std::pair<int64_t, int64_t>& b) {
+    return a.second > b.second || (a.second == b.second && a.first < b.first);
+  });
+  // degree groups: group index of each degree, (count, degree) per group (zero-degree vertices not counted)
+  int64_t c = 1, czero = 0;
+  for (int64_t i = 1; i < n; i++)
+    if (check[i].second != check[i - 1].second) c++;
+  for (int64_t i = 0; i < n; i++)
+    if (check[i].second == 0) czero++;
+  std::vector<int64_t> groupOf((size_t)check[0].second + 1, 0);
+  std::vector<std::pair<int64_t, int64_t>> perGroup(c, {0, 0});
+  int64_t a = 0;
+  for (int64_t i = 0; i < n; i++) {
+    if (i > 0 && check[i].second != check[i - 1].second) a++;
+    groupOf[check[i].second] = a;
+    if (i == 0 || check[i].second != 0) {
+      perGroup[a].first++;
+      perGroup[a].second = check[i].second;
+    }
+  }
+  std::vector<int64_t> edges(P, 0), vsize(P, 0);
+  std::vector<int64_t> perDeg((size_t)P * c, 0);  // [partition][group]
+  auto deal = [&](int64_t p, int64_t grp, int64_t deg, int64_t cnt) {
+    edges[p] += deg * cnt;
+    perDeg[(size_t)p * c + grp] += cnt;
+    vsize[p] += cnt;
+  };
+  for (int64_t i = 0; i < c; i++) {
+    const int64_t deg = perGroup[i].second, same = perGroup[i].first;
+    for (int64_t k = 0; k < same;) {
+      int64_t mx = edges[0], mn = edges[0], mnp = 0;
+      for (int64_t j = 1; j < P; j++) {
+        if (edges[j] < mn) {
+          mn = edges[j];
+          mnp = j;
+        }
+        if (edges[j] > mx) mx = edges[j];
+      }
+      const int64_t remain = (same - k) / P;
+      const int64_t take = (mx - mn > deg && remain > 1) ? remain : 1;
+      deal(mnp, groupOf[deg], deg, take);
+      k += take;
+    }
+  }
+  // zero-degree vertices even out the vertex counts
+  const int64_t avg = n / P, extra = n % P, zgrp = groupOf[0];
+  if (extra == 0 || czero / P != 0) {
+    for (int64_t p = 0; p < P; p++)
+      if (vsize[p] < avg) deal(p, zgrp, 0, avg - vsize[p]);
+    if (extra != 0)
+      for (int64_t p = 0; p < extra; p++) deal(p, zgrp, 0, 1);
+  } else {
+    for (int64_t z = 0; z < czero; z++) {
+      int64_t mn = vsize[0], mnp = 0;
+      for (int64_t p = 1; p < P; p++)
+        if (vsize[p] < mn) {
+          mn = vsize[p];
+          mnp = p;
+        }
+      deal(mnp, zgrp, 0, 1);
+    }
+  }
+  int64_t total = 0;
+  for (int64_t p = 0; p < P; p++) total += vsize[p];
+  if (total != n)
+    return fail(GG_ERR_PARTITION,
+                "gg_vebo: the zero-degree fill places %lld vertices for n=%lld (P=%d); the reference reads past "
+                "its vertex list here",
+                (long long)total, (long long)n, partitions);
+  std::vector<int64_t> start(P, 0), fill(P, 0);
+  for (int64_t p = 1; p < P; p++) start[p] = start[p - 1] + vsize[p - 1];
+  std::vector<uint32_t> old_of_new(n);
+  int64_t real = 0;
+  for (int64_t i = 0; i < c; i++)
+    for (int64_t p = 0; p < P; p++)
+      for (int64_t k = 0; k < perDeg[(size_t)p * c + i]; k++)
+        old_of_new[start[p] + fill[p]++] = (uint32_t)check[real++].first;
+  std::vector<uint32_t> nofo(n);
+  for (int64_t i = 0; i < n; i++) nofo[old_of_new[i]] = (uint32_t)i;
+  memset(out, 0, sizeof *out);
+  out->n = g->n;
+  out->m = m;
+  out->symmetric = g->symmetric;
+  out->weight_type = g->weight_type;
+  out->offsets = (uint32_t*)calloc((size_t)n + 1, sizeof(uint32_t));
+  out->indices = (uint32_t*)malloc(4 * (m ? m : 1));
+  if (g->weights) out->weights = malloc(4 * (m ? m : 1));
+  if (!out->offsets || !out->indices || (g->weights && !out->weights)) {
+    gg_host_graph_free(out);
+    return fail(GG_ERR_OOM, "gg_vebo: out of host memory");
+  }
+  for (int64_t i = 0; i < n; i++) {
+    const uint32_t o = old_of_new[i];
+    out->offsets[i + 1] = out->offsets[i] + (g->offsets[o + 1] - g->offsets[o]);
+  }
+  const uint32_t* w = (const uint32_t*)g->weights;
+  uint32_t* ow = (uint32_t*)out->weights;
+#pragma omp parallel for schedule(dynamic, 4096)
+  for (int64_t i = 0; i < n; i++) {
+    const uint32_t o = old_of_new[i];
+    uint32_t dst = out->offsets[i];
+    for (uint32_t j = g->offsets[o]; j < g->offsets[o + 1]; j++, dst++) {
+      out->indices[dst] = nofo[g->indices[j]];
+      if (ow) ow[dst] = w[j];
+    }
+  }
+  if (new_of_old) std::copy(nofo.begin(), nofo.end(), new_of_old);
+  if (part_sizes) std::copy(vsize.begin(), vsize.end(), part_sizes);
+  return GG_OK;
+}
+
 int gg_partition_sizes(const uint32_t* in_degrees, const uint32_t* out_degrees, uint32_t n, uint64_t m,
                        int32_t P, int32_t balance, int32_t part_how, int32_t relabel, int64_t* coo_sizes,
                        int64_t* csc_sizes) {

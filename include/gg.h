@@ -118,6 +118,15 @@ int gg_host_graph_write_adj(const gg_host_graph* g, const char* path);
 int gg_host_graph_write_gr(const gg_host_graph* g, const char* path);
 int gg_host_graph_read(const char* path, int32_t binary, int32_t symmetric,
                        int32_t weighted, gg_host_graph* out);
+/* VEBO reordering (graphtools/VEBO.C:56-395, the tool that prepares graphs
+ * for -o): vertices sorted by in-degree are dealt to `partitions` partitions
+ * that balance edges first and vertices second, and renumbered partition by
+ * partition.  out: the relabelled graph (out-edges of the old vertex at each
+ * new id, neighbour order kept, weights carried along); new_of_old[n] and
+ * part_sizes[partitions] may be NULL.  GG_ERR_PARTITION where the reference's
+ * zero-degree fill would place a different number of vertices than n. */
+int gg_vebo(const gg_host_graph* g, int32_t partitions, uint32_t* new_of_old, int64_t* part_sizes,
+            gg_host_graph* out);
 /* CSC (in-edges) of a host graph: in_offsets n+1, in_indices m, in_weights m. */
 int gg_host_graph_transpose(const gg_host_graph* g, gg_host_graph* out);
 void gg_host_graph_free(gg_host_graph* g);

@@ -20,7 +20,8 @@ def pytest_configure(config):
 
 
 def golden_names():
-    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and f != "partitions.npz")
+    """Golden graphs with app outputs (partition sizes and VEBO orders have their own fixtures)."""
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and f not in ("partitions.npz", "vebo.npz"))
 
 
 def load_golden(name):

@@ -11,6 +11,7 @@ from __future__ import annotations
 
 import argparse
 import os
+import subprocess
 import sys
 import tempfile
 
@@ -85,6 +86,40 @@ def partition_cases(tmp):
     print("partitions.npz")
 
 
+def read_adj_text(path):
+    """CSR of a PBBS AdjacencyGraph text file, neighbour order as written."""
+    tok = open(path).read().split()
+    assert tok[0] == "AdjacencyGraph"
+    n, m = int(tok[1]), int(tok[2])
+    off = np.array(tok[3:3 + n] + [m], np.int64)
+    idx = np.array(tok[3 + n:3 + n + m], np.int64)
+    return off, idx
+
+
+def vebo_cases(tmp):
+    """The reference's VEBO tool (graphtools/VEBO.C) on directed graphs; a
+    symmetric graph goes in as a directed file holding both directions, whose
+    in-degrees are its degrees."""
+    out = {}
+    cases = [("rmat10_P8", gg.HostGraph.rmat(10, 8, seed=11, symmetric=False), 8),
+             ("rmat10_P3", gg.HostGraph.rmat(10, 8, seed=11, symmetric=False), 3),
+             ("rmat12_P64", gg.HostGraph.rmat(12, 16, seed=14, symmetric=False), 64),
+             ("rmat11sym_P16", gg.HostGraph.rmat(11, 8, seed=15, symmetric=True), 16)]
+    for name, hg, P in cases:
+        gin = os.path.join(tmp, name + ".gr")
+        d = gg.HostGraph.from_csr(hg.offsets.copy(), hg.indices.copy(), symmetric=False)
+        d.write_gr(gin)
+        adj = os.path.join(tmp, name + ".vebo.adj")
+        r = subprocess.run([oracle.ref_binary("VEBO"), "-p", str(P), gin, adj], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr[-500:]
+        off, idx = read_adj_text(adj)
+        out.update({f"{name}_in_offsets": hg.offsets.copy(), f"{name}_in_indices": hg.indices.copy(),
+                    f"{name}_P": np.int32(P), f"{name}_sym": np.int32(hg.symmetric),
+                    f"{name}_offsets": off, f"{name}_indices": idx})
+        print(f"vebo {name}: n={hg.n} m={hg.m} P={P}")
+    np.savez_compressed(os.path.join(OUT, "vebo.npz"), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("GG_REFERENCE", "/root/reference"))
@@ -108,6 +143,7 @@ def main():
     two = [(0, 1), (1, 2), (2, 0), (4, 5), (5, 6), (6, 7), (7, 4), (4, 6)]
     run_case("twocomp10", hand_graph(two, 10, True), UNWEIGHTED, ["-s", "-c", "2"], 4, tmp)
     partition_cases(tmp)
+    vebo_cases(tmp)
 
 
 if __name__ == "__main__":

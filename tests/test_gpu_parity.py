@@ -213,3 +213,24 @@ def test_pagerank_converge_rmat14(gg, orc, sym):
         check_float(r, o)
         assert abs(float(r.sum()) - 1.0) <= 1e-5  # renormalised every iteration
         assert max_iter >= run.rounds >= int((l1 > 1e-5).sum())
+
+
+def test_vebo_graph_with_relabel_partitions(gg, orc):
+    """A VEBO-relabelled graph built with -o (partition boundaries at degree
+    rises) traverses to the same results, under the permutation."""
+    hg = gg.HostGraph.rmat(13, 16, seed=46, symmetric=False)
+    vg, new_of_old, _ = hg.vebo(32)
+    g = gg.Graph(vg, partitions=ok_partitions(vg, 32), relabel=True)
+    og = orc.Graph.from_host(hg)
+    _, olev, _ = og.bfs(100)
+    _, lev, _ = g.bfs(int(new_of_old[100]))
+    np.testing.assert_array_equal(lev[new_of_old], olev)
+    r, _ = g.pagerank(10)
+    o, _ = og.pagerank(10)
+    check_float(r[new_of_old], o)
+    # on a symmetric graph the component classes are invariant under relabelling
+    hs = gg.HostGraph.rmat(12, 4, seed=47, symmetric=True)
+    vs, nofo, _ = hs.vebo(16)
+    cn = gg.Graph(vs, partitions=ok_partitions(vs, 16), relabel=True).components()[0][nofo]
+    co = orc.Graph.from_host(hs).cc()[0]
+    assert len(set(zip(co.tolist(), cn.tolist()))) == len(set(co.tolist())) == len(set(cn.tolist()))
