@@ -127,6 +127,8 @@ struct gg_graph_s {
   uint64_t m_pad = 0;        // edge arrays hold m_pad entries (zero padded)
   gg::TileSet coo_tiles;
   bool has_coo = false;
+  bool coo_by_source = false;       // -P source: partitions of sources, destinations in d_coo_dst
+  uint32_t* d_coo_dst = nullptr;
   uint32_t *d_coo_src = nullptr, *d_coo_w = nullptr;
   uint16_t* d_coo_dloc = nullptr;
   uint64_t coo_len = 0;
@@ -725,6 +727,53 @@ __global__ void __launch_bounds__(kCooThreads, GG_COO_MIN_BLOCKS) k_pull_coo_w(c
     }
     if (a) atomicAdd(p.stats + 0, a);
     if (b2) atomicAdd(p.stats + 1, b2);
+  }
+}
+
+// ------------------------------------------ source-partitioned COO (-P source)
+// edgeMapDense over partitions of sources (graphgrind/graph-numa.h:1145-1171,
+// graphgrind/ligra-numa.h:803-866): a partition's edges reach destinations
+// anywhere, so every edge applies F's atomic update (edgeOpInAtomic) and the
+// output bit of a destination is counted once, by the thread that sets it.
+struct SrcParams {
+  const uint32_t* src;
+  const uint32_t* dst;
+  const uint32_t* wts;
+  uint64_t len;
+  const uint32_t* fr_bits;
+  uint32_t* next_bits;
+  const uint32_t* deg_off;
+  unsigned long long* stats;
+};
+
+template <class F, bool HW, bool ALL>
+__global__ void __launch_bounds__(256) k_coo_src(const SrcParams p, const F f) {
+  using V = typename F::value_t;
+  unsigned long long cnt = 0, deg = 0;
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < p.len;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t s = __ldg(p.src + e), d = __ldg(p.dst + e);
+    if (!ALL && !test_bit(p.fr_bits, s)) continue;
+    if (!F::kCondTrue && !f.cond(d)) continue;
+    const uint32_t w = HW ? __ldg(p.wts + e) : 1u;
+    if (F::kPositive) {  // sources outside the frontier carry negative values
+      const V v = f.gather(s, w);
+      if (v < F::identity()) continue;
+    }
+    if (f.update_atomic(s, d, w)) {
+      const uint32_t bit = 1u << (d & 31);
+      uint32_t* word = p.next_bits + (d >> 5);
+      if (!(__ldcg(word) & bit) && !(atomicOr(word, bit) & bit)) {
+        ++cnt;
+        deg += __ldg(p.deg_off + d + 1) - __ldg(p.deg_off + d);
+      }
+    }
+  }
+  cnt = warp_sum(cnt);
+  deg = warp_sum(deg);
+  if ((threadIdx.x & 31) == 0 && (cnt | deg)) {
+    atomicAdd(p.stats + 0, cnt);
+    atomicAdd(p.stats + 1, deg);
   }
 }
 

@@ -416,6 +416,109 @@ static int build_coo(gg_graph_s* g, const uint32_t* h_in_off) {
   return GG_OK;
 }
 
+// -P source (COOPartitionBySour, graphgrind/graph-numa.h:1145-1171): partition
+// p holds the out-edges of the sources in [coo_starts[p], coo_starts[p+1]),
+// which are contiguous in the CSR; they are Hilbert-ordered inside the
+// partition with the same key as the destination form (or left in CSR order).
+__global__ void k_coo_src_keys(const uint32_t* src, const uint32_t* dst, uint64_t m, const int64_t* starts, int P,
+                               const int64_t* part_side, int hilbert, uint64_t* keys, uint32_t* vals) {
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < m; j += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t s = src[j], d = dst[j];
+    uint64_t key;
+    if (hilbert) {
+      int lo = 0, hi = P;  // partition p with starts[p] <= s < starts[p+1]
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (starts[mid] <= (int64_t)s) lo = mid; else hi = mid;
+      }
+      key = (uint64_t)hilbert_xy2d(part_side[lo], (int64_t)s, (int64_t)d);
+    } else {
+      key = ((uint64_t)s << 32) | d;
+    }
+    keys[j] = key;
+    vals[j] = (uint32_t)j;
+  }
+}
+
+__global__ void k_coo_src_scatter(uint64_t m, const uint32_t* perm, const uint32_t* src, const uint32_t* dst,
+                                  const uint32_t* w, uint32_t* coo_src, uint32_t* coo_dst, uint32_t* coo_w) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t j = perm[i];
+    coo_src[i] = src[j];
+    coo_dst[i] = dst[j];
+    if (w) coo_w[i] = w[j];
+  }
+}
+
+static int build_coo_src(gg_graph_s* g) {
+  const uint32_t n = g->n;
+  const uint64_t m = g->m;
+  const int P = (int)g->coo_sizes.size();
+  const uint32_t* off = g->h_csr_off.data();
+  if (m >= (1ull << 31)) return fail(GG_ERR_SIZE, "source-partitioned COO exceeds the 2^31-edge sort limit");
+  std::vector<int64_t> side(P);
+  std::vector<int> seg_begin(P + 1);
+  for (int p = 0; p < P; ++p) {
+    seg_begin[p] = (int)off[g->coo_starts[p]];
+    side[p] = hilbert_side((int64_t)off[g->coo_starts[p + 1]] - (int64_t)off[g->coo_starts[p]]);
+  }
+  seg_begin[P] = (int)m;
+  GG_TRY(dev_alloc(g, &g->d_coo_src, m + 16));
+  GG_TRY(dev_alloc(g, &g->d_coo_dst, m + 16));
+  if (g->wtype != GG_W_NONE) GG_TRY(dev_alloc(g, &g->d_coo_w, m + 16));
+  uint32_t *d_src = nullptr, *d_vals = nullptr, *d_perm = nullptr;
+  uint64_t *d_keys = nullptr, *d_keys_out = nullptr;
+  int64_t *d_starts = nullptr, *d_side = nullptr;
+  int* d_seg = nullptr;
+  void* d_temp = nullptr;
+  size_t temp_bytes = 0;
+  int rc = GG_OK;
+  auto cleanup = [&]() {
+    cudaFree(d_src); cudaFree(d_vals); cudaFree(d_perm); cudaFree(d_keys); cudaFree(d_keys_out);
+    cudaFree(d_starts); cudaFree(d_side); cudaFree(d_seg); cudaFree(d_temp);
+  };
+#define GG_BUILD(call)                                                                      \
+  do {                                                                                      \
+    cudaError_t e__ = (call);                                                               \
+    if (e__ != cudaSuccess) {                                                               \
+      rc = fail(GG_ERR_CUDA, "COO build: %s: %s", #call, cudaGetErrorString(e__));          \
+      cleanup();                                                                            \
+      return rc;                                                                            \
+    }                                                                                       \
+  } while (0)
+  GG_BUILD(cudaMalloc(&d_src, 4 * m));
+  GG_BUILD(cudaMalloc(&d_vals, 4 * m));
+  GG_BUILD(cudaMalloc(&d_perm, 4 * m));
+  GG_BUILD(cudaMalloc(&d_keys, 8 * m));
+  GG_BUILD(cudaMalloc(&d_keys_out, 8 * m));
+  GG_BUILD(cudaMalloc(&d_starts, 8 * (P + 1)));
+  GG_BUILD(cudaMalloc(&d_side, 8 * P));
+  GG_BUILD(cudaMalloc(&d_seg, sizeof(int) * (P + 1)));
+  GG_BUILD(cudaMemcpy(d_starts, g->coo_starts.data(), 8 * (P + 1), cudaMemcpyHostToDevice));
+  GG_BUILD(cudaMemcpy(d_side, side.data(), 8 * P, cudaMemcpyHostToDevice));
+  GG_BUILD(cudaMemcpy(d_seg, seg_begin.data(), sizeof(int) * (P + 1), cudaMemcpyHostToDevice));
+  const int grid = g->num_sms * 8;
+  k_edge_dst<<<grid, 256>>>(g->d_csr_off, n, d_src);  // the row (source) of every CSR edge
+  k_coo_src_keys<<<grid, 256>>>(d_src, g->d_csr_idx, m, d_starts, P, d_side,
+                                g->opts.order == GG_ORDER_HILBERT ? 1 : 0, d_keys, d_vals);
+  GG_BUILD(cudaGetLastError());
+  GG_BUILD(cub::DeviceSegmentedRadixSort::SortPairs(nullptr, temp_bytes, d_keys, d_keys_out, d_vals, d_perm, (int)m,
+                                                    P, d_seg, d_seg + 1));
+  GG_BUILD(cudaMalloc(&d_temp, temp_bytes));
+  GG_BUILD(cub::DeviceSegmentedRadixSort::SortPairs(d_temp, temp_bytes, d_keys, d_keys_out, d_vals, d_perm, (int)m,
+                                                    P, d_seg, d_seg + 1));
+  k_coo_src_scatter<<<grid, 256>>>(m, d_perm, d_src, g->d_csr_idx, g->d_csr_w, g->d_coo_src, g->d_coo_dst,
+                                   g->d_coo_w);
+  GG_BUILD(cudaGetLastError());
+  GG_BUILD(cudaDeviceSynchronize());
+#undef GG_BUILD
+  cleanup();
+  g->coo_len = m;
+  g->coo_by_source = true;
+  g->has_coo = true;
+  return GG_OK;
+}
+
 static void graph_release(gg_graph_s* g) {
   if (!g) return;
   {
@@ -445,6 +548,7 @@ static void graph_release(gg_graph_s* g) {
   cudaFree(g->coo_tiles.d_tiles);
   cudaFree(g->d_coo_src);
   cudaFree(g->d_coo_dloc);
+  cudaFree(g->d_coo_dst);
   cudaFree(g->d_coo_w);
   cudaFree(g->ws.d_stats);
   cudaFree(g->ws.d_dedup);
@@ -473,8 +577,6 @@ static int graph_build(const gg_host_graph* hg, const gg_build_opts* opts_in, gg
   if (o.coo_dst_window <= 0) o.coo_dst_window = kSegBlock;
   o.coo_dst_window = std::min((o.coo_dst_window + kSegBlock - 1) / kSegBlock * kSegBlock, 1 << 16);
   if (o.order != GG_ORDER_CSR) o.order = GG_ORDER_HILBERT;
-  if (o.part_how == GG_PART_SOURCE)
-    return fail(GG_ERR_UNSUPPORTED, "-P source partitioning is not supported by this build");
   g->opts = o;
   g->n = n;
   g->m = m;
@@ -559,7 +661,8 @@ static int graph_build(const gg_host_graph* hg, const gg_build_opts* opts_in, gg
   }
   // partitioned COO: only for -v edge (graphgrind/graph-numa.h:661)
   const bool want_coo = o.balance == GG_BALANCE_EDGE && o.build_coo >= 0;
-  if (!rc && want_coo && m > 0) rc = build_coo(g, in->offsets);
+  if (!rc && want_coo && m > 0)
+    rc = o.part_how == GG_PART_SOURCE ? build_coo_src(g) : build_coo(g, in->offsets);
   if (!g->symmetric) gg_host_graph_free(&csc);
   if (rc) return rc;
   // workspace

@@ -76,6 +76,18 @@ template <class F, bool HW>
 int pull_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f, bool coo, bool no_out = false) {
   // a positive functor whose gathered values already mark the frontier needs no bitmap
   const bool all = in->bit || (F::kPositive && f.frontier_in_values);
+  if (coo && g->coo_by_source) {  // -P source: atomic updates over the source partitions
+    SrcParams sp{g->d_coo_src, g->d_coo_dst, g->d_coo_w, g->coo_len, in->d_bits, out->d_bits, g->out_off(),
+                 g->ws.d_stats};
+    const int grid = generic_grid(g, g->coo_len) ;
+    if (all)
+      k_coo_src<F, HW, true><<<grid, 256, 0, g->stream>>>(sp, f);
+    else
+      k_coo_src<F, HW, false><<<grid, 256, 0, g->stream>>>(sp, f);
+    GG_CUDA(cudaGetLastError());
+    g->kernels++;
+    return GG_OK;
+  }
   PullParams p{};
   const int orient = g->transposed ? 1 : 0;
   if (coo) {

@@ -86,6 +86,30 @@ def partition_cases(tmp):
     print("partitions.npz")
 
 
+def partition_src_cases(tmp):
+    """-P source on a directed graph: the reference's partition sizes for several
+    P, and its source-partitioned COO order (edges of each partition in its
+    sorted order) for one P."""
+    out = {}
+    g = gg.HostGraph.rmat(12, 16, seed=22, symmetric=False)
+    path = os.path.join(tmp, "parts_src.adj")
+    g.write_adj(path)
+    out.update({"offsets": g.offsets.copy(), "indices": g.indices.copy()})
+    for P in (1, 2, 8, 64):
+        for how in ("source", "dest"):
+            rc, dump, err = oracle.run_ref("BFS", "parts", path, os.path.join(tmp, "p.bin"), ["-c", str(P), "-P", how])
+            key = f"P{P}_{how}"
+            out[key + "_rc"] = np.int32(0 if rc == 0 else 1)
+            if rc == 0:
+                out[key + "_coo"] = dump["coo_sizes"]
+                out[key + "_csc"] = dump["csc_sizes"]
+                if P == 8 and how == "source":
+                    for k in ("coo_src", "coo_dst", "coo_bounds"):
+                        out["P8_source_" + k] = dump[k]
+    np.savez_compressed(os.path.join(OUT, "partitions_src.npz"), **out)
+    print("partitions_src.npz")
+
+
 def read_adj_text(path):
     """CSR of a PBBS AdjacencyGraph text file, neighbour order as written."""
     tok = open(path).read().split()
@@ -143,6 +167,7 @@ def main():
     two = [(0, 1), (1, 2), (2, 0), (4, 5), (5, 6), (6, 7), (7, 4), (4, 6)]
     run_case("twocomp10", hand_graph(two, 10, True), UNWEIGHTED, ["-s", "-c", "2"], 4, tmp)
     partition_cases(tmp)
+    partition_src_cases(tmp)
     vebo_cases(tmp)
 
 

@@ -234,3 +234,22 @@ def test_vebo_graph_with_relabel_partitions(gg, orc):
     cn = gg.Graph(vs, partitions=ok_partitions(vs, 16), relabel=True).components()[0][nofo]
     co = orc.Graph.from_host(hs).cc()[0]
     assert len(set(zip(co.tolist(), cn.tolist()))) == len(set(co.tolist())) == len(set(cn.tolist()))
+
+
+@pytest.mark.parametrize("sym", [True, False])
+def test_apps_with_source_partitions(gg, orc, sym):
+    """-P source: COO partitions of sources, dense COO steps with atomic updates."""
+    hg = gg.HostGraph.rmat(13, 16, seed=48, symmetric=sym).add_weights(gg.W_INT32, seed=4, lo=1, hi=100)
+    g = gg.Graph(hg, partitions=8, part_how=gg.PART_SOURCE)
+    assert g.info().has_coo
+    og = orc.Graph.from_host(hg)
+    for policy in (0, 2):  # reference rule, and every dense step through the COO
+        g.set_dense_policy(policy)
+        np.testing.assert_array_equal(g.bfs(9)[1], og.bfs(9)[1])
+        np.testing.assert_array_equal(g.components()[0], og.cc()[0])
+        np.testing.assert_array_equal(g.bellman_ford(9)[0], og.bellman_ford(9)[0])
+        r, _ = g.pagerank(10)
+        o, _ = og.pagerank(10)
+        check_float(r, o)
+        y, _ = g.spmv()
+        check_float(y, og.spmv()[0], rel=1e-6, mx=1e-6 * float(np.abs(og.spmv()[0]).max()))

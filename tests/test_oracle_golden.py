@@ -131,3 +131,38 @@ def test_hilbert_key_orders_reference_coo(gg, orc, name):
         assert all(a <= b for a, b in zip(keys, keys[1:])), f"partition {p} not ordered"
         assert np.all((d >= starts[p]) & (d < starts[p + 1]))
         assert ne == int(((dst_all >= starts[p]) & (dst_all < starts[p + 1])).sum())
+
+
+def test_source_partitions_match_reference(gg, orc):
+    """-P source on a directed graph: partition sizes balance out-degrees (COO)
+    and the destinations' out-degrees (compressed CSC), and each COO partition
+    holds the out-edges of its source range in Hilbert order."""
+    import os
+    from conftest import GOLDEN
+    z = np.load(os.path.join(GOLDEN, "partitions_src.npz"))
+    off = z["offsets"].astype(np.int64)
+    idx = z["indices"].astype(np.int64)
+    n, m = len(off) - 1, int(off[-1])
+    outd = np.diff(off).astype(np.uint32)
+    ind = np.bincount(idx, minlength=n).astype(np.uint32)
+    for P in (1, 2, 8, 64):
+        for how, code in (("source", 1), ("dest", 0)):
+            key = f"P{P}_{how}"
+            if int(z[key + "_rc"]):
+                with pytest.raises(gg.GGError):
+                    gg.partition_sizes(ind, outd, m, P, 0, code, False)
+                continue
+            pc, ps = gg.partition_sizes(ind, outd, m, P, 0, code, False)
+            np.testing.assert_array_equal(pc, z[key + "_coo"], err_msg=key)
+            np.testing.assert_array_equal(ps, z[key + "_csc"], err_msg=key)
+            rc, oc, os_ = orc.partition_sizes(ind, outd, m, P, 0, code, False)
+            assert rc == 0
+            np.testing.assert_array_equal(oc, z[key + "_coo"], err_msg=key)
+    src, dst, bounds = z["P8_source_coo_src"], z["P8_source_coo_dst"], z["P8_source_coo_bounds"]
+    starts = np.concatenate([[0], np.cumsum(z["P8_source_coo"])])
+    for p in range(len(bounds) - 1):
+        s, d = src[bounds[p]:bounds[p + 1]], dst[bounds[p]:bounds[p + 1]]
+        keys = [gg.hilbert_key(len(s), int(x), int(y)) for x, y in zip(s, d)]
+        assert all(a <= b for a, b in zip(keys, keys[1:])), f"partition {p} not ordered"
+        assert np.all((s >= starts[p]) & (s < starts[p + 1]))
+        assert len(s) == int(off[starts[p + 1]] - off[starts[p]])
