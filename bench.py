@@ -55,8 +55,8 @@ WORKLOAD = ("RMAT-24 directed (n=2^24, edge factor 16, a/b/c/d=.57/.19/.19/.05, 
 HBM_FALLBACK_GBS = 6650.0
 # DRAM bytes per PageRank-pull launch of the default workload, from one ncu
 # capture (profiles/dram_k_pull_coo_w_pagerank_rmat24.md)
-TRAFFIC_RMAT24_PR_PULL = 2175428096
-TRAFFIC_TILE_EDGES = 1 << 16
+TRAFFIC_RMAT24_PR_PULL = 2118674176
+TRAFFIC_TILE_EDGES = 1 << 17
 
 
 def log(*a):
