@@ -236,7 +236,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
                  3: "k_pull_coo_w (3-stage ring)", 4: "k_pull_coo_w (lane-contiguous)", 5: "k_pull_coo_w (prefetch)"}
     kernel_name = coo_names.get(g.get_tuning(gg.TUNE_COO_KERNEL), "k_pull_coo_w") if pr_kind == "coo_pull" \
         else "k_pull_seg"
-    # per-application dense-pull rooflines (SURVEY 8d bytes): PageRank 8m+16n, SpMV 12m+12n
+    # per-application dense-pull rooflines, algorithmic bytes: PageRank 8m+16n, SpMV 12m+12n
     roofline_by_app = {}
     for app, pf, bytes_ in (("pagerank", prof_pr, 8 * m + 16 * n), ("spmv", prof_sp, 12 * m + 12 * n)):
         kind = max(("coo_pull", "csc_pull"), key=lambda k: pf[k]["launches"])
