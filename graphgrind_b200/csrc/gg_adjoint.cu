@@ -107,12 +107,26 @@ __global__ void k_wpr_row_of(uint64_t m, uint32_t n, const uint32_t* off, uint32
   }
 }
 
-// perm[e] = position of out-edge e = u->v among v's in-edges (sorted by source).
-__global__ void k_wpr_perm(uint64_t m, const uint32_t* row_of, const uint32_t* out_idx, const uint32_t* in_off,
-                           const uint32_t* in_idx, uint32_t* perm, unsigned* err) {
+// Rows whose out-edge list is not sorted by destination (flag[u] = 1).
+__global__ void k_wpr_row_unsorted(uint64_t m, const uint32_t* row_of, const uint32_t* out_idx, uint32_t* flag) {
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x + 1; e < m; e += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t u = row_of[e];
+    if (row_of[e - 1] == u && out_idx[e - 1] > out_idx[e]) flag[u] = 1u;
+  }
+}
+
+// perm[e] = position of out-edge e = u->v among v's in-edges (sorted by
+// source).  An edge u->v present c > 1 times has c consecutive in-edge slots;
+// the copy of rank r among u's out-edges to v takes slot r of them (binary
+// search for the first copy in a sorted row, a scan of the row before e in an
+// unsorted one), so the map is a bijection.
+__global__ void k_wpr_perm(uint64_t m, const uint32_t* row_of, const uint32_t* out_off, const uint32_t* out_idx,
+                           const uint32_t* unsorted, const uint32_t* in_off, const uint32_t* in_idx, uint32_t* perm,
+                           unsigned* err) {
   for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t u = row_of[e], v = out_idx[e];
-    uint32_t lo = in_off[v], hi = in_off[v + 1];
+    const uint32_t end = in_off[v + 1];
+    uint32_t lo = in_off[v], hi = end;
     while (lo < hi) {
       const uint32_t mid = lo + (hi - lo) / 2;
       if (in_idx[mid] < u)
@@ -120,8 +134,25 @@ __global__ void k_wpr_perm(uint64_t m, const uint32_t* row_of, const uint32_t* o
       else
         hi = mid;
     }
-    if (lo < in_off[v + 1] && in_idx[lo] == u)
-      perm[e] = lo;
+    uint32_t r = 0;
+    if (lo + 1 < end && in_idx[lo] == u && in_idx[lo + 1] == u) {
+      const uint32_t rb = out_off[u];
+      if (unsorted[u]) {
+        for (uint32_t f = rb; f < (uint32_t)e; ++f) r += out_idx[f] == v;
+      } else {
+        uint32_t a = rb, b = (uint32_t)e;  // first copy of v in the sorted row
+        while (a < b) {
+          const uint32_t mid = a + (b - a) / 2;
+          if (out_idx[mid] < v)
+            a = mid + 1;
+          else
+            b = mid;
+        }
+        r = (uint32_t)e - a;
+      }
+    }
+    if (lo + r < end && in_idx[lo + r] == u)
+      perm[e] = lo + r;
     else
       atomicOr(err, 1u);
   }
@@ -205,8 +236,11 @@ static int wpr_build(gg_wpr_s* c) {
     GG_CUDA(cudaMemsetAsync(d_err, 0, 4, g->stream));
     const int grid = generic_grid(g, m);
     k_wpr_row_of<<<grid, kGenericThreads, 0, g->stream>>>(m, n, g->out_off(), c->row_of);
-    k_wpr_perm<<<grid, kGenericThreads, 0, g->stream>>>(m, c->row_of, g->out_idx(), g->in_off(), g->in_idx(), c->perm,
-                                                        d_err);
+    uint32_t* unsorted = reinterpret_cast<uint32_t*>(c->S);  // n flags; S is free until the first forward
+    GG_CUDA(cudaMemsetAsync(unsorted, 0, 4ull * n, g->stream));
+    k_wpr_row_unsorted<<<grid, kGenericThreads, 0, g->stream>>>(m, c->row_of, g->out_idx(), unsorted);
+    k_wpr_perm<<<grid, kGenericThreads, 0, g->stream>>>(m, c->row_of, g->out_off(), g->out_idx(), unsorted,
+                                                        g->in_off(), g->in_idx(), c->perm, d_err);
     unsigned h_err = 0;
     GG_CUDA(cudaMemcpyAsync(&h_err, d_err, 4, cudaMemcpyDeviceToHost, g->stream));
     GG_CUDA(cudaStreamSynchronize(g->stream));

@@ -549,14 +549,15 @@ static int ms_pull(gg_graph_s* g, bool vals, bool out, bool forward, const uint6
   p.vals = v;
   p.out = o;
   const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((p.nblocks + 7) / 8, (uint64_t)g->num_sms * 8));
-  static bool opted = false;
-  if (!opted) {
-    GG_CUDA(cudaFuncSetAttribute(k_ms_pull<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)ms_pull_smem<true>()));
-    GG_CUDA(cudaFuncSetAttribute(k_ms_pull<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)ms_pull_smem<true>()));
-    opted = true;
-  }
+  static DeviceOnce opted;
+  const int ok = opted.get(g->device, []() {
+    const bool a = cudaFuncSetAttribute(k_ms_pull<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)ms_pull_smem<true>()) == cudaSuccess;
+    const bool b = cudaFuncSetAttribute(k_ms_pull<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)ms_pull_smem<true>()) == cudaSuccess;
+    return a && b ? 1 : -1;
+  });
+  if (ok < 0) return fail(GG_ERR_CUDA, "cudaFuncSetAttribute failed for the multi-source pull");
   if (vals && out)
     k_ms_pull<true, true><<<grid, 256, ms_pull_smem<true>(), g->stream>>>(p);
   else if (vals)

@@ -3,6 +3,7 @@
 // gg_engine.cuh.  Mirrors graphgrind/ligra-numa.h:91-1082.
 #pragma once
 #include <algorithm>
+#include <atomic>
 
 #include "gg_engine.cuh"
 #include "gg_functors.cuh"
@@ -45,6 +46,25 @@ struct DevBuf {
   }
   ~DevBuf() {
     if (p) cudaFreeAsync(p, g->stream);
+  }
+};
+
+// Kernel attributes (dynamic shared memory opt-in) and occupancy are per
+// device: launchers cache them per device index, in atomics so that threads
+// driving different graphs may share them.
+constexpr int kMaxDevices = 16;
+struct DeviceOnce {
+  std::atomic<int> v[kMaxDevices];  // 0 = not yet set, else the cached value
+  // the cached value of device d, computing it with fn() once (uncached past kMaxDevices)
+  template <class Fn>
+  int get(int d, Fn fn) {
+    if (d < 0 || d >= kMaxDevices) return fn();
+    int x = v[d].load(std::memory_order_acquire);
+    if (x == 0) {
+      x = fn();
+      if (x > 0) v[d].store(x, std::memory_order_release);
+    }
+    return x;
   }
 };
 
@@ -119,15 +139,15 @@ int pull_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f
   p.tv = (uint32_t)g->opts.tile_vertices;
   const size_t smem_coo = pull_smem_bytes(true, kHW, 4, p.tv);
   const size_t smem_csc = pull_smem_bytes(false, kHW, 4);
-  // opt in once to the largest dynamic shared memory (widest tiles); the
-  // occupancy follows the tile width of this graph
-  static int occ[2][2] = {{-1, -1}, {-1, -1}};
-  auto launch = [&](auto kern, size_t smem, int& o) -> int {
-    if (o < 0) {
-      GG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)pull_smem_bytes(true, kHW, 4, kMaxTileVertices)));
-      o = 0;
-    }
+  // opt in once per device to the largest dynamic shared memory (widest
+  // tiles); the occupancy follows the tile width of this graph
+  static DeviceOnce opted_ring[2][2];
+  auto launch = [&](auto kern, size_t smem, DeviceOnce& once) -> int {
+    const int ok = once.get(g->device, [&]() {
+      return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)pull_smem_bytes(true, kHW, 4, kMaxTileVertices)) == cudaSuccess ? 1 : -1;
+    });
+    if (ok < 0) return fail(GG_ERR_CUDA, "cudaFuncSetAttribute failed for the dense pull");
     int blocks = 1;
     GG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kern, kPullThreads, smem));
     if (blocks < 1) blocks = 1;
@@ -138,16 +158,16 @@ int pull_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f
     return GG_OK;
   };
   if (coo && g->coo_kernel > 0) {  // per-warp COO pull: 0, 2 or 3 staging stages
-    static bool opted[2][4] = {};
-    static bool opted_pf[2] = {};
-    static bool opted_no[2] = {};
-    auto launch_w = [&](auto kern, int stages, bool& done) -> int {
+    static DeviceOnce opted[2][4];
+    static DeviceOnce opted_pf[2];
+    static DeviceOnce opted_no[2];
+    auto launch_w = [&](auto kern, int stages, DeviceOnce& once) -> int {
       const size_t smem = coo_w_smem_bytes(kHW, stages, 4, p.tv);
-      if (!done) {
-        GG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)coo_w_smem_bytes(kHW, stages, 4, kMaxTileVertices)));
-        done = true;
-      }
+      const int ok = once.get(g->device, [&]() {
+        return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)coo_w_smem_bytes(kHW, stages, 4, kMaxTileVertices)) == cudaSuccess ? 1 : -1;
+      });
+      if (ok < 0) return fail(GG_ERR_CUDA, "cudaFuncSetAttribute failed for the COO pull");
       int blocks = 1;
       GG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kern, kCooThreads, smem));
       if (blocks < 1) blocks = 1;
@@ -181,8 +201,8 @@ int pull_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f
     }
   }
   if (coo) {
-    if (all) return launch(k_pull<F, true, kHW, true>, smem_coo, occ[1][1]);
-    return launch(k_pull<F, true, kHW, false>, smem_coo, occ[1][0]);
+    if (all) return launch(k_pull<F, true, kHW, true>, smem_coo, opted_ring[1][1]);
+    return launch(k_pull<F, true, kHW, false>, smem_coo, opted_ring[1][0]);
   }
   (void)smem_csc;
   // CSC: the segmented pull over head bits
@@ -203,13 +223,16 @@ int pull_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f
   s.stats = p.stats;
   s.err = p.err;
   const size_t smem_seg = seg_smem_bytes(kHW, 4);
-  static int occ_seg[2] = {-1, -1};
-  auto launch_seg = [&](auto kern, int& o) -> int {
-    if (o < 0) {
-      GG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_seg));
-      GG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, kSegThreads, smem_seg));
-      if (o < 1) o = 1;
-    }
+  static DeviceOnce occ_seg[2];
+  auto launch_seg = [&](auto kern, DeviceOnce& once) -> int {
+    const int o = once.get(g->device, [&]() {
+      if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_seg) != cudaSuccess)
+        return -1;
+      int b = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, kSegThreads, smem_seg) != cudaSuccess) return -1;
+      return b < 1 ? 1 : b;
+    });
+    if (o < 0) return fail(GG_ERR_CUDA, "kernel set-up failed for the CSC pull");
     const int grid = (int)std::min<uint64_t>((uint64_t)g->num_sms * o, s.ntiles);
     kern<<<grid, kSegThreads, smem_seg, g->stream>>>(s, f);
     GG_CUDA(cudaGetLastError());

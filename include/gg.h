@@ -436,7 +436,11 @@ int gg_batch_bfs(gg_graph_batch_t b, const uint32_t* sources, int32_t* levels, g
  * which recomputes each segment from its checkpoint and reverses through it.
  * weights / grad_weights: host, m entries in the graph's out-edge order
  * (gg_host_graph offsets/indices of the current orientation); tele, x0, x_out,
- * grad_x, grad_tele, grad_x0: host, n entries (grad_* may be NULL). */
+ * grad_x, grad_tele, grad_x0: host, n entries (grad_* may be NULL).
+ * Repeated edges u->v carry one weight each.  create returns GG_ERR_FORMAT
+ * when an in-edge list of the current orientation is not sorted by source: the
+ * library builds a directed graph's in-edges sorted, the given rows are used as
+ * they are (a symmetric graph's in-edges, a transposed graph's in-edges). */
 typedef struct gg_wpr_s* gg_wpr_t;
 int gg_pagerank_weighted_create(gg_graph_t g, int32_t iters, float damping, int32_t checkpoint_every,
                                 int32_t normalize, gg_wpr_t* out);
