@@ -52,10 +52,21 @@ METRIC = "GTEPS"
 UNIT = "GTEPS"
 WORKLOAD = ("RMAT-24 directed (n=2^24, edge factor 16, a/b/c/d=.57/.19/.19/.05, seed 2, dedup, FP32 weights U(0,1]), "
             "P=384 edge-balanced Hilbert COO; step = BFS from 100 + PageRank 10 iterations + SpMV")
+
+
+def workload(scale: int, partitions: int, start: int) -> str:
+    """The workload line for the configuration actually run."""
+    if (scale, partitions, start) == (24, 384, 100):
+        return WORKLOAD
+    return (f"RMAT-{scale} directed (n=2^{scale}, edge factor 16, a/b/c/d=.57/.19/.19/.05, seed 2, dedup, FP32 "
+            f"weights U(0,1]), P={partitions} edge-balanced Hilbert COO; step = BFS from {start} + PageRank 10 "
+            "iterations + SpMV")
+
+
 HBM_FALLBACK_GBS = 6650.0
 # DRAM bytes per PageRank-pull launch of the default workload, from one ncu
 # capture (profiles/dram_k_pull_coo_w_pagerank_rmat24.md)
-TRAFFIC_RMAT24_PR_PULL = 2118674176
+TRAFFIC_RMAT24_PR_PULL = {0: 2118674176}  # by vertex order
 TRAFFIC_TILE_EDGES = 1 << 17
 
 
@@ -140,7 +151,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
     hg = make_graph(gg, args.scale, 2, gg.W_FLOAT32)
     log(f"[rank {rank}] generated RMAT-{args.scale}: n={hg.n} m={hg.m} in {time.time() - t0:.1f}s")
     t0 = time.time()
-    g = gg.Graph(hg, partitions=args.partitions, tile_edges=args.tile_edges)
+    g = gg.Graph(hg, partitions=args.partitions, tile_edges=args.tile_edges, vertex_order=args.vertex_order)
     g.set_dense_policy(args.dense_policy)
     info = g.info()
     log(f"[rank {rank}] device graph built in {time.time() - t0:.1f}s: {info.device_bytes / 2**30:.2f} GiB, "
@@ -248,8 +259,9 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
                                     "frac": round(ach / peak, 4)}
     traffic, traffic_src = args.traffic, "--traffic" if args.traffic else None
     if traffic is None and args.scale == 24 and args.partitions == 384 and args.dense_policy == 0 and \
-            args.tile_edges == TRAFFIC_TILE_EDGES and kernel_name == "k_pull_coo_w":
-        traffic = TRAFFIC_RMAT24_PR_PULL
+            args.tile_edges == TRAFFIC_TILE_EDGES and kernel_name == "k_pull_coo_w" and \
+            args.vertex_order in TRAFFIC_RMAT24_PR_PULL:
+        traffic = TRAFFIC_RMAT24_PR_PULL[args.vertex_order]
         traffic_src = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/dram_k_pull_coo_w_pagerank_rmat24.md"
     achieved = algo_bytes / (pull_ms / 1e3) / 1e9 if pull_ms > 0 else None
     out = {
@@ -257,9 +269,12 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
         "warmup": args.warmup, "ms_per_step": round(dev_ms / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 (PageRank/SpMV), u32 (BFS ids)",
         "data": "synthetic: seeded RMAT generated on the host (no dataset)",
-        "config": {"workload": WORKLOAD, "n": n, "m": m, "partitions": args.partitions,
+        "config": {"workload": workload(args.scale, args.partitions, args.start), "n": n, "m": m,
+                   "partitions": args.partitions,
                    "dense_policy": ["reference rule", "csc pull", "coo pull"][args.dense_policy],
                    "tile_edges": args.tile_edges,
+                   "vertex_order": ["given ids", "hottest sources first inside each partition (results in the "
+                                    "given ids)"][args.vertex_order],
                    "autotuned_knobs": knobs or None, "autotune_seconds": round(tune_s, 2),
                    "l2": "inputs larger than L2 (graph arrays > 3 GB vs 126 MB L2)",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
@@ -473,6 +488,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched / adjoint comparisons")
     ap.add_argument("--no-autotune", action="store_true", help="keep the library's default runtime knobs")
+    ap.add_argument("--vertex-order", type=int, default=1, choices=[0, 1],
+                    help="device numbering: 0 the given ids, 1 hottest sources first inside each partition")
     ap.add_argument("--tile-edges", type=int, default=1 << 17,
                     help="target edges per CTA tile (gg_autotune_build's choice for this workload)")
     ap.add_argument("--traffic", type=float, default=None,

@@ -37,6 +37,7 @@ W_NONE, W_INT32, W_FLOAT32 = 0, 1, 2
 BALANCE_EDGE, BALANCE_VERTEX = 0, 1
 PART_DEST, PART_SOURCE = 0, 1
 ORDER_CSR, ORDER_HILBERT = 0, 1
+VORDER_GIVEN, VORDER_HOT_FIRST = 0, 1
 EM_FORCE_SPARSE, EM_FORCE_CSC, EM_FORCE_COO, EM_NO_OUTPUT = 0x1, 0x2, 0x4, 0x8
 F_BFS, F_CC, F_PR, F_PRDELTA, F_SPMV, F_BF, F_BC, F_BC_BACK, F_BP = range(1, 10)
 
@@ -64,7 +65,7 @@ class BuildOpts(C.Structure):
     _fields_ = [("num_partitions", C.c_int32), ("balance", C.c_int32), ("part_how", C.c_int32),
                 ("relabel", C.c_int32), ("order", C.c_int32), ("tile_vertices", C.c_int32),
                 ("tile_edges", C.c_int32), ("build_coo", C.c_int32), ("coo_window", C.c_int32),
-                ("coo_dst_window", C.c_int32)]
+                ("coo_dst_window", C.c_int32), ("vertex_order", C.c_int32)]
 
 
 class TuneTrial(C.Structure):
@@ -141,12 +142,14 @@ _sig("gg_vebo", C.c_int, C.POINTER(HostGraphC), C.c_int32, _P, _P, C.POINTER(Hos
 _sig("gg_partition_sizes", C.c_int, _u32p, _u32p, C.c_uint32, C.c_uint64, C.c_int32, C.c_int32, C.c_int32,
      C.c_int32, _i64p, _i64p)
 _sig("gg_hilbert_key", C.c_int64, C.c_int64, C.c_int64, C.c_int64)
+_sig("gg_hot_first_order", C.c_int, C.POINTER(HostGraphC), C.POINTER(BuildOpts), _P, _P)
 _sig("gg_graph_build", C.c_int, C.POINTER(HostGraphC), C.POINTER(BuildOpts), C.POINTER(_P))
 _sig("gg_graph_destroy", C.c_int, _P)
 _sig("gg_graph_get_info", C.c_int, _P, C.POINTER(GraphInfo))
 _sig("gg_graph_partition_starts", C.c_int, _P, _i64p)
 _sig("gg_graph_transpose", C.c_int, _P)
 _sig("gg_graph_device_arrays", C.c_int, _P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), C.POINTER(_P))
+_sig("gg_graph_vertex_order", C.c_int, _P, _P)
 _sig("gg_frontier_single", C.c_int, _P, C.c_uint32, C.POINTER(_P))
 _sig("gg_frontier_all", C.c_int, _P, C.POINTER(_P))
 _sig("gg_frontier_empty", C.c_int, _P, C.POINTER(_P))
@@ -218,6 +221,7 @@ EXPORTED = [
     "gg_batch_create", "gg_batch_destroy", "gg_batch_info", "gg_batch_bfs",
     "gg_pagerank_weighted_create", "gg_pagerank_weighted_destroy", "gg_pagerank_weighted_fwd",
     "gg_pagerank_weighted_bwd", "gg_autotune", "gg_autotune_build", "gg_autotune_ppr_k",
+    "gg_hot_first_order", "gg_graph_vertex_order",
 ]
 
 
@@ -340,6 +344,15 @@ class HostGraph:
         t = HostGraphC()
         check(lib.gg_host_graph_transpose(C.byref(self.c), C.byref(t)), "gg_host_graph_transpose")
         return HostGraph(t)
+
+    def hot_first_order(self, partitions=384, balance=BALANCE_EDGE, part_how=PART_DEST, relabel=False):
+        """gg_hot_first_order: (new_of_old[n], COO partition starts[P+1]) of VORDER_HOT_FIRST."""
+        o = BuildOpts(partitions, balance, part_how, int(relabel), ORDER_HILBERT, 0, 0, 0, 0, 0, VORDER_HOT_FIRST)
+        new_of_old = np.empty(self.n, np.uint32)
+        starts = np.empty(partitions + 1, np.int64)
+        check(lib.gg_hot_first_order(C.byref(self.c), C.byref(o), _ptr(new_of_old), _ptr(starts)),
+              "gg_hot_first_order")
+        return new_of_old, starts
 
     def vebo(self, partitions=384):
         """VEBO reordering: (relabelled HostGraph, new_of_old[n], vertices per partition[P])."""
@@ -470,11 +483,12 @@ class Graph:
     """partitioned_graph on the device (gg_graph_build)."""
 
     def __init__(self, host: HostGraph, partitions=384, balance=BALANCE_EDGE, part_how=PART_DEST, relabel=False,
-                 order=ORDER_HILBERT, tile_vertices=0, tile_edges=0, build_coo=0, coo_window=0, coo_dst_window=0):
+                 order=ORDER_HILBERT, tile_vertices=0, tile_edges=0, build_coo=0, coo_window=0, coo_dst_window=0,
+                 vertex_order=VORDER_GIVEN):
         self.host = host
         self._deps = weakref.WeakSet()
         o = BuildOpts(partitions, balance, part_how, int(relabel), order, tile_vertices, tile_edges, build_coo,
-                      coo_window, coo_dst_window)
+                      coo_window, coo_dst_window, vertex_order)
         h = C.c_void_p()
         check(lib.gg_graph_build(C.byref(host.c), C.byref(o), C.byref(h)), "gg_graph_build")
         self.h = h
@@ -501,6 +515,12 @@ class Graph:
         s = np.zeros(P + 1, np.int64)
         check(lib.gg_graph_partition_starts(self.h, s.ctypes.data_as(_i64p)), "gg_graph_partition_starts")
         return s
+
+    def vertex_order(self) -> np.ndarray:
+        """new_of_old[n]: the device id of every given vertex (gg_graph_vertex_order)."""
+        a = np.empty(self.n, np.uint32)
+        check(lib.gg_graph_vertex_order(self.h, _ptr(a)), "gg_graph_vertex_order")
+        return a
 
     def transpose(self):
         check(lib.gg_graph_transpose(self.h), "gg_graph_transpose")
@@ -768,9 +788,10 @@ def autotune_build(host, app=APP_PAGERANK, start=0, candidates=()):
     """Build `host` under each candidate (dicts of Graph keyword options),
     autotune each, and return (best options dict, best trial dict)."""
     names = ("partitions", "balance", "part_how", "relabel", "order", "tile_vertices", "tile_edges", "build_coo",
-             "coo_window", "coo_dst_window")
+             "coo_window", "coo_dst_window", "vertex_order")
     defaults = dict(partitions=384, balance=BALANCE_EDGE, part_how=PART_DEST, relabel=0, order=ORDER_HILBERT,
-                    tile_vertices=0, tile_edges=0, build_coo=0, coo_window=0, coo_dst_window=0)
+                    tile_vertices=0, tile_edges=0, build_coo=0, coo_window=0, coo_dst_window=0,
+                    vertex_order=VORDER_GIVEN)
     cands = (BuildOpts * len(candidates))()
     for i, c in enumerate(candidates):
         d = dict(defaults, **c)

@@ -354,6 +354,9 @@ int gg_pagerank_weighted_create(gg_graph_t g, int32_t iters, float damping, int3
                                 int32_t normalize, gg_wpr_t* out) {
   if (!graph_live(g) || !out || iters < 0 || checkpoint_every < 1 || !(damping >= 0.f && damping <= 1.f))
     return fail(GG_ERR_INVALID_ARG, "gg_pagerank_weighted_create: iters >= 0, checkpoint_every >= 1, 0 <= damping <= 1");
+  if (g->relabeled)
+    return fail(GG_ERR_UNSUPPORTED, "gg_pagerank_weighted_create: weights follow the out-edge order of the given "
+                                    "ids; build the graph with vertex_order = GG_VORDER_GIVEN");
   gg_wpr_s* c = new (std::nothrow) gg_wpr_s;
   if (!c) return fail(GG_ERR_OOM, "weighted PageRank: out of host memory");
   c->g = g;

@@ -175,16 +175,28 @@ static int run_ppr_k(gg_graph_s* g, int32_t k, int32_t iters, float damping, con
   if (!brows.empty())
     GG_CUDA(cudaMemcpyAsync(d_brows, brows.data(), 4 * brows.size(), cudaMemcpyHostToDevice, g->stream));
   g->kernels = 0;
-  cudaEvent_t ea, eb;
-  cudaEventCreate(&ea);
-  cudaEventCreate(&eb);
-  // inputs are uploaded before the timed region
+  struct EvHold {
+    cudaEvent_t a = nullptr, b = nullptr;
+    ~EvHold() {
+      if (a) cudaEventDestroy(a);
+      if (b) cudaEventDestroy(b);
+    }
+  } ev;
+  cudaEventCreate(&ev.a);
+  cudaEventCreate(&ev.b);
+  cudaEvent_t ea = ev.a, eb = ev.b;
+  // inputs are uploaded before the timed region (a renumbered graph's teleport
+  // rows go through Y, which is written only later)
   if (tele_host) {
-    GG_CUDA(cudaMemcpyAsync(T, tele_host, 4 * nk, cudaMemcpyHostToDevice, g->stream));
+    GG_CUDA(cudaMemcpyAsync(g->relabeled ? Y : T, tele_host, 4 * nk, cudaMemcpyHostToDevice, g->stream));
     cudaEventRecord(ea, g->stream);
+    if (g->relabeled) GG_TRY(device_order<float>(g, Y, (uint32_t)k, T));
   } else {
+    std::vector<uint32_t> dev_seeds(seeds, seeds + k);
+    for (auto& v : dev_seeds) v = g->device_id(v);
     GG_CUDA(cudaMallocAsync((void**)&d_seeds, 4 * k, g->stream));
-    GG_CUDA(cudaMemcpyAsync(d_seeds, seeds, 4 * k, cudaMemcpyHostToDevice, g->stream));
+    GG_CUDA(cudaMemcpyAsync(d_seeds, dev_seeds.data(), 4 * k, cudaMemcpyHostToDevice, g->stream));
+    GG_CUDA(cudaStreamSynchronize(g->stream));  // dev_seeds leaves scope
     cudaEventRecord(ea, g->stream);
     GG_CUDA(cudaMemsetAsync(T, 0, 4 * nk, g->stream));
     k_ppr_onehot<<<1, 64, 0, g->stream>>>(d_seeds, (uint32_t)k, T);
@@ -235,15 +247,16 @@ static int run_ppr_k(gg_graph_s* g, int32_t k, int32_t iters, float damping, con
     g->kernels++;
   }
   if (iters == 0) GG_CUDA(cudaMemcpyAsync(Y, T, 4 * nk, cudaMemcpyDeviceToDevice, g->stream));
+  DevBuf<float> ty;
+  const float* res = Y;
+  GG_TRY(given_order<float>(g, Y, (uint32_t)k, ty, &res));
   GG_CUDA(cudaGetLastError());
   cudaEventRecord(eb, g->stream);
   GG_CUDA(cudaEventSynchronize(eb));
   float ms = 0;
   cudaEventElapsedTime(&ms, ea, eb);
-  cudaEventDestroy(ea);
-  cudaEventDestroy(eb);
   if (out) {
-    GG_CUDA(cudaMemcpyAsync(out, Y, 4 * nk, cudaMemcpyDeviceToHost, g->stream));
+    GG_CUDA(cudaMemcpyAsync(out, res, 4 * nk, cudaMemcpyDeviceToHost, g->stream));
     GG_CUDA(cudaStreamSynchronize(g->stream));
   }
   if (st) {
@@ -494,21 +507,27 @@ __global__ void k_ms_level_mask(uint32_t n, int32_t r, const int32_t* lvl, uint6
 }
 
 // (dep - 1/paths) / (1/paths), app/BC.C:220-222, into n x k outputs; NaN where unreached.
-__global__ void k_ms_bc_final(uint32_t n, uint32_t k, const float* dep, const float* sigma, float* dep_out,
-                              float* sigma_out) {
+// Output rows in the given vertex order: row u of the output is device row
+// new_of_old[u] (u itself when the graph keeps its given ids).
+__global__ void k_ms_bc_final(uint32_t n, uint32_t k, const uint32_t* new_of_old, const float* dep,
+                              const float* sigma, float* dep_out, float* sigma_out) {
   const uint64_t total = (uint64_t)n * k;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t v = i / k, j = i % k;
+    const uint64_t u = i / k, j = i % k;
+    const uint64_t v = new_of_old ? new_of_old[u] : u;
     const float inv = 1.0f / sigma[v * 64 + j];
     dep_out[i] = (dep[v * 64 + j] - inv) / inv;
     if (sigma_out) sigma_out[i] = sigma[v * 64 + j];
   }
 }
 
-__global__ void k_ms_levels_out(uint32_t n, uint32_t k, const int32_t* lvl, int32_t* out) {
+__global__ void k_ms_levels_out(uint32_t n, uint32_t k, const uint32_t* new_of_old, const int32_t* lvl, int32_t* out) {
   const uint64_t total = (uint64_t)n * k;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x)
-    out[i] = lvl[(i / k) * 64 + i % k];
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t u = i / k;
+    const uint64_t v = new_of_old ? new_of_old[u] : u;
+    out[i] = lvl[v * 64 + i % k];
+  }
 }
 
 // Device allocations released (stream-ordered) when the holder leaves scope.
@@ -568,9 +587,12 @@ static int ms_pull(gg_graph_s* g, bool vals, bool out, bool forward, const uint6
   return GG_OK;
 }
 
-static int run_ms(gg_graph_s* g, int32_t k, const uint32_t* sources, bool bc, int32_t* levels_out, float* dep_out,
-                  float* np_out, gg_run_stats* st) {
+static int run_ms(gg_graph_s* g, int32_t k, const uint32_t* given_sources, bool bc, int32_t* levels_out,
+                  float* dep_out, float* np_out, gg_run_stats* st) {
   const uint32_t n = g->n;
+  std::vector<uint32_t> dev_sources(given_sources, given_sources + k);
+  for (auto& v : dev_sources) v = g->device_id(v);
+  const uint32_t* sources = dev_sources.data();
   const uint64_t n64 = (uint64_t)n * 64;
   const uint64_t kmask = k == 64 ? ~0ull : ((1ull << k) - 1);
   DevAllocs mem(g->stream);
@@ -639,12 +661,13 @@ static int run_ms(gg_graph_s* g, int32_t k, const uint32_t* sources, bool bc, in
   if (bc) {
     GG_TRY(dout.alloc(g, nk));
     if (np_out) GG_TRY(sout.alloc(g, nk));
-    k_ms_bc_final<<<generic_grid(g, nk), kGenericThreads, 0, g->stream>>>(n, (uint32_t)k, dep, sigma, dout.p,
-                                                                          np_out ? sout.p : nullptr);
+    k_ms_bc_final<<<generic_grid(g, nk), kGenericThreads, 0, g->stream>>>(
+        n, (uint32_t)k, g->relabeled ? g->d_new_of_old : nullptr, dep, sigma, dout.p, np_out ? sout.p : nullptr);
     g->kernels++;
   } else if (levels_out) {
     GG_TRY(lout.alloc(g, nk));
-    k_ms_levels_out<<<generic_grid(g, nk), kGenericThreads, 0, g->stream>>>(n, (uint32_t)k, lvl, lout.p);
+    k_ms_levels_out<<<generic_grid(g, nk), kGenericThreads, 0, g->stream>>>(
+        n, (uint32_t)k, g->relabeled ? g->d_new_of_old : nullptr, lvl, lout.p);
     g->kernels++;
   }
   GG_CUDA(cudaGetLastError());

@@ -95,5 +95,8 @@ extern "C" int gg_bp(gg_graph_t g, int32_t iters, const float* vert_potential, c
                      float* vert_out, gg_run_stats* st) {
   if (!graph_live(g) || iters < 0 || !vert_potential || (g->m && !edge_potential) || !vert_out)
     return fail(GG_ERR_INVALID_ARG, "gg_bp: bad arguments");
+  if (g->relabeled)
+    return fail(GG_ERR_UNSUPPORTED, "gg_bp: edge potentials follow the in-edge slots of the given ids; build the "
+                                    "graph with vertex_order = GG_VORDER_GIVEN");
   return run_bp(g, iters, vert_potential, edge_potential, vert_out, st);
 }

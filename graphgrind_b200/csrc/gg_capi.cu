@@ -205,9 +205,19 @@ static int run_bfs(gg_graph_s* g, uint32_t start, int32_t* parents, int32_t* lev
     GG_TRY(edge_map(g, F.f, f, thr, 0, &out));
     F.reset(out);
   }
+  const int32_t* par_out = par.p;
+  const int32_t* lev_out = lev.p;
+  if (g->relabeled) {
+    int32_t* tp = reinterpret_cast<int32_t*>(g->ws.d_order[0]);
+    k_ids_to_given<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(n, g->d_new_of_old, g->d_old_of_new,
+                                                                          par.p, tp);
+    g->kernels++;
+    par_out = tp;
+  }
+  GG_TRY(given_order<int32_t>(g, lev.p, 1, &lev_out));
   const double ms = tm.stop();
-  GG_TRY(to_host(g, parents, par.p, n));
-  GG_TRY(to_host(g, levels, lev.p, n));
+  GG_TRY(to_host(g, parents, par_out, n));
+  GG_TRY(to_host(g, levels, lev_out, n));
   fill_stats(st, ms, round, trav, g->kernels);
   return GG_OK;
 }
@@ -220,7 +230,11 @@ static int run_cc(gg_graph_s* g, int32_t* ids_out, gg_run_stats* st) {
   GG_TRY(ids.alloc(g, n));
   GG_TRY(prev.alloc(g, n));
   EventTimer tm(g->stream);
-  k_iota<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>((uint32_t*)ids.p, n);
+  // IDs[i] = i (app/Components.C:206): the given id, also on a renumbered graph
+  if (g->relabeled)
+    GG_CUDA(cudaMemcpyAsync(ids.p, g->d_old_of_new, 4ull * n, cudaMemcpyDeviceToDevice, g->stream));
+  else
+    k_iota<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>((uint32_t*)ids.p, n);
   FrontierHold F;
   GG_TRY(gg_frontier_all(g, &F.f));
   int rounds = 0;
@@ -237,8 +251,10 @@ static int run_cc(gg_graph_s* g, int32_t* ids_out, gg_run_stats* st) {
     F.reset(out);
     ++rounds;
   }
+  const int32_t* ids_res = ids.p;
+  GG_TRY(given_order<int32_t>(g, ids.p, 0, &ids_res));
   const double ms = tm.stop();
-  GG_TRY(to_host(g, ids_out, ids.p, n));
+  GG_TRY(to_host(g, ids_out, ids_res, n));
   fill_stats(st, ms, rounds, trav, g->kernels);
   return GG_OK;
 }
@@ -298,8 +314,10 @@ static int run_pagerank(gg_graph_s* g, int max_iter, int bit_all, float* ranks, 
     if (bit_all) o->bit = true;  // output.bit = true
     F.reset(o);
   }
+  const float* res = last;
+  GG_TRY(given_order<float>(g, last, 0, &res));
   const double ms = tm.stop();
-  GG_TRY(to_host(g, ranks, last, n));
+  GG_TRY(to_host(g, ranks, res, n));
   fill_stats(st, ms, count, trav, g->kernels);
   return GG_OK;
 }
@@ -386,8 +404,10 @@ static int run_pagerank_converge(gg_graph_s* g, int32_t max_iter, double eps, fl
     ++count;
     std::swap(p_curr, p_next);
   }
+  const float* res = p_curr;
+  GG_TRY(given_order<float>(g, p_curr, 0, &res));
   const double ms = tm.stop();
-  GG_TRY(to_host(g, ranks, p_curr, n));
+  GG_TRY(to_host(g, ranks, res, n));
   fill_stats(st, ms, count, (uint64_t)count * g->m, g->kernels);
   return GG_OK;
 }
@@ -445,8 +465,10 @@ static int run_pagerank_delta(gg_graph_s* g, float* ranks, gg_run_stats* st) {
     if (l1 < eps) break;
     F.reset(A.release());
   }
+  const float* res = p.p;
+  GG_TRY(given_order<float>(g, p.p, 0, &res));
   const double ms = tm.stop();
-  GG_TRY(to_host(g, ranks, p.p, n));
+  GG_TRY(to_host(g, ranks, res, n));
   fill_stats(st, ms, round, trav, g->kernels);
   return GG_OK;
 }
@@ -458,9 +480,12 @@ static int run_spmv(gg_graph_s* g, const float* x_in, float* y_out, gg_run_stats
   DevBuf<float> x, y;
   GG_TRY(x.alloc(g, n));
   GG_TRY(y.alloc(g, n));
-  // the input vector is uploaded before the timed Compute loop (like the graph)
-  if (x_in) GG_CUDA(cudaMemcpyAsync(x.p, x_in, 4ull * n, cudaMemcpyHostToDevice, g->stream));
+  // the input vector is uploaded before the timed Compute loop (like the
+  // graph); a renumbered graph takes it through its given-order array
+  float* xg = g->relabeled ? reinterpret_cast<float*>(g->ws.d_order[0]) : x.p;
+  if (x_in) GG_CUDA(cudaMemcpyAsync(xg, x_in, 4ull * n, cudaMemcpyHostToDevice, g->stream));
   EventTimer tm(g->stream);
+  if (x_in && g->relabeled) GG_TRY(device_order<float>(g, xg, 1, x.p));
   if (!x_in) GG_TRY(fill<float>(g, x.p, n, (float)(1 / (double)n)));
   GG_TRY(fill<float>(g, y.p, n, 0.0f));
   FrontierHold F;
@@ -472,8 +497,10 @@ static int run_spmv(gg_graph_s* g, const float* x_in, float* y_out, gg_run_stats
   gg_frontier_s* out = nullptr;
   GG_TRY(edge_map(g, F.f, f, app_threshold(g), GG_EM_NO_OUTPUT, &out));  // output.del()
   frontier_free(out);
+  const float* res = y.p;
+  GG_TRY(given_order<float>(g, y.p, 1, &res));
   const double ms = tm.stop();
-  GG_TRY(to_host(g, y_out, y.p, n));
+  GG_TRY(to_host(g, y_out, res, n));
   fill_stats(st, ms, 1, g->m, g->kernels);
   return GG_OK;
 }
@@ -510,8 +537,10 @@ static int run_bf(gg_graph_s* g, uint32_t start, int32_t* dist, gg_run_stats* st
     F.reset(out);
     ++round;
   }
+  const int32_t* res = sp.p;
+  GG_TRY(given_order<int32_t>(g, sp.p, 0, &res));
   const double ms = tm.stop();
-  GG_TRY(to_host(g, dist, sp.p, n));
+  GG_TRY(to_host(g, dist, res, n));
   fill_stats(st, ms, (int)round, trav, g->kernels);
   return GG_OK;
 }
@@ -556,7 +585,11 @@ static int run_bc(gg_graph_s* g, uint32_t start, float* dep_out, float* np_out, 
     levels.push_back(out);
     F = out;
   }
-  if (np_out) GG_TRY(to_host(g, np_out, np.p, n));
+  if (np_out) {
+    const float* res = np.p;
+    GG_TRY(given_order<float>(g, np.p, 0, &res));
+    GG_TRY(to_host(g, np_out, res, n));
+  }
   GG_TRY(fill<float>(g, dep.p, n, 0.0f));
   k_invert<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(n, np.p);  // inverseNumPaths aliases NumPaths
   g->kernels++;
@@ -582,8 +615,10 @@ static int run_bc(gg_graph_s* g, uint32_t start, float* dep_out, float* np_out, 
   if (rc) return rc;
   k_bc_final<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(n, dep.p, np.p);
   g->kernels++;
+  const float* res = dep.p;
+  GG_TRY(given_order<float>(g, dep.p, 1, &res));
   const double ms = tm.stop();
-  GG_TRY(to_host(g, dep_out, dep.p, n));
+  GG_TRY(to_host(g, dep_out, res, n));
   fill_stats(st, ms, round, trav, g->kernels);
   return GG_OK;
 }
@@ -735,7 +770,7 @@ int gg_vertex_filter(gg_graph_t g, gg_frontier_t f, int32_t vid, const void* arg
 
 int gg_bfs(gg_graph_t g, uint32_t start, int32_t* parents, int32_t* levels, gg_run_stats* st) {
   if (!g || start >= g->n) return fail(GG_ERR_INVALID_ARG, "gg_bfs: bad arguments");
-  return run_bfs(g, start, parents, levels, st);
+  return run_bfs(g, g->device_id(start), parents, levels, st);
 }
 int gg_components(gg_graph_t g, int32_t* ids, gg_run_stats* st) {
   if (!g) return fail(GG_ERR_INVALID_ARG, "gg_components: null graph");
@@ -759,11 +794,11 @@ int gg_spmv(gg_graph_t g, const float* x, float* y, gg_run_stats* st) {
 }
 int gg_bellman_ford(gg_graph_t g, uint32_t start, int32_t* dist, gg_run_stats* st) {
   if (!g || start >= g->n) return fail(GG_ERR_INVALID_ARG, "gg_bellman_ford: bad arguments");
-  return run_bf(g, start, dist, st);
+  return run_bf(g, g->device_id(start), dist, st);
 }
 int gg_bc(gg_graph_t g, uint32_t start, float* dep, float* np, gg_run_stats* st) {
   if (!g || start >= g->n) return fail(GG_ERR_INVALID_ARG, "gg_bc: bad arguments");
-  return run_bc(g, start, dep, np, st);
+  return run_bc(g, g->device_id(start), dep, np, st);
 }
 
 }  // extern "C"

@@ -4,6 +4,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <string>
+#include <vector>
 
 #include "../../include/gg.h"
 
@@ -20,6 +21,16 @@ int fail(int code, const char* fmt, ...);
     int r__ = (expr);             \
     if (r__ != GG_OK) return r__; \
   } while (0)
+
+// Rows of g renumbered: new vertex i holds the out-edges of old vertex
+// old_of_new[i], in their order, with neighbour ids mapped through new_of_old
+// and the weights carried along.  out is allocated like gg_host_graph_read's.
+int relabel_host_graph(const gg_host_graph* g, const uint32_t* old_of_new, const uint32_t* new_of_old,
+                       gg_host_graph* out);
+// GG_VORDER_HOT_FIRST: inside every [starts[p], starts[p+1]) the vertices by
+// descending out-degree, ties by id.  starts has P+1 ascending entries, 0 .. n.
+void hot_first_order(const gg_host_graph* g, const int64_t* starts, int32_t P, uint32_t* old_of_new,
+                     uint32_t* new_of_old);
 
 inline uint64_t mix64(uint64_t z) {
   // SplitMix64 output function (Steele, Lea & Flood, OOPSLA 2014).

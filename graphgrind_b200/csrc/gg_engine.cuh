@@ -104,6 +104,7 @@ struct Workspace {
   double* d_red = nullptr;                // reduction scratch (double)
   double* h_red = nullptr;                // pinned
   unsigned long long* d_loop = nullptr;   // state of the device-driven level loop (16 words)
+  uint32_t* d_order[2] = {nullptr, nullptr};  // renumbered graphs: n-entry arrays for the given-order copies
 };
 
 }  // namespace gg
@@ -141,7 +142,13 @@ struct gg_graph_s {
   int dense_policy = 0;
   int sparse_div = 20;  // the apps' edgeMap threshold is m / sparse_div (app/*.C pass m/20)
   int device_loop = 1;  // BFS runs consecutive sparse levels in one cooperative launch
-  int coo_kernel = 1;  // 0 CTA ring (k_pull), 1 per-warp direct loads (fastest measured), 2/3 per-warp bulk-copy rings
+  int coo_kernel = 6;  // 0 CTA ring (k_pull), 1 per-warp direct loads, 2/3 per-warp bulk-copy rings, 6 direct loads
+                       // with cross-lane run merging (fastest measured)
+  // gg_build_opts.vertex_order: device ids differ from the given ids
+  bool relabeled = false;
+  std::vector<uint32_t> h_new_of_old, h_old_of_new;
+  uint32_t *d_new_of_old = nullptr, *d_old_of_new = nullptr;
+  uint32_t device_id(uint32_t v) const { return relabeled ? h_new_of_old[v] : v; }
   uint64_t device_bytes = 0;
   int kernels = 0;  // kernels launched since the counter was last reset
   std::unordered_set<gg_frontier_s*> frontiers;  // live frontiers (freed with the graph)
@@ -465,7 +472,12 @@ __host__ __device__ constexpr size_t coo_w_smem_bytes(bool hw, int stages, int v
 // NOOUT: the caller discards edgeMap's output (GG_EM_NO_OUTPUT) and F's
 // commit of the identity is a no-op (sums): no touched flags, no next-frontier
 // bits, no stats; destinations with a non-identity sum are committed.
-template <class F, bool HW, bool ALL, int STAGES, bool CONTIG = false, bool PF = false, bool NOOUT = false>
+// MERGE: destination runs that continue across lanes are combined with warp
+// shuffles before the shared-memory accumulation, so a destination appears in
+// at most one accumulation per block (instead of one per lane it spans, all
+// on one address).
+template <class F, bool HW, bool ALL, int STAGES, bool CONTIG = false, bool PF = false, bool NOOUT = false,
+          bool MERGE = false>
 __global__ void __launch_bounds__(kCooThreads, GG_COO_MIN_BLOCKS) k_pull_coo_w(const PullParams p, const F f) {
   static_assert(!NOOUT || F::kIdentityCommitNoop, "discarding the output needs a no-op identity commit");
   static_assert(!CONTIG || STAGES == 0, "lane-contiguous edges use direct loads");
@@ -655,6 +667,55 @@ __global__ void __launch_bounds__(kCooThreads, GG_COO_MIN_BLOCKS) k_pull_coo_w(c
         }
         continue;
       }
+      auto flush = [&](int l, V v) {
+        F::atomic_combine(&s_acc[l], v);
+        if (!F::kPositive && !NOOUT) s_touch[l] = 1;
+      };
+      if constexpr (MERGE) {
+        // The block is sorted by destination, so a lane's middle runs are
+        // complete and go straight to shared memory, while its first run
+        // (held back when the lane has two or more) and its last run may
+        // continue in the neighbouring lanes.
+        int cur = -1, hd = -1;
+        V acc = F::identity(), ha = F::identity();
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          if (!vld[k]) continue;
+          const int l = (int)dv[k];
+          if (l != cur) {
+            if (cur >= 0) {
+              if (hd < 0) {
+                hd = cur;
+                ha = acc;
+              } else {
+                flush(cur, acc);
+              }
+            }
+            cur = l;
+            acc = val[k];
+          } else {
+            acc = F::combine(acc, val[k]);
+          }
+        }
+        // a held-back first run joins the previous lane's last run
+        const int nhd = __shfl_down_sync(0xffffffffu, hd, 1);
+        const V nha = __shfl_down_sync(0xffffffffu, ha, 1);
+        const int ptl = __shfl_up_sync(0xffffffffu, cur, 1);
+        if (lane < 31 && nhd >= 0 && nhd == cur) acc = F::combine(acc, nha);
+        if (hd >= 0 && !(lane > 0 && ptl == hd)) flush(hd, ha);
+        // last runs: equal destinations sit in consecutive lanes; a segmented
+        // reduction leaves each segment's total in its last lane
+        const uint32_t heads = __ballot_sync(0xffffffffu, lane == 0 || cur != ptl);
+        const int s0 = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+          const V t = __shfl_up_sync(0xffffffffu, acc, d);
+          if (lane - d >= s0) acc = F::combine(t, acc);
+        }
+        const bool seg_end = lane == 31 || ((heads >> (lane + 1)) & 1u);
+        if (seg_end && cur >= 0) flush(cur, acc);
+        continue;
+      }
       int cur = -1;
       V acc = F::identity();
 #pragma unroll
@@ -662,10 +723,7 @@ __global__ void __launch_bounds__(kCooThreads, GG_COO_MIN_BLOCKS) k_pull_coo_w(c
         if (!vld[k]) continue;
         const int l = (int)dv[k];
         if (l != cur) {
-          if (cur >= 0) {
-            F::atomic_combine(&s_acc[cur], acc);
-            if (!F::kPositive && !NOOUT) s_touch[cur] = 1;
-          }
+          if (cur >= 0) flush(cur, acc);
           cur = l;
           acc = val[k];
         } else {

@@ -556,6 +556,9 @@ static void graph_release(gg_graph_s* g) {
   cudaFree(g->ws.d_bsum);
   cudaFree(g->ws.d_red);
   cudaFree(g->ws.d_loop);
+  cudaFree(g->d_new_of_old);
+  cudaFree(g->d_old_of_new);
+  for (auto* a : g->ws.d_order) cudaFree(a);
   if (g->ws.h_stats) cudaFreeHost(g->ws.h_stats);
   if (g->ws.h_red) cudaFreeHost(g->ws.h_red);
   for (auto& e : g->prof_ev)
@@ -564,11 +567,14 @@ static void graph_release(gg_graph_s* g) {
   delete g;
 }
 
-static int graph_build(const gg_host_graph* hg, const gg_build_opts* opts_in, gg_graph_s* g) {
+static int graph_build(const gg_host_graph* hg_given, const gg_build_opts* opts_in, gg_graph_s* g) {
+  const gg_host_graph* hg = hg_given;
   const uint32_t n = hg->n;
   const uint64_t m = hg->m;
   gg_build_opts o{};
   if (opts_in) o = *opts_in;
+  if (o.vertex_order != GG_VORDER_GIVEN && o.vertex_order != GG_VORDER_HOT_FIRST)
+    return fail(GG_ERR_INVALID_ARG, "gg_graph_build: unknown vertex_order %d", o.vertex_order);
   if (o.num_partitions <= 0) o.num_partitions = 384;
   if (o.tile_vertices <= 0 || o.tile_vertices > kMaxTileVertices) o.tile_vertices = kMaxTileVertices;
   if (o.tile_edges <= 0) o.tile_edges = 1 << 16;
@@ -613,6 +619,43 @@ static int graph_build(const gg_host_graph* hg, const gg_build_opts* opts_in, gg
   for (int p = 0; p < P; ++p) {
     g->coo_starts[p + 1] = g->coo_starts[p] + g->coo_sizes[p];
     g->csc_starts[p + 1] = g->csc_starts[p] + g->csc_sizes[p];
+  }
+  // vertex_order: the device graph is the given graph renumbered inside every
+  // COO partition; the partitions (computed above on the given ids) keep
+  // their vertex sets and sizes
+  struct HostHold {
+    gg_host_graph h{};
+    ~HostHold() { gg_host_graph_free(&h); }
+  } renum;
+  if (o.vertex_order == GG_VORDER_HOT_FIRST) {
+    if (g->coo_starts[P] != (int64_t)n) {
+      if (!g->symmetric) gg_host_graph_free(&csc);
+      return fail(GG_ERR_PARTITION, "partition sizes sum to %lld, not n=%u", (long long)g->coo_starts[P], n);
+    }
+    g->relabeled = true;
+    g->h_old_of_new.resize(n);
+    g->h_new_of_old.resize(n);
+    hot_first_order(hg, g->coo_starts.data(), P, g->h_old_of_new.data(), g->h_new_of_old.data());
+    if (!g->symmetric) gg_host_graph_free(&csc);
+    GG_TRY(relabel_host_graph(hg, g->h_old_of_new.data(), g->h_new_of_old.data(), &renum.h));
+    hg = &renum.h;
+    in = hg;
+    if (!g->symmetric) {
+      GG_TRY(gg_host_graph_transpose(hg, &csc));
+      in = &csc;
+    }
+    g->h_csr_off.assign(hg->offsets, hg->offsets + n + 1);
+    g->h_csc_off.assign(in->offsets, in->offsets + n + 1);
+    rc = dev_alloc(g, &g->d_new_of_old, n);
+    if (!rc) rc = dev_alloc(g, &g->d_old_of_new, n);
+    if (!rc && cudaMemcpy(g->d_new_of_old, g->h_new_of_old.data(), 4ull * n, cudaMemcpyHostToDevice) != cudaSuccess)
+      rc = fail(GG_ERR_CUDA, "vertex order upload failed");
+    if (!rc && cudaMemcpy(g->d_old_of_new, g->h_old_of_new.data(), 4ull * n, cudaMemcpyHostToDevice) != cudaSuccess)
+      rc = fail(GG_ERR_CUDA, "vertex order upload failed");
+    if (rc) {
+      if (!g->symmetric) gg_host_graph_free(&csc);
+      return rc;
+    }
   }
   auto up = [&](uint32_t** d, const void* h, size_t count, size_t pad) -> int {
     GG_TRY(dev_alloc(g, d, count + pad));
@@ -674,6 +717,8 @@ static int graph_build(const gg_host_graph* hg, const gg_build_opts* opts_in, gg
   GG_TRY(dev_alloc(g, &g->ws.d_scan, (size_t)n + 4));
   GG_TRY(dev_alloc(g, &g->ws.d_red, 64));
   GG_TRY(dev_alloc(g, &g->ws.d_loop, 16));
+  if (g->relabeled)
+    for (auto& a : g->ws.d_order) GG_TRY(dev_alloc(g, &a, (size_t)n + 4));
   GG_CUDA(cudaMallocHost((void**)&g->ws.h_red, 64 * sizeof(double)));
   // keep stream-ordered allocations (frontiers) cached in the pool
   cudaMemPool_t pool;
@@ -777,7 +822,7 @@ int gg_graph_set_tuning(gg_graph_t g, int32_t key, int64_t value) {
     case GG_TUNE_DENSE_POLICY:
       return gg_graph_set_dense_policy(g, (int32_t)value);
     case GG_TUNE_COO_KERNEL:
-      if (value < 0 || value > 5) return fail(GG_ERR_INVALID_ARG, "COO kernel must be 0..5");
+      if (value < 0 || value > 6) return fail(GG_ERR_INVALID_ARG, "COO kernel must be 0..6");
       g->coo_kernel = (int)value;
       return GG_OK;
     case GG_TUNE_SPARSE_DIV:
@@ -816,6 +861,12 @@ int gg_graph_get_tuning(gg_graph_t g, int32_t key, int64_t* value) {
 int gg_graph_transpose(gg_graph_t g) {
   if (!g) return fail(GG_ERR_INVALID_ARG, "gg_graph_transpose: null graph");
   if (!g->symmetric) g->transposed = !g->transposed;  // graphgrind/graph-numa.h:598-611
+  return GG_OK;
+}
+
+int gg_graph_vertex_order(gg_graph_t g, uint32_t* new_of_old) {
+  if (!graph_live(g) || !new_of_old) return fail(GG_ERR_INVALID_ARG, "gg_graph_vertex_order: bad arguments");
+  for (uint32_t v = 0; v < g->n; ++v) new_of_old[v] = g->device_id(v);
   return GG_OK;
 }
 

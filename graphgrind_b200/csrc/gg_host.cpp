@@ -139,6 +139,55 @@ struct RmatGen {
   }
 };
 
+int relabel_host_graph(const gg_host_graph* g, const uint32_t* old_of_new, const uint32_t* new_of_old,
+                       gg_host_graph* out) {
+  const int64_t n = g->n;
+  const uint64_t m = g->m;
+  memset(out, 0, sizeof *out);
+  out->n = g->n;
+  out->m = m;
+  out->symmetric = g->symmetric;
+  out->weight_type = g->weight_type;
+  out->offsets = (uint32_t*)calloc((size_t)n + 1, sizeof(uint32_t));
+  out->indices = (uint32_t*)malloc(4 * (m ? m : 1));
+  if (g->weights) out->weights = malloc(4 * (m ? m : 1));
+  if (!out->offsets || !out->indices || (g->weights && !out->weights)) {
+    gg_host_graph_free(out);
+    return fail(GG_ERR_OOM, "relabel: out of host memory");
+  }
+  for (int64_t i = 0; i < n; i++) {
+    const uint32_t o = old_of_new[i];
+    out->offsets[i + 1] = out->offsets[i] + (g->offsets[o + 1] - g->offsets[o]);
+  }
+  const uint32_t* w = (const uint32_t*)g->weights;
+  uint32_t* ow = (uint32_t*)out->weights;
+#pragma omp parallel for schedule(dynamic, 4096)
+  for (int64_t i = 0; i < n; i++) {
+    const uint32_t o = old_of_new[i];
+    uint32_t dst = out->offsets[i];
+    for (uint32_t j = g->offsets[o]; j < g->offsets[o + 1]; j++, dst++) {
+      out->indices[dst] = new_of_old[g->indices[j]];
+      if (ow) ow[dst] = w[j];
+    }
+  }
+  return GG_OK;
+}
+
+void hot_first_order(const gg_host_graph* g, const int64_t* starts, int32_t P, uint32_t* old_of_new,
+                     uint32_t* new_of_old) {
+  const uint32_t* off = g->offsets;
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int32_t p = 0; p < P; p++) {
+    const int64_t a = starts[p], b = starts[p + 1];
+    for (int64_t v = a; v < b; v++) old_of_new[v] = (uint32_t)v;
+    std::stable_sort(old_of_new + a, old_of_new + b, [off](uint32_t x, uint32_t y) {
+      return off[x + 1] - off[x] > off[y + 1] - off[y];
+    });
+  }
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < (int64_t)g->n; i++) new_of_old[old_of_new[i]] = (uint32_t)i;
+}
+
 }  // namespace gg
 
 using namespace gg;
@@ -705,33 +754,7 @@ int gg_vebo(const gg_host_graph* g, int32_t partitions, uint32_t* new_of_old, in
         old_of_new[start[p] + fill[p]++] = (uint32_t)check[real++].first;
   std::vector<uint32_t> nofo(n);
   for (int64_t i = 0; i < n; i++) nofo[old_of_new[i]] = (uint32_t)i;
-  memset(out, 0, sizeof *out);
-  out->n = g->n;
-  out->m = m;
-  out->symmetric = g->symmetric;
-  out->weight_type = g->weight_type;
-  out->offsets = (uint32_t*)calloc((size_t)n + 1, sizeof(uint32_t));
-  out->indices = (uint32_t*)malloc(4 * (m ? m : 1));
-  if (g->weights) out->weights = malloc(4 * (m ? m : 1));
-  if (!out->offsets || !out->indices || (g->weights && !out->weights)) {
-    gg_host_graph_free(out);
-    return fail(GG_ERR_OOM, "gg_vebo: out of host memory");
-  }
-  for (int64_t i = 0; i < n; i++) {
-    const uint32_t o = old_of_new[i];
-    out->offsets[i + 1] = out->offsets[i] + (g->offsets[o + 1] - g->offsets[o]);
-  }
-  const uint32_t* w = (const uint32_t*)g->weights;
-  uint32_t* ow = (uint32_t*)out->weights;
-#pragma omp parallel for schedule(dynamic, 4096)
-  for (int64_t i = 0; i < n; i++) {
-    const uint32_t o = old_of_new[i];
-    uint32_t dst = out->offsets[i];
-    for (uint32_t j = g->offsets[o]; j < g->offsets[o + 1]; j++, dst++) {
-      out->indices[dst] = nofo[g->indices[j]];
-      if (ow) ow[dst] = w[j];
-    }
-  }
+  GG_TRY_HOST(relabel_host_graph(g, old_of_new.data(), nofo.data(), out));
   if (new_of_old) std::copy(nofo.begin(), nofo.end(), new_of_old);
   if (part_sizes) std::copy(vsize.begin(), vsize.end(), part_sizes);
   return GG_OK;
@@ -794,6 +817,32 @@ int gg_partition_sizes(const uint32_t* in_degrees, const uint32_t* out_degrees, 
 // HilbertEdgeSort::xy2d with the reference's grid side, see gg_hilbert.h.
 int64_t gg_hilbert_key(int64_t side_edges, int64_t x, int64_t y) {
   return gg::hilbert_xy2d(gg::hilbert_side(side_edges), x, y);
+}
+
+int gg_hot_first_order(const gg_host_graph* g, const gg_build_opts* opts, uint32_t* new_of_old,
+                       int64_t* starts) {
+  if (!g || !g->offsets || (g->m && !g->indices) || g->n == 0 || !new_of_old)
+    return fail(GG_ERR_INVALID_ARG, "gg_hot_first_order: bad arguments");
+  const uint32_t n = g->n;
+  gg_build_opts o{};
+  if (opts) o = *opts;
+  const int32_t P = o.num_partitions > 0 ? o.num_partitions : 384;
+  std::vector<uint32_t> outdeg(n), indeg(n, 0);
+  for (uint32_t v = 0; v < n; v++) outdeg[v] = g->offsets[v + 1] - g->offsets[v];
+  if (g->symmetric) {
+    indeg = outdeg;
+  } else {
+    for (uint64_t j = 0; j < g->m; j++) indeg[g->indices[j]]++;
+  }
+  std::vector<int64_t> coo(P), csc(P), st((size_t)P + 1, 0);
+  GG_TRY_HOST(gg_partition_sizes(indeg.data(), outdeg.data(), n, g->m, P, o.balance, o.part_how, o.relabel,
+                                 coo.data(), csc.data()));
+  for (int32_t p = 0; p < P; p++) st[p + 1] = st[p] + coo[p];
+  if (st[P] != (int64_t)n) return fail(GG_ERR_PARTITION, "partition sizes sum to %lld, not n=%u", (long long)st[P], n);
+  std::vector<uint32_t> oofn(n);
+  hot_first_order(g, st.data(), P, oofn.data(), new_of_old);
+  if (starts) std::copy(st.begin(), st.end(), starts);
+  return GG_OK;
 }
 
 }  // extern "C"

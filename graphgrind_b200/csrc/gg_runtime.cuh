@@ -78,6 +78,71 @@ inline int generic_grid(const gg_graph_s* g, uint64_t work) {
   return (int)std::min<uint64_t>(b, cap);
 }
 
+// ------------------------------------------ given ids <-> device ids
+// Graphs built with a vertex_order hold their vertices renumbered; the
+// applications move per-vertex arrays (rows of k entries) between the two
+// orders at their boundary.  The renumbering stays inside partitions, so both
+// directions read and write within one partition's stretch of the array.
+// to_given: out[u] = in[new_of_old[u]];  to_device: out[i] = in[old_of_new[i]].
+template <class T>
+__global__ void k_permute_rows(uint32_t n, uint32_t k, const uint32_t* map, const T* in, T* out) {
+  const uint64_t total = (uint64_t)n * k;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = in[(uint64_t)map[i / k] * k + i % k];
+}
+// vertex ids held as values (BFS parents): the given id of the value, for the
+// given vertex u
+static __global__ void k_ids_to_given(uint32_t n, const uint32_t* new_of_old, const uint32_t* old_of_new,
+                               const int32_t* in, int32_t* out) {
+  for (uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; u < n; u += (uint64_t)gridDim.x * blockDim.x) {
+    const int32_t v = in[new_of_old[u]];
+    out[u] = v < 0 ? v : (int32_t)old_of_new[v];
+  }
+}
+
+// `dev` (n rows of k, device order) in the given order: dev itself on a graph
+// with its given ids, else a permuted copy in tmp.
+template <class T>
+int given_order(gg_graph_s* g, const T* dev, uint32_t k, DevBuf<T>& tmp, const T** res) {
+  *res = dev;
+  if (!g->relabeled) return GG_OK;
+  GG_TRY(tmp.alloc(g, (uint64_t)g->n * k));
+  k_permute_rows<T><<<generic_grid(g, (uint64_t)g->n * k), kGenericThreads, 0, g->stream>>>(g->n, k, g->d_new_of_old,
+                                                                                             dev, tmp.p);
+  GG_CUDA(cudaGetLastError());
+  g->kernels++;
+  *res = tmp.p;
+  return GG_OK;
+}
+// The same for one 4-byte value per vertex, into the graph's given-order
+// array `slot` (0 or 1; nothing is allocated on the application's path).
+template <class T>
+int given_order(gg_graph_s* g, const T* dev, int slot, const T** res) {
+  static_assert(sizeof(T) == 4, "the given-order arrays hold 4-byte values");
+  *res = dev;
+  if (!g->relabeled) return GG_OK;
+  T* out = reinterpret_cast<T*>(g->ws.d_order[slot]);
+  k_permute_rows<T><<<generic_grid(g, g->n), kGenericThreads, 0, g->stream>>>(g->n, 1, g->d_new_of_old, dev, out);
+  GG_CUDA(cudaGetLastError());
+  g->kernels++;
+  *res = out;
+  return GG_OK;
+}
+// `given` (n rows of k, given order, device memory) into `dev` in device order
+// (a copy when the graph keeps its given ids).
+template <class T>
+int device_order(gg_graph_s* g, const T* given, uint32_t k, T* dev) {
+  if (!g->relabeled) {
+    GG_CUDA(cudaMemcpyAsync(dev, given, sizeof(T) * (uint64_t)g->n * k, cudaMemcpyDeviceToDevice, g->stream));
+    return GG_OK;
+  }
+  k_permute_rows<T><<<generic_grid(g, (uint64_t)g->n * k), kGenericThreads, 0, g->stream>>>(g->n, k, g->d_old_of_new,
+                                                                                             given, dev);
+  GG_CUDA(cudaGetLastError());
+  g->kernels++;
+  return GG_OK;
+}
+
 // ------------------------------------------------------------ frontiers
 int frontier_new(gg_graph_s* g, gg_frontier_s** out);
 int frontier_ensure_bits(gg_frontier_s* f, bool zero);
@@ -160,7 +225,8 @@ int pull_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f
   if (coo && g->coo_kernel > 0) {  // per-warp COO pull: 0, 2 or 3 staging stages
     static DeviceOnce opted[2][4];
     static DeviceOnce opted_pf[2];
-    static DeviceOnce opted_no[2];
+    static DeviceOnce opted_no[2][2];
+    static DeviceOnce opted_mg[2];
     auto launch_w = [&](auto kern, int stages, DeviceOnce& once) -> int {
       const size_t smem = coo_w_smem_bytes(kHW, stages, 4, p.tv);
       const int ok = once.get(g->device, [&]() {
@@ -179,10 +245,16 @@ int pull_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f
     };
     if constexpr (F::kIdentityCommitNoop) {
       if (no_out && g->coo_kernel == 1)
-        return all ? launch_w(k_pull_coo_w<F, kHW, true, 0, false, false, true>, 0, opted_no[1])
-                   : launch_w(k_pull_coo_w<F, kHW, false, 0, false, false, true>, 0, opted_no[0]);
+        return all ? launch_w(k_pull_coo_w<F, kHW, true, 0, false, false, true>, 0, opted_no[0][1])
+                   : launch_w(k_pull_coo_w<F, kHW, false, 0, false, false, true>, 0, opted_no[0][0]);
+      if (no_out && g->coo_kernel == 6)
+        return all ? launch_w(k_pull_coo_w<F, kHW, true, 0, false, false, true, true>, 0, opted_no[1][1])
+                   : launch_w(k_pull_coo_w<F, kHW, false, 0, false, false, true, true>, 0, opted_no[1][0]);
     }
     switch (g->coo_kernel) {
+      case 6:
+        return all ? launch_w(k_pull_coo_w<F, kHW, true, 0, false, false, false, true>, 0, opted_mg[1])
+                   : launch_w(k_pull_coo_w<F, kHW, false, 0, false, false, false, true>, 0, opted_mg[0]);
       case 5:
         return all ? launch_w(k_pull_coo_w<F, kHW, true, 0, false, true>, 0, opted_pf[1])
                    : launch_w(k_pull_coo_w<F, kHW, false, 0, false, true>, 0, opted_pf[0]);

@@ -68,7 +68,22 @@ typedef struct gg_build_opts {
                                warp's 32 gathers share cache lines          */
   int32_t coo_dst_window;   /* GPU: edges per destination-ordered window when
                                coo_window == 0 (multiple of 256; 0 = 256)    */
+  int32_t vertex_order;     /* GPU: gg_vertex_order (0 = the given ids)      */
 } gg_build_opts;
+
+/* Device-side vertex numbering of a graph (gg_build_opts.vertex_order).
+ * GG_VORDER_HOT_FIRST renumbers the vertices inside every stretch between two
+ * partition boundaries (of the COO and of the compressed-CSC partitioner) by
+ * descending out-degree, ties by id: each partition keeps its vertex set and
+ * sizes, and the sources a dense pull gathers most share cache lines.  The
+ * applications (gg_bfs ... gg_msbc) take and return the given ids and arrays
+ * in the given order, with results equal to the unrenumbered graph's (FP32
+ * sums up to their summation order; BFS parents are another valid tree).
+ * The low-level API (frontiers, edgeMap / vertexMap arrays, device arrays,
+ * gg_bfs_push_step_noalloc on the device arrays) speaks the device ids:
+ * gg_graph_vertex_order gives the map.  gg_bp and gg_pagerank_weighted_*,
+ * whose inputs are per-edge arrays, return GG_ERR_UNSUPPORTED on such graphs. */
+enum gg_vertex_order { GG_VORDER_GIVEN = 0, GG_VORDER_HOT_FIRST = 1 };
 
 typedef struct gg_graph_info {
   uint32_t n;
@@ -141,6 +156,14 @@ void gg_host_graph_free(gg_host_graph* g);
 int gg_partition_sizes(const uint32_t* in_degrees, const uint32_t* out_degrees, uint32_t n,
                        uint64_t m, int32_t P, int32_t balance, int32_t part_how,
                        int32_t relabel, int64_t* coo_sizes, int64_t* csc_sizes);
+/* GG_VORDER_HOT_FIRST for graph g built with opts (num_partitions, balance,
+ * part_how, relabel): the COO partition starts (P+1 entries, may be NULL) of
+ * the given ids, and new_of_old[n], the device id gg_graph_build gives each
+ * vertex: inside every partition, the vertices by descending out-degree, ties
+ * by id.  Host-only; gg_graph_build with vertex_order = GG_VORDER_HOT_FIRST
+ * uses the same order. */
+int gg_hot_first_order(const gg_host_graph* g, const gg_build_opts* opts, uint32_t* new_of_old,
+                       int64_t* starts);
 /* Hilbert key of edge (x=src, y=dst) on the reference's grid, whose side is
  * roundUpPow2(edges in the partition) (graphgrind/graph-numa.h:353-386, 487). */
 int64_t gg_hilbert_key(int64_t side_edges, int64_t x, int64_t y);
@@ -162,6 +185,9 @@ int gg_graph_partition_starts(gg_graph_t g, int64_t* starts);
  * out/in roles of CSR and CSC for symmetric=0 graphs; the COO partitions are
  * NOT transposed, as in the reference. */
 int gg_graph_transpose(gg_graph_t g);
+/* new_of_old[n]: the device id of every given vertex id (the identity unless
+ * the graph was built with a vertex_order). */
+int gg_graph_vertex_order(gg_graph_t g, uint32_t* new_of_old);
 /* Out-degree of every vertex in the current orientation (device pointer). */
 int gg_graph_device_arrays(gg_graph_t g, const uint32_t** out_offsets,
                            const uint32_t** out_indices, const uint32_t** in_offsets,
@@ -259,7 +285,9 @@ int gg_graph_set_dense_policy(gg_graph_t g, int32_t policy);
  *                         and one shared-memory accumulation per edge (the
  *                         default for graphs built with coo_window > 0),
  *                         5 per-warp direct loads with the next block's edge
- *                         stream prefetched into registers
+ *                         stream prefetched into registers, 6 per-warp direct
+ *                         loads with destination runs merged across lanes (the
+ *                         default for graphs built with coo_window == 0)
  *   GG_TUNE_SPARSE_DIV    the application loops (gg_bfs ... gg_bc) call edgeMap
  *                         with threshold m / value (20 in the reference apps)
  *   GG_TUNE_DEVICE_LOOP   1 (default): gg_bfs runs consecutive sparse levels in

@@ -140,12 +140,14 @@ def _check_parents(par, lev, hg, start):
     assert par[start] == start and np.all(par[lev < 0] == -1)
 
 
+@pytest.mark.parametrize("vorder", [0, 1])
 @pytest.mark.parametrize("policy", [0, 1, 2])
 @pytest.mark.parametrize("name", CASES)
-def test_traversals(gg, orc, name, policy):
-    """BFS (parents valid, levels bit-exact), Components, BellmanFord and BC."""
+def test_traversals(gg, orc, name, policy, vorder):
+    """BFS (parents valid, levels bit-exact), Components, BellmanFord and BC,
+    on the given ids and renumbered hottest-first."""
     hg, og, pref = _case(gg, orc, name)
-    g = gg.Graph(hg, partitions=_partitions(gg, hg, pref))
+    g = gg.Graph(hg, partitions=_partitions(gg, hg, pref), vertex_order=vorder)
     g.set_dense_policy(policy)
     ids, _ = g.components()
     np.testing.assert_array_equal(ids, og.cc()[0])
@@ -175,11 +177,12 @@ def test_device_loop_off(gg, orc, name):
         np.testing.assert_array_equal(g.bfs(s)[1], og.bfs(s)[1])
 
 
+@pytest.mark.parametrize("vorder", [0, 1])
 @pytest.mark.parametrize("name", CASES)
-def test_rank_apps(gg, orc, name):
+def test_rank_apps(gg, orc, name, vorder):
     """PageRank, PageRankBit, PageRankDelta, SPMV and PageRankConverage."""
     hg, og, pref = _case(gg, orc, name)
-    g = gg.Graph(hg, partitions=_partitions(gg, hg, pref))
+    g = gg.Graph(hg, partitions=_partitions(gg, hg, pref), vertex_order=vorder)
     for bit in (False, True):
         o = _oracle_or_none(og.pagerank, 10, bit)
         if o is None:
@@ -208,11 +211,12 @@ def test_rank_apps(gg, orc, name):
         assert 100 >= run.rounds >= int((o[2] > 1e-5).sum())
 
 
+@pytest.mark.parametrize("vorder", [0, 1])
 @pytest.mark.parametrize("name", CASES)
-def test_batched_traversals(gg, orc, name):
+def test_batched_traversals(gg, orc, name, vorder):
     """k-column personalised PageRank, multi-source BFS and BC."""
     hg, og, pref = _case(gg, orc, name)
-    g = gg.Graph(hg, partitions=_partitions(gg, hg, pref))
+    g = gg.Graph(hg, partitions=_partitions(gg, hg, pref), vertex_order=vorder)
     rng = np.random.default_rng(7)
     for k in (1, 32, 64):
         seeds = rng.integers(0, hg.n, k).astype(np.uint32)
@@ -329,7 +333,7 @@ def test_source_partitions(gg, orc, name):
         _close(g.spmv()[0], og.spmv()[0], rel=1e-6, mx=1e-6)
 
 
-@pytest.mark.parametrize("kernel", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("kernel", [0, 1, 2, 3, 4, 5, 6])
 def test_coo_kernels_on_multigraph(gg, orc, kernel):
     """Every COO pull kernel on repeated edges and loops (coo_window builds
     give kernel 4 its lane-contiguous layout)."""

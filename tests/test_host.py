@@ -151,3 +151,24 @@ def test_device_calls_fail_cleanly_without_gpu(gg):
     with pytest.raises(gg.GGError) as e:
         gg.GraphBatch([g, g])
     assert "NO_DEVICE" in str(e.value)
+
+
+@pytest.mark.parametrize("sym", [True, False])
+@pytest.mark.parametrize("P,balance,part_how", [(16, 0, 0), (7, 1, 0), (16, 0, 1), (1, 0, 0)])
+def test_hot_first_order(gg, sym, P, balance, part_how):
+    """gg_hot_first_order: the reference's COO partitions keep their vertex
+    sets, and inside each the vertices go by descending out-degree, ties by id."""
+    hg = gg.HostGraph.rmat(11, 8, seed=21, symmetric=sym)
+    outd = hg.degrees()
+    ind = outd if sym else hg.transpose().degrees()
+    coo, _ = gg.partition_sizes(ind, outd, hg.m, P, balance, part_how, False)
+    nofo, starts = hg.hot_first_order(P, balance, part_how)
+    np.testing.assert_array_equal(starts, np.concatenate([[0], np.cumsum(coo)]))
+    oofn = np.empty(hg.n, np.int64)
+    oofn[nofo] = np.arange(hg.n)
+    assert sorted(nofo.tolist()) == list(range(hg.n))
+    for p in range(P):
+        a, b = int(starts[p]), int(starts[p + 1])
+        ids = np.arange(a, b)
+        want = ids[np.lexsort((ids, -outd[a:b].astype(np.int64)))]
+        np.testing.assert_array_equal(oofn[a:b], want, err_msg=f"partition {p}")
