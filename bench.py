@@ -66,7 +66,7 @@ def workload(scale: int, partitions: int, start: int) -> str:
 HBM_FALLBACK_GBS = 6650.0
 # DRAM bytes per PageRank-pull launch of the default workload, from one ncu
 # capture (profiles/dram_k_pull_coo_w_pagerank_rmat24.md)
-TRAFFIC_RMAT24_PR_PULL = {0: 2118674176}  # by vertex order
+TRAFFIC_RMAT24_PR_PULL = {1: 1919532928}  # by vertex order (merged-run COO kernel)
 TRAFFIC_TILE_EDGES = 1 << 17
 
 
