@@ -7,6 +7,8 @@
 // the personalised form of PR_F / PR_Vertex_F (app/PageRank.C:256-315) with a
 // teleport matrix T (n x k, row-major) in place of the uniform 1/n, all
 // vertices active (PageRankBit, app/PageRankBit.C:145).
+#include <cub/cub.cuh>
+
 #include <algorithm>
 #include <functional>
 #include <vector>
@@ -449,44 +451,115 @@ __global__ void __launch_bounds__(256, GG_MS_MIN_BLOCKS) k_ms_pull(MsPull p) {
   }
 }
 
-// Sources: seen = visit = bit j at sources[j], level 0, one path.
+// Sources: seen = visit = bit j at sources[j], level 0, one path.  The
+// levels go to lvl (n x 64, device rows) and/or straight to out_lv (n x k,
+// given rows: old_of_new[v], or v when the graph keeps its ids).
 __global__ void k_ms_seed(const uint32_t* src, uint32_t k, uint64_t* seen, uint64_t* visit, int32_t* lvl,
-                          float* sigma) {
+                          int32_t* out_lv, const uint32_t* old_of_new, float* sigma) {
   const uint32_t j = threadIdx.x;
   if (j >= k) return;
   const uint32_t s = src[j];
   atomicOr(reinterpret_cast<unsigned long long*>(seen + s), 1ull << j);
   atomicOr(reinterpret_cast<unsigned long long*>(visit + s), 1ull << j);
-  lvl[(uint64_t)s * 64 + j] = 0;
+  if (lvl) lvl[(uint64_t)s * 64 + j] = 0;
+  if (out_lv) out_lv[(uint64_t)(old_of_new ? old_of_new[s] : s) * k + j] = 0;
   if (sigma) sigma[(uint64_t)s * 64 + j] = 1.f;
 }
 
-// After a forward level r: the new frontier masks become visit, join seen and
-// set the level of each new (vertex, source) pair; stats[0] += vertices in the
-// frontier, stats[1] += sum of out-degree x sources over it.
+// After a forward level r: the new frontier masks become visit and join
+// seen; the frontier's vertices are appended to queue (with their
+// out-degrees in qdeg) for a push of the next level; the levels of the new
+// (vertex, source) pairs are written by the whole warp, one vertex at a time
+// with lanes over sources (whole-row stores).  stats[0] = frontier vertices
+// (the queue length), stats[1] += sum of out-degree x sources over it,
+// stats[2] += sum of out-degree (the edges a push expands).
 __global__ void k_ms_fwd_vertex(uint32_t n, int32_t r, uint64_t* seen, uint64_t* visit, uint64_t* next, int32_t* lvl,
-                                const uint32_t* out_off, unsigned long long* stats) {
-  unsigned long long cnt = 0, trav = 0;
-  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x) {
-    uint64_t nm = next[v];
-    visit[v] = nm;
+                                int32_t* out_lv, uint32_t out_k, const uint32_t* old_of_new, const uint32_t* out_off,
+                                uint32_t* queue, uint32_t* qdeg, unsigned long long* stats) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t w0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  unsigned long long trav = 0, edges = 0;
+  for (uint64_t base = w0 * 32; base < n; base += nw * 32) {
+    const uint64_t v = base + lane;
+    uint64_t nm = 0;
+    uint32_t d = 0;
+    if (v < n) {
+      nm = next[v];
+      visit[v] = nm;
+      if (nm) {
+        next[v] = 0;
+        seen[v] |= nm;
+        d = out_off[v + 1] - out_off[v];
+        trav += (unsigned long long)d * __popcll(nm);
+        edges += d;
+      }
+    }
+    uint32_t act = __ballot_sync(0xffffffffu, nm != 0);
+    if (!act) continue;
+    uint32_t pos = 0;
+    if (lane == 0) pos = (uint32_t)atomicAdd(stats, (unsigned long long)__popc(act));
+    pos = __shfl_sync(0xffffffffu, pos, 0) + __popc(act & ((1u << lane) - 1u));
     if (nm) {
-      next[v] = 0;
-      seen[v] |= nm;
-      ++cnt;
-      trav += (unsigned long long)(out_off[v + 1] - out_off[v]) * __popcll(nm);
-      while (nm) {
-        const int j = __ffsll((long long)nm) - 1;
-        nm &= nm - 1;
-        lvl[v * 64 + j] = r;
+      queue[pos] = (uint32_t)v;
+      qdeg[pos] = d;
+    }
+    while (act) {
+      const int b = __ffs(act) - 1;
+      act &= act - 1;
+      const uint64_t vv = base + b;
+      const uint64_t mm = __shfl_sync(0xffffffffu, nm, b);
+      const bool lo = (mm >> lane) & 1u, hi = (mm >> (lane + 32)) & 1u;
+      if (lvl) {
+        if (lo) lvl[vv * 64 + lane] = r;
+        if (hi) lvl[vv * 64 + 32 + lane] = r;
+      }
+      if (out_lv) {
+        const uint64_t row = (uint64_t)(old_of_new ? old_of_new[vv] : vv) * out_k;
+        if (lo) out_lv[row + lane] = r;
+        if (hi) out_lv[row + 32 + lane] = r;
       }
     }
   }
-  cnt = warp_sum(cnt);
   trav = warp_sum(trav);
-  if ((threadIdx.x & 31) == 0 && (cnt | trav)) {
-    atomicAdd(stats, cnt);
+  edges = warp_sum(edges);
+  if (lane == 0 && (trav | edges)) {
     atomicAdd(stats + 1, trav);
+    atomicAdd(stats + 2, edges);
+  }
+}
+
+// Push of a sparse forward level (the frontier's out-edges are few): one
+// thread per frontier edge, load-balanced through the exclusive degree sums
+// qoff of the frontier queue; each edge (u, v) ORs the sources reaching u
+// for the first time at v into next[v], and for BC adds u's path counts of
+// those sources to v's.  The pairs (v, j) written are unreached ones, the
+// (u, j) read are frontier ones, so sigma is updated in place.
+__global__ void k_ms_push(const uint32_t* queue, const uint32_t* qoff, uint32_t nq, uint64_t edges,
+                          const uint32_t* out_off, const uint32_t* out_idx, const uint64_t* visit,
+                          const uint64_t* seen, uint64_t kmask, uint64_t* next, float* sigma) {
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < edges;
+       t += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = nq - 1;  // the last queue entry whose first edge is <= t
+    while (lo < hi) {
+      const uint32_t mid = lo + (hi - lo + 1) / 2;
+      if (qoff[mid] <= t)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const uint32_t u = queue[lo];
+    const uint32_t v = out_idx[out_off[u] + (uint32_t)(t - qoff[lo])];
+    uint64_t m = visit[u] & ~seen[v] & kmask;
+    if (!m) continue;
+    atomicOr(reinterpret_cast<unsigned long long*>(next + v), (unsigned long long)m);
+    if (sigma) {
+      while (m) {
+        const int j = __ffsll((long long)m) - 1;
+        m &= m - 1;
+        atomicAdd(sigma + (uint64_t)v * 64 + j, sigma[(uint64_t)u * 64 + j]);
+      }
+    }
   }
 }
 
@@ -518,15 +591,6 @@ __global__ void k_ms_bc_final(uint32_t n, uint32_t k, const uint32_t* new_of_old
     const float inv = 1.0f / sigma[v * 64 + j];
     dep_out[i] = (dep[v * 64 + j] - inv) / inv;
     if (sigma_out) sigma_out[i] = sigma[v * 64 + j];
-  }
-}
-
-__global__ void k_ms_levels_out(uint32_t n, uint32_t k, const uint32_t* new_of_old, const int32_t* lvl, int32_t* out) {
-  const uint64_t total = (uint64_t)n * k;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t u = i / k;
-    const uint64_t v = new_of_old ? new_of_old[u] : u;
-    out[i] = lvl[v * 64 + i % k];
   }
 }
 
@@ -594,50 +658,97 @@ static int run_ms(gg_graph_s* g, int32_t k, const uint32_t* given_sources, bool 
   for (auto& v : dev_sources) v = g->device_id(v);
   const uint32_t* sources = dev_sources.data();
   const uint64_t n64 = (uint64_t)n * 64;
+  const uint64_t nk = (uint64_t)n * k;
   const uint64_t kmask = k == 64 ? ~0ull : ((1ull << k) - 1);
   DevAllocs mem(g->stream);
   uint64_t *seen, *visit, *next, *mask_a, *mask_b;
-  int32_t* lvl;
+  int32_t* lvl = nullptr;  // n x 64 levels, kept for the BC backward pass
   float *sigma = nullptr, *dep = nullptr;
-  uint32_t* d_src;
+  uint32_t *d_src, *queue, *qdeg, *qoff;
+  unsigned char* scan_tmp;
   unsigned long long* d_stats;
   GG_TRY(mem.get(&seen, n));
   GG_TRY(mem.get(&visit, n));
   GG_TRY(mem.get(&next, n));
-  GG_TRY(mem.get(&lvl, n64));
   GG_TRY(mem.get(&d_src, 64));
-  GG_TRY(mem.get(&d_stats, 2));
+  GG_TRY(mem.get(&d_stats, 4));
+  GG_TRY(mem.get(&queue, n));
+  GG_TRY(mem.get(&qdeg, n));
+  GG_TRY(mem.get(&qoff, n));
+  size_t scan_bytes = 0;
+  GG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, qdeg, qoff, (int)n, g->stream));
+  GG_TRY(mem.get(&scan_tmp, scan_bytes));
   if (bc) {
+    GG_TRY(mem.get(&lvl, n64));
     GG_TRY(mem.get(&sigma, n64));
     GG_TRY(mem.get(&dep, n64));
   }
+  // multi-source BFS writes its levels straight into the n x k output
+  DevBuf<int32_t> lout;
+  int32_t* out_lv = nullptr;
+  if (!bc && levels_out) {
+    GG_TRY(lout.alloc(g, nk));
+    out_lv = lout.p;
+  }
+  const uint32_t* old_of_new = g->relabeled ? g->d_old_of_new : nullptr;
+  // the first frontier: the distinct sources, with their first-edge offsets
+  std::vector<uint32_t> uq(sources, sources + k);
+  std::sort(uq.begin(), uq.end());
+  uq.erase(std::unique(uq.begin(), uq.end()), uq.end());
+  std::vector<uint32_t> uoff(uq.size());
+  uint64_t f_edges = 0;
+  for (size_t i = 0; i < uq.size(); ++i) {
+    uoff[i] = (uint32_t)f_edges;
+    f_edges += g->h_out_off()[uq[i] + 1] - g->h_out_off()[uq[i]];
+  }
+  uint64_t f_cnt = uq.size();
   unsigned long long* h_stats = reinterpret_cast<unsigned long long*>(g->ws.h_red);
   g->kernels = 0;
   EventTimer tm(g->stream);
   GG_CUDA(cudaMemcpyAsync(d_src, sources, 4 * k, cudaMemcpyHostToDevice, g->stream));
+  GG_CUDA(cudaMemcpyAsync(queue, uq.data(), 4 * uq.size(), cudaMemcpyHostToDevice, g->stream));
+  GG_CUDA(cudaMemcpyAsync(qoff, uoff.data(), 4 * uoff.size(), cudaMemcpyHostToDevice, g->stream));
   GG_CUDA(cudaMemsetAsync(seen, 0, 8 * (uint64_t)n, g->stream));
   GG_CUDA(cudaMemsetAsync(visit, 0, 8 * (uint64_t)n, g->stream));
   GG_CUDA(cudaMemsetAsync(next, 0, 8 * (uint64_t)n, g->stream));
-  GG_CUDA(cudaMemsetAsync(lvl, 0xff, 4 * n64, g->stream));
+  if (lvl) GG_CUDA(cudaMemsetAsync(lvl, 0xff, 4 * n64, g->stream));
+  if (out_lv) GG_CUDA(cudaMemsetAsync(out_lv, 0xff, 4 * nk, g->stream));
   if (bc) GG_CUDA(cudaMemsetAsync(sigma, 0, 4 * n64, g->stream));
-  k_ms_seed<<<1, 64, 0, g->stream>>>(d_src, (uint32_t)k, seen, visit, lvl, sigma);
+  k_ms_seed<<<1, 64, 0, g->stream>>>(d_src, (uint32_t)k, seen, visit, lvl, out_lv, old_of_new, sigma);
   g->kernels++;
   uint64_t trav = 0;
   for (int32_t j = 0; j < k; ++j) trav += g->h_out_off()[sources[j] + 1] - g->h_out_off()[sources[j]];
   std::vector<uint64_t> level_trav{trav};
   int32_t L = 0;
   const int vgrid = generic_grid(g, n);
+  const int64_t thr = app_threshold(g);
   for (int32_t r = 1;; ++r) {
-    GG_TRY(ms_pull(g, bc, true, true, seen, ~0ull, kmask, visit, sigma, next));
-    GG_CUDA(cudaMemsetAsync(d_stats, 0, 16, g->stream));
-    k_ms_fwd_vertex<<<vgrid, kGenericThreads, 0, g->stream>>>(n, r, seen, visit, next, lvl, g->out_off(), d_stats);
+    // edgeMap's direction rule on the frontier (vertices + out-edges against
+    // m / 20): a sparse frontier pushes its out-edges, a dense one is pulled
+    if ((int64_t)(f_cnt + f_edges) <= thr) {
+      if (f_edges > 0) {
+        k_ms_push<<<generic_grid(g, f_edges), kGenericThreads, 0, g->stream>>>(
+            queue, qoff, (uint32_t)f_cnt, f_edges, g->out_off(), g->out_idx(), visit, seen, kmask, next, sigma);
+        g->kernels++;
+      }
+    } else {
+      GG_TRY(ms_pull(g, bc, true, true, seen, ~0ull, kmask, visit, sigma, next));
+    }
+    GG_CUDA(cudaMemsetAsync(d_stats, 0, 32, g->stream));
+    k_ms_fwd_vertex<<<vgrid, kGenericThreads, 0, g->stream>>>(n, r, seen, visit, next, lvl, out_lv, (uint32_t)k,
+                                                              old_of_new, g->out_off(), queue, qdeg, d_stats);
     g->kernels++;
-    GG_CUDA(cudaMemcpyAsync(h_stats, d_stats, 16, cudaMemcpyDeviceToHost, g->stream));
+    GG_CUDA(cudaMemcpyAsync(h_stats, d_stats, 24, cudaMemcpyDeviceToHost, g->stream));
     GG_CUDA(cudaStreamSynchronize(g->stream));
     if (h_stats[0] == 0) break;
     L = r;
     level_trav.push_back(h_stats[1]);
     trav += h_stats[1];
+    f_cnt = h_stats[0];
+    f_edges = h_stats[2];
+    if ((int64_t)(f_cnt + f_edges) <= thr && f_edges > 0) {
+      GG_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, qdeg, qoff, (int)f_cnt, g->stream));
+    }
   }
   if (bc) {
     GG_TRY(mem.get(&mask_a, n));
@@ -656,18 +767,11 @@ static int run_ms(gg_graph_s* g, int32_t k, const uint32_t* given_sources, bool 
     }
   }
   DevBuf<float> dout, sout;
-  DevBuf<int32_t> lout;
-  const uint64_t nk = (uint64_t)n * k;
   if (bc) {
     GG_TRY(dout.alloc(g, nk));
     if (np_out) GG_TRY(sout.alloc(g, nk));
     k_ms_bc_final<<<generic_grid(g, nk), kGenericThreads, 0, g->stream>>>(
         n, (uint32_t)k, g->relabeled ? g->d_new_of_old : nullptr, dep, sigma, dout.p, np_out ? sout.p : nullptr);
-    g->kernels++;
-  } else if (levels_out) {
-    GG_TRY(lout.alloc(g, nk));
-    k_ms_levels_out<<<generic_grid(g, nk), kGenericThreads, 0, g->stream>>>(
-        n, (uint32_t)k, g->relabeled ? g->d_new_of_old : nullptr, lvl, lout.p);
     g->kernels++;
   }
   GG_CUDA(cudaGetLastError());

@@ -82,6 +82,32 @@ def test_msbc_matches_brandes(rmat12, k):
         assert rel_l1(dep[fin, j], odep[fin]) <= 1e-4, s
 
 
+@pytest.mark.parametrize("div", [1, 20, 1 << 20])
+def test_multi_source_push_and_pull_levels(gg, orc, rmat12, div):
+    """Sparse levels push the frontier's out-edges, dense ones pull; every
+    level pushed (div 1), the reference's rule (20) and every level pulled
+    (2^20) give the oracle's levels and path counts."""
+    hg, g, og = rmat12
+    g.set_tuning(gg.TUNE_SPARSE_DIV, div)
+    src = np.random.default_rng(div).integers(0, hg.n, 40).astype(np.uint32)
+    src[5] = src[9]
+    lev, run = g.msbfs(src)
+    dep, npth, _ = g.msbc(src[:12])
+    g.set_tuning(gg.TUNE_SPARSE_DIV, 20)
+    trav = 0
+    for j, s in enumerate(src):
+        _, olev, ost = og.bfs(int(s))
+        np.testing.assert_array_equal(lev[:, j], olev, err_msg=f"source {s}")
+        trav += ost.edges_traversed
+    assert run.edges_traversed == trav
+    for j, s in enumerate(src[:12]):
+        odep, onp = og.bc_brandes(int(s))
+        np.testing.assert_allclose(npth[:, j], onp, rtol=1e-6)
+        np.testing.assert_array_equal(np.isnan(dep[:, j]), np.isnan(odep))
+        fin = np.isfinite(odep)
+        assert rel_l1(dep[fin, j], odep[fin]) <= 1e-4, s
+
+
 def test_msbc_equals_single_source_on_symmetric(gg, orc):
     hg = gg.HostGraph.rmat(11, 16, seed=95, symmetric=True)
     g = gg.Graph(hg, partitions=ok_partitions(hg, 16))
