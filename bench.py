@@ -12,7 +12,8 @@ each run through the library's C ABI (gg_bfs / gg_pagerank / gg_spmv).
            loops (CUDA events on the library's stream), graph resident in HBM
   e2e    = same edges / host wall time of the same C-ABI calls, including the
            H2D copy of the SpMV input vector from pinned memory and the D2H
-           copies of every result array (BFS parents+levels, ranks, y)
+           copies of every result array of the reference's apps (BFS parents,
+           PageRank ranks, SpMV y)
   roofline = the dense-pull kernel of the PageRank iterations: algorithmic
            bytes 8m + 16n per launch over its CUDA-event duration
   cpu_baseline = the reference's own OpenMP build (oracle/_ref) on the host
@@ -159,7 +160,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
     n, m = hg.n, hg.m
     x = gg.PinnedArray(n, np.float32)
     x.array[:] = np.random.default_rng(7).random(n, dtype=np.float32)
-    par, lev = gg.PinnedArray(n, np.int32), gg.PinnedArray(n, np.int32)
+    par = gg.PinnedArray(n, np.int32)
     ranks, y = gg.PinnedArray(n, np.float32), gg.PinnedArray(n, np.float32)
 
     # runtime knobs per application, chosen by the library's autotuner on this graph
@@ -182,7 +183,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
 
     def step():
         use("bfs")
-        _, _, b = g.bfs(args.start, out=(par.array, lev.array))
+        _, _, b = g.bfs(args.start, out=(par.array, None))  # app/BFS.C's result is Parents
         use("pagerank")
         _, p = g.pagerank(10, out=ranks.array)
         use("spmv")
@@ -289,7 +290,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
         "roofline_by_app": roofline_by_app,
         "kernel_profile": {k: {"launches": v["launches"], "ms": round(v["ms"], 3)} for k, v in prof.items()},
         "e2e": {"value": round(e2e, 4), "unit": UNIT, "h2d_bytes_per_step": 4 * n + 4,
-                "d2h_bytes_per_step": 16 * n},
+                "d2h_bytes_per_step": 12 * n},
         "gpu_launches": launches_all,
         "clocks": clk,
     }

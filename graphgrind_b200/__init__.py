@@ -143,6 +143,8 @@ _sig("gg_partition_sizes", C.c_int, _u32p, _u32p, C.c_uint32, C.c_uint64, C.c_in
      C.c_int32, _i64p, _i64p)
 _sig("gg_hilbert_key", C.c_int64, C.c_int64, C.c_int64, C.c_int64)
 _sig("gg_hot_first_order", C.c_int, C.POINTER(HostGraphC), C.POINTER(BuildOpts), _P, _P)
+_sig("gg_host_graph_read_gpu", C.c_int, C.c_char_p, C.c_int32, C.c_int32, C.c_int32, C.c_int64,
+     C.POINTER(HostGraphC))
 _sig("gg_graph_build", C.c_int, C.POINTER(HostGraphC), C.POINTER(BuildOpts), C.POINTER(_P))
 _sig("gg_graph_destroy", C.c_int, _P)
 _sig("gg_graph_get_info", C.c_int, _P, C.POINTER(GraphInfo))
@@ -221,7 +223,7 @@ EXPORTED = [
     "gg_batch_create", "gg_batch_destroy", "gg_batch_info", "gg_batch_bfs",
     "gg_pagerank_weighted_create", "gg_pagerank_weighted_destroy", "gg_pagerank_weighted_fwd",
     "gg_pagerank_weighted_bwd", "gg_autotune", "gg_autotune_build", "gg_autotune_ppr_k",
-    "gg_hot_first_order", "gg_graph_vertex_order",
+    "gg_hot_first_order", "gg_graph_vertex_order", "gg_host_graph_read_gpu",
 ]
 
 
@@ -308,6 +310,14 @@ class HostGraph:
         g = HostGraphC()
         check(lib.gg_host_graph_read(str(path).encode(), int(binary), int(symmetric), int(weighted), C.byref(g)),
               "gg_host_graph_read")
+        return HostGraph(g)
+
+    @staticmethod
+    def read_gpu(path, binary=False, symmetric=False, weighted=False, chunk_bytes=0) -> "HostGraph":
+        """gg_host_graph_read_gpu: the PBBS text body parsed on the GPU."""
+        g = HostGraphC()
+        check(lib.gg_host_graph_read_gpu(str(path).encode(), int(binary), int(symmetric), int(weighted),
+                                         int(chunk_bytes), C.byref(g)), "gg_host_graph_read_gpu")
         return HostGraph(g)
 
     @staticmethod
@@ -585,9 +595,10 @@ class Graph:
 
     # applications
     def bfs(self, start=100, out=None):
+        """app/BFS.C: (parents, levels, Run); out=(parents, None) skips the levels."""
         par, lev = out if out is not None else (np.empty(self.n, np.int32), np.empty(self.n, np.int32))
         st = RunStats()
-        check(lib.gg_bfs(self.h, start, _ptr(par), _ptr(lev), C.byref(st)), "gg_bfs")
+        check(lib.gg_bfs(self.h, start, _ptr(par), None if lev is None else _ptr(lev), C.byref(st)), "gg_bfs")
         return par, lev, _run(st)
 
     def components(self):

@@ -207,14 +207,14 @@ static int run_bfs(gg_graph_s* g, uint32_t start, int32_t* parents, int32_t* lev
   }
   const int32_t* par_out = par.p;
   const int32_t* lev_out = lev.p;
-  if (g->relabeled) {
+  if (g->relabeled && parents) {
     int32_t* tp = reinterpret_cast<int32_t*>(g->ws.d_order[0]);
     k_ids_to_given<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(n, g->d_new_of_old, g->d_old_of_new,
                                                                           par.p, tp);
     g->kernels++;
     par_out = tp;
   }
-  GG_TRY(given_order<int32_t>(g, lev.p, 1, &lev_out));
+  if (levels) GG_TRY(given_order<int32_t>(g, lev.p, 1, &lev_out));
   const double ms = tm.stop();
   GG_TRY(to_host(g, parents, par_out, n));
   GG_TRY(to_host(g, levels, lev_out, n));

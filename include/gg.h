@@ -72,10 +72,10 @@ typedef struct gg_build_opts {
 } gg_build_opts;
 
 /* Device-side vertex numbering of a graph (gg_build_opts.vertex_order).
- * GG_VORDER_HOT_FIRST renumbers the vertices inside every stretch between two
- * partition boundaries (of the COO and of the compressed-CSC partitioner) by
- * descending out-degree, ties by id: each partition keeps its vertex set and
- * sizes, and the sources a dense pull gathers most share cache lines.  The
+ * GG_VORDER_HOT_FIRST renumbers the vertices inside every partition of the
+ * COO partitioner (computed on the given ids) by descending out-degree, ties
+ * by id: each partition keeps its vertex set and size, and the sources a
+ * dense pull gathers most share cache lines.  The
  * applications (gg_bfs ... gg_msbc) take and return the given ids and arrays
  * in the given order, with results equal to the unrenumbered graph's (FP32
  * sums up to their summation order; BFS parents are another valid tree).
@@ -133,6 +133,16 @@ int gg_host_graph_write_adj(const gg_host_graph* g, const char* path);
 int gg_host_graph_write_gr(const gg_host_graph* g, const char* path);
 int gg_host_graph_read(const char* path, int32_t binary, int32_t symmetric,
                        int32_t weighted, gg_host_graph* out);
+/* The same reader with the PBBS text body parsed on the GPU (readGraphFromFile,
+ * graphgrind/IO.h:136-199): the file is read once into pinned memory, its
+ * header on the host, and the body crosses to the device in chunks of
+ * chunk_bytes (0 = 256 MiB; cut where a number ends), where the numbers are
+ * found, converted and range-checked in parallel.  Same result and the same
+ * GG_ERR_FORMAT cases as gg_host_graph_read (a number of more than 18 digits
+ * is also one); binary != 0 reads a .gr file as gg_host_graph_read does.
+ * Needs a CUDA device; the device memory it takes is released on return. */
+int gg_host_graph_read_gpu(const char* path, int32_t binary, int32_t symmetric,
+                           int32_t weighted, int64_t chunk_bytes, gg_host_graph* out);
 /* VEBO reordering (graphtools/VEBO.C:56-395, the tool that prepares graphs
  * for -o): vertices sorted by in-degree are dealt to `partitions` partitions
  * that balance edges first and vertices second, and renumbered partition by
@@ -369,7 +379,8 @@ typedef struct gg_run_stats {
   int32_t kernels;          /* kernels launched by the loop                  */
 } gg_run_stats;
 
-/* app/BFS.C:77-101: parents[n] (-1 unreached), levels[n] (-1 unreached). */
+/* app/BFS.C:77-101: parents[n] (-1 unreached), levels[n] (-1 unreached); either
+ * output may be NULL (app/BFS.C's result is the parents). */
 int gg_bfs(gg_graph_t g, uint32_t start, int32_t* parents, int32_t* levels, gg_run_stats* st);
 /* app/Components.C:202-227: ids[n]. */
 int gg_components(gg_graph_t g, int32_t* ids, gg_run_stats* st);

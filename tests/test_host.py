@@ -151,6 +151,12 @@ def test_device_calls_fail_cleanly_without_gpu(gg):
     with pytest.raises(gg.GGError) as e:
         gg.GraphBatch([g, g])
     assert "NO_DEVICE" in str(e.value)
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "g.adj")
+        g.write_adj(p)
+        with pytest.raises(gg.GGError) as e:
+            gg.HostGraph.read_gpu(p)
+        assert "NO_DEVICE" in str(e.value)
 
 
 @pytest.mark.parametrize("sym", [True, False])
