@@ -26,6 +26,9 @@ each run through the library's C ABI (gg_bfs / gg_pagerank / gg_spmv).
            persistent launch vs plain per-graph BFS on a sample; weighted
            PageRank adjoint (RMAT-22 seed 6, 30 iterations, checkpoints every 5)
            backward vs forward time
+  stress   = (N=1, outside the timed step) BFS from 100 and Components on the
+           4096^2 grid with 0.1 % long-range edges (seed 3, high diameter,
+           sparse frontiers) and on Erdos-Renyi n=2^24, m=2^28 (seed 4, dense)
 
 Multi-GPU: the path does not shard across GPUs in this build (one GPU per
 graph); --gpus N runs N independent replicas under torchrun and reports the
@@ -393,6 +396,49 @@ def run_batched(gg):
     return out
 
 
+def _accepted_partitions(gg, hg, preferred):
+    """The largest P <= preferred that the reference partitioner accepts."""
+    outd = hg.degrees()
+    ind = outd if hg.symmetric else hg.transpose().degrees()
+    for P in range(preferred, 0, -1):
+        try:
+            gg.partition_sizes(ind, outd, hg.m, P)
+            return P
+        except gg.GGError:
+            continue
+    return 1
+
+
+def run_stress(gg):
+    """Sparse-frontier / high-diameter stress against the dense-pull case: BFS
+    and Components on the 4096^2 grid with 0.1 % long-range edges (seed 3) and
+    on Erdos-Renyi n = 2^24, m = 2^28 (seed 4, directed)."""
+    out = {}
+    t0 = time.time()
+    for name, make in (("grid4096", lambda: gg.HostGraph.grid(4096, 0.001, seed=3)),
+                       ("er24", lambda: gg.HostGraph.er(1 << 24, 1 << 28, seed=4, symmetric=False))):
+        hg = make()
+        P = _accepted_partitions(gg, hg, 384)
+        g = gg.Graph(hg, partitions=P, tile_edges=1 << 17)
+        par = np.empty(hg.n, np.int32)
+        ids = np.empty(hg.n, np.int32)
+        g.bfs(100, out=(par, None))
+        rb = g.bfs(100, out=(par, None))[2]
+        bfs_ms = _best(lambda: g.bfs(100, out=(par, None))[2].ms, 3)
+        g.components()
+        rc = g.components()[1]
+        cc_ms = _best(lambda: g.components()[1].ms, 2)
+        out[name] = {"n": hg.n, "m": hg.m, "partitions": P,
+                     "bfs": {"ms": round(bfs_ms, 3), "levels": rb.rounds,
+                             "gteps": round(rb.edges_traversed / bfs_ms / 1e6, 2)},
+                     "components": {"ms": round(cc_ms, 3), "rounds": rc.rounds,
+                                    "gteps": round(rc.edges_traversed / cc_ms / 1e6, 2)}}
+        g.close()
+        del hg
+    out["seconds"] = round(time.time() - t0, 1)
+    return out
+
+
 # ------------------------------------------------------- the reference (CPU)
 def reference_sample(scale: int, partitions: int, rounds: int, workdir: str):
     """Time the reference's own BFS, PageRank and SPMV (OpenMP build of
@@ -489,6 +535,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched / adjoint comparisons")
     ap.add_argument("--no-autotune", action="store_true", help="keep the library's default runtime knobs")
+    ap.add_argument("--no-stress", action="store_true", help="skip the grid / Erdos-Renyi BFS and Components lines")
     ap.add_argument("--vertex-order", type=int, default=1, choices=[0, 1],
                     help="device numbering: 0 the given ids, 1 hottest sources first inside each partition")
     ap.add_argument("--tile-edges", type=int, default=1 << 17,
@@ -524,6 +571,12 @@ def main():
                 out["batched"] = run_batched(gg)
             except Exception as e:  # reported, the headline line still prints
                 out["batched"] = {"error": str(e)[:300]}
+        if world == 1 and not args.no_stress:
+            import graphgrind_b200 as gg
+            try:
+                out["stress"] = run_stress(gg)
+            except Exception as e:
+                out["stress"] = {"error": str(e)[:300]}
         print(json.dumps(out))
     if dist:
         dist.barrier()

@@ -451,31 +451,31 @@ __global__ void __launch_bounds__(256, GG_MS_MIN_BLOCKS) k_ms_pull(MsPull p) {
   }
 }
 
-// Sources: seen = visit = bit j at sources[j], level 0, one path.  The
-// levels go to lvl (n x 64, device rows) and/or straight to out_lv (n x k,
-// given rows: old_of_new[v], or v when the graph keeps its ids).
-__global__ void k_ms_seed(const uint32_t* src, uint32_t k, uint64_t* seen, uint64_t* visit, int32_t* lvl,
-                          int32_t* out_lv, const uint32_t* old_of_new, float* sigma) {
+// Sources: seen = visit = bit j at sources[j], level 0, one path.  Levels
+// go straight to out_lv (n x k, given rows: old_of_new[v], or v when the
+// graph keeps its ids), when given.
+__global__ void k_ms_seed(const uint32_t* src, uint32_t k, uint64_t* seen, uint64_t* visit, int32_t* out_lv,
+                          const uint32_t* old_of_new, float* sigma) {
   const uint32_t j = threadIdx.x;
   if (j >= k) return;
   const uint32_t s = src[j];
   atomicOr(reinterpret_cast<unsigned long long*>(seen + s), 1ull << j);
   atomicOr(reinterpret_cast<unsigned long long*>(visit + s), 1ull << j);
-  if (lvl) lvl[(uint64_t)s * 64 + j] = 0;
   if (out_lv) out_lv[(uint64_t)(old_of_new ? old_of_new[s] : s) * k + j] = 0;
   if (sigma) sigma[(uint64_t)s * 64 + j] = 1.f;
 }
 
 // After a forward level r: the new frontier masks become visit and join
 // seen; the frontier's vertices are appended to queue (with their
-// out-degrees in qdeg) for a push of the next level; the levels of the new
+// out-degrees in qdeg, and for BC their new masks in qmask) for a push of the
+// next level and for the backward pass; the levels of the new
 // (vertex, source) pairs are written by the whole warp, one vertex at a time
 // with lanes over sources (whole-row stores).  stats[0] = frontier vertices
 // (the queue length), stats[1] += sum of out-degree x sources over it,
 // stats[2] += sum of out-degree (the edges a push expands).
-__global__ void k_ms_fwd_vertex(uint32_t n, int32_t r, uint64_t* seen, uint64_t* visit, uint64_t* next, int32_t* lvl,
+__global__ void k_ms_fwd_vertex(uint32_t n, int32_t r, uint64_t* seen, uint64_t* visit, uint64_t* next,
                                 int32_t* out_lv, uint32_t out_k, const uint32_t* old_of_new, const uint32_t* out_off,
-                                uint32_t* queue, uint32_t* qdeg, unsigned long long* stats) {
+                                uint32_t* queue, uint32_t* qdeg, uint64_t* qmask, unsigned long long* stats) {
   const int lane = threadIdx.x & 31;
   const uint64_t w0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -503,6 +503,7 @@ __global__ void k_ms_fwd_vertex(uint32_t n, int32_t r, uint64_t* seen, uint64_t*
     if (nm) {
       queue[pos] = (uint32_t)v;
       qdeg[pos] = d;
+      if (qmask) qmask[pos] = nm;
     }
     while (act) {
       const int b = __ffs(act) - 1;
@@ -510,10 +511,6 @@ __global__ void k_ms_fwd_vertex(uint32_t n, int32_t r, uint64_t* seen, uint64_t*
       const uint64_t vv = base + b;
       const uint64_t mm = __shfl_sync(0xffffffffu, nm, b);
       const bool lo = (mm >> lane) & 1u, hi = (mm >> (lane + 32)) & 1u;
-      if (lvl) {
-        if (lo) lvl[vv * 64 + lane] = r;
-        if (hi) lvl[vv * 64 + 32 + lane] = r;
-      }
       if (out_lv) {
         const uint64_t row = (uint64_t)(old_of_new ? old_of_new[vv] : vv) * out_k;
         if (lo) out_lv[row + lane] = r;
@@ -563,19 +560,48 @@ __global__ void k_ms_push(const uint32_t* queue, const uint32_t* qoff, uint32_t 
   }
 }
 
-// Backward level r: mask[v] = sources with level r at v, and dep[v][j] =
-// 1/paths[v][j] there (BC_Back_Vertex_F, app/BC.C:140-154).  One warp per vertex.
-__global__ void k_ms_level_mask(uint32_t n, int32_t r, const int32_t* lvl, uint64_t* mask, const float* sigma,
-                                float* dep) {
+// Backward level r from the level's vertex list (recorded by the forward
+// pass): mask[v] = the sources with level r at v and dep[v][j] = 1/paths[v][j]
+// there (BC_Back_Vertex_F, app/BC.C:140-154).  One warp per listed vertex.
+__global__ void k_ms_level_seed(const uint32_t* list, const uint64_t* masks, uint32_t cnt, uint64_t* mask,
+                                const float* sigma, float* dep) {
   const int lane = threadIdx.x & 31;
   const uint64_t w0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  for (uint64_t v = w0; v < n; v += nw) {
-    const int32_t l0 = lvl[v * 64 + lane], l1 = lvl[v * 64 + 32 + lane];
-    const uint32_t lo = __ballot_sync(0xffffffffu, l0 == r), hi = __ballot_sync(0xffffffffu, l1 == r);
-    if (lane == 0) mask[v] = (uint64_t)lo | ((uint64_t)hi << 32);
-    if (l0 == r) dep[v * 64 + lane] = 1.f / sigma[v * 64 + lane];
-    if (l1 == r) dep[v * 64 + 32 + lane] = 1.f / sigma[v * 64 + 32 + lane];
+  for (uint64_t i = w0; i < cnt; i += nw) {
+    const uint64_t v = list[i];
+    const uint64_t mk = masks[i];
+    if (lane == 0) mask[v] = mk;
+    if ((mk >> lane) & 1u) dep[v * 64 + lane] = 1.f / sigma[v * 64 + lane];
+    if ((mk >> (lane + 32)) & 1u) dep[v * 64 + 32 + lane] = 1.f / sigma[v * 64 + 32 + lane];
+  }
+}
+
+// Backward step of a sparse level: one thread per out-edge (x, y) of the
+// level-r vertices (load-balanced through the exclusive degree sums qoff of
+// the list); dep[x][j] += dep[y][j] for the sources j at level r at x and
+// r + 1 at y.  The pairs written (level r) and read (level r + 1) differ.
+__global__ void k_ms_back_edges(const uint32_t* list, const uint32_t* qoff, uint32_t cnt, uint64_t edges,
+                                const uint32_t* out_off, const uint32_t* out_idx, const uint64_t* cur,
+                                const uint64_t* prev, float* dep) {
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < edges;
+       t += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = cnt - 1;  // the last list entry whose first edge is <= t
+    while (lo < hi) {
+      const uint32_t mid = lo + (hi - lo + 1) / 2;
+      if (qoff[mid] <= t)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const uint32_t x = list[lo];
+    const uint32_t y = out_idx[out_off[x] + (uint32_t)(t - qoff[lo])];
+    uint64_t b = cur[x] & prev[y];
+    while (b) {
+      const int j = __ffsll((long long)b) - 1;
+      b &= b - 1;
+      atomicAdd(dep + (uint64_t)x * 64 + j, dep[(uint64_t)y * 64 + j]);
+    }
   }
 }
 
@@ -661,8 +687,7 @@ static int run_ms(gg_graph_s* g, int32_t k, const uint32_t* given_sources, bool 
   const uint64_t nk = (uint64_t)n * k;
   const uint64_t kmask = k == 64 ? ~0ull : ((1ull << k) - 1);
   DevAllocs mem(g->stream);
-  uint64_t *seen, *visit, *next, *mask_a, *mask_b;
-  int32_t* lvl = nullptr;  // n x 64 levels, kept for the BC backward pass
+  uint64_t *seen, *visit, *next, *mask_a, *mask_b, *qmask = nullptr;
   float *sigma = nullptr, *dep = nullptr;
   uint32_t *d_src, *queue, *qdeg, *qoff;
   unsigned char* scan_tmp;
@@ -679,9 +704,9 @@ static int run_ms(gg_graph_s* g, int32_t k, const uint32_t* given_sources, bool 
   GG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, qdeg, qoff, (int)n, g->stream));
   GG_TRY(mem.get(&scan_tmp, scan_bytes));
   if (bc) {
-    GG_TRY(mem.get(&lvl, n64));
     GG_TRY(mem.get(&sigma, n64));
     GG_TRY(mem.get(&dep, n64));
+    GG_TRY(mem.get(&qmask, n));
   }
   // multi-source BFS writes its levels straight into the n x k output
   DevBuf<int32_t> lout;
@@ -702,6 +727,18 @@ static int run_ms(gg_graph_s* g, int32_t k, const uint32_t* given_sources, bool 
     f_edges += g->h_out_off()[uq[i] + 1] - g->h_out_off()[uq[i]];
   }
   uint64_t f_cnt = uq.size();
+  // BC: every level's vertices, their level masks and out-degrees, for the
+  // backward pass (level 0: the distinct sources)
+  std::vector<uint32_t*> r_list, r_deg;
+  std::vector<uint64_t*> r_mask;
+  std::vector<uint64_t> r_cnt, r_edges;
+  std::vector<uint64_t> umask(uq.size(), 0);
+  std::vector<uint32_t> udeg(uq.size());
+  for (size_t i = 0; i < uq.size(); ++i) {
+    udeg[i] = g->h_out_off()[uq[i] + 1] - g->h_out_off()[uq[i]];
+    for (int32_t j = 0; j < k; ++j)
+      if (sources[j] == uq[i]) umask[i] |= 1ull << j;
+  }
   unsigned long long* h_stats = reinterpret_cast<unsigned long long*>(g->ws.h_red);
   g->kernels = 0;
   EventTimer tm(g->stream);
@@ -711,10 +748,24 @@ static int run_ms(gg_graph_s* g, int32_t k, const uint32_t* given_sources, bool 
   GG_CUDA(cudaMemsetAsync(seen, 0, 8 * (uint64_t)n, g->stream));
   GG_CUDA(cudaMemsetAsync(visit, 0, 8 * (uint64_t)n, g->stream));
   GG_CUDA(cudaMemsetAsync(next, 0, 8 * (uint64_t)n, g->stream));
-  if (lvl) GG_CUDA(cudaMemsetAsync(lvl, 0xff, 4 * n64, g->stream));
   if (out_lv) GG_CUDA(cudaMemsetAsync(out_lv, 0xff, 4 * nk, g->stream));
-  if (bc) GG_CUDA(cudaMemsetAsync(sigma, 0, 4 * n64, g->stream));
-  k_ms_seed<<<1, 64, 0, g->stream>>>(d_src, (uint32_t)k, seen, visit, lvl, out_lv, old_of_new, sigma);
+  if (bc) {
+    GG_CUDA(cudaMemsetAsync(sigma, 0, 4 * n64, g->stream));
+    uint32_t *l0, *d0;
+    uint64_t* m0;
+    GG_TRY(mem.get(&l0, uq.size()));
+    GG_TRY(mem.get(&d0, uq.size()));
+    GG_TRY(mem.get(&m0, uq.size()));
+    GG_CUDA(cudaMemcpyAsync(l0, uq.data(), 4 * uq.size(), cudaMemcpyHostToDevice, g->stream));
+    GG_CUDA(cudaMemcpyAsync(d0, udeg.data(), 4 * uq.size(), cudaMemcpyHostToDevice, g->stream));
+    GG_CUDA(cudaMemcpyAsync(m0, umask.data(), 8 * uq.size(), cudaMemcpyHostToDevice, g->stream));
+    r_list.push_back(l0);
+    r_deg.push_back(d0);
+    r_mask.push_back(m0);
+    r_cnt.push_back(uq.size());
+    r_edges.push_back(f_edges);
+  }
+  k_ms_seed<<<1, 64, 0, g->stream>>>(d_src, (uint32_t)k, seen, visit, out_lv, old_of_new, sigma);
   g->kernels++;
   uint64_t trav = 0;
   for (int32_t j = 0; j < k; ++j) trav += g->h_out_off()[sources[j] + 1] - g->h_out_off()[sources[j]];
@@ -735,8 +786,8 @@ static int run_ms(gg_graph_s* g, int32_t k, const uint32_t* given_sources, bool 
       GG_TRY(ms_pull(g, bc, true, true, seen, ~0ull, kmask, visit, sigma, next));
     }
     GG_CUDA(cudaMemsetAsync(d_stats, 0, 32, g->stream));
-    k_ms_fwd_vertex<<<vgrid, kGenericThreads, 0, g->stream>>>(n, r, seen, visit, next, lvl, out_lv, (uint32_t)k,
-                                                              old_of_new, g->out_off(), queue, qdeg, d_stats);
+    k_ms_fwd_vertex<<<vgrid, kGenericThreads, 0, g->stream>>>(n, r, seen, visit, next, out_lv, (uint32_t)k,
+                                                              old_of_new, g->out_off(), queue, qdeg, qmask, d_stats);
     g->kernels++;
     GG_CUDA(cudaMemcpyAsync(h_stats, d_stats, 24, cudaMemcpyDeviceToHost, g->stream));
     GG_CUDA(cudaStreamSynchronize(g->stream));
@@ -746,6 +797,21 @@ static int run_ms(gg_graph_s* g, int32_t k, const uint32_t* given_sources, bool 
     trav += h_stats[1];
     f_cnt = h_stats[0];
     f_edges = h_stats[2];
+    if (bc) {  // keep this level's vertex list for the backward pass
+      uint32_t *lr, *dr;
+      uint64_t* mr;
+      GG_TRY(mem.get(&lr, f_cnt));
+      GG_TRY(mem.get(&dr, f_cnt));
+      GG_TRY(mem.get(&mr, f_cnt));
+      GG_CUDA(cudaMemcpyAsync(lr, queue, 4 * f_cnt, cudaMemcpyDeviceToDevice, g->stream));
+      GG_CUDA(cudaMemcpyAsync(dr, qdeg, 4 * f_cnt, cudaMemcpyDeviceToDevice, g->stream));
+      GG_CUDA(cudaMemcpyAsync(mr, qmask, 8 * f_cnt, cudaMemcpyDeviceToDevice, g->stream));
+      r_list.push_back(lr);
+      r_deg.push_back(dr);
+      r_mask.push_back(mr);
+      r_cnt.push_back(f_cnt);
+      r_edges.push_back(f_edges);
+    }
     if ((int64_t)(f_cnt + f_edges) <= thr && f_edges > 0) {
       GG_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, qdeg, qoff, (int)f_cnt, g->stream));
     }
@@ -753,14 +819,27 @@ static int run_ms(gg_graph_s* g, int32_t k, const uint32_t* given_sources, bool 
   if (bc) {
     GG_TRY(mem.get(&mask_a, n));
     GG_TRY(mem.get(&mask_b, n));
+    GG_CUDA(cudaMemsetAsync(mask_b, 0, 8 * (uint64_t)n, g->stream));
     GG_CUDA(cudaMemsetAsync(dep, 0, 4 * n64, g->stream));
-    const int wgrid = generic_grid(g, (uint64_t)n * 32);
     uint64_t *cur = mask_a, *prev = mask_b;
     for (int32_t r = L; r >= 0; --r) {
-      k_ms_level_mask<<<wgrid, kGenericThreads, 0, g->stream>>>(n, r, lvl, cur, sigma, dep);
+      // cur = the level-r masks (zero elsewhere), dep seeded with 1/paths there
+      GG_CUDA(cudaMemsetAsync(cur, 0, 8 * (uint64_t)n, g->stream));
+      k_ms_level_seed<<<generic_grid(g, r_cnt[r] * 32), kGenericThreads, 0, g->stream>>>(r_list[r], r_mask[r],
+                                                                                         (uint32_t)r_cnt[r], cur,
+                                                                                         sigma, dep);
       g->kernels++;
       if (r < L) {
-        GG_TRY(ms_pull(g, true, false, false, cur, 0, kmask, prev, dep, nullptr));
+        if ((int64_t)(r_cnt[r] + r_edges[r]) <= thr) {  // few edges leave level r: walk only them
+          if (r_edges[r] > 0) {
+            GG_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, r_deg[r], qoff, (int)r_cnt[r], g->stream));
+            k_ms_back_edges<<<generic_grid(g, r_edges[r]), kGenericThreads, 0, g->stream>>>(
+                r_list[r], qoff, (uint32_t)r_cnt[r], r_edges[r], g->out_off(), g->out_idx(), cur, prev, dep);
+            g->kernels++;
+          }
+        } else {
+          GG_TRY(ms_pull(g, true, false, false, cur, 0, kmask, prev, dep, nullptr));
+        }
         trav += level_trav[r + 1];
       }
       std::swap(cur, prev);
