@@ -462,8 +462,16 @@ constexpr int kCooThreads = kCooWarps * 32;
 __host__ __device__ constexpr size_t coo_w_stage_bytes(bool hw) {
   return (size_t)kSegBlock * 4 + (size_t)kSegBlock * 2 + (hw ? (size_t)kSegBlock * 4 : 0);
 }
-__host__ __device__ constexpr size_t coo_w_smem_bytes(bool hw, int stages, int vbytes, uint32_t tv) {
-  return 256 + (size_t)kCooWarps * stages * coo_w_stage_bytes(hw) + (size_t)((tv + 3) & ~3u) * (vbytes + 2);
+// Per tile destination: the accumulator plus a "touched" byte (functors whose
+// identity does not mark untouched destinations, when the output is kept)
+// and a "cond" byte (functors with a condition on the destination).
+template <class F, bool NOOUT>
+__host__ __device__ constexpr int coo_w_flag_bytes() {
+  return (!F::kPositive && !NOOUT ? 1 : 0) + (F::kCondTrue ? 0 : 1);
+}
+__host__ __device__ constexpr size_t coo_w_smem_bytes(bool hw, int stages, int vbytes, uint32_t tv, int flag_bytes = 2) {
+  return (stages > 0 ? 256 : 0) + (size_t)kCooWarps * stages * coo_w_stage_bytes(hw) +
+         (size_t)((tv + 3) & ~3u) * (vbytes + flag_bytes);
 }
 
 #ifndef GG_COO_MIN_BLOCKS
@@ -486,11 +494,12 @@ __global__ void __launch_bounds__(kCooThreads, GG_COO_MIN_BLOCKS) k_pull_coo_w(c
   extern __shared__ __align__(128) unsigned char smem[];
   constexpr uint32_t SB = (uint32_t)coo_w_stage_bytes(HW);
   const uint32_t tv4 = (p.tv + 3) & ~3u;
+  constexpr bool kTouch = !F::kPositive && !NOOUT;
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
-  unsigned char* stages = smem + 256;
+  unsigned char* stages = smem + (STAGES > 0 ? 256 : 0);
   V* s_acc = reinterpret_cast<V*>(stages + (size_t)kCooWarps * STAGES * SB);
-  uint8_t* s_touch = reinterpret_cast<uint8_t*>(s_acc + tv4);
-  uint8_t* s_cond = s_touch + tv4;
+  uint8_t* s_touch = reinterpret_cast<uint8_t*>(s_acc + tv4);  // kTouch only
+  uint8_t* s_cond = s_touch + (kTouch ? tv4 : 0);              // !F::kCondTrue only
   __shared__ uint32_t s_tile;
   __shared__ unsigned long long s_red[2][kCooWarps];
   __shared__ int s_fail;
@@ -515,8 +524,8 @@ __global__ void __launch_bounds__(kCooThreads, GG_COO_MIN_BLOCKS) k_pull_coo_w(c
     const uint32_t v0 = td.x, nv = td.y, e0 = td.z, ne = td.w;  // e0, ne multiples of 8
     for (uint32_t i = tid; i < nv; i += kCooThreads) {
       s_acc[i] = F::identity();
-      if (!F::kPositive && !NOOUT) s_touch[i] = 0;
-      s_cond[i] = (F::kCondTrue || f.cond(v0 + i)) ? 1 : 0;
+      if (kTouch) s_touch[i] = 0;
+      if (!F::kCondTrue) s_cond[i] = f.cond(v0 + i) ? 1 : 0;
     }
     __syncthreads();
     const uint32_t nb = (ne + kSegBlock - 1) / kSegBlock;
@@ -663,13 +672,13 @@ __global__ void __launch_bounds__(kCooThreads, GG_COO_MIN_BLOCKS) k_pull_coo_w(c
         for (int k = 0; k < 8; ++k) {
           if (!vld[k]) continue;
           F::atomic_combine(&s_acc[dv[k]], val[k]);
-          if (!F::kPositive && !NOOUT) s_touch[dv[k]] = 1;
+          if (kTouch) s_touch[dv[k]] = 1;
         }
         continue;
       }
       auto flush = [&](int l, V v) {
         F::atomic_combine(&s_acc[l], v);
-        if (!F::kPositive && !NOOUT) s_touch[l] = 1;
+        if (kTouch) s_touch[l] = 1;
       };
       if constexpr (MERGE) {
         // The block is sorted by destination, so a lane's middle runs are
@@ -737,18 +746,18 @@ __global__ void __launch_bounds__(kCooThreads, GG_COO_MIN_BLOCKS) k_pull_coo_w(c
         for (int o = 16; o > 0; o >>= 1) r = F::combine(r, __shfl_xor_sync(0xffffffffu, r, o));
         if (lane == 0) {
           F::atomic_combine(&s_acc[c0], r);
-          if (!F::kPositive && !NOOUT) s_touch[c0] = 1;
+          if (kTouch) s_touch[c0] = 1;
         }
       } else if (cur >= 0) {
         F::atomic_combine(&s_acc[cur], acc);
-        if (!F::kPositive && !NOOUT) s_touch[cur] = 1;
+        if (kTouch) s_touch[cur] = 1;
       }
     }
     __syncthreads();
     if (s_fail) break;
     if constexpr (NOOUT) {
       for (uint32_t l = tid; l < nv; l += kCooThreads)
-        if (s_acc[l] != F::identity() && s_cond[l]) f.commit(v0 + l, s_acc[l]);
+        if (s_acc[l] != F::identity() && (F::kCondTrue || s_cond[l])) f.commit(v0 + l, s_acc[l]);
       __syncthreads();
       continue;
     }
@@ -759,7 +768,7 @@ __global__ void __launch_bounds__(kCooThreads, GG_COO_MIN_BLOCKS) k_pull_coo_w(c
       if (v >= v0 && v < v0 + nv) {
         const uint32_t l = v - v0;
         const bool touched = F::kPositive ? (s_acc[l] != F::identity()) : (s_touch[l] != 0);
-        if (touched && s_cond[l]) act = f.commit(v, s_acc[l]);
+        if (touched && (F::kCondTrue || s_cond[l])) act = f.commit(v, s_acc[l]);
       }
       const uint32_t word = __ballot_sync(0xffffffffu, act);
       if (act) my_deg += __ldg(p.deg_off + v + 1) - __ldg(p.deg_off + v);

@@ -227,11 +227,14 @@ int pull_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f
     static DeviceOnce opted_pf[2];
     static DeviceOnce opted_no[2][2];
     static DeviceOnce opted_mg[2];
-    auto launch_w = [&](auto kern, int stages, DeviceOnce& once) -> int {
-      const size_t smem = coo_w_smem_bytes(kHW, stages, 4, p.tv);
+    constexpr int kFlags = coo_w_flag_bytes<F, false>(), kFlagsNoOut = coo_w_flag_bytes<F, true>();
+    auto launch_w = [&](auto kern, int stages, DeviceOnce& once, int flags) -> int {
+      const size_t smem = coo_w_smem_bytes(kHW, stages, 4, p.tv, flags);
       const int ok = once.get(g->device, [&]() {
         return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)coo_w_smem_bytes(kHW, stages, 4, kMaxTileVertices)) == cudaSuccess ? 1 : -1;
+                                    (int)coo_w_smem_bytes(kHW, stages, 4, kMaxTileVertices, flags)) == cudaSuccess
+                   ? 1
+                   : -1;
       });
       if (ok < 0) return fail(GG_ERR_CUDA, "cudaFuncSetAttribute failed for the COO pull");
       int blocks = 1;
@@ -245,31 +248,32 @@ int pull_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f
     };
     if constexpr (F::kIdentityCommitNoop) {
       if (no_out && g->coo_kernel == 1)
-        return all ? launch_w(k_pull_coo_w<F, kHW, true, 0, false, false, true>, 0, opted_no[0][1])
-                   : launch_w(k_pull_coo_w<F, kHW, false, 0, false, false, true>, 0, opted_no[0][0]);
+        return all ? launch_w(k_pull_coo_w<F, kHW, true, 0, false, false, true>, 0, opted_no[0][1], kFlagsNoOut)
+                   : launch_w(k_pull_coo_w<F, kHW, false, 0, false, false, true>, 0, opted_no[0][0], kFlagsNoOut);
       if (no_out && g->coo_kernel == 6)
-        return all ? launch_w(k_pull_coo_w<F, kHW, true, 0, false, false, true, true>, 0, opted_no[1][1])
-                   : launch_w(k_pull_coo_w<F, kHW, false, 0, false, false, true, true>, 0, opted_no[1][0]);
+        return all ? launch_w(k_pull_coo_w<F, kHW, true, 0, false, false, true, true>, 0, opted_no[1][1], kFlagsNoOut)
+                   : launch_w(k_pull_coo_w<F, kHW, false, 0, false, false, true, true>, 0, opted_no[1][0],
+                              kFlagsNoOut);
     }
     switch (g->coo_kernel) {
       case 6:
-        return all ? launch_w(k_pull_coo_w<F, kHW, true, 0, false, false, false, true>, 0, opted_mg[1])
-                   : launch_w(k_pull_coo_w<F, kHW, false, 0, false, false, false, true>, 0, opted_mg[0]);
+        return all ? launch_w(k_pull_coo_w<F, kHW, true, 0, false, false, false, true>, 0, opted_mg[1], kFlags)
+                   : launch_w(k_pull_coo_w<F, kHW, false, 0, false, false, false, true>, 0, opted_mg[0], kFlags);
       case 5:
-        return all ? launch_w(k_pull_coo_w<F, kHW, true, 0, false, true>, 0, opted_pf[1])
-                   : launch_w(k_pull_coo_w<F, kHW, false, 0, false, true>, 0, opted_pf[0]);
+        return all ? launch_w(k_pull_coo_w<F, kHW, true, 0, false, true>, 0, opted_pf[1], kFlags)
+                   : launch_w(k_pull_coo_w<F, kHW, false, 0, false, true>, 0, opted_pf[0], kFlags);
       case 4:
-        return all ? launch_w(k_pull_coo_w<F, kHW, true, 0, true>, 0, opted[1][0])
-                   : launch_w(k_pull_coo_w<F, kHW, false, 0, true>, 0, opted[0][0]);
+        return all ? launch_w(k_pull_coo_w<F, kHW, true, 0, true>, 0, opted[1][0], kFlags)
+                   : launch_w(k_pull_coo_w<F, kHW, false, 0, true>, 0, opted[0][0], kFlags);
       case 1:
-        return all ? launch_w(k_pull_coo_w<F, kHW, true, 0>, 0, opted[1][1])
-                   : launch_w(k_pull_coo_w<F, kHW, false, 0>, 0, opted[0][1]);
+        return all ? launch_w(k_pull_coo_w<F, kHW, true, 0>, 0, opted[1][1], kFlags)
+                   : launch_w(k_pull_coo_w<F, kHW, false, 0>, 0, opted[0][1], kFlags);
       case 2:
-        return all ? launch_w(k_pull_coo_w<F, kHW, true, 2>, 2, opted[1][2])
-                   : launch_w(k_pull_coo_w<F, kHW, false, 2>, 2, opted[0][2]);
+        return all ? launch_w(k_pull_coo_w<F, kHW, true, 2>, 2, opted[1][2], kFlags)
+                   : launch_w(k_pull_coo_w<F, kHW, false, 2>, 2, opted[0][2], kFlags);
       default:
-        return all ? launch_w(k_pull_coo_w<F, kHW, true, 3>, 3, opted[1][3])
-                   : launch_w(k_pull_coo_w<F, kHW, false, 3>, 3, opted[0][3]);
+        return all ? launch_w(k_pull_coo_w<F, kHW, true, 3>, 3, opted[1][3], kFlags)
+                   : launch_w(k_pull_coo_w<F, kHW, false, 3>, 3, opted[0][3], kFlags);
     }
   }
   if (coo) {
