@@ -431,8 +431,15 @@ def run_stress(gg):
         out[name] = {"n": hg.n, "m": hg.m, "partitions": P,
                      "bfs": {"ms": round(bfs_ms, 3), "levels": rb.rounds,
                              "gteps": round(rb.edges_traversed / bfs_ms / 1e6, 2)},
-                     "components": {"ms": round(cc_ms, 3), "rounds": rc.rounds,
-                                    "gteps": round(rc.edges_traversed / cc_ms / 1e6, 2)}}
+                     "components": {"algorithm": "label propagation (app/Components.C)", "ms": round(cc_ms, 3),
+                                    "rounds": rc.rounds, "gteps": round(rc.edges_traversed / cc_ms / 1e6, 2)}}
+        if hg.symmetric:  # the same labels by union-find (GG_TUNE_CC_ALGO 1)
+            g.set_tuning(gg.TUNE_CC_ALGO, 1)
+            g.components()
+            uf_ms = _best(lambda: g.components()[1].ms, 3)
+            g.set_tuning(gg.TUNE_CC_ALGO, 0)
+            out[name]["components_union_find"] = {"ms": round(uf_ms, 3),
+                                                  "speedup_vs_label_propagation": round(cc_ms / uf_ms, 1)}
         g.close()
         del hg
     out["seconds"] = round(time.time() - t0, 1)

@@ -222,8 +222,109 @@ static int run_bfs(gg_graph_s* g, uint32_t start, int32_t* parents, int32_t* lev
   return GG_OK;
 }
 
+// ------------------------------------------------ union-find components
+// On a symmetric graph the fixed point of app/Components.C's label
+// propagation is the smallest id of each connected component.  Union-find
+// reaches it in one pass over the edges: every parent pointer goes to a
+// smaller id, so a tree's root is its smallest vertex, and hooking always
+// puts the larger of two roots under the smaller one (a CAS on the root's
+// own pointer; a failed CAS continues from the root's new parent).
+__device__ __forceinline__ uint32_t uf_find(uint32_t* par, uint32_t v) {
+  uint32_t cur = __ldcg(par + v);
+  if (cur == v) return v;
+  uint32_t prev = v;
+  for (;;) {
+    const uint32_t next = __ldcg(par + cur);
+    if (next == cur) return cur;
+    par[prev] = next;  // path halving: any ancestor is a valid parent
+    prev = cur;
+    cur = next;
+  }
+}
+
+__global__ void k_uf_init(uint32_t n, uint32_t* par, uint32_t* minid) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x) {
+    par[v] = (uint32_t)v;
+    if (minid) minid[v] = 0xffffffffu;
+  }
+}
+
+// One thread per CSR edge (row found by binary search over the offsets);
+// each undirected edge is taken once, from its larger end.
+__global__ void k_uf_hook(uint64_t m, uint32_t n, const uint32_t* off, const uint32_t* idx, uint32_t* par) {
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = n - 1;
+    while (lo < hi) {
+      const uint32_t mid = lo + (hi - lo + 1) / 2;
+      if (off[mid] <= e)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const uint32_t u = lo, v = idx[e];
+    if (v >= u) continue;
+    uint32_t ru = uf_find(par, u), rv = uf_find(par, v);
+    while (ru != rv) {
+      if (ru < rv) {
+        const uint32_t t = ru;
+        ru = rv;
+        rv = t;
+      }
+      const uint32_t old = atomicCAS(par + ru, ru, rv);  // hook the larger root under the smaller
+      if (old == ru) break;
+      ru = uf_find(par, old);
+      rv = uf_find(par, rv);
+    }
+  }
+}
+
+// minid[root] = the smallest given id of the root's component (renumbered graphs).
+__global__ void k_uf_min_given(uint32_t n, uint32_t* par, const uint32_t* old_of_new, uint32_t* minid) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x)
+    atomicMin(minid + uf_find(par, (uint32_t)v), old_of_new[v]);
+}
+
+__global__ void k_uf_label(uint32_t n, uint32_t* par, const uint32_t* minid, int32_t* ids) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t r = uf_find(par, (uint32_t)v);
+    ids[v] = (int32_t)(minid ? minid[r] : r);
+  }
+}
+
+static int run_cc_union_find(gg_graph_s* g, int32_t* ids_out, gg_run_stats* st) {
+  const uint32_t n = g->n;
+  g->kernels = 0;
+  DevBuf<uint32_t> par, minid;
+  DevBuf<int32_t> ids;
+  GG_TRY(par.alloc(g, n));
+  GG_TRY(ids.alloc(g, n));
+  if (g->relabeled) GG_TRY(minid.alloc(g, n));
+  EventTimer tm(g->stream);
+  const int grid = generic_grid(g, n);
+  k_uf_init<<<grid, kGenericThreads, 0, g->stream>>>(n, par.p, g->relabeled ? minid.p : nullptr);
+  g->kernels++;
+  if (g->m) {
+    k_uf_hook<<<generic_grid(g, g->m), kGenericThreads, 0, g->stream>>>(g->m, n, g->out_off(), g->out_idx(), par.p);
+    g->kernels++;
+  }
+  if (g->relabeled) {
+    k_uf_min_given<<<grid, kGenericThreads, 0, g->stream>>>(n, par.p, g->d_old_of_new, minid.p);
+    g->kernels++;
+  }
+  k_uf_label<<<grid, kGenericThreads, 0, g->stream>>>(n, par.p, g->relabeled ? minid.p : nullptr, ids.p);
+  g->kernels++;
+  GG_CUDA(cudaGetLastError());
+  const int32_t* res = ids.p;
+  GG_TRY(given_order<int32_t>(g, ids.p, 0, &res));
+  const double ms = tm.stop();
+  GG_TRY(to_host(g, ids_out, res, n));
+  fill_stats(st, ms, 1, g->m, g->kernels);
+  return GG_OK;
+}
+
 // app/Components.C:202-227
 static int run_cc(gg_graph_s* g, int32_t* ids_out, gg_run_stats* st) {
+  if (g->cc_algo == 1 && g->symmetric) return run_cc_union_find(g, ids_out, st);
   const uint32_t n = g->n;
   g->kernels = 0;
   DevBuf<int32_t> ids, prev;

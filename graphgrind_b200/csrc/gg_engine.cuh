@@ -142,6 +142,7 @@ struct gg_graph_s {
   int dense_policy = 0;
   int sparse_div = 20;  // the apps' edgeMap threshold is m / sparse_div (app/*.C pass m/20)
   int device_loop = 1;  // BFS runs consecutive sparse levels in one cooperative launch
+  int cc_algo = 0;      // Components on symmetric graphs: 0 label propagation, 1 union-find
   int coo_kernel = 6;  // 0 CTA ring (k_pull), 1 per-warp direct loads, 2/3 per-warp bulk-copy rings, 6 direct loads
                        // with cross-lane run merging (fastest measured)
   // gg_build_opts.vertex_order: device ids differ from the given ids

@@ -833,6 +833,10 @@ int gg_graph_set_tuning(gg_graph_t g, int32_t key, int64_t value) {
       if (value != 0 && value != 1) return fail(GG_ERR_INVALID_ARG, "device loop switch must be 0 or 1");
       g->device_loop = (int)value;
       return GG_OK;
+    case GG_TUNE_CC_ALGO:
+      if (value != 0 && value != 1) return fail(GG_ERR_INVALID_ARG, "components algorithm must be 0 or 1");
+      g->cc_algo = (int)value;
+      return GG_OK;
     default:
       return fail(GG_ERR_INVALID_ARG, "unknown tuning key %d", key);
   }
@@ -852,6 +856,9 @@ int gg_graph_get_tuning(gg_graph_t g, int32_t key, int64_t* value) {
       return GG_OK;
     case GG_TUNE_DEVICE_LOOP:
       *value = g->device_loop;
+      return GG_OK;
+    case GG_TUNE_CC_ALGO:
+      *value = g->cc_algo;
       return GG_OK;
     default:
       return fail(GG_ERR_INVALID_ARG, "unknown tuning key %d", key);

@@ -1,6 +1,7 @@
 // Autotuner: picks the engine's knobs for one application on one graph by
 // timing it.  Runtime knobs (dense-pull layout policy, COO pull kernel,
-// push/pull threshold m/div) are searched on a built graph; build knobs
+// push/pull threshold m/div, and for Components on a symmetric graph the
+// union-find pass) are searched on a built graph; build knobs
 // (partition count, CTA tile size, COO window order) by building the graph
 // once per candidate; the personalised-PageRank column count by timing one
 // k-column pass per candidate k.  Every knob leaves edgeMap's results as they
@@ -70,6 +71,7 @@ int set_knobs(gg_graph_t g, const gg_tune_trial& t) {
   GG_TRY_HOST(gg_graph_set_tuning(g, GG_TUNE_DENSE_POLICY, t.dense_policy));
   GG_TRY_HOST(gg_graph_set_tuning(g, GG_TUNE_COO_KERNEL, t.coo_kernel));
   GG_TRY_HOST(gg_graph_set_tuning(g, GG_TUNE_SPARSE_DIV, t.sparse_div));
+  GG_TRY_HOST(gg_graph_set_tuning(g, GG_TUNE_CC_ALGO, t.cc_algo));
   return GG_OK;
 }
 
@@ -82,10 +84,11 @@ int gg_autotune(gg_graph_t g, int32_t app, uint32_t start, gg_tune_trial* trials
   gg_graph_info info{};
   GG_TRY_HOST(gg_graph_get_info(g, &info));
   if (start >= info.n) return gg::fail(GG_ERR_INVALID_ARG, "gg_autotune: start %u out of range", start);
-  int64_t keep[3];
+  int64_t keep[4];
   GG_TRY_HOST(gg_graph_get_tuning(g, GG_TUNE_DENSE_POLICY, &keep[0]));
   GG_TRY_HOST(gg_graph_get_tuning(g, GG_TUNE_COO_KERNEL, &keep[1]));
   GG_TRY_HOST(gg_graph_get_tuning(g, GG_TUNE_SPARSE_DIV, &keep[2]));
+  GG_TRY_HOST(gg_graph_get_tuning(g, GG_TUNE_CC_ALGO, &keep[3]));
   HostBufs bufs(info.n);
   std::vector<gg_tune_trial> tried;
   const bool has_coo = info.num_coo_tiles > 0;
@@ -97,6 +100,7 @@ int gg_autotune(gg_graph_t g, int32_t app, uint32_t start, gg_tune_trial* trials
     gg_graph_set_tuning(g, GG_TUNE_DENSE_POLICY, keep[0]);
     gg_graph_set_tuning(g, GG_TUNE_COO_KERNEL, keep[1]);
     gg_graph_set_tuning(g, GG_TUNE_SPARSE_DIV, keep[2]);
+    gg_graph_set_tuning(g, GG_TUNE_CC_ALGO, keep[3]);
   };
   for (int pol : policies) {
     if (pol == 2 && !has_coo) continue;
@@ -117,6 +121,21 @@ int gg_autotune(gg_graph_t g, int32_t app, uint32_t start, gg_tune_trial* trials
         tried.push_back(t);
       }
     }
+  }
+  if (app == GG_APP_COMPONENTS && info.symmetric) {  // union-find: no edgeMap knob applies
+    gg_tune_trial t{};
+    t.dense_policy = 0;
+    t.coo_kernel = kernels[0];
+    t.sparse_div = 20;
+    t.cc_algo = 1;
+    int rc = set_knobs(g, t);
+    if (!rc) rc = time_app(g, app, start, bufs, 3, &t.ms);
+    if (rc) {
+      const std::string keep_msg = gg_last_error_string();
+      restore();
+      return gg::fail(rc, "%s", keep_msg.c_str());
+    }
+    tried.push_back(t);
   }
   std::stable_sort(tried.begin(), tried.end(), [](const gg_tune_trial& a, const gg_tune_trial& b) { return a.ms < b.ms; });
   if (tried.empty()) {  // unreachable: policy 0 is always tried

@@ -302,11 +302,19 @@ int gg_graph_set_dense_policy(gg_graph_t g, int32_t policy);
  *                         with threshold m / value (20 in the reference apps)
  *   GG_TUNE_DEVICE_LOOP   1 (default): gg_bfs runs consecutive sparse levels in
  *                         one cooperative launch that applies the direction
- *                         rule on the device; 0: one host round trip per level */
+ *                         rule on the device; 0: one host round trip per level
+ *   GG_TUNE_CC_ALGO       0 (default): gg_components runs app/Components.C's
+ *                         label propagation through edgeMap; 1: on symmetric
+ *                         graphs, a union-find pass over the edges (each root
+ *                         hooked under the smaller one), which ends with the
+ *                         same labels (the smallest id of each component) and
+ *                         reports 1 round; directed graphs keep label
+ *                         propagation, whose labels are not components */
 #define GG_TUNE_DENSE_POLICY 1
 #define GG_TUNE_COO_KERNEL 2
 #define GG_TUNE_SPARSE_DIV 3
 #define GG_TUNE_DEVICE_LOOP 4
+#define GG_TUNE_CC_ALGO 5
 int gg_graph_set_tuning(gg_graph_t g, int32_t key, int64_t value);
 int gg_graph_get_tuning(gg_graph_t g, int32_t key, int64_t* value);
 
@@ -512,11 +520,12 @@ typedef struct gg_tune_trial {
   int32_t tile_vertices;
   int32_t tile_edges;
   int32_t coo_window;
-  int32_t pad;
+  int32_t cc_algo;        /* GG_TUNE_CC_ALGO                            */
   double ms;              /* best of 3 device times of the application  */
 } gg_tune_trial;
 /* Runtime search on a built graph: every combination of dense policy, COO
- * kernel (where a COO exists) and threshold divisor {20, 10, 40}; the fastest
+ * kernel (where a COO exists) and threshold divisor {20, 10, 40}, plus the
+ * union-find pass for GG_APP_COMPONENTS on a symmetric graph; the fastest
  * is left set on g.  trials[max_trials] (may be NULL) receives the trials,
  * fastest first; *n_trials the number run. */
 int gg_autotune(gg_graph_t g, int32_t app, uint32_t start, gg_tune_trial* trials, int32_t max_trials,
