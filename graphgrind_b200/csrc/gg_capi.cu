@@ -249,31 +249,52 @@ __global__ void k_uf_init(uint32_t n, uint32_t* par, uint32_t* minid) {
   }
 }
 
-// One thread per CSR edge (row found by binary search over the offsets);
-// each undirected edge is taken once, from its larger end.
-__global__ void k_uf_hook(uint64_t m, uint32_t n, const uint32_t* off, const uint32_t* idx, uint32_t* par) {
-  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (uint64_t)gridDim.x * blockDim.x) {
-    uint32_t lo = 0, hi = n - 1;
-    while (lo < hi) {
-      const uint32_t mid = lo + (hi - lo + 1) / 2;
-      if (off[mid] <= e)
-        lo = mid;
-      else
-        hi = mid - 1;
+__device__ __forceinline__ void uf_union(uint32_t* par, uint32_t u, uint32_t v) {
+  uint32_t ru = uf_find(par, u), rv = uf_find(par, v);
+  while (ru != rv) {
+    if (ru < rv) {
+      const uint32_t t = ru;
+      ru = rv;
+      rv = t;
     }
-    const uint32_t u = lo, v = idx[e];
-    if (v >= u) continue;
-    uint32_t ru = uf_find(par, u), rv = uf_find(par, v);
-    while (ru != rv) {
-      if (ru < rv) {
-        const uint32_t t = ru;
-        ru = rv;
-        rv = t;
-      }
-      const uint32_t old = atomicCAS(par + ru, ru, rv);  // hook the larger root under the smaller
-      if (old == ru) break;
-      ru = uf_find(par, old);
-      rv = uf_find(par, rv);
+    const uint32_t old = atomicCAS(par + ru, ru, rv);  // hook the larger root under the smaller
+    if (old == ru) break;
+    ru = uf_find(par, old);
+    rv = uf_find(par, rv);
+  }
+}
+
+constexpr uint32_t kUfSmallDegree = 32;
+
+// Each undirected edge is taken once, from its larger end.  One thread per
+// vertex of degree <= 32; larger vertices are listed for k_uf_hook_big.
+__global__ void k_uf_hook_small(uint32_t n, const uint32_t* off, const uint32_t* idx, uint32_t* par, uint32_t* big,
+                                uint32_t* nbig) {
+  for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < n; x += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t u = (uint32_t)x, e0 = off[u], e1 = off[u + 1];
+    if (e1 - e0 > kUfSmallDegree) {
+      big[atomicAdd(nbig, 1u)] = u;
+      continue;
+    }
+    for (uint32_t e = e0; e < e1; ++e) {
+      const uint32_t v = idx[e];
+      if (v < u) uf_union(par, u, v);
+    }
+  }
+}
+
+// One warp per listed vertex, lanes over its edges.
+__global__ void k_uf_hook_big(const uint32_t* big, const uint32_t* nbig, const uint32_t* off, const uint32_t* idx,
+                              uint32_t* par) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t w0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint32_t cnt = *nbig;
+  for (uint64_t i = w0; i < cnt; i += nw) {
+    const uint32_t u = big[i];
+    for (uint32_t e = off[u] + lane; e < off[u + 1]; e += 32) {
+      const uint32_t v = idx[e];
+      if (v < u) uf_union(par, u, v);
     }
   }
 }
@@ -294,18 +315,23 @@ __global__ void k_uf_label(uint32_t n, uint32_t* par, const uint32_t* minid, int
 static int run_cc_union_find(gg_graph_s* g, int32_t* ids_out, gg_run_stats* st) {
   const uint32_t n = g->n;
   g->kernels = 0;
-  DevBuf<uint32_t> par, minid;
+  DevBuf<uint32_t> par, minid, big;
   DevBuf<int32_t> ids;
   GG_TRY(par.alloc(g, n));
   GG_TRY(ids.alloc(g, n));
+  GG_TRY(big.alloc(g, n));  // n + 4 entries: the list, then its length at [n]
   if (g->relabeled) GG_TRY(minid.alloc(g, n));
   EventTimer tm(g->stream);
   const int grid = generic_grid(g, n);
   k_uf_init<<<grid, kGenericThreads, 0, g->stream>>>(n, par.p, g->relabeled ? minid.p : nullptr);
   g->kernels++;
   if (g->m) {
-    k_uf_hook<<<generic_grid(g, g->m), kGenericThreads, 0, g->stream>>>(g->m, n, g->out_off(), g->out_idx(), par.p);
-    g->kernels++;
+    uint32_t* nbig = big.p + n;
+    GG_CUDA(cudaMemsetAsync(nbig, 0, sizeof(uint32_t), g->stream));
+    k_uf_hook_small<<<grid, kGenericThreads, 0, g->stream>>>(n, g->out_off(), g->out_idx(), par.p, big.p, nbig);
+    k_uf_hook_big<<<(int)g->num_sms * 8, kGenericThreads, 0, g->stream>>>(big.p, nbig, g->out_off(), g->out_idx(),
+                                                                           par.p);
+    g->kernels += 2;
   }
   if (g->relabeled) {
     k_uf_min_given<<<grid, kGenericThreads, 0, g->stream>>>(n, par.p, g->d_old_of_new, minid.p);
