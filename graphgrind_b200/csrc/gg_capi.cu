@@ -372,6 +372,12 @@ static int run_cc(gg_graph_s* g, int32_t* ids_out, gg_run_stats* st) {
     CcF f;
     f.ids = ids.p;
     f.prev = prev.p;
+    // A vertex outside the frontier has prevIDs == IDs, unchanged since the
+    // round it last was in the frontier, when every out-neighbour took a
+    // label <= it; so its value cannot lower any destination, and the dense
+    // pull may gather every source without testing the frontier bitmap
+    // (same labels, outputs and rounds).
+    f.outside_inert = true;
     trav += F.f->out_edges;
     gg_frontier_s* out = nullptr;
     GG_TRY(edge_map(g, F.f, f, app_threshold(g), 0, &out));

@@ -12,6 +12,7 @@ struct MinI32 {
   using value_t = int32_t;
   static constexpr bool kIdentityCommitNoop = false;
   bool frontier_in_values = false;  // gathered values already mark frontier membership
+  bool outside_inert = false;       // a source outside the frontier cannot change any result
   __device__ static value_t identity() { return 0x7fffffff; }
   __device__ static value_t combine(value_t a, value_t b) { return a < b ? a : b; }
   __device__ static void atomic_combine(value_t* s, value_t v) { atomicMin(s, v); }
@@ -20,6 +21,7 @@ struct MinU32 {
   using value_t = uint32_t;
   static constexpr bool kIdentityCommitNoop = false;
   bool frontier_in_values = false;  // gathered values already mark frontier membership
+  bool outside_inert = false;       // a source outside the frontier cannot change any result
   __device__ static value_t identity() { return 0xffffffffu; }
   __device__ static value_t combine(value_t a, value_t b) { return a < b ? a : b; }
   __device__ static void atomic_combine(value_t* s, value_t v) { atomicMin(s, v); }
@@ -28,6 +30,7 @@ struct SumF32 {
   using value_t = float;
   static constexpr bool kIdentityCommitNoop = false;  // set by functors whose commit is "+= acc" alone
   bool frontier_in_values = false;  // gathered values already mark frontier membership
+  bool outside_inert = false;       // a source outside the frontier cannot change any result
   __device__ static value_t identity() { return 0.0f; }
   __device__ static value_t combine(value_t a, value_t b) { return a + b; }
   __device__ static void atomic_combine(value_t* s, value_t v) { atomicAdd(s, v); }

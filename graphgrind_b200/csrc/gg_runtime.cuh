@@ -160,7 +160,7 @@ int read_stats(gg_graph_s* g);  // blocks; checks the device error word
 template <class F, bool HW>
 int pull_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f, bool coo, bool no_out = false) {
   // a positive functor whose gathered values already mark the frontier needs no bitmap
-  const bool all = in->bit || (F::kPositive && f.frontier_in_values);
+  const bool all = in->bit || (F::kPositive && f.frontier_in_values) || f.outside_inert;
   if (coo && g->coo_by_source) {  // -P source: atomic updates over the source partitions
     SrcParams sp{g->d_coo_src, g->d_coo_dst, g->d_coo_w, g->coo_len, in->d_bits, out->d_bits, g->out_off(),
                  g->ws.d_stats};
