@@ -26,6 +26,8 @@ each run through the library's C ABI (gg_bfs / gg_pagerank / gg_spmv).
            persistent launch vs plain per-graph BFS on a sample; weighted
            PageRank adjoint (RMAT-22 seed 6, 30 iterations, checkpoints every 5)
            backward vs forward time
+  other_apps = (N=1, outside the timed step) Components, PageRankDelta and
+           BellmanFord (uint32 weights in [1,100]) on the same RMAT-24 graph
   stress   = (N=1, outside the timed step) BFS from 100 and Components on the
            4096^2 grid with 0.1 % long-range edges (seed 3, high diameter,
            sparse frontiers) and on Erdos-Renyi n=2^24, m=2^28 (seed 4, dense)
@@ -297,6 +299,33 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
         "gpu_launches": launches_all,
         "clocks": clk,
     }
+    if world == 1 and not args.no_stress:
+        out["other_apps"] = run_other_apps(gg, hg, g, args)
+    return out
+
+
+def run_other_apps(gg, hg, g, args):
+    """The rest of the RMAT-24 application list (Components, PageRankDelta with
+    eps 1e-7, BellmanFord from the start vertex on uint32 weights in [1,100]),
+    outside the timed step, each the best of 3 device times."""
+    out = {}
+    ids = np.empty(hg.n, np.int32)
+    ranks = np.empty(hg.n, np.float32)
+    for name, fn in (("components", lambda: g.components()[1]),
+                     ("pagerank_delta", lambda: g.pagerank_delta()[1])):
+        fn()
+        runs = [fn() for _ in range(3)]
+        r = min(runs, key=lambda x: x.ms)
+        out[name] = {"ms": round(r.ms, 3), "rounds": r.rounds, "gteps": round(r.edges_traversed / r.ms / 1e6, 2)}
+    hw = make_graph(gg, args.scale, 2, gg.W_INT32)
+    gw = gg.Graph(hw, partitions=args.partitions, tile_edges=args.tile_edges, vertex_order=args.vertex_order)
+    gw.bellman_ford(args.start)
+    runs = [gw.bellman_ford(args.start)[1] for _ in range(3)]
+    r = min(runs, key=lambda x: x.ms)
+    out["bellman_ford"] = {"ms": round(r.ms, 3), "rounds": r.rounds,
+                           "gteps": round(r.edges_traversed / r.ms / 1e6, 2)}
+    gw.close()
+    del ids, ranks
     return out
 
 
@@ -542,7 +571,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched / adjoint comparisons")
     ap.add_argument("--no-autotune", action="store_true", help="keep the library's default runtime knobs")
-    ap.add_argument("--no-stress", action="store_true", help="skip the grid / Erdos-Renyi BFS and Components lines")
+    ap.add_argument("--no-stress", action="store_true",
+                    help="skip the other RMAT-24 apps and the grid / Erdos-Renyi BFS and Components lines")
     ap.add_argument("--vertex-order", type=int, default=1, choices=[0, 1],
                     help="device numbering: 0 the given ids, 1 hottest sources first inside each partition")
     ap.add_argument("--tile-edges", type=int, default=1 << 17,
