@@ -72,8 +72,8 @@ def workload(scale: int, partitions: int, start: int) -> str:
 HBM_FALLBACK_GBS = 6650.0
 # DRAM bytes per PageRank-pull launch of the default workload, from one ncu
 # capture (profiles/dram_k_pull_coo_w_pagerank_rmat24.md)
-TRAFFIC_RMAT24_PR_PULL = {1: 1919532928}  # by vertex order (merged-run COO kernel)
-TRAFFIC_TILE_EDGES = 1 << 17
+TRAFFIC_RMAT24_PR_PULL = {1: 1897370112}  # by vertex order (merged-run COO kernel)
+TRAFFIC_TILE_EDGES = 1 << 18
 
 
 def log(*a):
@@ -575,7 +575,7 @@ def main():
                     help="skip the other RMAT-24 apps and the grid / Erdos-Renyi BFS and Components lines")
     ap.add_argument("--vertex-order", type=int, default=1, choices=[0, 1],
                     help="device numbering: 0 the given ids, 1 hottest sources first inside each partition")
-    ap.add_argument("--tile-edges", type=int, default=1 << 17,
+    ap.add_argument("--tile-edges", type=int, default=1 << 18,
                     help="target edges per CTA tile (gg_autotune_build's choice for this workload)")
     ap.add_argument("--traffic", type=float, default=None,
                     help="DRAM bytes per dense-pull launch from an ncu capture (reported as roofline.traffic)")
