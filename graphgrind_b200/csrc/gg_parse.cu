@@ -6,6 +6,7 @@
 // compacts those positions, and one thread per number converts and range-checks
 // it into its slot of the offsets / neighbours / weights arrays.
 #include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
 #include <fcntl.h>
 #include <sys/stat.h>
 #include <unistd.h>
@@ -161,7 +162,7 @@ static int parse_adj(const char* path, int32_t symmetric, int32_t weighted, int6
   GG_PARSE_CUDA(cudaMalloc(&b.d_err, sizeof(unsigned)));
   GG_PARSE_CUDA(cudaMemsetAsync(b.d_err, 0, sizeof(unsigned), b.st));
   size_t tmp_bytes = 0;
-  cub::CountingInputIterator<uint32_t> pos(0);
+  thrust::counting_iterator<uint32_t> pos(0);
   GG_PARSE_CUDA(cub::DeviceSelect::If(nullptr, tmp_bytes, pos, b.d_starts, b.d_count, (int)(chunk + kMaxToken),
                                       TokenStart{b.d_chunk}, b.st));
   GG_PARSE_CUDA(cudaMalloc(&b.d_tmp, tmp_bytes));
