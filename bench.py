@@ -150,6 +150,19 @@ def make_graph(gg, scale: int, seed: int, weights: int):
     return hg
 
 
+def aggregate_ranks(dist, dev_ms, wall_s, edges, launches, device="cuda"):
+    """Whole-job figures of N replicas: the slowest rank's device and wall
+    times (max over ranks), the edges and kernel launches of all ranks (sum)."""
+    if not dist:
+        return dev_ms, wall_s, float(edges), int(launches)
+    import torch
+    t = torch.tensor([dev_ms, wall_s], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e = torch.tensor([edges, launches], dtype=torch.float64, device=device)
+    dist.all_reduce(e, op=dist.ReduceOp.SUM)
+    return float(t[0]), float(t[1]), float(e[0]), int(e[1])
+
+
 def run_ours(args, rank: int, world: int, local_rank: int, dist):
     import graphgrind_b200 as gg
 
@@ -234,16 +247,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
     for k in ("csc_pull", "coo_pull"):
         if prof_pr[k]["launches"] >= pr_prof["launches"]:
             pr_kind, pr_prof = k, prof_pr[k]
-    if dist:
-        import torch
-        t = torch.tensor([dev_ms, wall_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dev_ms, wall_s = float(t[0]), float(t[1])
-        e = torch.tensor([edges, launches], dtype=torch.float64, device="cuda")
-        dist.all_reduce(e, op=dist.ReduceOp.SUM)
-        edges_all, launches_all = float(e[0]), int(e[1])
-    else:
-        edges_all, launches_all = float(edges), launches
+    dev_ms, wall_s, edges_all, launches_all = aggregate_ranks(dist, dev_ms, wall_s, edges, launches)
     value = edges_all / (dev_ms / 1e3) / 1e9
     e2e = edges_all / wall_s / 1e9
     peak, peak_kind = peak_hbm()
