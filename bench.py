@@ -254,7 +254,8 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
     pull_ms = pr_prof["ms"] / max(pr_prof["launches"], 1)
     algo_bytes = 8 * m + 16 * n
     coo_names = {0: "k_pull (CTA ring)", 1: "k_pull_coo_w", 2: "k_pull_coo_w (2-stage ring)",
-                 3: "k_pull_coo_w (3-stage ring)", 4: "k_pull_coo_w (lane-contiguous)", 5: "k_pull_coo_w (prefetch)"}
+                 3: "k_pull_coo_w (3-stage ring)", 4: "k_pull_coo_w (lane-contiguous)", 5: "k_pull_coo_w (prefetch)",
+                 6: "k_pull_coo_w (merged runs)"}
     kernel_name = coo_names.get(g.get_tuning(gg.TUNE_COO_KERNEL), "k_pull_coo_w") if pr_kind == "coo_pull" \
         else "k_pull_seg"
     # per-application dense-pull rooflines, algorithmic bytes: PageRank 8m+16n, SpMV 12m+12n
