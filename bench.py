@@ -256,8 +256,8 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
     coo_names = {0: "k_pull (CTA ring)", 1: "k_pull_coo_w", 2: "k_pull_coo_w (2-stage ring)",
                  3: "k_pull_coo_w (3-stage ring)", 4: "k_pull_coo_w (lane-contiguous)", 5: "k_pull_coo_w (prefetch)",
                  6: "k_pull_coo_w (merged runs)"}
-    kernel_name = coo_names.get(g.get_tuning(gg.TUNE_COO_KERNEL), "k_pull_coo_w") if pr_kind == "coo_pull" \
-        else "k_pull_seg"
+    pr_coo_kernel = knobs["pagerank"]["coo_kernel"] if "pagerank" in knobs else g.get_tuning(gg.TUNE_COO_KERNEL)
+    kernel_name = coo_names.get(pr_coo_kernel, "k_pull_coo_w") if pr_kind == "coo_pull" else "k_pull_seg"
     # per-application dense-pull rooflines, algorithmic bytes: PageRank 8m+16n, SpMV 12m+12n
     roofline_by_app = {}
     for app, pf, bytes_ in (("pagerank", prof_pr, 8 * m + 16 * n), ("spmv", prof_sp, 12 * m + 12 * n)):
@@ -270,7 +270,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
                                     "frac": round(ach / peak, 4)}
     traffic, traffic_src = args.traffic, "--traffic" if args.traffic else None
     if traffic is None and args.scale == 24 and args.partitions == 384 and args.dense_policy == 0 and \
-            args.tile_edges == TRAFFIC_TILE_EDGES and kernel_name == "k_pull_coo_w" and \
+            args.tile_edges == TRAFFIC_TILE_EDGES and pr_kind == "coo_pull" and pr_coo_kernel == 6 and \
             args.vertex_order in TRAFFIC_RMAT24_PR_PULL:
         traffic = TRAFFIC_RMAT24_PR_PULL[args.vertex_order]
         traffic_src = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/dram_k_pull_coo_w_pagerank_rmat24.md"
