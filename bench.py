@@ -268,6 +268,16 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
             roofline_by_app[app] = {"kernel": kind, "launch_ms": round(lm, 4), "algorithmic_bytes": bytes_,
                                     "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
                                     "frac": round(ach / peak, 4)}
+    # BFS as a whole (device loop, pulls, result copy): 4 B per traversed edge
+    # plus 12 B per reached vertex (parent and level written, offset read)
+    reached = int(np.count_nonzero(par.array >= 0))
+    bfs_ms = per_app["bfs"][1] / args.steps
+    if bfs_ms > 0:
+        bfs_bytes = 4 * (per_app["bfs"][0] // args.steps) + 12 * reached
+        ach = bfs_bytes / (bfs_ms / 1e3) / 1e9
+        roofline_by_app["bfs"] = {"kernel": "whole application", "ms": round(bfs_ms, 4), "reached": reached,
+                                  "algorithmic_bytes": int(bfs_bytes), "achieved": round(ach, 1), "peak": peak,
+                                  "unit": "GB/s", "frac": round(ach / peak, 4)}
     traffic, traffic_src = args.traffic, "--traffic" if args.traffic else None
     if traffic is None and args.scale == 24 and args.partitions == 384 and args.dense_policy == 0 and \
             args.tile_edges == TRAFFIC_TILE_EDGES and pr_kind == "coo_pull" and pr_coo_kernel == 6 and \
