@@ -392,41 +392,354 @@ static int run_cc(gg_graph_s* g, int32_t* ids_out, gg_run_stats* st) {
   return GG_OK;
 }
 
+// ---------------------------------------------- PageRank as a CUDA graph
+// The iteration loop of app/PageRank.C:353-376 captured once per graph handle
+// and knob setting, then replayed per call.  The top graph holds the
+// initialisation and the first iteration, then a while node whose body runs
+// the next iteration with the rank buffers one way round and, under an if
+// node, the one after with them the other way round, so that the swap needs
+// no host work.  After every iteration a one-thread check kernel decides on
+// the device what the host loop decides after its read-back: stop when
+// L1 < eps (:371) or after max_iter iterations, and hand the loop back to
+// the host when the next edgeMap would not take the dense COO pull that the
+// graph holds (ligra-numa.h:953-960 evaluated on the output's count and
+// out-degree sum).  One read-back per call replaces two per iteration.
+struct PrLoopCtl {
+  unsigned long long trav;       // out-degree sums of the input frontiers so far
+  unsigned long long dm;         // last output frontier: active vertices
+  unsigned long long out_edges;  //   and their out-degree sum
+  unsigned long long in_dm;      // input frontier of the last iteration
+  unsigned long long in_edges;
+  unsigned long long err;        // device error word seen by a check
+  double l1;                     // L1 of the last iteration
+  double eps;
+  long long threshold;           // edgeMap's threshold (m / div)
+  long long dense_threshold;     // m / 2
+  uint32_t count;                // iterations done
+  uint32_t max_iter;
+  uint32_t reason;               // 0 running, 1 converged, 2 max_iter, 3 handed back, 4 device error
+  uint32_t coo_always;           // the dense policy pins the COO pull (else the m/2 rule)
+};
+
+struct PrLoop {
+  float* buf[3] = {nullptr, nullptr, nullptr};  // ranks (two) and the contributions, n + 4 each
+  uint32_t* bits[2] = {nullptr, nullptr};       // output bitmaps of odd / even iterations
+  PrLoopCtl* d_ctl = nullptr;
+  PrLoopCtl* h_ctl = nullptr;  // pinned
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int key[3] = {-1, -1, -1};   // bit_all, COO kernel, transposed of the captured graph
+  uint64_t bytes = 0;
+};
+
+void pr_loop_free(gg_graph_s* g) {
+  PrLoop* L = g->pr_loop;
+  if (!L) return;
+  if (L->exec) cudaGraphExecDestroy(L->exec);
+  if (L->graph) cudaGraphDestroy(L->graph);
+  for (float* b : L->buf) cudaFree(b);
+  for (uint32_t* b : L->bits) cudaFree(b);
+  cudaFree(L->d_ctl);
+  if (L->h_ctl) cudaFreeHost(L->h_ctl);
+  g->device_bytes -= L->bytes;
+  delete L;
+  g->pr_loop = nullptr;
+}
+
+__global__ void k_pr_loop_check(PrLoopCtl* c, unsigned long long* stats, double* red, cudaGraphConditionalHandle h_loop,
+                                cudaGraphConditionalHandle h_odd, int set_odd) {
+  const double l1 = red[0];
+  const unsigned long long dm = stats[0], oe = stats[1], err = stats[3];
+  red[0] = 0;  // the next epilogue's L1 and the next pull's counters start from zero
+  for (int i = 0; i < 8; ++i) stats[i] = 0;
+  const uint32_t count = c->count + 1;
+  c->count = count;
+  c->l1 = l1;
+  c->dm = dm;
+  c->out_edges = oe;
+  uint32_t reason = 0;
+  if (err) {
+    c->err = err;
+    reason = 4;
+  } else if (l1 < c->eps) {
+    reason = 1;
+  } else if (count >= c->max_iter) {
+    reason = 2;
+  } else {
+    const long long fm = (long long)dm, tot = (long long)oe;
+    const bool pull = tot > 0 && fm + tot > c->threshold && (c->coo_always || fm + tot > c->dense_threshold);
+    if (pull) {
+      c->trav += oe;
+      c->in_dm = dm;
+      c->in_edges = oe;
+    } else {
+      reason = 3;
+    }
+  }
+  c->reason = reason;
+  cudaGraphSetConditional(h_loop, reason == 0 ? 1u : 0u);
+  if (set_odd) cudaGraphSetConditional(h_odd, reason == 0 ? 1u : 0u);
+}
+
+// One PageRank iteration's launches (the COO pull, as edgeMap picks it for a
+// dense frontier, and the epilogue) into buffers of the loop.
+static int pr_iteration(gg_graph_s* g, PrLoop* L, bool first, bool bit_all, float* p_curr, float* p_next,
+                        uint32_t* in_bits, uint32_t* out_bits) {
+  const uint32_t n = g->n;
+  GG_TRY(fill<uint32_t>(g, out_bits, (uint64_t)g->words() + 4, 0u));
+  gg_frontier_s in{}, out{};
+  in.g = out.g = g;
+  in.n = out.n = n;
+  in.bit = first || bit_all;  // the first input is all vertices; PageRankBit keeps output.bit set
+  in.has_dense = !in.bit;
+  in.d_bits = in_bits;
+  out.d_bits = out_bits;
+  const bool masked = !bit_all;  // the dense output marks the next contributions
+  PrPosF f;
+  f.contrib = L->buf[2];
+  f.acc_out = p_next;
+  f.frontier_in_values = !first && masked;
+  GG_TRY((pull_launch<PrPosF, false>(g, &in, &out, f, true, false)));
+  const float added = (float)((1 - 0.85) * (1 / (double)n));
+  k_pr_epilogue<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(
+      n, in.bit ? 1 : 0, in_bits, p_curr, p_next, g->out_off(), 0.85f, added, L->buf[2], g->ws.d_red,
+      masked ? out_bits : nullptr);
+  GG_CUDA(cudaGetLastError());
+  return GG_OK;
+}
+
+// Captures the launches of fn into graph (after nothing) and returns the last
+// captured node.
+template <class Fn>
+static int capture_into(gg_graph_s* g, cudaGraph_t graph, Fn fn, cudaGraphNode_t* last) {
+  cudaStream_t s = g->stream;
+  GG_CUDA(cudaStreamBeginCaptureToGraph(s, graph, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+  int rc = fn();
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  if (!rc) {
+    if (cudaStreamGetCaptureInfo(s, &cs, nullptr, nullptr, &deps, &nd) != cudaSuccess || nd != 1)
+      rc = fail(GG_ERR_CUDA, "PageRank graph: capture did not end in one node");
+    else
+      *last = deps[0];
+  }
+  cudaGraph_t out = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(s, &out);
+  if (!rc && e != cudaSuccess) rc = fail(GG_ERR_CUDA, "PageRank graph: capture failed (%s)", cudaGetErrorString(e));
+  return rc;
+}
+
+static int add_conditional(cudaGraph_t graph, cudaGraphNode_t dep, cudaGraphConditionalHandle h,
+                           cudaGraphConditionalNodeType type, cudaGraph_t* body) {
+  cudaGraphNodeParams np{};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = h;
+  np.conditional.type = type;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  GG_CUDA(cudaGraphAddNode(&node, graph, &dep, 1, &np));
+  *body = np.conditional.phGraph_out[0];
+  return GG_OK;
+}
+
+static int pr_loop_capture(gg_graph_s* g, PrLoop* L, bool bit_all) {
+  const uint32_t n = g->n;
+  cudaGraph_t graph = nullptr;
+  GG_CUDA(cudaGraphCreate(&graph, 0));
+  float *A = L->buf[0], *B = L->buf[1], *C = L->buf[2];
+  uint32_t *X = L->bits[0], *Y = L->bits[1];
+  cudaGraphConditionalHandle h_loop = 0, h_odd = 0;
+  cudaGraph_t body = nullptr, odd = nullptr;
+  cudaGraphNode_t last = nullptr;
+  auto check = [&](int set_odd) -> int {
+    k_pr_loop_check<<<1, 1, 0, g->stream>>>(L->d_ctl, g->ws.d_stats, g->ws.d_red, h_loop, h_odd, set_odd);
+    GG_CUDA(cudaGetLastError());
+    return GG_OK;
+  };
+  int rc = cudaGraphConditionalHandleCreate(&h_loop, graph, 0, cudaGraphCondAssignDefault) == cudaSuccess
+               ? GG_OK
+               : fail(GG_ERR_CUDA, "PageRank graph: no conditional handle");
+  // initialisation and iteration 1 (ranks into B, output bits into X)
+  if (!rc)
+    rc = capture_into(g, graph, [&]() -> int {
+      GG_CUDA(cudaMemsetAsync(g->ws.d_stats, 0, sizeof(unsigned long long) * 8, g->stream));
+      GG_CUDA(cudaMemsetAsync(g->ws.d_red, 0, sizeof(double), g->stream));
+      GG_TRY(fill<float>(g, A, n, (float)(1 / (double)n)));
+      GG_TRY(fill<float>(g, B, n, 0.0f));
+      k_div_outdeg<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(n, A, g->out_off(), C);
+      GG_CUDA(cudaGetLastError());
+      GG_TRY(pr_iteration(g, L, true, bit_all, A, B, Y, X));
+      return check(0);
+    }, &last);
+  if (!rc) rc = add_conditional(graph, last, h_loop, cudaGraphCondTypeWhile, &body);
+  if (!rc && cudaGraphConditionalHandleCreate(&h_odd, body, 0, cudaGraphCondAssignDefault) != cudaSuccess)
+    rc = fail(GG_ERR_CUDA, "PageRank graph: no conditional handle");
+  // even iterations: ranks into A, output bits into Y
+  if (!rc)
+    rc = capture_into(g, body, [&]() -> int {
+      GG_TRY(pr_iteration(g, L, false, bit_all, B, A, X, Y));
+      return check(1);
+    }, &last);
+  if (!rc) rc = add_conditional(body, last, h_odd, cudaGraphCondTypeIf, &odd);
+  // odd iterations: ranks into B, output bits into X
+  if (!rc)
+    rc = capture_into(g, odd, [&]() -> int {
+      GG_TRY(pr_iteration(g, L, false, bit_all, A, B, Y, X));
+      return check(0);
+    }, &last);
+  cudaGraphExec_t exec = nullptr;
+  if (!rc && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess)
+    rc = fail(GG_ERR_CUDA, "PageRank graph: instantiation refused");
+  if (rc) {
+    cudaGetLastError();
+    cudaGraphDestroy(graph);
+    return rc;
+  }
+  if (L->exec) cudaGraphExecDestroy(L->exec);
+  if (L->graph) cudaGraphDestroy(L->graph);
+  L->graph = graph;
+  L->exec = exec;
+  return GG_OK;
+}
+
+// The loop of this graph handle for bit_all, captured (again) when a knob it
+// depends on changed since.
+static int pr_loop_get(gg_graph_s* g, bool bit_all, PrLoop** out) {
+  if (!g->pr_loop) {
+    PrLoop* L = new (std::nothrow) PrLoop;
+    if (!L) return fail(GG_ERR_OOM, "PageRank graph: out of host memory");
+    g->pr_loop = L;
+    const uint64_t fb = 4ull * ((uint64_t)g->n + 4), bb = 4ull * ((uint64_t)g->words() + 4);
+    int rc = GG_OK;
+    for (float*& b : L->buf)
+      if (!rc && cudaMalloc((void**)&b, fb) != cudaSuccess) rc = fail(GG_ERR_OOM, "PageRank graph: buffers");
+    for (uint32_t*& b : L->bits)
+      if (!rc && cudaMalloc((void**)&b, bb) != cudaSuccess) rc = fail(GG_ERR_OOM, "PageRank graph: bitmaps");
+    if (!rc && cudaMalloc((void**)&L->d_ctl, sizeof(PrLoopCtl)) != cudaSuccess)
+      rc = fail(GG_ERR_OOM, "PageRank graph: control block");
+    if (!rc && cudaMallocHost((void**)&L->h_ctl, sizeof(PrLoopCtl)) != cudaSuccess)
+      rc = fail(GG_ERR_OOM, "PageRank graph: pinned control block");
+    if (rc) {
+      cudaGetLastError();
+      pr_loop_free(g);
+      return rc;
+    }
+    L->bytes = 3 * fb + 2 * bb + sizeof(PrLoopCtl);
+    g->device_bytes += L->bytes;
+  }
+  PrLoop* L = g->pr_loop;
+  const int key[3] = {bit_all ? 1 : 0, g->coo_kernel, g->transposed ? 1 : 0};
+  if (!L->exec || !std::equal(key, key + 3, L->key)) {
+    L->key[0] = -1;
+    GG_TRY(pr_loop_capture(g, L, bit_all));
+    std::copy(key, key + 3, L->key);
+  }
+  *out = L;
+  return GG_OK;
+}
+
 // app/PageRank.C:330-378 (bit_all: app/PageRankBit.C:145)
-static int run_pagerank(gg_graph_s* g, int max_iter, int bit_all, float* ranks, gg_run_stats* st,
-                        const float* x_dev_init = nullptr) {
+static int run_pagerank(gg_graph_s* g, int max_iter, int bit_all, float* ranks, gg_run_stats* st) {
   const uint32_t n = g->n;
   g->kernels = 0;
-  DevBuf<float> a, b, contrib;
-  GG_TRY(a.alloc(g, n));
-  GG_TRY(b.alloc(g, n));
-  GG_TRY(contrib.alloc(g, n));
   const float damping = 0.85f;
   const float added = (float)((1 - 0.85) * (1 / (double)n));
   const double eps = 0.0000001;
+  const int64_t m = (int64_t)g->m, threshold = app_threshold(g);
+  // the graph holds the COO pull: only where edgeMap picks it for all vertices
+  const bool ref_rule = g->dense_policy == 0 || g->transposed;
+  const bool coo_first = m > 0 && (int64_t)n + m > threshold && g->has_coo &&
+                         (ref_rule ? (int64_t)n + m > m / 2 : g->dense_policy == 2);
+  PrLoop* L = nullptr;
+  if (g->pr_graph && !g->profiling && coo_first && pr_loop_get(g, bit_all != 0, &L) != GG_OK) {
+    g->pr_graph = 0;  // refused by the driver: the host loop from now on
+    L = nullptr;
+  }
+  g->kernels = 0;  // launches captured above are not this call's
+  DevBuf<float> a, b, contrib;
+  float *A, *B, *C;
+  if (L) {
+    A = L->buf[0];
+    B = L->buf[1];
+    C = L->buf[2];
+  } else {
+    GG_TRY(a.alloc(g, n));
+    GG_TRY(b.alloc(g, n));
+    GG_TRY(contrib.alloc(g, n));
+    A = a.p;
+    B = b.p;
+    C = contrib.p;
+  }
   EventTimer tm(g->stream);
-  float* p_curr = a.p;
-  float* p_next = b.p;
-  if (x_dev_init) GG_CUDA(cudaMemcpyAsync(p_curr, x_dev_init, 4ull * n, cudaMemcpyDeviceToDevice, g->stream));
-  else GG_TRY(fill<float>(g, p_curr, n, (float)(1 / (double)n)));
-  GG_TRY(fill<float>(g, p_next, n, 0.0f));
-  k_div_outdeg<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(n, p_curr, g->out_off(), contrib.p);
-  g->kernels++;
-  FrontierHold F;
-  GG_TRY(gg_frontier_all(g, &F.f));
+  float* p_curr = A;
+  float* p_next = B;
+  float* last = p_next;
   int count = 0;
   uint64_t trav = 0;
-  float* last = p_next;
   bool masked = false;  // contrib marks the frontier (sources outside hold -1)
-  while (count < max_iter) {
+  bool done = false;
+  FrontierHold F;
+  if (L) {
+    PrLoopCtl& c = *L->h_ctl;
+    c = PrLoopCtl{};
+    c.trav = g->m;  // the first input: all vertices (bits(part, n, m))
+    c.in_dm = n;
+    c.in_edges = g->m;
+    c.eps = eps;
+    c.threshold = threshold;
+    c.dense_threshold = m / 2;
+    c.max_iter = (uint32_t)max_iter;
+    c.coo_always = ref_rule ? 0u : 1u;
+    GG_CUDA(cudaMemcpyAsync(L->d_ctl, L->h_ctl, sizeof(PrLoopCtl), cudaMemcpyHostToDevice, g->stream));
+    GG_CUDA(cudaGraphLaunch(L->exec, g->stream));
+    GG_CUDA(cudaMemcpyAsync(L->h_ctl, L->d_ctl, sizeof(PrLoopCtl), cudaMemcpyDeviceToHost, g->stream));
+    GG_CUDA(cudaStreamSynchronize(g->stream));
+    if (c.reason == 4) return fail(GG_ERR_TIMEOUT, "device wait budget exhausted (error word %llu)", c.err);
+    if (c.reason < 1 || c.reason > 3 || c.count < 1) return fail(GG_ERR_CUDA, "PageRank graph: bad loop state");
+    count = (int)c.count;
+    trav = c.trav;
+    g->kernels = 7 + 4 * (count - 1);  // 3 initial fills, then bitmap fill, pull, epilogue and check per iteration
+    g->last = gg_edge_map_stats{};
+    g->last.kind = 3;
+    g->last.frontier_active = c.in_dm;
+    g->last.frontier_out_edges = c.in_edges;
+    g->last.output_active = c.dm;
+    g->last.output_out_edges = c.out_edges;
+    last = (count & 1) ? B : A;
+    if (c.reason == 3) {  // the next edgeMap leaves the COO pull: continue on the host
+      p_curr = last;
+      p_next = last == A ? B : A;
+      gg_frontier_s* o = nullptr;
+      GG_TRY(frontier_new(g, &o));
+      F.reset(o);
+      GG_TRY(frontier_ensure_bits(o, false));
+      GG_CUDA(cudaMemcpyAsync(o->d_bits, L->bits[(count & 1) ? 0 : 1], 4ull * (g->words() + 4),
+                              cudaMemcpyDeviceToDevice, g->stream));
+      o->has_dense = true;
+      o->dm = c.dm;
+      o->out_edges = c.out_edges;
+      if (bit_all) o->bit = true;
+      masked = !bit_all;
+    } else {
+      done = true;
+    }
+  } else {
+    GG_TRY(fill<float>(g, p_curr, n, (float)(1 / (double)n)));
+    GG_TRY(fill<float>(g, p_next, n, 0.0f));
+    k_div_outdeg<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(n, p_curr, g->out_off(), C);
+    g->kernels++;
+    GG_TRY(gg_frontier_all(g, &F.f));
+  }
+  while (!done && count < max_iter) {
     ++count;
     PrPosF f;  // frontier sources have p > 0
-    f.contrib = contrib.p;
+    f.contrib = C;
     f.acc_out = p_next;
     f.frontier_in_values = masked;
     trav += F.f->out_edges;
     gg_frontier_s* out = nullptr;
-    GG_TRY(edge_map(g, F.f, f, app_threshold(g), 0, &out));
+    GG_TRY(edge_map(g, F.f, f, threshold, 0, &out));
     FrontierHold O;
     O.f = out;
     if (!F.f->bit && !F.f->has_dense) GG_TRY(frontier_to_dense(F.f));
@@ -434,7 +747,7 @@ static int run_pagerank(gg_graph_s* g, int max_iter, int bit_all, float* ranks, 
     masked = !bit_all && out->n == n && out->has_dense;
     GG_CUDA(cudaMemsetAsync(g->ws.d_red, 0, sizeof(double), g->stream));
     k_pr_epilogue<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(
-        n, F.f->bit ? 1 : 0, F.f->d_bits, p_curr, p_next, g->out_off(), damping, added, contrib.p, g->ws.d_red,
+        n, F.f->bit ? 1 : 0, F.f->d_bits, p_curr, p_next, g->out_off(), damping, added, C, g->ws.d_red,
         masked ? out->d_bits : nullptr);
     GG_CUDA(cudaGetLastError());
     g->kernels++;

@@ -107,6 +107,8 @@ struct Workspace {
   uint32_t* d_order[2] = {nullptr, nullptr};  // renumbered graphs: n-entry arrays for the given-order copies
 };
 
+struct PrLoop;  // PageRank iterations captured as a CUDA graph (buffers, graph, control block)
+
 }  // namespace gg
 
 struct gg_graph_s {
@@ -143,6 +145,8 @@ struct gg_graph_s {
   int sparse_div = 20;  // the apps' edgeMap threshold is m / sparse_div (app/*.C pass m/20)
   int device_loop = 1;  // BFS runs consecutive sparse levels in one cooperative launch
   int cc_algo = 0;      // Components on symmetric graphs: 0 label propagation, 1 union-find
+  int pr_graph = 1;     // PageRank iterations replayed as one CUDA graph (0: one host round trip per iteration)
+  gg::PrLoop* pr_loop = nullptr;  // created by the first graph-driven PageRank call
   int coo_kernel = 6;  // 0 CTA ring (k_pull), 1 per-warp direct loads, 2/3 per-warp bulk-copy rings, 6 direct loads
                        // with cross-lane run merging (fastest measured)
   // gg_build_opts.vertex_order: device ids differ from the given ids
@@ -485,9 +489,10 @@ __host__ __device__ constexpr size_t coo_w_smem_bytes(bool hw, int stages, int v
 // shuffles before the shared-memory accumulation, so a destination appears in
 // at most one accumulation per block (instead of one per lane it spans, all
 // on one address).
-template <class F, bool HW, bool ALL, int STAGES, bool CONTIG = false, bool PF = false, bool NOOUT = false,
-          bool MERGE = false>
-__global__ void __launch_bounds__(kCooThreads, GG_COO_MIN_BLOCKS) k_pull_coo_w(const PullParams p, const F f) {
+// The pull as a device function, so that a persistent loop kernel can run it
+// once per iteration (k_pull_coo_w is one call of it).
+template <class F, bool HW, bool ALL, int STAGES, bool CONTIG, bool PF, bool NOOUT, bool MERGE>
+__device__ __forceinline__ void pull_coo_w_run(const PullParams& p, const F& f) {
   static_assert(!NOOUT || F::kIdentityCommitNoop, "discarding the output needs a no-op identity commit");
   static_assert(!CONTIG || STAGES == 0, "lane-contiguous edges use direct loads");
   static_assert(!PF || (STAGES == 0 && !CONTIG), "register prefetch applies to direct loads");
@@ -796,6 +801,12 @@ __global__ void __launch_bounds__(kCooThreads, GG_COO_MIN_BLOCKS) k_pull_coo_w(c
     if (a) atomicAdd(p.stats + 0, a);
     if (b2) atomicAdd(p.stats + 1, b2);
   }
+}
+
+template <class F, bool HW, bool ALL, int STAGES, bool CONTIG = false, bool PF = false, bool NOOUT = false,
+          bool MERGE = false>
+__global__ void __launch_bounds__(kCooThreads, GG_COO_MIN_BLOCKS) k_pull_coo_w(const PullParams p, const F f) {
+  pull_coo_w_run<F, HW, ALL, STAGES, CONTIG, PF, NOOUT, MERGE>(p, f);
 }
 
 // ------------------------------------------ source-partitioned COO (-P source)

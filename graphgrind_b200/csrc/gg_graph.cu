@@ -529,6 +529,7 @@ static void graph_release(gg_graph_s* g) {
   const std::vector<gg_frontier_s*> fl(g->frontiers.begin(), g->frontiers.end());
   for (gg_frontier_s* f : fl) frontier_free(f);
   if (g->stream) cudaStreamSynchronize(g->stream);
+  pr_loop_free(g);
   for (void* a : g->arrays) cudaFree(a);
   g->arrays.clear();
   cudaFree(g->d_csr_off);
@@ -837,6 +838,10 @@ int gg_graph_set_tuning(gg_graph_t g, int32_t key, int64_t value) {
       if (value != 0 && value != 1) return fail(GG_ERR_INVALID_ARG, "components algorithm must be 0 or 1");
       g->cc_algo = (int)value;
       return GG_OK;
+    case GG_TUNE_PR_GRAPH:
+      if (value != 0 && value != 1) return fail(GG_ERR_INVALID_ARG, "PageRank graph switch must be 0 or 1");
+      g->pr_graph = (int)value;
+      return GG_OK;
     default:
       return fail(GG_ERR_INVALID_ARG, "unknown tuning key %d", key);
   }
@@ -859,6 +864,9 @@ int gg_graph_get_tuning(gg_graph_t g, int32_t key, int64_t* value) {
       return GG_OK;
     case GG_TUNE_CC_ALGO:
       *value = g->cc_algo;
+      return GG_OK;
+    case GG_TUNE_PR_GRAPH:
+      *value = g->pr_graph;
       return GG_OK;
     default:
       return fail(GG_ERR_INVALID_ARG, "unknown tuning key %d", key);

@@ -309,12 +309,23 @@ int gg_graph_set_dense_policy(gg_graph_t g, int32_t policy);
  *                         hooked under the smaller one), which ends with the
  *                         same labels (the smallest id of each component) and
  *                         reports 1 round; directed graphs keep label
- *                         propagation, whose labels are not components */
+ *                         propagation, whose labels are not components
+ *   GG_TUNE_PR_GRAPH      1 (default): gg_pagerank runs its iterations as one
+ *                         CUDA graph (a while node; L1, the iteration count and
+ *                         the direction rule are checked on the device) while
+ *                         each edgeMap takes the dense COO pull, and hands the
+ *                         loop back to the host otherwise; the graph and its
+ *                         rank buffers (12 bytes per vertex) stay with the
+ *                         graph handle.  Falls back to 0 by itself when the
+ *                         driver refuses the capture; profiling (see
+ *                         gg_graph_set_profiling) also takes the host loop.
+ *                         0: one host round trip per iteration */
 #define GG_TUNE_DENSE_POLICY 1
 #define GG_TUNE_COO_KERNEL 2
 #define GG_TUNE_SPARSE_DIV 3
 #define GG_TUNE_DEVICE_LOOP 4
 #define GG_TUNE_CC_ALGO 5
+#define GG_TUNE_PR_GRAPH 6
 int gg_graph_set_tuning(gg_graph_t g, int32_t key, int64_t value);
 int gg_graph_get_tuning(gg_graph_t g, int32_t key, int64_t* value);
 
