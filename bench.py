@@ -172,6 +172,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
     t0 = time.time()
     g = gg.Graph(hg, partitions=args.partitions, tile_edges=args.tile_edges, vertex_order=args.vertex_order)
     g.set_dense_policy(args.dense_policy)
+    g.set_tuning(gg.TUNE_PR_GRAPH, 1 if args.pr_loop == "graph" else 0)
     info = g.info()
     log(f"[rank {rank}] device graph built in {time.time() - t0:.1f}s: {info.device_bytes / 2**30:.2f} GiB, "
         f"{info.num_coo_tiles} COO tiles, {info.num_csc_tiles} CSC tiles")
@@ -298,6 +299,8 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
                    "partitions": args.partitions,
                    "dense_policy": ["reference rule", "csc pull", "coo pull"][args.dense_policy],
                    "tile_edges": args.tile_edges,
+                   "pagerank_loop": {"graph": "iterations replayed as one CUDA graph",
+                                     "host": "one host round trip per iteration"}[args.pr_loop],
                    "vertex_order": ["given ids", "hottest sources first inside each partition (results in the "
                                     "given ids)"][args.vertex_order],
                    "autotuned_knobs": knobs or None, "autotune_seconds": round(tune_s, 2),
@@ -596,6 +599,8 @@ def main():
                     help="device numbering: 0 the given ids, 1 hottest sources first inside each partition")
     ap.add_argument("--tile-edges", type=int, default=1 << 18,
                     help="target edges per CTA tile (gg_autotune_build's choice for this workload)")
+    ap.add_argument("--pr-loop", choices=["graph", "host"], default="graph",
+                    help="PageRank iterations as one CUDA graph (GG_TUNE_PR_GRAPH 1) or host-driven")
     ap.add_argument("--traffic", type=float, default=None,
                     help="DRAM bytes per dense-pull launch from an ncu capture (reported as roofline.traffic)")
     args = ap.parse_args()
