@@ -70,9 +70,10 @@ def workload(scale: int, partitions: int, start: int) -> str:
 
 
 HBM_FALLBACK_GBS = 6650.0
-# DRAM bytes per PageRank-pull launch of the default workload, from one ncu
-# capture (profiles/dram_k_pull_coo_w_pagerank_rmat24.md)
-TRAFFIC_RMAT24_PR_PULL = {1: 1897370112}  # by vertex order (merged-run COO kernel)
+# DRAM bytes per PageRank-pull launch of the default workload (the merged-run
+# COO kernel with the vertex step at its commits), from one ncu capture
+# (profiles/dram_k_pull_coo_w_pagerank_rmat24.md)
+TRAFFIC_RMAT24_PR_PULL = {1: 2110578176}  # by vertex order
 TRAFFIC_TILE_EDGES = 1 << 18
 
 
@@ -257,15 +258,23 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
     e2e = edges_all / wall_s / 1e9
     peak, peak_kind = peak_hbm()
     pull_ms = pr_prof["ms"] / max(pr_prof["launches"], 1)
-    algo_bytes = 8 * m + 16 * n
+    # the per-warp COO kernels run PageRank's vertex step at their commits:
+    # 8 B per edge (index, gathered contribution) and 24 B per vertex (offset,
+    # accumulator and previous rank read; rank, reset and next contribution written)
+    pr_coo_kernel = knobs["pagerank"]["coo_kernel"] if "pagerank" in knobs else g.get_tuning(gg.TUNE_COO_KERNEL)
+    pr_fused = pr_kind == "coo_pull" and pr_coo_kernel > 0
+    pr_bytes = 8 * m + (24 if pr_fused else 16) * n
+    algo_bytes = pr_bytes
     coo_names = {0: "k_pull (CTA ring)", 1: "k_pull_coo_w", 2: "k_pull_coo_w (2-stage ring)",
                  3: "k_pull_coo_w (3-stage ring)", 4: "k_pull_coo_w (lane-contiguous)", 5: "k_pull_coo_w (prefetch)",
                  6: "k_pull_coo_w (merged runs)"}
-    pr_coo_kernel = knobs["pagerank"]["coo_kernel"] if "pagerank" in knobs else g.get_tuning(gg.TUNE_COO_KERNEL)
     kernel_name = coo_names.get(pr_coo_kernel, "k_pull_coo_w") if pr_kind == "coo_pull" else "k_pull_seg"
-    # per-application dense-pull rooflines, algorithmic bytes: PageRank 8m+16n, SpMV 12m+12n
+    if pr_fused:
+        kernel_name += " with the vertex step"
+    # per-application dense-pull rooflines, algorithmic bytes: PageRank as
+    # above (8m+16n without the vertex step), SpMV 12m+12n
     roofline_by_app = {}
-    for app, pf, bytes_ in (("pagerank", prof_pr, 8 * m + 16 * n), ("spmv", prof_sp, 12 * m + 12 * n)):
+    for app, pf, bytes_ in (("pagerank", prof_pr, pr_bytes), ("spmv", prof_sp, 12 * m + 12 * n)):
         kind = max(("coo_pull", "csc_pull"), key=lambda k: pf[k]["launches"])
         if pf[kind]["launches"]:
             lm = pf[kind]["ms"] / pf[kind]["launches"]

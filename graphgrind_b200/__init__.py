@@ -81,7 +81,7 @@ class GraphInfo(C.Structure):
     _fields_ = [("n", C.c_uint32), ("m", C.c_uint64), ("symmetric", C.c_int32),
                 ("weight_type", C.c_int32), ("num_partitions", C.c_int32), ("has_coo", C.c_int32),
                 ("transposed", C.c_int32), ("num_csc_tiles", C.c_int32),
-                ("num_coo_tiles", C.c_int32), ("device_bytes", C.c_uint64)]
+                ("num_coo_tiles", C.c_int32), ("device_bytes", C.c_uint64), ("num_coo_gaps", C.c_int32)]
 
 
 class RunStats(C.Structure):

@@ -422,7 +422,7 @@ struct PrLoopCtl {
 };
 
 struct PrLoop {
-  float* buf[3] = {nullptr, nullptr, nullptr};  // ranks (two) and the contributions, n + 4 each
+  float* buf[4] = {nullptr, nullptr, nullptr, nullptr};  // ranks (two) and contributions (two), n + 4 each
   uint32_t* bits[2] = {nullptr, nullptr};       // output bitmaps of odd / even iterations
   PrLoopCtl* d_ctl = nullptr;
   PrLoopCtl* h_ctl = nullptr;  // pinned
@@ -481,10 +481,51 @@ __global__ void k_pr_loop_check(PrLoopCtl* c, unsigned long long* stats, double*
   if (set_odd) cudaGraphSetConditional(h_odd, reason == 0 ? 1u : 0u);
 }
 
+// The per-warp COO pull applies PrFinishF's vertex step at its commits (the
+// CTA-ring and source-partition kernels commit with PrT's sum alone).
+static bool pr_fused(const gg_graph_s* g) { return g->coo_kernel > 0 && !g->coo_by_source; }
+
+static PrFinishF pr_functor(gg_graph_s* g, const float* contrib, float* contrib_next, float* p_curr, float* p_next,
+                            const uint32_t* fbits, bool frontier_in_values, bool masked) {
+  PrFinishF f;
+  f.contrib = contrib;
+  f.acc_out = p_next;
+  f.frontier_in_values = frontier_in_values;
+  f.p_prev = p_curr;
+  f.fbits = fbits;
+  f.contrib_next = contrib_next;
+  f.l1 = g->ws.d_red;
+  f.damping = 0.85f;
+  f.added = (float)((1 - 0.85) * (1 / (double)g->n));
+  f.masked = masked ? 1 : 0;
+  return f;
+}
+
+// The vertex step for the destination ranges no COO tile covers (no in-edges).
+__global__ void k_pr_finish_gaps(const uint2* gaps, uint32_t ngaps, const PrFinishF f, const uint32_t* off) {
+  double acc = 0;
+  for (uint32_t r = blockIdx.x; r < ngaps; r += gridDim.x) {
+    const uint2 gr = gaps[r];
+    for (uint32_t v = gr.x + threadIdx.x; v < gr.x + gr.y; v += blockDim.x)
+      acc += f.finish(v, false, 0.0f, off[v + 1] - off[v]);
+  }
+  block_add_double(acc, f.l1);
+}
+
+static int pr_finish_gaps(gg_graph_s* g, const PrFinishF& f) {
+  if (!g->coo_gap_count) return GG_OK;
+  const int grid = (int)std::min<uint32_t>(g->coo_gap_count, (uint32_t)g->num_sms * 4);
+  k_pr_finish_gaps<<<grid, kGenericThreads, 0, g->stream>>>(g->d_coo_gaps, g->coo_gap_count, f, g->out_off());
+  GG_CUDA(cudaGetLastError());
+  g->kernels++;
+  return GG_OK;
+}
+
 // One PageRank iteration's launches (the COO pull, as edgeMap picks it for a
-// dense frontier, and the epilogue) into buffers of the loop.
-static int pr_iteration(gg_graph_s* g, PrLoop* L, bool first, bool bit_all, float* p_curr, float* p_next,
-                        uint32_t* in_bits, uint32_t* out_bits) {
+// dense frontier, with the vertex step at its commits or as the epilogue)
+// into buffers of the loop.
+static int pr_iteration(gg_graph_s* g, bool first, bool bit_all, float* p_curr, float* p_next, const float* contrib,
+                        float* contrib_next, uint32_t* in_bits, uint32_t* out_bits) {
   const uint32_t n = g->n;
   GG_TRY(fill<uint32_t>(g, out_bits, (uint64_t)g->words() + 4, 0u));
   gg_frontier_s in{}, out{};
@@ -495,14 +536,12 @@ static int pr_iteration(gg_graph_s* g, PrLoop* L, bool first, bool bit_all, floa
   in.d_bits = in_bits;
   out.d_bits = out_bits;
   const bool masked = !bit_all;  // the dense output marks the next contributions
-  PrPosF f;
-  f.contrib = L->buf[2];
-  f.acc_out = p_next;
-  f.frontier_in_values = !first && masked;
-  GG_TRY((pull_launch<PrPosF, false>(g, &in, &out, f, true, false)));
-  const float added = (float)((1 - 0.85) * (1 / (double)n));
+  const PrFinishF f = pr_functor(g, contrib, contrib_next, p_curr, p_next, in.bit ? nullptr : in_bits,
+                                 !first && masked, masked);
+  GG_TRY((pull_launch<PrFinishF, false>(g, &in, &out, f, true, false)));
+  if (pr_fused(g)) return pr_finish_gaps(g, f);
   k_pr_epilogue<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(
-      n, in.bit ? 1 : 0, in_bits, p_curr, p_next, g->out_off(), 0.85f, added, L->buf[2], g->ws.d_red,
+      n, in.bit ? 1 : 0, in_bits, p_curr, p_next, g->out_off(), f.damping, f.added, contrib_next, g->ws.d_red,
       masked ? out_bits : nullptr);
   GG_CUDA(cudaGetLastError());
   return GG_OK;
@@ -547,7 +586,7 @@ static int pr_loop_capture(gg_graph_s* g, PrLoop* L, bool bit_all) {
   const uint32_t n = g->n;
   cudaGraph_t graph = nullptr;
   GG_CUDA(cudaGraphCreate(&graph, 0));
-  float *A = L->buf[0], *B = L->buf[1], *C = L->buf[2];
+  float *A = L->buf[0], *B = L->buf[1], *C0 = L->buf[2], *C1 = L->buf[3];
   uint32_t *X = L->bits[0], *Y = L->bits[1];
   cudaGraphConditionalHandle h_loop = 0, h_odd = 0;
   cudaGraph_t body = nullptr, odd = nullptr;
@@ -567,25 +606,25 @@ static int pr_loop_capture(gg_graph_s* g, PrLoop* L, bool bit_all) {
       GG_CUDA(cudaMemsetAsync(g->ws.d_red, 0, sizeof(double), g->stream));
       GG_TRY(fill<float>(g, A, n, (float)(1 / (double)n)));
       GG_TRY(fill<float>(g, B, n, 0.0f));
-      k_div_outdeg<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(n, A, g->out_off(), C);
+      k_div_outdeg<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(n, A, g->out_off(), C0);
       GG_CUDA(cudaGetLastError());
-      GG_TRY(pr_iteration(g, L, true, bit_all, A, B, Y, X));
+      GG_TRY(pr_iteration(g, true, bit_all, A, B, C0, C1, Y, X));
       return check(0);
     }, &last);
   if (!rc) rc = add_conditional(graph, last, h_loop, cudaGraphCondTypeWhile, &body);
   if (!rc && cudaGraphConditionalHandleCreate(&h_odd, body, 0, cudaGraphCondAssignDefault) != cudaSuccess)
     rc = fail(GG_ERR_CUDA, "PageRank graph: no conditional handle");
-  // even iterations: ranks into A, output bits into Y
+  // even iterations: ranks into A, contributions into C0, output bits into Y
   if (!rc)
     rc = capture_into(g, body, [&]() -> int {
-      GG_TRY(pr_iteration(g, L, false, bit_all, B, A, X, Y));
+      GG_TRY(pr_iteration(g, false, bit_all, B, A, C1, C0, X, Y));
       return check(1);
     }, &last);
   if (!rc) rc = add_conditional(body, last, h_odd, cudaGraphCondTypeIf, &odd);
-  // odd iterations: ranks into B, output bits into X
+  // odd iterations: ranks into B, contributions into C1, output bits into X
   if (!rc)
     rc = capture_into(g, odd, [&]() -> int {
-      GG_TRY(pr_iteration(g, L, false, bit_all, A, B, Y, X));
+      GG_TRY(pr_iteration(g, false, bit_all, A, B, C0, C1, Y, X));
       return check(0);
     }, &last);
   cudaGraphExec_t exec = nullptr;
@@ -625,7 +664,7 @@ static int pr_loop_get(gg_graph_s* g, bool bit_all, PrLoop** out) {
       pr_loop_free(g);
       return rc;
     }
-    L->bytes = 3 * fb + 2 * bb + sizeof(PrLoopCtl);
+    L->bytes = 4 * fb + 2 * bb + sizeof(PrLoopCtl);
     g->device_bytes += L->bytes;
   }
   PrLoop* L = g->pr_loop;
@@ -657,24 +696,30 @@ static int run_pagerank(gg_graph_s* g, int max_iter, int bit_all, float* ranks, 
     L = nullptr;
   }
   g->kernels = 0;  // launches captured above are not this call's
-  DevBuf<float> a, b, contrib;
-  float *A, *B, *C;
+  // contributions are double-buffered: the vertex step at the COO pull's
+  // commits writes the next ones while other tiles still gather these
+  DevBuf<float> a, b, c0, c1;
+  float *A, *B, *Cb[2];
   if (L) {
     A = L->buf[0];
     B = L->buf[1];
-    C = L->buf[2];
+    Cb[0] = L->buf[2];
+    Cb[1] = L->buf[3];
   } else {
     GG_TRY(a.alloc(g, n));
     GG_TRY(b.alloc(g, n));
-    GG_TRY(contrib.alloc(g, n));
+    GG_TRY(c0.alloc(g, n));
+    GG_TRY(c1.alloc(g, n));
     A = a.p;
     B = b.p;
-    C = contrib.p;
+    Cb[0] = c0.p;
+    Cb[1] = c1.p;
   }
   EventTimer tm(g->stream);
   float* p_curr = A;
   float* p_next = B;
   float* last = p_next;
+  int cur = 0;  // the contributions the next pull gathers
   int count = 0;
   uint64_t trav = 0;
   bool masked = false;  // contrib marks the frontier (sources outside hold -1)
@@ -699,7 +744,10 @@ static int run_pagerank(gg_graph_s* g, int max_iter, int bit_all, float* ranks, 
     if (c.reason < 1 || c.reason > 3 || c.count < 1) return fail(GG_ERR_CUDA, "PageRank graph: bad loop state");
     count = (int)c.count;
     trav = c.trav;
-    g->kernels = 7 + 4 * (count - 1);  // 3 initial fills, then bitmap fill, pull, epilogue and check per iteration
+    // 2 fills and the first contributions, then per iteration the bitmap fill,
+    // the pull, the vertex step's pass (uncovered ranges or the epilogue) and the check
+    const int per_iter = 3 + (pr_fused(g) && g->coo_gap_count == 0 ? 0 : 1);
+    g->kernels = 3 + per_iter * count;
     g->last = gg_edge_map_stats{};
     g->last.kind = 3;
     g->last.frontier_active = c.in_dm;
@@ -707,6 +755,7 @@ static int run_pagerank(gg_graph_s* g, int max_iter, int bit_all, float* ranks, 
     g->last.output_active = c.dm;
     g->last.output_out_edges = c.out_edges;
     last = (count & 1) ? B : A;
+    cur = count & 1;
     if (c.reason == 3) {  // the next edgeMap leaves the COO pull: continue on the host
       p_curr = last;
       p_next = last == A ? B : A;
@@ -727,35 +776,41 @@ static int run_pagerank(gg_graph_s* g, int max_iter, int bit_all, float* ranks, 
   } else {
     GG_TRY(fill<float>(g, p_curr, n, (float)(1 / (double)n)));
     GG_TRY(fill<float>(g, p_next, n, 0.0f));
-    k_div_outdeg<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(n, p_curr, g->out_off(), C);
+    k_div_outdeg<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(n, p_curr, g->out_off(), Cb[0]);
     g->kernels++;
     GG_TRY(gg_frontier_all(g, &F.f));
   }
   while (!done && count < max_iter) {
     ++count;
-    PrPosF f;  // frontier sources have p > 0
-    f.contrib = C;
-    f.acc_out = p_next;
-    f.frontier_in_values = masked;
     trav += F.f->out_edges;
+    // the vertex step reads the input frontier's bitmap during the pull
+    if (!F.f->bit && !F.f->has_dense) GG_TRY(frontier_to_dense(F.f));
+    GG_CUDA(cudaMemsetAsync(g->ws.d_red, 0, sizeof(double), g->stream));
+    // frontier sources have p > 0; a COO pull's output is dense, so it marks
+    // the next contributions unless PageRankBit keeps every vertex active
+    const PrFinishF f = pr_functor(g, Cb[cur], Cb[cur ^ 1], p_curr, p_next, F.f->bit ? nullptr : F.f->d_bits,
+                                   masked, !bit_all);
     gg_frontier_s* out = nullptr;
     GG_TRY(edge_map(g, F.f, f, threshold, 0, &out));
     FrontierHold O;
     O.f = out;
-    if (!F.f->bit && !F.f->has_dense) GG_TRY(frontier_to_dense(F.f));
     // the output becomes the next frontier: mark it in the next contributions
     masked = !bit_all && out->n == n && out->has_dense;
-    GG_CUDA(cudaMemsetAsync(g->ws.d_red, 0, sizeof(double), g->stream));
-    k_pr_epilogue<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(
-        n, F.f->bit ? 1 : 0, F.f->d_bits, p_curr, p_next, g->out_off(), damping, added, C, g->ws.d_red,
-        masked ? out->d_bits : nullptr);
-    GG_CUDA(cudaGetLastError());
-    g->kernels++;
+    if (g->last.kind == 3 && pr_fused(g)) {  // the pull's commits ran the vertex step
+      GG_TRY(pr_finish_gaps(g, f));
+    } else {
+      k_pr_epilogue<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(
+          n, F.f->bit ? 1 : 0, F.f->d_bits, p_curr, p_next, g->out_off(), damping, added, Cb[cur ^ 1],
+          g->ws.d_red, masked ? out->d_bits : nullptr);
+      GG_CUDA(cudaGetLastError());
+      g->kernels++;
+    }
     last = p_next;
     double l1;
     GG_TRY(read_red(g, &l1));
     if (l1 < eps) break;
     std::swap(p_curr, p_next);
+    cur ^= 1;
     gg_frontier_s* o = O.release();
     if (bit_all) o->bit = true;  // output.bit = true
     F.reset(o);

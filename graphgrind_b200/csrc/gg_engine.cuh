@@ -129,6 +129,8 @@ struct gg_graph_s {
   gg::SegIndex seg[2];       // row structure of the pulled stream, same indexing
   uint64_t m_pad = 0;        // edge arrays hold m_pad entries (zero padded)
   gg::TileSet coo_tiles;
+  uint2* d_coo_gaps = nullptr;  // {first, count} of the destination ranges outside every COO tile
+  uint32_t coo_gap_count = 0;
   bool has_coo = false;
   bool coo_by_source = false;       // -P source: partitions of sources, destinations in d_coo_dst
   uint32_t* d_coo_dst = nullptr;
@@ -461,6 +463,17 @@ __global__ void __launch_bounds__(kPullThreads, 2) k_pull(const PullParams p, co
 // STAGES > 0 through a private bulk-copy ring in shared memory, STAGES == 0
 // with direct 16-byte loads (no staging; all of L1 left to the source
 // gathers).  No CTA-wide barrier per block.
+// F::kFinish when the functor declares it (a vertex step the per-warp COO
+// pull applies to every destination of a tile at its commit), else false
+template <class F, class = void>
+struct finishes {
+  static constexpr bool value = false;
+};
+template <class F>
+struct finishes<F, decltype((void)F::kFinish)> {
+  static constexpr bool value = F::kFinish;
+};
+
 constexpr int kCooWarps = 8;
 constexpr int kCooThreads = kCooWarps * 32;
 
@@ -494,6 +507,8 @@ __host__ __device__ constexpr size_t coo_w_smem_bytes(bool hw, int stages, int v
 template <class F, bool HW, bool ALL, int STAGES, bool CONTIG, bool PF, bool NOOUT, bool MERGE>
 __device__ __forceinline__ void pull_coo_w_run(const PullParams& p, const F& f) {
   static_assert(!NOOUT || F::kIdentityCommitNoop, "discarding the output needs a no-op identity commit");
+  constexpr bool kFin = finishes<F>::value;  // the vertex step runs at the commit (PrFinishF)
+  static_assert(!kFin || (!NOOUT && F::kPositive && F::kCondTrue), "the vertex step needs the output");
   static_assert(!CONTIG || STAGES == 0, "lane-contiguous edges use direct loads");
   static_assert(!PF || (STAGES == 0 && !CONTIG), "register prefetch applies to direct loads");
   using V = typename F::value_t;
@@ -508,6 +523,7 @@ __device__ __forceinline__ void pull_coo_w_run(const PullParams& p, const F& f) 
   uint8_t* s_cond = s_touch + (kTouch ? tv4 : 0);              // !F::kCondTrue only
   __shared__ uint32_t s_tile;
   __shared__ unsigned long long s_red[2][kCooWarps];
+  __shared__ double s_l1[kFin ? kCooWarps : 1];
   __shared__ int s_fail;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -520,6 +536,7 @@ __device__ __forceinline__ void pull_coo_w_run(const PullParams& p, const F& f) 
   __syncthreads();
   uint32_t parity = 0;
   unsigned long long my_cnt = 0, my_deg = 0;
+  double my_l1 = 0;
 
   for (;;) {
     if (tid == 0) s_tile = (uint32_t)atomicAdd(p.tile_counter, 1ull);
@@ -771,13 +788,24 @@ __device__ __forceinline__ void pull_coo_w_run(const PullParams& p, const F& f) 
     for (uint32_t bb = base0 + (uint32_t)warp * 32u; bb < v0 + nv; bb += kCooThreads) {
       const uint32_t v = bb + (uint32_t)lane;
       bool act = false;
+      uint32_t dg = 0;
       if (v >= v0 && v < v0 + nv) {
         const uint32_t l = v - v0;
         const bool touched = F::kPositive ? (s_acc[l] != F::identity()) : (s_touch[l] != 0);
-        if (touched && (F::kCondTrue || s_cond[l])) act = f.commit(v, s_acc[l]);
+        if constexpr (kFin) {
+          dg = __ldg(p.deg_off + v + 1) - __ldg(p.deg_off + v);
+          my_l1 += f.finish(v, touched, s_acc[l], dg);
+          act = touched;
+        } else if (touched && (F::kCondTrue || s_cond[l])) {
+          act = f.commit(v, s_acc[l]);
+        }
       }
       const uint32_t word = __ballot_sync(0xffffffffu, act);
-      if (act) my_deg += __ldg(p.deg_off + v + 1) - __ldg(p.deg_off + v);
+      if (kFin) {
+        if (act) my_deg += dg;
+      } else if (act) {
+        my_deg += __ldg(p.deg_off + v + 1) - __ldg(p.deg_off + v);
+      }
       if (lane == 0 && word) {
         atomicOr(p.next_bits + (bb >> 5), word);
         my_cnt += __popc(word);
@@ -787,19 +815,26 @@ __device__ __forceinline__ void pull_coo_w_run(const PullParams& p, const F& f) 
   }
   my_deg = warp_sum(my_deg);
   my_cnt = warp_sum(my_cnt);
+  if (kFin) my_l1 = warp_sum(my_l1);
   if (lane == 0) {
     s_red[0][warp] = my_cnt;
     s_red[1][warp] = my_deg;
+    if (kFin) s_l1[warp] = my_l1;
   }
   __syncthreads();
   if (tid == 0) {
     unsigned long long a = 0, b2 = 0;
+    double l1 = 0;
     for (int w = 0; w < kCooWarps; ++w) {
       a += s_red[0][w];
       b2 += s_red[1][w];
+      if (kFin) l1 += s_l1[w];
     }
     if (a) atomicAdd(p.stats + 0, a);
     if (b2) atomicAdd(p.stats + 1, b2);
+    if constexpr (kFin) {
+      if (l1 != 0) atomicAdd(f.l1, l1);
+    }
   }
 }
 

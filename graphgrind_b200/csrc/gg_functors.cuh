@@ -121,6 +121,41 @@ struct PrT : SumF32 {
 using PrF = PrT<false>;
 using PrPosF = PrT<true>;
 
+// PageRank's pull with the vertex step of app/PageRank.C (PR_Vertex_F and
+// PR_Vertex_Reset, :84-100, and the L1 term of :136-139) applied where the
+// per-warp COO pull commits a tile's destinations (each destination belongs
+// to one tile, so its sum is final there): rank = the accumulated sum, for
+// input-frontier members damping * rank + (1 - damping)/n; L1 += |previous -
+// rank|; the previous-rank buffer becomes the next accumulator (0 for members,
+// the difference for the others); the next contribution rank/outdeg, -1 for
+// sources outside the output when the output marks the frontier.  The
+// contributions are double-buffered: the pull reads contrib and writes
+// contrib_next.  Other kernels apply PrT's commit and leave the vertex step
+// to a separate pass.
+struct PrFinishF : PrT<true> {
+  static constexpr bool kFinish = true;
+  static constexpr bool kIdentityCommitNoop = false;  // the vertex step visits every destination
+  float* p_prev;            // ranks of the previous iteration, reset in place
+  const uint32_t* fbits;    // input frontier (null: every vertex)
+  float* contrib_next;
+  double* l1;
+  float damping, added;
+  int masked;               // the output marks the next frontier in contrib_next
+  // vertex v of the tile: s = its accumulated sum (touched: s came from an
+  // edge), d = its out-degree; returns its L1 term
+  __device__ float finish(uint32_t v, bool touched, float s, uint32_t d) const {
+    float pn = acc_out[v];
+    if (touched) pn += s;
+    const bool in = !fbits || ((fbits[v >> 5] >> (v & 31)) & 1u);
+    if (in) pn = damping * pn + added;
+    const float diff = fabsf(p_prev[v] - pn);
+    acc_out[v] = pn;
+    p_prev[v] = in ? 0.0f : diff;
+    contrib_next[v] = d ? ((!masked || touched) ? pn / (float)d : -1.0f) : 0.0f;
+    return diff;
+  }
+};
+
 // SPMV_F, app/SPMV.C:7-47: p_next[d] += p_curr[s] * edgeLen.  Weights are
 // the reference's int edge lengths, or FP32 when the graph carries FP32 weights.
 struct SpmvF : SumF32 {

@@ -411,6 +411,20 @@ static int build_coo(gg_graph_s* g, const uint32_t* h_in_off) {
   for (size_t t = 0; t < segs.size(); ++t)
     tiles[t] = make_uint4(segs[t].x, segs[t].y, pad_start[t], (segs[t].w + 7u) & ~7u);
   GG_TRY(upload_tiles(g, g->coo_tiles, tiles));
+  // destination ranges that no tile covers (no in-edges at all): a vertex
+  // step run at the tiles' commits visits them separately
+  std::vector<uint2> gaps;
+  uint32_t covered = 0;
+  for (const uint4& sg : segs) {
+    if (sg.x > covered) gaps.push_back(make_uint2(covered, sg.x - covered));
+    covered = sg.x + sg.y;
+  }
+  if (covered < n) gaps.push_back(make_uint2(covered, n - covered));
+  g->coo_gap_count = (uint32_t)gaps.size();
+  if (!gaps.empty()) {
+    GG_TRY(dev_alloc(g, &g->d_coo_gaps, gaps.size()));
+    GG_CUDA(cudaMemcpy(g->d_coo_gaps, gaps.data(), sizeof(uint2) * gaps.size(), cudaMemcpyHostToDevice));
+  }
   g->has_coo = true;
   if (g->opts.coo_window > 0) g->coo_kernel = 4;  // the lane-contiguous pull matches source-ordered windows
   return GG_OK;
@@ -547,6 +561,7 @@ static void graph_release(gg_graph_s* g) {
     cudaFree(s.d_rows);
   }
   cudaFree(g->coo_tiles.d_tiles);
+  cudaFree(g->d_coo_gaps);
   cudaFree(g->d_coo_src);
   cudaFree(g->d_coo_dloc);
   cudaFree(g->d_coo_dst);
@@ -785,6 +800,7 @@ int gg_graph_get_info(gg_graph_t g, gg_graph_info* info) {
   info->num_csc_tiles = (int32_t)g->csc_tiles[0].count;
   info->num_coo_tiles = (int32_t)g->coo_tiles.count;
   info->device_bytes = g->device_bytes;
+  info->num_coo_gaps = (int32_t)g->coo_gap_count;
   return GG_OK;
 }
 

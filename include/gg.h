@@ -58,7 +58,8 @@ typedef struct gg_build_opts {
   int32_t part_how;         /* -P   gg_part_how                             */
   int32_t relabel;          /* -o   partition boundaries at degree rises    */
   int32_t order;            /* EDGES_HILBERT: gg_order                      */
-  int32_t tile_vertices;    /* GPU: max destinations per CTA tile (<=8192)  */
+  int32_t tile_vertices;    /* GPU: max destinations per CTA tile (<=4096;
+                               0 or larger values give 4096)             */
   int32_t tile_edges;       /* GPU: target edges per CTA tile               */
   int32_t build_coo;        /* 1 = build the partitioned COO (default when balance==edge) */
   int32_t coo_window;       /* GPU: order inside a COO tile after the Hilbert sort:
@@ -96,6 +97,7 @@ typedef struct gg_graph_info {
   int32_t num_csc_tiles;
   int32_t num_coo_tiles;
   uint64_t device_bytes;    /* HBM held by the graph */
+  int32_t num_coo_gaps;     /* destination ranges with no in-edges, outside every COO tile */
 } gg_graph_info;
 
 /* ==================================================== host-only: graphs */
@@ -315,7 +317,7 @@ int gg_graph_set_dense_policy(gg_graph_t g, int32_t policy);
  *                         the direction rule are checked on the device) while
  *                         each edgeMap takes the dense COO pull, and hands the
  *                         loop back to the host otherwise; the graph and its
- *                         rank buffers (12 bytes per vertex) stay with the
+ *                         rank buffers (16 bytes per vertex) stay with the
  *                         graph handle.  Falls back to 0 by itself when the
  *                         driver refuses the capture; profiling (see
  *                         gg_graph_set_profiling) also takes the host loop.
