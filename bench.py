@@ -322,7 +322,11 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
                      "frac": round(achieved / peak, 4) if achieved else None, "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": algo_bytes, "launch_ms": round(pull_ms, 4),
                      "launches": pr_prof["launches"], "traffic": traffic,
-                     "traffic_source": traffic_src},
+                     "traffic_source": traffic_src,
+                     # the same launch counted at the pull's 8m + 16n (its
+                     # vertex step's 8 B per vertex left out)
+                     "frac_pull_bytes_only": round((8 * m + 16 * n) / (pull_ms / 1e3) / 1e9 / peak, 4)
+                     if pull_ms > 0 else None},
         "roofline_by_app": roofline_by_app,
         "kernel_profile": {k: {"launches": v["launches"], "ms": round(v["ms"], 3)} for k, v in prof.items()},
         "e2e": {"value": round(e2e, 4), "unit": UNIT, "h2d_bytes_per_step": 4 * n + 4,
