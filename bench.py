@@ -201,6 +201,10 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
             g.set_tuning(gg.TUNE_COO_KERNEL, kb["coo_kernel"])
             g.set_tuning(gg.TUNE_SPARSE_DIV, kb["sparse_div"])
 
+    # results leave for the pinned host arrays on the library's copy stream
+    # while the next application runs; the step ends when all have arrived
+    g.set_tuning(gg.TUNE_ASYNC_RESULTS, 1 if args.copies == "overlap" else 0)
+
     def step():
         use("bfs")
         _, _, b = g.bfs(args.start, out=(par.array, None))  # app/BFS.C's result is Parents
@@ -208,6 +212,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
         _, p = g.pagerank(10, out=ranks.array)
         use("spmv")
         _, s = g.spmv(x.array, out=y.array)
+        g.synchronize()
         return b, p, s
 
     for _ in range(args.warmup):
@@ -249,6 +254,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
         g.spmv(x.array, out=y.array)
     prof_sp = g.profile()
     g.set_profiling(False)
+    g.synchronize()
     clk = clocks.stop()
     for k in ("csc_pull", "coo_pull"):
         if prof_pr[k]["launches"] >= pr_prof["launches"]:
@@ -310,6 +316,9 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
                    "tile_edges": args.tile_edges,
                    "pagerank_loop": {"graph": "iterations replayed as one CUDA graph",
                                      "host": "one host round trip per iteration"}[args.pr_loop],
+                   "result_copies": {"overlap": "to pinned host arrays on a copy stream, overlapping the next "
+                                                "application; the step waits for all (gg_graph_synchronize)",
+                                     "wait": "each call returns after its copy"}[args.copies],
                    "vertex_order": ["given ids", "hottest sources first inside each partition (results in the "
                                     "given ids)"][args.vertex_order],
                    "autotuned_knobs": knobs or None, "autotune_seconds": round(tune_s, 2),
@@ -612,6 +621,9 @@ def main():
                     help="device numbering: 0 the given ids, 1 hottest sources first inside each partition")
     ap.add_argument("--tile-edges", type=int, default=1 << 18,
                     help="target edges per CTA tile (gg_autotune_build's choice for this workload)")
+    ap.add_argument("--copies", choices=["overlap", "wait"], default="overlap",
+                    help="result copies to the host overlap the next application (GG_TUNE_ASYNC_RESULTS 1) "
+                         "or finish inside each call")
     ap.add_argument("--pr-loop", choices=["graph", "host"], default="graph",
                     help="PageRank iterations as one CUDA graph (GG_TUNE_PR_GRAPH 1) or host-driven")
     ap.add_argument("--traffic", type=float, default=None,

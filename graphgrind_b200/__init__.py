@@ -147,6 +147,7 @@ _sig("gg_host_graph_read_gpu", C.c_int, C.c_char_p, C.c_int32, C.c_int32, C.c_in
      C.POINTER(HostGraphC))
 _sig("gg_graph_build", C.c_int, C.POINTER(HostGraphC), C.POINTER(BuildOpts), C.POINTER(_P))
 _sig("gg_graph_destroy", C.c_int, _P)
+_sig("gg_graph_synchronize", C.c_int, _P)
 _sig("gg_graph_get_info", C.c_int, _P, C.POINTER(GraphInfo))
 _sig("gg_graph_partition_starts", C.c_int, _P, _i64p)
 _sig("gg_graph_transpose", C.c_int, _P)
@@ -171,6 +172,7 @@ _sig("gg_graph_set_dense_policy", C.c_int, _P, C.c_int32)
 _sig("gg_graph_set_tuning", C.c_int, _P, C.c_int32, C.c_int64)
 _sig("gg_graph_get_tuning", C.c_int, _P, C.c_int32, C.POINTER(C.c_int64))
 TUNE_DENSE_POLICY, TUNE_COO_KERNEL, TUNE_SPARSE_DIV, TUNE_DEVICE_LOOP, TUNE_CC_ALGO, TUNE_PR_GRAPH = 1, 2, 3, 4, 5, 6
+TUNE_ASYNC_RESULTS = 7
 APP_BFS, APP_COMPONENTS, APP_PAGERANK, APP_PAGERANK_DELTA, APP_SPMV, APP_BELLMAN_FORD, APP_BC = range(1, 8)
 _sig("gg_vertex_map", C.c_int, _P, _P, C.c_int32, _P)
 _sig("gg_vertex_filter", C.c_int, _P, _P, C.c_int32, _P, C.POINTER(_P))
@@ -210,7 +212,7 @@ EXPORTED = [
     "gg_last_error_string", "gg_version", "gg_gen_rmat", "gg_gen_grid", "gg_gen_er",
     "gg_host_graph_add_weights", "gg_host_graph_write_adj", "gg_host_graph_write_gr",
     "gg_host_graph_read", "gg_host_graph_transpose", "gg_host_graph_free", "gg_partition_sizes",
-    "gg_hilbert_key", "gg_graph_build", "gg_graph_destroy", "gg_graph_get_info",
+    "gg_hilbert_key", "gg_graph_build", "gg_graph_destroy", "gg_graph_synchronize", "gg_graph_get_info",
     "gg_graph_partition_starts", "gg_graph_transpose", "gg_graph_device_arrays",
     "gg_frontier_single", "gg_frontier_all", "gg_frontier_empty", "gg_frontier_from_mask",
     "gg_frontier_from_list", "gg_frontier_destroy", "gg_frontier_stats", "gg_frontier_to_mask",
@@ -534,6 +536,10 @@ class Graph:
 
     def transpose(self):
         check(lib.gg_graph_transpose(self.h), "gg_graph_transpose")
+
+    def synchronize(self):
+        """Waits for the result copies TUNE_ASYNC_RESULTS leaves in flight."""
+        check(lib.gg_graph_synchronize(self.h), "gg_graph_synchronize")
 
     def set_profiling(self, enable=True):
         check(lib.gg_graph_set_profiling(self.h, int(enable)), "gg_graph_set_profiling")

@@ -159,6 +159,21 @@ static void fill_stats(gg_run_stats* st, double ms, int rounds, uint64_t trav, i
 template <class T>
 static int to_host(gg_graph_s* g, T* host, const T* dev, uint64_t n) {
   if (!host) return GG_OK;
+  // asynchronous results: a result staged in a given-order array leaves on
+  // the copy stream into pinned memory, and the call does not wait for it
+  int slot = -1;
+  for (int k = 0; k < 2; ++k)
+    if (g->ws.d_order[k] && reinterpret_cast<const void*>(dev) == g->ws.d_order[k]) slot = k;
+  cudaPointerAttributes pa{};
+  if (g->async_results && slot >= 0 && cudaPointerGetAttributes(&pa, host) == cudaSuccess &&
+      pa.type == cudaMemoryTypeHost) {
+    GG_CUDA(cudaEventRecord(g->result_ready, g->stream));
+    GG_CUDA(cudaStreamWaitEvent(g->copy_stream, g->result_ready, 0));
+    GG_CUDA(cudaMemcpyAsync(host, dev, sizeof(T) * n, cudaMemcpyDeviceToHost, g->copy_stream));
+    GG_CUDA(cudaEventRecord(g->slot_copied[slot], g->copy_stream));
+    return GG_OK;
+  }
+  cudaGetLastError();  // a pageable pointer is not an error
   GG_CUDA(cudaMemcpyAsync(host, dev, sizeof(T) * n, cudaMemcpyDeviceToHost, g->stream));
   GG_CUDA(cudaStreamSynchronize(g->stream));
   return GG_OK;
@@ -209,11 +224,13 @@ static int run_bfs(gg_graph_s* g, uint32_t start, int32_t* parents, int32_t* lev
   const int32_t* lev_out = lev.p;
   if (g->relabeled && parents) {
     int32_t* tp = reinterpret_cast<int32_t*>(g->ws.d_order[0]);
+    GG_TRY(slot_write_wait(g, 0));
     k_ids_to_given<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(n, g->d_new_of_old, g->d_old_of_new,
                                                                           par.p, tp);
     g->kernels++;
     par_out = tp;
   }
+  if (parents && !g->relabeled) GG_TRY(given_order<int32_t>(g, par.p, 0, &par_out));
   if (levels) GG_TRY(given_order<int32_t>(g, lev.p, 1, &lev_out));
   const double ms = tm.stop();
   GG_TRY(to_host(g, parents, par_out, n));
@@ -982,8 +999,11 @@ static int run_spmv(gg_graph_s* g, const float* x_in, float* y_out, gg_run_stats
   GG_TRY(x.alloc(g, n));
   GG_TRY(y.alloc(g, n));
   // the input vector is uploaded before the timed Compute loop (like the
-  // graph); a renumbered graph takes it through its given-order array
-  float* xg = g->relabeled ? reinterpret_cast<float*>(g->ws.d_order[0]) : x.p;
+  // graph); a renumbered graph takes it through its given-order array 1,
+  // which the result uses after it (array 0 may still be leaving for the
+  // host with an earlier result)
+  float* xg = g->relabeled ? reinterpret_cast<float*>(g->ws.d_order[1]) : x.p;
+  if (x_in && g->relabeled) GG_TRY(slot_write_wait(g, 1));
   if (x_in) GG_CUDA(cudaMemcpyAsync(xg, x_in, 4ull * n, cudaMemcpyHostToDevice, g->stream));
   EventTimer tm(g->stream);
   if (x_in && g->relabeled) GG_TRY(device_order<float>(g, xg, 1, x.p));

@@ -148,6 +148,12 @@ struct gg_graph_s {
   int device_loop = 1;  // BFS runs consecutive sparse levels in one cooperative launch
   int cc_algo = 0;      // Components on symmetric graphs: 0 label propagation, 1 union-find
   int pr_graph = 1;     // PageRank iterations replayed as one CUDA graph (0: one host round trip per iteration)
+  // GG_TUNE_ASYNC_RESULTS: results bound for pinned host memory leave from the
+  // given-order arrays on copy_stream, and the call returns without waiting
+  int async_results = 0;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t result_ready = nullptr;                // on stream: the result to copy is complete
+  cudaEvent_t slot_copied[2] = {nullptr, nullptr};  // on copy_stream: the last copy out of ws.d_order[k]
   gg::PrLoop* pr_loop = nullptr;  // created by the first graph-driven PageRank call
   int coo_kernel = 6;  // 0 CTA ring (k_pull), 1 per-warp direct loads, 2/3 per-warp bulk-copy rings, 6 direct loads
                        // with cross-lane run merging (fastest measured)

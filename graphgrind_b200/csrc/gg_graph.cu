@@ -543,6 +543,7 @@ static void graph_release(gg_graph_s* g) {
   const std::vector<gg_frontier_s*> fl(g->frontiers.begin(), g->frontiers.end());
   for (gg_frontier_s* f : fl) frontier_free(f);
   if (g->stream) cudaStreamSynchronize(g->stream);
+  if (g->copy_stream) cudaStreamSynchronize(g->copy_stream);
   pr_loop_free(g);
   for (void* a : g->arrays) cudaFree(a);
   g->arrays.clear();
@@ -579,6 +580,10 @@ static void graph_release(gg_graph_s* g) {
   if (g->ws.h_red) cudaFreeHost(g->ws.h_red);
   for (auto& e : g->prof_ev)
     if (e) cudaEventDestroy(e);
+  for (auto& e : g->slot_copied)
+    if (e) cudaEventDestroy(e);
+  if (g->result_ready) cudaEventDestroy(g->result_ready);
+  if (g->copy_stream) cudaStreamDestroy(g->copy_stream);
   if (g->stream) cudaStreamDestroy(g->stream);
   delete g;
 }
@@ -781,6 +786,13 @@ int gg_graph_build(const gg_host_graph* hg, const gg_build_opts* opts, gg_graph_
   return GG_OK;
 }
 
+int gg_graph_synchronize(gg_graph_t g) {
+  if (!graph_live(g)) return fail(GG_ERR_INVALID_ARG, "gg_graph_synchronize: not a live graph");
+  if (g->copy_stream) GG_CUDA(cudaStreamSynchronize(g->copy_stream));
+  GG_CUDA(cudaStreamSynchronize(g->stream));
+  return GG_OK;
+}
+
 int gg_graph_destroy(gg_graph_t g) {
   if (!graph_live(g)) return fail(GG_ERR_INVALID_ARG, "gg_graph_destroy: not a live graph");
   cudaStreamSynchronize(g->stream);
@@ -858,6 +870,18 @@ int gg_graph_set_tuning(gg_graph_t g, int32_t key, int64_t value) {
       if (value != 0 && value != 1) return fail(GG_ERR_INVALID_ARG, "PageRank graph switch must be 0 or 1");
       g->pr_graph = (int)value;
       return GG_OK;
+    case GG_TUNE_ASYNC_RESULTS:
+      if (value != 0 && value != 1) return fail(GG_ERR_INVALID_ARG, "asynchronous results switch must be 0 or 1");
+      if (value && !g->copy_stream) {
+        GG_CUDA(cudaStreamCreateWithFlags(&g->copy_stream, cudaStreamNonBlocking));
+        GG_CUDA(cudaEventCreateWithFlags(&g->result_ready, cudaEventDisableTiming));
+        for (auto& e : g->slot_copied) GG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      }
+      if (value && !g->ws.d_order[0])  // results of graphs with their given ids are staged there too
+        for (auto& a : g->ws.d_order) GG_TRY(dev_alloc(g, &a, (size_t)g->n + 4));
+      if (!value && g->copy_stream) GG_CUDA(cudaStreamSynchronize(g->copy_stream));
+      g->async_results = (int)value;
+      return GG_OK;
     default:
       return fail(GG_ERR_INVALID_ARG, "unknown tuning key %d", key);
   }
@@ -883,6 +907,9 @@ int gg_graph_get_tuning(gg_graph_t g, int32_t key, int64_t* value) {
       return GG_OK;
     case GG_TUNE_PR_GRAPH:
       *value = g->pr_graph;
+      return GG_OK;
+    case GG_TUNE_ASYNC_RESULTS:
+      *value = g->async_results;
       return GG_OK;
     default:
       return fail(GG_ERR_INVALID_ARG, "unknown tuning key %d", key);

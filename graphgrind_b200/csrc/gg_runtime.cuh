@@ -114,14 +114,28 @@ int given_order(gg_graph_s* g, const T* dev, uint32_t k, DevBuf<T>& tmp, const T
   *res = tmp.p;
   return GG_OK;
 }
+// Before the stream writes the given-order array `slot`: wait until a copy to
+// the host that still reads it (GG_TUNE_ASYNC_RESULTS) is done.
+inline int slot_write_wait(gg_graph_s* g, int slot) {
+  if (g->slot_copied[slot]) GG_CUDA(cudaStreamWaitEvent(g->stream, g->slot_copied[slot], 0));
+  return GG_OK;
+}
 // The same for one 4-byte value per vertex, into the graph's given-order
 // array `slot` (0 or 1; nothing is allocated on the application's path).
+// With asynchronous results the array also stages results of graphs that
+// keep their given ids, so that they can leave while the stream goes on.
 template <class T>
 int given_order(gg_graph_s* g, const T* dev, int slot, const T** res) {
   static_assert(sizeof(T) == 4, "the given-order arrays hold 4-byte values");
   *res = dev;
-  if (!g->relabeled) return GG_OK;
+  if (!g->relabeled && !g->async_results) return GG_OK;
   T* out = reinterpret_cast<T*>(g->ws.d_order[slot]);
+  GG_TRY(slot_write_wait(g, slot));
+  if (!g->relabeled) {
+    GG_CUDA(cudaMemcpyAsync(out, dev, sizeof(T) * (uint64_t)g->n, cudaMemcpyDeviceToDevice, g->stream));
+    *res = out;
+    return GG_OK;
+  }
   k_permute_rows<T><<<generic_grid(g, g->n), kGenericThreads, 0, g->stream>>>(g->n, 1, g->d_new_of_old, dev, out);
   GG_CUDA(cudaGetLastError());
   g->kernels++;

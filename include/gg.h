@@ -189,6 +189,9 @@ typedef struct gg_frontier_s* gg_frontier_t;
  * Hilbert/CSR-sorted partitioned COO, cut into CTA tiles sized to shared memory. */
 int gg_graph_build(const gg_host_graph* g, const gg_build_opts* opts, gg_graph_t* out);
 int gg_graph_destroy(gg_graph_t g);
+/* Waits for the graph's work and for the result copies that
+ * GG_TUNE_ASYNC_RESULTS left in flight. */
+int gg_graph_synchronize(gg_graph_t g);
 int gg_graph_get_info(gg_graph_t g, gg_graph_info* info);
 /* Partition starts (P+1 entries) of the COO partitioner (partitioner::start_of,
  * graphgrind/partitioner.h:153-165). */
@@ -321,13 +324,24 @@ int gg_graph_set_dense_policy(gg_graph_t g, int32_t policy);
  *                         graph handle.  Falls back to 0 by itself when the
  *                         driver refuses the capture; profiling (see
  *                         gg_graph_set_profiling) also takes the host loop.
- *                         0: one host round trip per iteration */
+ *                         0: one host round trip per iteration
+ *   GG_TUNE_ASYNC_RESULTS 0 (default): the applications return once their
+ *                         results are in the host arrays; 1: a result bound
+ *                         for pinned host memory (cudaMallocHost or
+ *                         cudaHostRegister) is copied on a second stream
+ *                         while the call returns, so that the copy overlaps
+ *                         the next call's work; gg_graph_synchronize waits
+ *                         for every such copy (read the arrays after it).
+ *                         Pageable arrays are filled before the call
+ *                         returns in both modes.  Graphs that keep their
+ *                         given ids then hold two n-entry staging arrays */
 #define GG_TUNE_DENSE_POLICY 1
 #define GG_TUNE_COO_KERNEL 2
 #define GG_TUNE_SPARSE_DIV 3
 #define GG_TUNE_DEVICE_LOOP 4
 #define GG_TUNE_CC_ALGO 5
 #define GG_TUNE_PR_GRAPH 6
+#define GG_TUNE_ASYNC_RESULTS 7
 int gg_graph_set_tuning(gg_graph_t g, int32_t key, int64_t value);
 int gg_graph_get_tuning(gg_graph_t g, int32_t key, int64_t* value);
 
