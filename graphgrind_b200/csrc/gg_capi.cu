@@ -1008,18 +1008,23 @@ static int run_spmv(gg_graph_s* g, const float* x_in, float* y_out, gg_run_stats
   EventTimer tm(g->stream);
   if (x_in && g->relabeled) GG_TRY(device_order<float>(g, xg, 1, x.p));
   if (!x_in) GG_TRY(fill<float>(g, x.p, n, (float)(1 / (double)n)));
-  GG_TRY(fill<float>(g, y.p, n, 0.0f));
+  // a renumbered graph's sums go straight to the given ids, in array 1 (the
+  // input staged there was consumed above)
+  float* yd = g->relabeled ? reinterpret_cast<float*>(g->ws.d_order[1]) : y.p;
+  if (g->relabeled && !x_in) GG_TRY(slot_write_wait(g, 1));
+  GG_TRY(fill<float>(g, yd, n, 0.0f));
   FrontierHold F;
   GG_TRY(gg_frontier_all(g, &F.f));
   SpmvF f;
   f.x = x.p;
-  f.y = y.p;
+  f.y = yd;
   f.float_w = g->wtype == GG_W_FLOAT32;
+  f.y_map = g->relabeled ? g->d_old_of_new : nullptr;
   gg_frontier_s* out = nullptr;
   GG_TRY(edge_map(g, F.f, f, app_threshold(g), GG_EM_NO_OUTPUT, &out));  // output.del()
   frontier_free(out);
-  const float* res = y.p;
-  GG_TRY(given_order<float>(g, y.p, 1, &res));
+  const float* res = yd;
+  if (!g->relabeled) GG_TRY(given_order<float>(g, y.p, 1, &res));
   const double ms = tm.stop();
   GG_TRY(to_host(g, y_out, res, n));
   fill_stats(st, ms, 1, g->m, g->kernels);

@@ -167,15 +167,17 @@ struct SpmvF : SumF32 {
   const float* x;
   float* y;
   int float_w;
+  const uint32_t* y_map = nullptr;  // y is indexed by y_map[d] (the given ids of a renumbered graph), else by d
   __device__ float wv(uint32_t w) const { return float_w ? __uint_as_float(w) : (float)(int32_t)w; }
+  __device__ uint32_t yi(uint32_t d) const { return y_map ? __ldg(y_map + d) : d; }
   __device__ bool cond(uint32_t) const { return true; }
   __device__ value_t gather(uint32_t s, uint32_t w) const { return __ldg(x + s) * wv(w); }
   __device__ bool commit(uint32_t d, value_t acc) const {
-    y[d] += acc;
+    y[yi(d)] += acc;
     return true;
   }
   __device__ bool update_atomic(uint32_t s, uint32_t d, uint32_t w) const {
-    atomicAdd(y + d, __ldg(x + s) * wv(w));
+    atomicAdd(y + yi(d), __ldg(x + s) * wv(w));
     return true;
   }
 };
