@@ -278,9 +278,12 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
     if pr_fused:
         kernel_name += " with the vertex step"
     # per-application dense-pull rooflines, algorithmic bytes: PageRank as
-    # above (8m+16n without the vertex step), SpMV 12m+12n
+    # above (8m+16n without the vertex step), SpMV 12m+12n, plus 4 B per
+    # vertex on a renumbered graph, whose commits read the given id of
+    # every destination and write its sum there
+    spmv_bytes = 12 * m + (16 if args.vertex_order else 12) * n
     roofline_by_app = {}
-    for app, pf, bytes_ in (("pagerank", prof_pr, pr_bytes), ("spmv", prof_sp, 12 * m + 12 * n)):
+    for app, pf, bytes_ in (("pagerank", prof_pr, pr_bytes), ("spmv", prof_sp, spmv_bytes)):
         kind = max(("coo_pull", "csc_pull"), key=lambda k: pf[k]["launches"])
         if pf[kind]["launches"]:
             lm = pf[kind]["ms"] / pf[kind]["launches"]
