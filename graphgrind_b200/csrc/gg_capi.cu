@@ -463,8 +463,31 @@ void pr_loop_free(gg_graph_s* g) {
   g->pr_loop = nullptr;
 }
 
+// The graph's first pass: ranks 1/n, accumulators 0, first contributions
+// (k_div_outdeg's quotient) and the first output bitmap cleared.
+__global__ void k_pr_loop_init(uint32_t n, float* p, float* acc, const uint32_t* off, float* contrib, uint32_t* bits,
+                               uint32_t words) {
+  const float p0 = (float)(1 / (double)n);
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint32_t d = off[i + 1] - off[i];
+    p[i] = p0;
+    acc[i] = 0.0f;
+    contrib[i] = d ? p0 / (float)d : 0.0f;
+  }
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < words; i += stride) bits[i] = 0;
+}
+
+// After iteration i: thread 0 decides (below); every thread clears the
+// iteration's input bitmap, read by nothing after its pull and uncovered-range
+// pass, which the next iteration writes as its output.
 __global__ void k_pr_loop_check(PrLoopCtl* c, unsigned long long* stats, double* red, cudaGraphConditionalHandle h_loop,
-                                cudaGraphConditionalHandle h_odd, int set_odd) {
+                                cudaGraphConditionalHandle h_odd, int set_odd, uint32_t* clear_bits,
+                                uint32_t clear_words) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < clear_words;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    clear_bits[i] = 0;
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
   const double l1 = red[0];
   const unsigned long long dm = stats[0], oe = stats[1], err = stats[3];
   red[0] = 0;  // the next epilogue's L1 and the next pull's counters start from zero
@@ -543,8 +566,7 @@ static int pr_finish_gaps(gg_graph_s* g, const PrFinishF& f) {
 // into buffers of the loop.
 static int pr_iteration(gg_graph_s* g, bool first, bool bit_all, float* p_curr, float* p_next, const float* contrib,
                         float* contrib_next, uint32_t* in_bits, uint32_t* out_bits) {
-  const uint32_t n = g->n;
-  GG_TRY(fill<uint32_t>(g, out_bits, (uint64_t)g->words() + 4, 0u));
+  const uint32_t n = g->n;  // out_bits arrives cleared (initial pass, or the previous check)
   gg_frontier_s in{}, out{};
   in.g = out.g = g;
   in.n = out.n = n;
@@ -608,8 +630,10 @@ static int pr_loop_capture(gg_graph_s* g, PrLoop* L, bool bit_all) {
   cudaGraphConditionalHandle h_loop = 0, h_odd = 0;
   cudaGraph_t body = nullptr, odd = nullptr;
   cudaGraphNode_t last = nullptr;
-  auto check = [&](int set_odd) -> int {
-    k_pr_loop_check<<<1, 1, 0, g->stream>>>(L->d_ctl, g->ws.d_stats, g->ws.d_red, h_loop, h_odd, set_odd);
+  const uint32_t words = g->words() + 4;
+  auto check = [&](int set_odd, uint32_t* in_bits) -> int {
+    k_pr_loop_check<<<generic_grid(g, words), kGenericThreads, 0, g->stream>>>(
+        L->d_ctl, g->ws.d_stats, g->ws.d_red, h_loop, h_odd, set_odd, in_bits, words);
     GG_CUDA(cudaGetLastError());
     return GG_OK;
   };
@@ -621,12 +645,10 @@ static int pr_loop_capture(gg_graph_s* g, PrLoop* L, bool bit_all) {
     rc = capture_into(g, graph, [&]() -> int {
       GG_CUDA(cudaMemsetAsync(g->ws.d_stats, 0, sizeof(unsigned long long) * 8, g->stream));
       GG_CUDA(cudaMemsetAsync(g->ws.d_red, 0, sizeof(double), g->stream));
-      GG_TRY(fill<float>(g, A, n, (float)(1 / (double)n)));
-      GG_TRY(fill<float>(g, B, n, 0.0f));
-      k_div_outdeg<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(n, A, g->out_off(), C0);
+      k_pr_loop_init<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(n, A, B, g->out_off(), C0, X, words);
       GG_CUDA(cudaGetLastError());
       GG_TRY(pr_iteration(g, true, bit_all, A, B, C0, C1, Y, X));
-      return check(0);
+      return check(0, Y);
     }, &last);
   if (!rc) rc = add_conditional(graph, last, h_loop, cudaGraphCondTypeWhile, &body);
   if (!rc && cudaGraphConditionalHandleCreate(&h_odd, body, 0, cudaGraphCondAssignDefault) != cudaSuccess)
@@ -635,14 +657,14 @@ static int pr_loop_capture(gg_graph_s* g, PrLoop* L, bool bit_all) {
   if (!rc)
     rc = capture_into(g, body, [&]() -> int {
       GG_TRY(pr_iteration(g, false, bit_all, B, A, C1, C0, X, Y));
-      return check(1);
+      return check(1, X);
     }, &last);
   if (!rc) rc = add_conditional(body, last, h_odd, cudaGraphCondTypeIf, &odd);
   // odd iterations: ranks into B, contributions into C1, output bits into X
   if (!rc)
     rc = capture_into(g, odd, [&]() -> int {
       GG_TRY(pr_iteration(g, false, bit_all, A, B, C0, C1, Y, X));
-      return check(0);
+      return check(0, Y);
     }, &last);
   cudaGraphExec_t exec = nullptr;
   if (!rc && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess)
@@ -761,10 +783,10 @@ static int run_pagerank(gg_graph_s* g, int max_iter, int bit_all, float* ranks, 
     if (c.reason < 1 || c.reason > 3 || c.count < 1) return fail(GG_ERR_CUDA, "PageRank graph: bad loop state");
     count = (int)c.count;
     trav = c.trav;
-    // 2 fills and the first contributions, then per iteration the bitmap fill,
-    // the pull, the vertex step's pass (uncovered ranges or the epilogue) and the check
-    const int per_iter = 3 + (pr_fused(g) && g->coo_gap_count == 0 ? 0 : 1);
-    g->kernels = 3 + per_iter * count;
+    // the initial pass, then per iteration the pull, the vertex step's pass
+    // (uncovered ranges or the epilogue) and the check
+    const int per_iter = 2 + (pr_fused(g) && g->coo_gap_count == 0 ? 0 : 1);
+    g->kernels = 1 + per_iter * count;
     g->last = gg_edge_map_stats{};
     g->last.kind = 3;
     g->last.frontier_active = c.in_dm;

@@ -12,13 +12,13 @@ pytestmark = pytest.mark.gpu
 
 
 def graph_kernels(gg, g, rounds):
-    """Kernels of a run that the captured graph finished: two fills and the
-    first contributions, then per iteration the bitmap fill, the pull, the
-    check and, unless the pull's commits ran the vertex step over every
-    vertex, one more pass (the uncovered ranges, or the epilogue)."""
+    """Kernels of a run that the captured graph finished: the initial pass,
+    then per iteration the pull, the check and, unless the pull's commits ran
+    the vertex step over every vertex, one more pass (the uncovered ranges,
+    or the epilogue)."""
     fused = g.get_tuning(gg.TUNE_COO_KERNEL) > 0
-    per_iter = 3 if fused and g.info().num_coo_gaps == 0 else 4
-    return 3 + per_iter * rounds
+    per_iter = 2 if fused and g.info().num_coo_gaps == 0 else 3
+    return 1 + per_iter * rounds
 
 
 def check_ranks(r, o):
