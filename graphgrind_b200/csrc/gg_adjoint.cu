@@ -4,7 +4,7 @@
 //   x_{t+1}[v] = d * sum_{e = u->v} a_e x_t[u] + (1 - d) * tele[v]
 //
 // the weighted form of PR_F / PR_Vertex_F (app/PageRank.C:28-100) with a_e in
-// place of 1/outdeg(u), and SPMV_F (app/SPMV.C:7-47) at one step with d = 1.
+// place of 1/outdeg(u), and SPMV_F (app/SPMV.C:7-48) at one step with d = 1.
 // Forward steps pull over the in-edges (CSC); the adjoint is the transposed
 // traversal, a pull over the out-edges (CSR):
 //   lambda_T = dL/dx_T

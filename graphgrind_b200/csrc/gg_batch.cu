@@ -4,7 +4,7 @@
 //
 //   X_0 = T,  X_{t+1} = d * A X_t + (1 - d) * T,  A[v,u] = 1/outdeg(u) for u->v
 //
-// the personalised form of PR_F / PR_Vertex_F (app/PageRank.C:256-315) with a
+// the personalised form of PR_F / PR_Vertex_F (app/PageRank.C:28-87) with a
 // teleport matrix T (n x k, row-major) in place of the uniform 1/n, all
 // vertices active (PageRankBit, app/PageRankBit.C:145).
 #include <cub/cub.cuh>
@@ -562,7 +562,7 @@ __global__ void k_ms_push(const uint32_t* queue, const uint32_t* qoff, uint32_t 
 
 // Backward level r from the level's vertex list (recorded by the forward
 // pass): mask[v] = the sources with level r at v and dep[v][j] = 1/paths[v][j]
-// there (BC_Back_Vertex_F, app/BC.C:140-154).  One warp per listed vertex.
+// there (BC_Back_Vertex_F, app/BC.C:142-154).  One warp per listed vertex.
 __global__ void k_ms_level_seed(const uint32_t* list, const uint64_t* masks, uint32_t cnt, uint64_t* mask,
                                 const float* sigma, float* dep) {
   const int lane = threadIdx.x & 31;

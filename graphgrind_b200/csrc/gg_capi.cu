@@ -63,7 +63,7 @@ __device__ __forceinline__ void block_add_double(double v, double* out) {
   }
 }
 
-// PageRank iteration epilogue (app/PageRank.C:361-371), fused:
+// PageRank iteration epilogue (app/PageRank.C:133-142), fused:
 //   vertexMap(F, PR_Vertex_F)            p_next[i] = d*p_next[i] + (1-d)/n, i in F
 //   p_curr[j] = |p_curr[j] - p_next[j]|  for every j, L1 = sum
 //   vertexMap(F, PR_Vertex_Reset)        p_curr[i] = 0, i in F
@@ -365,7 +365,7 @@ static int run_cc_union_find(gg_graph_s* g, int32_t* ids_out, gg_run_stats* st) 
   return GG_OK;
 }
 
-// app/Components.C:202-227
+// app/Components.C:101-126
 static int run_cc(gg_graph_s* g, int32_t* ids_out, gg_run_stats* st) {
   if (g->cc_algo == 1 && g->symmetric) return run_cc_union_find(g, ids_out, st);
   const uint32_t n = g->n;
@@ -374,7 +374,7 @@ static int run_cc(gg_graph_s* g, int32_t* ids_out, gg_run_stats* st) {
   GG_TRY(ids.alloc(g, n));
   GG_TRY(prev.alloc(g, n));
   EventTimer tm(g->stream);
-  // IDs[i] = i (app/Components.C:206): the given id, also on a renumbered graph
+  // IDs[i] = i (app/Components.C:112): the given id, also on a renumbered graph
   if (g->relabeled)
     GG_CUDA(cudaMemcpyAsync(ids.p, g->d_old_of_new, 4ull * n, cudaMemcpyDeviceToDevice, g->stream));
   else
@@ -410,7 +410,7 @@ static int run_cc(gg_graph_s* g, int32_t* ids_out, gg_run_stats* st) {
 }
 
 // ---------------------------------------------- PageRank as a CUDA graph
-// The iteration loop of app/PageRank.C:353-376 captured once per graph handle
+// The iteration loop of app/PageRank.C:129-146 captured once per graph handle
 // and knob setting, then replayed per call.  The top graph holds the
 // initialisation and the first iteration, then a while node whose body runs
 // the next iteration with the rank buffers one way round and, under an if
@@ -717,7 +717,7 @@ static int pr_loop_get(gg_graph_s* g, bool bit_all, PrLoop** out) {
   return GG_OK;
 }
 
-// app/PageRank.C:330-378 (bit_all: app/PageRankBit.C:145)
+// app/PageRank.C:102-150 (bit_all: app/PageRankBit.C:145)
 static int run_pagerank(gg_graph_s* g, int max_iter, int bit_all, float* ranks, gg_run_stats* st) {
   const uint32_t n = g->n;
   g->kernels = 0;
@@ -862,7 +862,7 @@ static int run_pagerank(gg_graph_s* g, int max_iter, int bit_all, float* ranks, 
   return GG_OK;
 }
 
-// PageRankConverage (app/PageRankConverage.C:243-310) kernels.  Sums are
+// PageRankConverage (app/PageRankConverage.C:235-315) kernels.  Sums are
 // accumulated in FP64 like the reference's sum()/normdiff().
 // Next contributions: add_factor = (0.85 / outdeg) * p (sinks are never gathered).
 __global__ void k_prc_contrib(uint32_t n, const float* p, const uint32_t* off, float* contrib) {
@@ -1013,7 +1013,7 @@ static int run_pagerank_delta(gg_graph_s* g, float* ranks, gg_run_stats* st) {
   return GG_OK;
 }
 
-// app/SPMV.C:65-93
+// app/SPMV.C:64-92
 static int run_spmv(gg_graph_s* g, const float* x_in, float* y_out, gg_run_stats* st) {
   const uint32_t n = g->n;
   g->kernels = 0;

@@ -64,7 +64,7 @@ struct BfsF : MinU32 {
   }
 };
 
-// CC_F, app/Components.C:127-186.  Pull = the cached form (:158-180):
+// CC_F, app/Components.C:26-85.  Pull = the cached form (:57-79):
 // min over prevIDs[s]; output iff the label drops and IDs[d]==prevIDs[d].
 // Push = updateAtomic (:152-157): writeMin(IDs[d], IDs[s]) && orig==prevIDs[d].
 struct CcF : MinI32 {
@@ -91,7 +91,7 @@ struct CcF : MinI32 {
   }
 };
 
-// PR_F, app/PageRank.C:256-298: p_next[d] += p_curr[s]/outdeg(s).  The
+// PR_F, app/PageRank.C:28-70: p_next[d] += p_curr[s]/outdeg(s).  The
 // division is done once per source (contrib[s] = p_curr[s]/outdeg(s)) by the
 // iteration's vertex pass; the per-edge value is the same FP32 quotient.
 // Also PageRankDelta's PR_F (app/PageRankDelta.C:29-71) with contrib = Delta/outdeg.
@@ -156,7 +156,7 @@ struct PrFinishF : PrT<true> {
   }
 };
 
-// SPMV_F, app/SPMV.C:7-47: p_next[d] += p_curr[s] * edgeLen.  Weights are
+// SPMV_F, app/SPMV.C:7-48: p_next[d] += p_curr[s] * edgeLen.  Weights are
 // the reference's int edge lengths, or FP32 when the graph carries FP32 weights.
 struct SpmvF : SumF32 {
   static constexpr bool kIdentityCommitNoop = true;  // commit is y[d] += acc
@@ -182,7 +182,7 @@ struct SpmvF : SumF32 {
   }
 };
 
-// BF_F, app/BellmanFord.C:28-92.  Pull = cached form: min of SP[s]+w over the
+// BF_F, app/BellmanFord.C:28-91.  Pull = cached form: min of SP[s]+w over the
 // frontier in-neighbours; output iff it lowers SP[d] and Visited[d] was 0.
 // Push = writeMin(SP[d], SP[s]+w) && CAS(Visited[d], 0, 1).
 struct BfF : MinI32 {
@@ -212,7 +212,7 @@ struct BfF : MinI32 {
   }
 };
 
-// BC_F / BC_Back_F, app/BC.C:28-117: value[d] += value[s] for unvisited d;
+// BC_F / BC_Back_F, app/BC.C:28-126: value[d] += value[s] for unvisited d;
 // output iff value[d] was 0 before (first path reaching d).
 struct BcF : SumF32 {
   static constexpr bool kPositive = false;
@@ -234,7 +234,7 @@ struct BcF : SumF32 {
 };
 
 // ------------------------------------------------------- vertex functors
-// CC_Vertex_F, app/Components.C:189-200
+// CC_Vertex_F, app/Components.C:88-99
 struct VCcCopy {
   int32_t* ids;
   int32_t* prev;
@@ -243,7 +243,7 @@ struct VCcCopy {
     return true;
   }
 };
-// PR_Vertex_F, app/PageRank.C:301-315
+// PR_Vertex_F, app/PageRank.C:73-87
 struct VPrUpdate {
   float* p_next;
   float damping, added;
@@ -261,7 +261,7 @@ struct VFill {
     return true;
   }
 };
-// PR_Vertex_F_FirstRound, app/PageRankDelta.C:73-90
+// PR_Vertex_F_FirstRound, app/PageRankDelta.C:73-89
 struct VPrdFirst {
   float* p;
   float* delta;
@@ -276,7 +276,7 @@ struct VPrdFirst {
     return fabsf(d) > eps2 * pi;
   }
 };
-// PR_Vertex_F, app/PageRankDelta.C:92-106
+// PR_Vertex_F, app/PageRankDelta.C:91-105
 struct VPrd {
   float* p;
   float* delta;
@@ -290,7 +290,7 @@ struct VPrd {
     return fabsf(d) > eps2 * pi;
   }
 };
-// BC_Vertex_F, app/BC.C:119-128
+// BC_Vertex_F, app/BC.C:129-138
 struct VBcMark {
   uint8_t* visited;
   __device__ bool operator()(uint32_t i) const {
@@ -298,7 +298,7 @@ struct VBcMark {
     return true;
   }
 };
-// BC_Back_Vertex_F, app/BC.C:131-143
+// BC_Back_Vertex_F, app/BC.C:142-154
 struct VBcBack {
   uint8_t* visited;
   float* dep;

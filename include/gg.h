@@ -234,14 +234,14 @@ int gg_frontier_repr(gg_frontier_t f);
  * point at device vertex arrays allocated with gg_vertex_array_alloc. */
 enum gg_functor_id {
   GG_F_BFS = 1,            /* app/BFS.C:26-75            args: gg_bfs_args      */
-  GG_F_CC = 2,             /* app/Components.C:127-186   args: gg_cc_args       */
-  GG_F_PR = 3,             /* app/PageRank.C:256-298     args: gg_pr_args       */
+  GG_F_CC = 2,             /* app/Components.C:26-85     args: gg_cc_args       */
+  GG_F_PR = 3,             /* app/PageRank.C:28-70       args: gg_pr_args       */
   GG_F_PRDELTA = 4,        /* app/PageRankDelta.C:29-71  args: gg_prdelta_args  */
-  GG_F_SPMV = 5,           /* app/SPMV.C:7-47            args: gg_spmv_args     */
-  GG_F_BF = 6,             /* app/BellmanFord.C:28-92    args: gg_bf_args       */
-  GG_F_BC = 7,             /* app/BC.C:28-71 (BC_F)      args: gg_bc_args       */
-  GG_F_BC_BACK = 8,        /* app/BC.C:73-117 (BC_Back_F) args: gg_bc_args      */
-  GG_F_BP = 9              /* app/BP.C:54-130            args: gg_bp_args       */
+  GG_F_SPMV = 5,           /* app/SPMV.C:7-48            args: gg_spmv_args     */
+  GG_F_BF = 6,             /* app/BellmanFord.C:28-91    args: gg_bf_args       */
+  GG_F_BC = 7,             /* app/BC.C:28-77 (BC_F)      args: gg_bc_args       */
+  GG_F_BC_BACK = 8,        /* app/BC.C:79-126 (BC_Back_F) args: gg_bc_args      */
+  GG_F_BP = 9              /* app/BP.C:54-133            args: gg_bp_args       */
 };
 typedef struct { int32_t* parents; int32_t* levels; int32_t round; } gg_bfs_args;
 typedef struct { int32_t* ids; int32_t* prev_ids; } gg_cc_args;
@@ -347,14 +347,14 @@ int gg_graph_get_tuning(gg_graph_t g, int32_t key, int64_t* value);
 
 /* Vertex functors for vertexMap / vertexFilter (graphgrind/ligra-numa.h:1023-1082). */
 enum gg_vertex_functor_id {
-  GG_V_CC_COPY = 101,      /* app/Components.C:189-200  prevIDs[i]=IDs[i]      args gg_cc_args   */
-  GG_V_PR_UPDATE = 102,    /* app/PageRank.C:301-315    p=d*p+(1-d)/n          args gg_pr_vertex_args */
+  GG_V_CC_COPY = 101,      /* app/Components.C:88-99    prevIDs[i]=IDs[i]      args gg_cc_args   */
+  GG_V_PR_UPDATE = 102,    /* app/PageRank.C:73-87      p=d*p+(1-d)/n          args gg_pr_vertex_args */
   GG_V_FILL_F32 = 103,     /* PR/SPMV reset: a[i]=value                        args gg_fill_args */
   GG_V_FILL_I32 = 104,     /* BF_Vertex_F: a[i]=value                          args gg_fill_args */
-  GG_V_PRDELTA_FIRST = 105,/* app/PageRankDelta.C:73-90 (filter)             args gg_prdelta_vertex_args */
-  GG_V_PRDELTA = 106,      /* app/PageRankDelta.C:92-106 (filter)            args gg_prdelta_vertex_args */
-  GG_V_BC_MARK = 107,      /* app/BC.C:119-128 Visited[i]=1                  args gg_bc_args */
-  GG_V_BC_BACK = 108,      /* app/BC.C:131-143                               args gg_bc_back_vertex_args */
+  GG_V_PRDELTA_FIRST = 105,/* app/PageRankDelta.C:73-89 (filter)             args gg_prdelta_vertex_args */
+  GG_V_PRDELTA = 106,      /* app/PageRankDelta.C:91-105 (filter)            args gg_prdelta_vertex_args */
+  GG_V_BC_MARK = 107,      /* app/BC.C:129-138 Visited[i]=1                  args gg_bc_args */
+  GG_V_BC_BACK = 108,      /* app/BC.C:142-154                               args gg_bc_back_vertex_args */
   GG_V_FILL_U8 = 109       /* a[i]=value (bytes)                              args gg_fill_args */
 };
 typedef struct { float* p_next; float damping; uint32_t n; } gg_pr_vertex_args;
@@ -417,19 +417,19 @@ typedef struct gg_run_stats {
 /* app/BFS.C:77-101: parents[n] (-1 unreached), levels[n] (-1 unreached); either
  * output may be NULL (app/BFS.C's result is the parents). */
 int gg_bfs(gg_graph_t g, uint32_t start, int32_t* parents, int32_t* levels, gg_run_stats* st);
-/* app/Components.C:202-227: ids[n]. */
+/* app/Components.C:101-126: ids[n]. */
 int gg_components(gg_graph_t g, int32_t* ids, gg_run_stats* st);
-/* app/PageRank.C:330-378 (bit_all=0) and app/PageRankBit.C (bit_all=1):
+/* app/PageRank.C:102-150 (bit_all=0) and app/PageRankBit.C (bit_all=1):
  * ranks[n] in FP32, max_iter iterations (10 in the reference). */
 int gg_pagerank(gg_graph_t g, int32_t max_iter, int32_t bit_all, float* ranks, gg_run_stats* st);
-/* app/PageRankConverage.C:243-310: PageRank whose dangling mass is spread
+/* app/PageRankConverage.C:235-315: PageRank whose dangling mass is spread
  * evenly and whose ranks are renormalised every iteration, until the L1
  * change is at most eps or max_iter iterations ran (100 and 1e-7 in the
  * reference).  ranks[n]; st->rounds = iterations. */
 int gg_pagerank_converge(gg_graph_t g, int32_t max_iter, double eps, float* ranks, gg_run_stats* st);
 /* app/PageRankDelta.C:120-174: ranks[n]. */
 int gg_pagerank_delta(gg_graph_t g, float* ranks, gg_run_stats* st);
-/* app/SPMV.C:65-93 with x = 1/n (x_in == NULL) or x_in[n]: y[n] = A^T-weighted sum. */
+/* app/SPMV.C:64-92 with x = 1/n (x_in == NULL) or x_in[n]: y[n] = A^T-weighted sum. */
 int gg_spmv(gg_graph_t g, const float* x_in, float* y, gg_run_stats* st);
 /* app/BellmanFord.C:106-145: dist[n] (1073741823 = unreached). */
 int gg_bellman_ford(gg_graph_t g, uint32_t start, int32_t* dist, gg_run_stats* st);
@@ -447,7 +447,7 @@ int gg_bp(gg_graph_t g, int32_t iters, const float* vert_potential, const float*
 
 /* ============================================================ batching */
 /* k-column personalised PageRank, the batched form of PR_F/PR_Vertex_F
- * (app/PageRank.C:256-315) with every vertex active (app/PageRankBit.C:145)
+ * (app/PageRank.C:28-87) with every vertex active (app/PageRankBit.C:145)
  * and a teleport matrix in place of the uniform 1/n:
  *   X_0 = T,  X_{t+1} = damping * A X_t + (1 - damping) * T,  A[v,u] = 1/outdeg(u)
  * k = 32 or 64 runs all columns in one SpMM-shaped pull per iteration (each
@@ -503,7 +503,7 @@ int gg_batch_bfs(gg_graph_batch_t b, const uint32_t* sources, int32_t* levels, g
  *   x_{t+1}[v] = damping * sum_{e = u->v} a_e x_t[u] + (1 - damping) * tele[v]
  * for t < iters from x_0 (x0, or 1/n when x0 == NULL): PR_F / PR_Vertex_F
  * (app/PageRank.C:28-100) with a_e in place of 1/outdeg(u) (a_e = 1/outdeg(u),
- * tele = 1/n gives PageRankBit), and SPMV_F (app/SPMV.C:7-47) at iters = 1,
+ * tele = 1/n gives PageRankBit), and SPMV_F (app/SPMV.C:7-48) at iters = 1,
  * damping = 1.  Its adjoint is the transposed traversal (a pull over the
  * out-edges where the forward pulls the in-edges).  A context holds the
  * forward's checkpoints (x_t every checkpoint_every steps) for the backward,

@@ -23,13 +23,18 @@ LIB = os.path.join(HERE, "liboracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
 
 
+def reference_tree() -> str:
+    """The GraphGrind source tree: $GG_REFERENCE, or a checkout named
+    `reference` beside this repository."""
+    return os.environ.get("GG_REFERENCE") or os.path.normpath(os.path.join(HERE, "..", "..", "reference"))
+
+
 def build(ref: bool = False) -> None:
     """Compile liboracle.so (and the reference harness when ref=True and the
     reference tree is present)."""
     subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
-    if ref and os.path.isdir(os.environ.get("GG_REFERENCE", "/root/reference")):
-        subprocess.run(["make", "-s", "-C", HERE, "ref", "REF=" + os.environ.get("GG_REFERENCE", "/root/reference")],
-                       check=True)
+    if ref and os.path.isdir(os.path.join(reference_tree(), "graphgrind")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", "REF=" + reference_tree()], check=True)
 
 
 if not os.path.exists(LIB):
@@ -65,10 +70,17 @@ for name, args in {
     "or_wpr_backward": [C.POINTER(OrGraph), _P, _P, _P, C.c_int32, C.c_double, C.c_int32, _P, _P, _P, _P],
     "or_partition_sizes": [_P, _P, C.c_uint32, C.c_uint64, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, _P],
     "or_hilbert_key": [C.c_int64, C.c_int64, C.c_int64],
+    "or_gen_rmat": [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_uint64, C.c_int32, _P,
+                    C.POINTER(C.c_void_p), C.POINTER(C.c_uint64)],
+    "or_add_weights": [C.c_uint32, _P, _P, C.c_int32, C.c_int32, C.c_uint64, C.c_int32, C.c_int32, _P],
+    "or_csc": [C.c_uint32, C.c_uint64, _P, _P, _P, _P, _P, _P],
+    "or_write_gr": [C.c_char_p, C.c_uint32, C.c_uint64, _P, _P, _P, C.c_int32],
 }.items():
     f = getattr(_lib, name)
     f.argtypes = args
     f.restype = C.c_int64 if name == "or_hilbert_key" else C.c_int
+_lib.or_free.argtypes = [C.c_void_p]
+_lib.or_free.restype = None
 
 
 def _p(a):
@@ -76,17 +88,16 @@ def _p(a):
 
 
 def csc_of(offsets, indices, weights=None):
-    """In-edge CSC of a CSR, in-lists ordered by source id (numpy, host)."""
-    offsets = np.asarray(offsets, np.int64)
-    n = len(offsets) - 1
-    src = np.repeat(np.arange(n, dtype=np.int64), np.diff(offsets))
-    dst = np.asarray(indices, np.int64)
-    order = np.lexsort((src, dst))
-    in_idx = src[order].astype(np.uint32)
-    in_off = np.zeros(n + 1, np.int64)
-    np.cumsum(np.bincount(dst, minlength=n), out=in_off[1:])
-    in_w = None if weights is None else np.asarray(weights)[order]
-    return in_off.astype(np.uint32), in_idx, in_w
+    """In-edge CSC of a CSR, in-lists ordered by source id (host; or_csc)."""
+    off = np.ascontiguousarray(offsets, np.uint32)
+    idx = np.ascontiguousarray(indices, np.uint32)
+    n, m = len(off) - 1, len(idx)
+    w = None if weights is None else np.ascontiguousarray(weights, np.float64)
+    in_off = np.empty(n + 1, np.uint32)
+    in_idx = np.empty(max(m, 1), np.uint32)
+    in_w = None if w is None else np.empty(max(m, 1), np.float64)
+    assert _lib.or_csc(n, m, _p(off), _p(idx), _p(w), _p(in_off), _p(in_idx), _p(in_w)) == 0
+    return in_off, in_idx[:m], None if in_w is None else in_w[:m]
 
 
 class Graph:
@@ -227,6 +238,48 @@ def partition_sizes(in_deg, out_deg, m, P, balance=0, part_how=0, relabel=False)
 
 def hilbert_key(side_edges, x, y):
     return int(_lib.or_hilbert_key(side_edges, x, y))
+
+
+# ------------------------------------------------ inputs without the library
+class RmatGraph:
+    """A seeded R-MAT CSR made by the oracle's restatement of the library's
+    generator (or_gen_rmat), for processes that must not load the library."""
+
+    def __init__(self, scale, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=1, symmetric=False):
+        n = 1 << scale
+        self.n, self.symmetric = n, bool(symmetric)
+        self.offsets = np.empty(n + 1, np.uint32)
+        ptr, m = C.c_void_p(), C.c_uint64()
+        rc = _lib.or_gen_rmat(scale, edge_factor, a, b, c, seed, int(symmetric), _p(self.offsets), C.byref(ptr),
+                              C.byref(m))
+        if rc:
+            raise RuntimeError(f"or_gen_rmat failed ({rc})")
+        self.m = int(m.value)
+        try:
+            self.indices = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_uint32)), (max(self.m, 1),))[:self.m].copy()
+        finally:
+            _lib.or_free(ptr)
+        self.weights = None
+
+    def add_weights(self, as_float: bool, seed: int, lo: int = 1, hi: int = 100):
+        w = np.empty(max(self.m, 1), np.float32 if as_float else np.int32)
+        assert _lib.or_add_weights(self.n, _p(self.offsets), _p(self.indices), int(self.symmetric), int(as_float),
+                                   seed, lo, hi, _p(w)) == 0
+        self.weights = w[:self.m]
+        return self
+
+    def write_gr(self, path: str):
+        """Galois .gr (plus path_t for a directed graph); float weights are
+        written rounded to integers, as the library's writer does."""
+        w = None
+        if self.weights is not None:
+            w = self.weights if self.weights.dtype == np.int32 else np.rint(self.weights).astype(np.int32)
+            w = np.ascontiguousarray(w)
+        assert _lib.or_write_gr(path.encode(), self.n, self.m, _p(self.offsets), _p(self.indices), _p(w),
+                                int(self.symmetric)) == 0, f"cannot write {path}"
+
+    def out_degrees(self):
+        return np.diff(self.offsets.astype(np.int64))
 
 
 # ------------------------------------------------------- reference harness

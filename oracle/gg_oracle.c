@@ -296,7 +296,7 @@ int or_bfs(const or_graph* g, uint32_t start, int64_t* parents, int32_t* levels,
 }
 
 /* ================================================================ Components */
-/* app/Components.C:127-200 */
+/* app/Components.C:26-99 */
 typedef struct { int64_t* ids; int64_t* prev; } cc_ctx;
 static int cc_cond(void* c, uint32_t d) { (void)c; (void)d; return 1; }
 static int cc_update(void* c, uint32_t s, uint32_t d, double w, int64_t pos) {
@@ -343,7 +343,7 @@ static int cc_vertex(void* c, uint32_t i) {
 }
 
 int or_cc(const or_graph* g, int64_t* ids, or_stats* st) {
-  /* app/Components.C:202-227 */
+  /* app/Components.C:101-126 */
   if (!g) return -1;
   eng_t e = {g, 0, st, 0};
   int64_t* prev = (int64_t*)malloc(sizeof(int64_t) * (g->n ? g->n : 1));
@@ -363,7 +363,7 @@ int or_cc(const or_graph* g, int64_t* ids, or_stats* st) {
 }
 
 /* ================================================================== PageRank */
-/* app/PageRank.C:256-328 */
+/* app/PageRank.C:28-100 */
 typedef struct { double* p_curr; double* p_next; const eng_t* e; double damping, added; } pr_ctx;
 static int true_cond(void* c, uint32_t d) { (void)c; (void)d; return 1; }
 static int pr_update(void* c, uint32_t s, uint32_t d, double w, int64_t pos) {
@@ -391,7 +391,7 @@ static int pr_reset(void* c, uint32_t i) {
 }
 
 int or_pagerank(const or_graph* g, int32_t max_iter, int32_t bit_all, double* ranks, or_stats* st) {
-  /* app/PageRank.C:330-378; bit_all reproduces app/PageRankBit.C:145 */
+  /* app/PageRank.C:102-150; bit_all reproduces app/PageRankBit.C:145 */
   if (!g) return -1;
   const uint32_t n = g->n;
   eng_t e = {g, 0, st, 0};
@@ -519,7 +519,7 @@ int or_pagerank_delta(const or_graph* g, double* ranks, or_stats* st) {
 }
 
 /* ===================================================================== SPMV */
-/* app/SPMV.C:7-93 */
+/* app/SPMV.C:7-92 */
 typedef struct { const double* x; double* y; } spmv_ctx;
 static int spmv_update(void* c, uint32_t s, uint32_t d, double w, int64_t pos) {
   (void)pos;

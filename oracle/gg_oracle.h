@@ -5,7 +5,7 @@
  * baseline leg may load it; the product never does.
  *
  * FP64 throughout for PageRank / PageRankDelta / SPMV / BC (the reference's
- * PR/PRDelta/SPMV are double, app/PageRank.C:258, and BC's float is widened,
+ * PR/PRDelta/SPMV are double, app/PageRank.C:30, and BC's float is widened,
  * app/BC.C:26); integer apps use int64 like the reference's intT.
  */
 #ifndef GG_ORACLE_H
@@ -59,7 +59,7 @@ int or_bp(const or_graph* g, int32_t iters, const double* vert_pot, const double
  * k-column personalised form uses this per column): x_{t+1} = d*A x_t + (1-d)*tele. */
 int or_ppr(const or_graph* g, int32_t iters, double damping, const double* tele, double* x);
 
-/* app/PageRankConverage.C:243-310: PageRank with the dangling mass spread
+/* app/PageRankConverage.C:235-315: PageRank with the dangling mass spread
  * evenly and the ranks renormalised every iteration, until the L1 change
  * drops to eps or max_iter iterations ran.  ranks[n]; *iters = iterations;
  * l1[max_iter] (may be NULL) = each iteration's L1 change. */
@@ -68,7 +68,7 @@ int or_pagerank_converge(const or_graph* g, int32_t max_iter, double eps, double
 
 /* Weighted PageRank and its adjoint (no reference counterpart; the weighted
  * form of PR_F / PR_Vertex_F, app/PageRank.C:28-100, with the edge weight in
- * place of 1/outdeg, and SPMV_F, app/SPMV.C:7-47, at iters = 1, damping = 1):
+ * place of 1/outdeg, and SPMV_F, app/SPMV.C:7-48, at iters = 1, damping = 1):
  *   a_e = w_e (or w_e / sum of w over the source's out-edges when normalize)
  *   x_{t+1}[v] = damping * sum_{e = u->v} a_e x_t[u] + (1 - damping) * tele[v]
  * weights in out-edge (CSR) order; x0 NULL means 1/n.  The backward takes
@@ -85,6 +85,22 @@ int or_partition_sizes(const uint32_t* in_deg, const uint32_t* out_deg, uint32_t
                        int32_t P, int32_t balance, int32_t part_how, int32_t relabel,
                        int64_t* coo_sizes, int64_t* csc_sizes);
 int64_t or_hilbert_key(int64_t side_edges, int64_t x, int64_t y);
+
+/* Inputs without the GPU library (gg_oracle_gen.c). */
+/* The library's seeded R-MAT generator restated (gg_gen_rmat): offsets[n+1]
+ * filled, *indices malloc'd (release with or_free), *m set. */
+int or_gen_rmat(int32_t scale, int32_t edge_factor, double a, double b, double c, uint64_t seed,
+                int32_t symmetric, uint32_t* offsets, uint32_t** indices, uint64_t* m);
+void or_free(void* p);
+/* gg_host_graph_add_weights restated: int32 in [lo,hi] or float in (0,1]. */
+int or_add_weights(uint32_t n, const uint32_t* offsets, const uint32_t* indices, int32_t symmetric,
+                   int32_t as_float, uint64_t seed, int32_t lo, int32_t hi, void* weights);
+/* In-edge CSC (in-lists ascending by source); weights follow when given. */
+int or_csc(uint32_t n, uint64_t m, const uint32_t* out_off, const uint32_t* out_idx, const double* out_w,
+           uint32_t* in_off, uint32_t* in_idx, double* in_w);
+/* Galois .gr v1 (graphgrind/IO.h:365-450); directed graphs also get path_t. */
+int or_write_gr(const char* path, uint32_t n, uint64_t m, const uint32_t* off, const uint32_t* idx,
+                const int32_t* w, int32_t symmetric);
 
 #ifdef __cplusplus
 }

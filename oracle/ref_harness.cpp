@@ -119,7 +119,7 @@ static void replay(G& GA, long start) {  // app/BFS.C:77-101
 }
 #elif defined(GG_APP_CC)
 template <class G>
-static void replay(G& GA, long) {  // app/Components.C:202-227
+static void replay(G& GA, long) {  // app/Components.C:101-126
   const intT n = GA.n, m = GA.m;
   const partitioner& part = GA.get_partitioner();
   mmap_ptr<intT> IDs, prevIDs;
@@ -143,7 +143,7 @@ static void replay(G& GA, long) {  // app/Components.C:202-227
 }
 #elif defined(GG_APP_PR) || defined(GG_APP_PRBIT)
 template <class G>
-static void replay(G& GA, long) {  // app/PageRank.C:330-378, app/PageRankBit.C:131-147
+static void replay(G& GA, long) {  // app/PageRank.C:102-150, app/PageRankBit.C:103-151
   typedef typename G::vertex_type vertex;
   const partitioner& part = GA.get_partitioner();
   graph<vertex>& WG = GA.get_partition();
@@ -184,7 +184,7 @@ static void replay(G& GA, long) {  // app/PageRank.C:330-378, app/PageRankBit.C:
 }
 #elif defined(GG_APP_PRC)
 template <class G>
-static void replay(G& GA, long) {  // app/PageRankConverage.C:243-310
+static void replay(G& GA, long) {  // app/PageRankConverage.C:235-315
   typedef typename G::vertex_type vertex;
   const partitioner& part = GA.get_partitioner();
   graph<vertex>& WG = GA.get_partition();
@@ -266,7 +266,7 @@ static void replay(G& GA, long) {  // app/PageRankDelta.C:120-174
 }
 #elif defined(GG_APP_SPMV)
 template <class G>
-static void replay(G& GA, long) {  // app/SPMV.C:65-93
+static void replay(G& GA, long) {  // app/SPMV.C:64-92
   typedef typename G::vertex_type vertex;
   const partitioner& part = GA.get_partitioner();
   const intT n = GA.n, m = GA.m;

@@ -5,7 +5,8 @@ by `make -C oracle ref` (oracle/ref_harness.cpp), on small graphs and stores
 inputs (CSR) and outputs as .npz files.  Run it in a container that has the
 reference tree; the fixtures are committed and the tests only read them.
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py [--reference <GraphGrind tree>]
+    (default: $GG_REFERENCE, or a checkout named `reference` beside this repository)
 """
 from __future__ import annotations
 
@@ -146,7 +147,7 @@ def vebo_cases(tmp):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("GG_REFERENCE", "/root/reference"))
+    ap.add_argument("--reference", default=oracle.reference_tree())
     a = ap.parse_args()
     os.environ["GG_REFERENCE"] = a.reference
     oracle.build(ref=True)
