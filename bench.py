@@ -16,8 +16,9 @@ each run through the library's C ABI (gg_bfs / gg_pagerank / gg_spmv).
            PageRank ranks, SpMV y)
   roofline = the dense-pull kernel of the PageRank iterations: algorithmic
            bytes 8m + 16n per launch over its CUDA-event duration
-  cpu_baseline = the reference's own OpenMP build (oracle/_ref) on the host
-           cores, on a bounded RMAT-22 sample of the same workload
+  cpu_baseline = the reference's own OpenMP build (oracle/_ref, compiled from
+           GraphGrind's sources) on the host cores, on the same graph written
+           as Galois .gr, -c 384 -r 100 (2 rounds after 1 warm-up)
   batched  = (N=1, outside the timed step) the batched and differentiated
            forms against the plain form on the same GPU: k=64 personalised
            PageRank (RMAT-22 seed 5, 20 iterations) vs 64 single-column runs;
@@ -31,6 +32,12 @@ each run through the library's C ABI (gg_bfs / gg_pagerank / gg_spmv).
   stress   = (N=1, outside the timed step) BFS from 100 and Components on the
            4096^2 grid with 0.1 % long-range edges (seed 3, high diameter,
            sparse frontiers) and on Erdos-Renyi n=2^24, m=2^28 (seed 4, dense)
+
+--impl reference times the same step with the reference's own build: the
+graph is generated by the oracle's restatement of the library's generator (so
+that process loads no library of the product), written as .gr, and each of
+BFS, PageRank and SPMV runs W + K rounds through the reference's own driver
+("Running : t", Compute only); a one-thread round of each is reported beside.
 
 Multi-GPU: the path does not shard across GPUs in this build (one GPU per
 graph); --gpus N runs N independent replicas under torchrun and reports the
@@ -151,6 +158,40 @@ def make_graph(gg, scale: int, seed: int, weights: int):
     return hg
 
 
+# ------------------------------------------------ the workloads' other inputs
+# (the full-size parity tests import these, so that they check the results of
+# exactly the inputs measured here)
+def spmv_input(n: int) -> np.ndarray:
+    """x of the step's SpMV: uniform [0, 1) FP32."""
+    return np.random.default_rng(7).random(n, dtype=np.float32)
+
+
+def ppr_seeds(n: int) -> np.ndarray:
+    """The 64 one-hot teleport vertices of the k=64 personalised PageRank."""
+    return np.random.default_rng(5).integers(0, n, 64).astype(np.uint32)
+
+
+def multi_sources(n: int) -> np.ndarray:
+    """The 64 sources of the multi-source BFS / BC."""
+    return np.random.default_rng(105).integers(0, n, 64).astype(np.uint32)
+
+
+def many_graph_shapes(count: int = 1024):
+    """(scale, edge factor) of each graph of the many-graph BFS."""
+    rng = np.random.default_rng(11)
+    return rng.integers(10, 17, count), rng.integers(8, 33, count)
+
+
+def adjoint_inputs(n: int, m: int):
+    """Weighted PageRank adjoint: edge weights U(0,1] (normalised per source
+    inside the function), teleport 1/n, loss weights N(0,1)."""
+    rng = np.random.default_rng(6)
+    w = rng.uniform(0, 1, m).astype(np.float32)
+    w[w == 0] = 0.5
+    c = rng.standard_normal(n).astype(np.float32)
+    return w, np.full(n, 1.0 / n, np.float32), c
+
+
 def aggregate_ranks(dist, dev_ms, wall_s, edges, launches, device="cuda"):
     """Whole-job figures of N replicas: the slowest rank's device and wall
     times (max over ranks), the edges and kernel launches of all ranks (sum)."""
@@ -179,7 +220,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
         f"{info.num_coo_tiles} COO tiles, {info.num_csc_tiles} CSC tiles")
     n, m = hg.n, hg.m
     x = gg.PinnedArray(n, np.float32)
-    x.array[:] = np.random.default_rng(7).random(n, dtype=np.float32)
+    x.array[:] = spmv_input(n)
     par = gg.PinnedArray(n, np.int32)
     ranks, y = gg.PinnedArray(n, np.float32), gg.PinnedArray(n, np.float32)
 
@@ -313,9 +354,9 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
         "warmup": args.warmup, "ms_per_step": round(dev_ms / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 (PageRank/SpMV), u32 (BFS ids)",
         "data": "synthetic: seeded RMAT generated on the host (no dataset)",
-        "config": {"workload": workload(args.scale, args.partitions, args.start), "n": n, "m": m,
-                   "partitions": args.partitions,
-                   "dense_policy": ["reference rule", "csc pull", "coo pull"][args.dense_policy],
+        "config": common_config(args, n, m),
+        "parallelism": "replicas" if world > 1 else "single GPU",
+        "engine": {"dense_policy": ["reference rule", "csc pull", "coo pull"][args.dense_policy],
                    "tile_edges": args.tile_edges,
                    "pagerank_loop": {"graph": "iterations replayed as one CUDA graph",
                                      "host": "one host round trip per iteration"}[args.pr_loop],
@@ -324,9 +365,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
                                      "wait": "each call returns after its copy"}[args.copies],
                    "vertex_order": ["given ids", "hottest sources first inside each partition (results in the "
                                     "given ids)"][args.vertex_order],
-                   "autotuned_knobs": knobs or None, "autotune_seconds": round(tune_s, 2),
-                   "l2": "inputs larger than L2 (graph arrays > 3 GB vs 126 MB L2)",
-                   "parallelism": "replicas" if world > 1 else "single GPU"},
+                   "autotuned_knobs": knobs or None, "autotune_seconds": round(tune_s, 2)},
         "apps": {k: {"edges": int(v[0]), "ms": round(v[1] / args.steps, 4),
                      "gteps": round(v[0] / (v[1] / 1e3) / 1e9, 4) if v[1] else None} for k, v in per_app.items()},
         "roofline": {"bound": "hbm", "kernel": f"{kernel_name} (PageRank dense pull)",
@@ -348,6 +387,11 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
     }
     if world == 1 and not args.no_stress:
         out["other_apps"] = run_other_apps(gg, hg, g, args)
+    if world == 1 and not args.no_cpu_baseline:
+        g.close()
+        per_step = {"BFS": per_app["bfs"][0] // args.steps, "PR": per_app["pagerank"][0] // args.steps,
+                    "SPMV": per_app["spmv"][0] // args.steps}
+        out["cpu_baseline"] = cpu_baseline_for_ours(args, hg, per_step)
     return out
 
 
@@ -389,7 +433,7 @@ def run_batched(gg):
     hg = gg.HostGraph.rmat(22, 16, 0.57, 0.19, 0.19, seed=5, symmetric=False)
     g = gg.Graph(hg, partitions=96)
     m = hg.m
-    seeds = rng.integers(0, hg.n, 64).astype(np.uint32)
+    seeds = ppr_seeds(hg.n)
     o64 = np.empty((hg.n, 64), np.float32)
     o1 = np.empty((hg.n, 1), np.float32)
     g.ppr_k(64, 20, 0.85, seeds=seeds, out=o64)
@@ -404,7 +448,7 @@ def run_batched(gg):
                       "batched_ms": round(k64, 3), "batched_gteps": round(64 * 20 * m / k64 / 1e6, 2),
                       "plain_64x_ms": round(plain, 3), "plain_gteps": round(64 * 20 * m / plain / 1e6, 2),
                       "speedup": round(plain / k64, 2), "max_rel_l1_vs_plain_cols0_3": max(diffs)}
-    src = rng.integers(0, hg.n, 64).astype(np.uint32)
+    src = multi_sources(hg.n)
     lev = np.empty((hg.n, 64), np.int32)
     g.msbfs(src, out=lev)
     r = g.msbfs(src, out=lev)[1]
@@ -423,7 +467,7 @@ def run_batched(gg):
     g.close()
     # 1,024 independent graphs in one persistent launch
     count = 1024
-    scales, efs = rng.integers(10, 17, count), rng.integers(8, 33, count)
+    scales, efs = many_graph_shapes(count)
     hgs = [gg.HostGraph.rmat(int(sc), int(ef), 0.57, 0.19, 0.19, seed=1000 + i, symmetric=False)
            for i, (sc, ef) in enumerate(zip(scales, efs))]
     b = gg.GraphBatch(hgs)
@@ -452,10 +496,7 @@ def run_batched(gg):
     # weighted PageRank adjoint
     hw = gg.HostGraph.rmat(22, 16, 0.57, 0.19, 0.19, seed=6, symmetric=False)
     gw = gg.Graph(hw, partitions=96)
-    w = rng.uniform(0, 1, hw.m).astype(np.float32)
-    w[w == 0] = 0.5
-    tele = np.full(hw.n, 1.0 / hw.n, np.float32)
-    c = rng.standard_normal(hw.n).astype(np.float32)
+    w, tele, c = adjoint_inputs(hw.n, hw.m)
     wpr = gg.WeightedPageRank(gw, 30, 0.85, 5, True)
     wpr.forward(w, tele)
     wpr.backward(c)
@@ -523,33 +564,50 @@ def run_stress(gg):
 
 
 # ------------------------------------------------------- the reference (CPU)
-def reference_sample(scale: int, partitions: int, rounds: int, workdir: str):
-    """Time the reference's own BFS, PageRank and SPMV (OpenMP build of
-    GraphGrind, oracle/_ref) on an RMAT sample of the workload.  Returns
-    (per-round GTEPS list, info dict)."""
-    import graphgrind_b200 as gg
+REF_APPS = ("BFS", "PR", "SPMV")
+REF_SPMV_WEIGHTS = ("SpMV reads uint32 weights U[1,100] (hash seed 102) where the GPU reads FP32 U(0,1]: the "
+                    "reference takes integer weights only (graphgrind/graph-numa.h:78-89)")
+
+
+def common_config(args, n: int, m: int) -> dict:
+    """The workload block both arms print: same graph, partitions and step."""
+    return {"workload": workload(args.scale, args.partitions, args.start), "n": n, "m": m,
+            "partitions": args.partitions, "start": args.start, "pagerank_iterations": 10,
+            "l2": "inputs larger than L2 (graph arrays > 3 GB vs 126 MB L2)"}
+
+
+def reference_inputs(workdir: str, scale: int, start: int):
+    """The step's graph and its edge counts from the oracle alone (no library
+    of the product is loaded): R-MAT `scale`, seed 2, directed, written as
+    Galois .gr (+ _t) unweighted for BFS/PageRank and with uint32 weights for
+    SpMV; traversed edges per application as the library counts them
+    (graphgrind/ligra-numa.h:944-945)."""
     import oracle
 
-    for app in ("BFS", "PR", "SPMV"):
+    r = oracle.RmatGraph(scale, 16, 0.57, 0.19, 0.19, seed=2, symmetric=False)
+    pu, pw = os.path.join(workdir, "g.gr"), os.path.join(workdir, "gw.gr")
+    r.write_gr(pu)
+    og = oracle.Graph(r.offsets, r.indices)
+    _, _, bst = og.bfs(start)
+    pr_edges, _ = og.pagerank_edges(10)
+    del og
+    r.add_weights(False, seed=102, lo=1, hi=100)
+    r.write_gr(pw)
+    return r.n, r.m, {"BFS": bst.edges_traversed, "PR": pr_edges, "SPMV": r.m}, {"BFS": pu, "PR": pu, "SPMV": pw}
+
+
+def time_reference(paths: dict, partitions: int, start: int, rounds: int, threads=None) -> dict:
+    """The reference's own driver (parallel_main, graphgrind/ligra-numa.h:1095)
+    on each file: its 'Running : t' seconds per round (Compute only, graph
+    load and partition build excluded, :1150-1161)."""
+    import oracle
+
+    for app in REF_APPS:
         if not oracle.ref_available(app):
             raise RuntimeError(f"reference binary {oracle.ref_binary(app)} not built")
-    hg = make_graph(gg, scale, 5, gg.W_NONE)
-    hw = make_graph(gg, scale, 5, gg.W_INT32)
-    pu, pw = os.path.join(workdir, "g.gr"), os.path.join(workdir, "gw.gr")
-    hg.write_gr(pu)
-    hw.write_gr(pw)
-    og = oracle.Graph.from_host(hg)
-    _, _, bst = og.bfs(100)
-    _, pst = og.pagerank(10)
-    edges = {"BFS": bst.edges_traversed, "PR": pst.edges_traversed, "SPMV": hw.m}
-    times = {}
-    for app, path in (("BFS", pu), ("PR", pu), ("SPMV", pw)):
-        times[app] = oracle.time_ref(app, path, ["-b", "-c", str(partitions), "-r", "100"], rounds=rounds)
-    per_round = [sum(edges.values()) / sum(times[a][r] for a in times) / 1e9 for r in range(rounds)]
-    info = {"n": hg.n, "m": hg.m, "edges_per_step": sum(edges.values()),
-            "seconds_per_step": [round(sum(times[a][r] for a in times), 5) for r in range(rounds)],
-            "apps_s": {a: [round(t, 5) for t in v] for a, v in times.items()}}
-    return per_round, info
+    flags = ["-b", "-c", str(partitions), "-r", str(start)]
+    return {app: oracle.time_ref(app, paths[app], flags, rounds=rounds, threads=threads, timeout=1800)
+            for app in REF_APPS}
 
 
 def cpu_model():
@@ -562,42 +620,67 @@ def cpu_model():
     return "unknown"
 
 
+def _per_round(edges: dict, times: dict, first: int):
+    secs = [sum(times[a][r] for a in REF_APPS) for r in range(first, len(times[REF_APPS[0]]))]
+    return secs, sum(edges.values()) * len(secs) / sum(secs) / 1e9
+
+
 def run_reference_arm(args):
+    """bench.py --impl reference: GraphGrind's own OpenMP build (oracle/_ref,
+    compiled from the reference's sources) on this host's cores, on the same
+    graph file, partitions and step as the GPU arm; W warm-up rounds, then K
+    timed rounds of each application.  This process loads only the oracle."""
     cores = os.cpu_count() or 1
-    sample = f"RMAT-{args.ref_scale} directed, same generator parameters (seed 5), -b -c {args.ref_partitions}"
-    base = {"impl": "reference", "metric": METRIC, "unit": UNIT, "higher_is_better": True, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64 (PageRank/SpMV), int64 (BFS ids)", "data": "synthetic: seeded RMAT",
-            "config": {"workload": WORKLOAD, "sample": sample, "parallelism": "host cores (OpenMP)"}}
     try:
         with tempfile.TemporaryDirectory() as d:
-            per_round, info = reference_sample(args.ref_scale, args.ref_partitions, args.warmup + args.steps, d)
+            n, m, edges, paths = reference_inputs(d, args.scale, args.start)
+            times = time_reference(paths, args.partitions, args.start, args.warmup + args.steps)
+            one = None
+            if not args.no_one_thread:
+                t1 = time_reference(paths, args.partitions, args.start, 1, threads=1)
+                one = {"value": round(_per_round(edges, t1, 0)[1], 4), "unit": UNIT, "cores": 1,
+                       "sample": "one round of each application, OMP_NUM_THREADS=1",
+                       "seconds": {a: round(t1[a][0], 4) for a in REF_APPS}}
     except Exception as e:
         print(json.dumps({"impl": "reference", "unavailable": f"reference build/run failed: {e}"[:300]}))
         return
-    timed = per_round[args.warmup:]
-    secs = info["seconds_per_step"][args.warmup:]
-    value = info["edges_per_step"] * len(secs) / sum(secs) / 1e9
-    base.update({"value": round(value, 4), "ms_per_step": round(1e3 * sum(secs) / len(secs), 3),
-                 "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": cores, "kind": "reference",
-                                  "cpu": cpu_model(), "sample": sample + f"; {info['edges_per_step']} edges per step",
-                                  "per_round_gteps": [round(v, 4) for v in timed]},
-                 "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-                 "reference_detail": info})
-    print(json.dumps(base))
+    secs, value = _per_round(edges, times, args.warmup)
+    sample = (f"the GPU arm's graph (R-MAT-{args.scale} seed 2, directed) as Galois .gr, -b -c {args.partitions} "
+              f"-r {args.start}; {args.steps} timed rounds after {args.warmup} warm-up; {REF_SPMV_WEIGHTS}")
+    out = {"impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * sum(secs) / len(secs), 3),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64 (PageRank/SpMV), int64 (BFS ids)", "data": "synthetic: seeded RMAT (no dataset)",
+           "config": common_config(args, n, m), "parallelism": f"host cores (OpenMP, {cores} threads)",
+           "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": cores, "kind": "reference",
+                            "cpu": cpu_model(), "sample": sample},
+           "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "one_thread": one,
+           "reference_detail": {"edges_per_step": sum(edges.values()), "edges": edges,
+                                "seconds_per_round": {a: [round(t, 5) for t in times[a]] for a in REF_APPS}}}
+    print(json.dumps(out))
 
 
-def cpu_baseline_for_ours(args):
+def cpu_baseline_for_ours(args, hg, edges: dict):
+    """The reference's own build on the GPU arm's graph (written from the same
+    host CSR), 3 rounds of each application, the first dropped."""
+    import graphgrind_b200 as gg
+
     cores = os.cpu_count() or 1
-    sample = f"RMAT-{args.ref_scale} directed sample (seed 5), reference OpenMP build, -b -c {args.ref_partitions}"
+    sample = (f"the same graph as Galois .gr, reference OpenMP build, -b -c {args.partitions} -r {args.start}; "
+              f"mean of 2 rounds after 1 warm-up; {REF_SPMV_WEIGHTS}")
     try:
         with tempfile.TemporaryDirectory() as d:
-            per_round, info = reference_sample(args.ref_scale, args.ref_partitions, 3, d)
-        secs = info["seconds_per_step"][1:]
-        value = info["edges_per_step"] * len(secs) / sum(secs) / 1e9
+            pu, pw = os.path.join(d, "g.gr"), os.path.join(d, "gw.gr")
+            gu = gg.HostGraph.from_csr(hg.offsets, hg.indices, None, symmetric=False)
+            gu.write_gr(pu)
+            gu.add_weights(gg.W_INT32, seed=102, lo=1, hi=100)
+            gu.write_gr(pw)
+            del gu
+            times = time_reference({"BFS": pu, "PR": pu, "SPMV": pw}, args.partitions, args.start, 3)
+        _, value = _per_round(edges, times, 1)
         return {"value": round(value, 4), "unit": UNIT, "cores": cores, "kind": "reference", "cpu": cpu_model(),
-                "sample": sample + f"; BFS+PageRank(10)+SPMV, {info['edges_per_step']} edges per step, "
-                                   f"mean of 2 rounds after 1 warm-up"}
+                "sample": sample}
     except Exception as e:
         return {"value": None, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample,
                 "error": str(e)[:200]}
@@ -613,8 +696,8 @@ def main():
     ap.add_argument("--partitions", type=int, default=384)
     ap.add_argument("--start", type=int, default=100)
     ap.add_argument("--dense-policy", type=int, default=0, help="0 reference rule, 1 CSC pull, 2 COO pull")
-    ap.add_argument("--ref-scale", type=int, default=22)
-    ap.add_argument("--ref-partitions", type=int, default=256)
+    ap.add_argument("--no-one-thread", action="store_true",
+                    help="reference arm: skip the one-thread round of each application")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched / adjoint comparisons")
     ap.add_argument("--no-autotune", action="store_true", help="keep the library's default runtime knobs")
@@ -652,8 +735,6 @@ def main():
         dist = tdist
     out = run_ours(args, rank, world, local_rank, dist)
     if rank == 0:
-        if world == 1 and not args.no_cpu_baseline:
-            out["cpu_baseline"] = cpu_baseline_for_ours(args)
         if world == 1 and not args.no_batched:
             import graphgrind_b200 as gg
             try:

@@ -33,6 +33,8 @@ ERRORS = {
     -1: "INVALID_ARG", -2: "CUDA", -3: "OOM", -4: "PARTITION", -5: "IO", -6: "FORMAT",
     -7: "NO_DEVICE", -8: "UNSUPPORTED", -9: "TIMEOUT", -10: "SIZE",
 }
+ERR_INVALID_ARG, ERR_CUDA, ERR_OOM, ERR_PARTITION, ERR_IO, ERR_FORMAT = -1, -2, -3, -4, -5, -6
+ERR_NO_DEVICE, ERR_UNSUPPORTED, ERR_TIMEOUT, ERR_SIZE = -7, -8, -9, -10
 W_NONE, W_INT32, W_FLOAT32 = 0, 1, 2
 BALANCE_EDGE, BALANCE_VERTEX = 0, 1
 PART_DEST, PART_SOURCE = 0, 1
@@ -139,6 +141,7 @@ _sig("gg_host_graph_read", C.c_int, C.c_char_p, C.c_int32, C.c_int32, C.c_int32,
 _sig("gg_host_graph_transpose", C.c_int, C.POINTER(HostGraphC), C.POINTER(HostGraphC))
 _sig("gg_host_graph_free", None, C.POINTER(HostGraphC))
 _sig("gg_vebo", C.c_int, C.POINTER(HostGraphC), C.c_int32, _P, _P, C.POINTER(HostGraphC))
+_sig("gg_vebo_gpu", C.c_int, C.POINTER(HostGraphC), C.c_int32, _P, _P, C.POINTER(HostGraphC))
 _sig("gg_partition_sizes", C.c_int, _u32p, _u32p, C.c_uint32, C.c_uint64, C.c_int32, C.c_int32, C.c_int32,
      C.c_int32, _i64p, _i64p)
 _sig("gg_hilbert_key", C.c_int64, C.c_int64, C.c_int64, C.c_int64)
@@ -153,6 +156,8 @@ _sig("gg_graph_partition_starts", C.c_int, _P, _i64p)
 _sig("gg_graph_transpose", C.c_int, _P)
 _sig("gg_graph_device_arrays", C.c_int, _P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), C.POINTER(_P))
 _sig("gg_graph_vertex_order", C.c_int, _P, _P)
+_sig("gg_graph_device_weights", C.c_int, _P, C.POINTER(_P), C.POINTER(_P))
+_sig("gg_graph_coo_layout", C.c_int, _P, C.POINTER(C.c_uint64), _P, C.POINTER(C.c_uint64), _P, _P)
 _sig("gg_frontier_single", C.c_int, _P, C.c_uint32, C.POINTER(_P))
 _sig("gg_frontier_all", C.c_int, _P, C.POINTER(_P))
 _sig("gg_frontier_empty", C.c_int, _P, C.POINTER(_P))
@@ -173,6 +178,7 @@ _sig("gg_graph_set_tuning", C.c_int, _P, C.c_int32, C.c_int64)
 _sig("gg_graph_get_tuning", C.c_int, _P, C.c_int32, C.POINTER(C.c_int64))
 TUNE_DENSE_POLICY, TUNE_COO_KERNEL, TUNE_SPARSE_DIV, TUNE_DEVICE_LOOP, TUNE_CC_ALGO, TUNE_PR_GRAPH = 1, 2, 3, 4, 5, 6
 TUNE_ASYNC_RESULTS = 7
+TUNE_LOOP_WAIT_BUDGET = 8
 APP_BFS, APP_COMPONENTS, APP_PAGERANK, APP_PAGERANK_DELTA, APP_SPMV, APP_BELLMAN_FORD, APP_BC = range(1, 8)
 _sig("gg_vertex_map", C.c_int, _P, _P, C.c_int32, _P)
 _sig("gg_vertex_filter", C.c_int, _P, _P, C.c_int32, _P, C.POINTER(_P))
@@ -225,7 +231,8 @@ EXPORTED = [
     "gg_batch_create", "gg_batch_destroy", "gg_batch_info", "gg_batch_bfs",
     "gg_pagerank_weighted_create", "gg_pagerank_weighted_destroy", "gg_pagerank_weighted_fwd",
     "gg_pagerank_weighted_bwd", "gg_autotune", "gg_autotune_build", "gg_autotune_ppr_k",
-    "gg_hot_first_order", "gg_graph_vertex_order", "gg_host_graph_read_gpu",
+    "gg_hot_first_order", "gg_graph_vertex_order", "gg_host_graph_read_gpu", "gg_graph_device_weights",
+    "gg_graph_coo_layout", "gg_vebo_gpu",
 ]
 
 
@@ -372,6 +379,14 @@ class HostGraph:
         new_of_old = np.empty(self.n, np.uint32)
         sizes = np.empty(partitions, np.int64)
         check(lib.gg_vebo(C.byref(self.c), partitions, _ptr(new_of_old), _ptr(sizes), C.byref(t)), "gg_vebo")
+        return HostGraph(t), new_of_old, sizes
+
+    def vebo_gpu(self, partitions=384):
+        """gg_vebo_gpu: vebo() computed on the GPU, the same result."""
+        t = HostGraphC()
+        new_of_old = np.empty(self.n, np.uint32)
+        sizes = np.empty(partitions, np.int64)
+        check(lib.gg_vebo_gpu(C.byref(self.c), partitions, _ptr(new_of_old), _ptr(sizes), C.byref(t)), "gg_vebo_gpu")
         return HostGraph(t), new_of_old, sizes
 
 
@@ -527,6 +542,19 @@ class Graph:
         s = np.zeros(P + 1, np.int64)
         check(lib.gg_graph_partition_starts(self.h, s.ctypes.data_as(_i64p)), "gg_graph_partition_starts")
         return s
+
+    def coo_layout(self):
+        """The device COO (gg_graph_coo_layout): (tiles[T, 4] {first vertex,
+        vertices, first slot, slots} in work order, src[slots], dst[slots];
+        padding slots hold 0xffffffff)."""
+        nt, ln = C.c_uint64(), C.c_uint64()
+        check(lib.gg_graph_coo_layout(self.h, C.byref(nt), None, C.byref(ln), None, None), "gg_graph_coo_layout")
+        tiles = np.empty((max(nt.value, 1), 4), np.uint32)
+        src = np.empty(max(ln.value, 1), np.uint32)
+        dst = np.empty(max(ln.value, 1), np.uint32)
+        check(lib.gg_graph_coo_layout(self.h, C.byref(nt), _ptr(tiles), C.byref(ln), _ptr(src), _ptr(dst)),
+              "gg_graph_coo_layout")
+        return tiles[:nt.value], src[:ln.value], dst[:ln.value]
 
     def vertex_order(self) -> np.ndarray:
         """new_of_old[n]: the device id of every given vertex (gg_graph_vertex_order)."""

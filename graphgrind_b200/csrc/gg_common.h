@@ -4,6 +4,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/gg.h"
@@ -31,6 +32,12 @@ int relabel_host_graph(const gg_host_graph* g, const uint32_t* old_of_new, const
 // descending out-degree, ties by id.  starts has P+1 ascending entries, 0 .. n.
 void hot_first_order(const gg_host_graph* g, const int64_t* starts, int32_t P, uint32_t* old_of_new,
                      uint32_t* new_of_old);
+
+// The deal of VEBO over runs of equal in-degree (degree, vertices) of the
+// vertices sorted by (in-degree descending, id): perDeg[p * runs + i] and
+// vsize[p]; GG_ERR_PARTITION where the reference's zero-degree fill breaks.
+int vebo_deal(const std::vector<std::pair<int64_t, int64_t>>& runs, int64_t n, int64_t P, std::vector<int64_t>& perDeg,
+              std::vector<int64_t>& vsize);
 
 inline uint64_t mix64(uint64_t z) {
   // SplitMix64 output function (Steele, Lea & Flood, OOPSLA 2014).

@@ -147,6 +147,7 @@ struct gg_graph_s {
   int sparse_div = 20;  // the apps' edgeMap threshold is m / sparse_div (app/*.C pass m/20)
   int device_loop = 1;  // BFS runs consecutive sparse levels in one cooperative launch
   int cc_algo = 0;      // Components on symmetric graphs: 0 label propagation, 1 union-find
+  uint32_t loop_wait_budget = 1u << 22;  // spins of the BFS level loop's grid-barrier wait
   int pr_graph = 1;     // PageRank iterations replayed as one CUDA graph (0: one host round trip per iteration)
   // GG_TUNE_ASYNC_RESULTS: results bound for pinned host memory leave from the
   // given-order arrays on copy_stream, and the call returns without waiting

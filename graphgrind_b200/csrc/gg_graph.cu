@@ -822,6 +822,59 @@ int gg_graph_partition_starts(gg_graph_t g, int64_t* starts) {
   return GG_OK;
 }
 
+namespace gg {
+__global__ void k_coo_unpack(const uint4* tiles, uint32_t ntiles, const uint32_t* src, const uint16_t* dloc,
+                             uint32_t* out_src, uint32_t* out_dst) {
+  for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const uint4 tl = tiles[t];  // {v0, nv, first slot, padded edge count}
+    for (uint32_t i = threadIdx.x; i < tl.w; i += blockDim.x) {
+      const uint32_t s = src[tl.z + i];
+      out_src[tl.z + i] = s;
+      out_dst[tl.z + i] = s == 0xffffffffu ? 0xffffffffu : tl.x + dloc[tl.z + i];
+    }
+  }
+}
+}  // namespace gg
+
+int gg_graph_coo_layout(gg_graph_t g, uint64_t* num_tiles, uint32_t* tiles, uint64_t* coo_len, uint32_t* src,
+                        uint32_t* dst) {
+  if (!graph_live(g) || !num_tiles || !coo_len)
+    return fail(GG_ERR_INVALID_ARG, "gg_graph_coo_layout: bad arguments");
+  if (!g->has_coo) return fail(GG_ERR_UNSUPPORTED, "gg_graph_coo_layout: the graph has no partitioned COO");
+  std::vector<uint4> tl;
+  if (g->coo_by_source) {
+    const int P = (int)g->coo_sizes.size();
+    for (int p = 0; p < P; ++p) {
+      const uint32_t a = (uint32_t)g->coo_starts[p], b = (uint32_t)g->coo_starts[p + 1];
+      tl.push_back(make_uint4(a, b - a, g->h_csr_off[a], g->h_csr_off[b] - g->h_csr_off[a]));
+    }
+  } else {
+    tl = g->coo_tiles.host;
+  }
+  *num_tiles = tl.size();
+  *coo_len = g->coo_len;
+  if (tiles) memcpy(tiles, tl.data(), sizeof(uint4) * tl.size());
+  if (!src && !dst) return GG_OK;
+  if (!src || !dst) return fail(GG_ERR_INVALID_ARG, "gg_graph_coo_layout: give both src and dst");
+  if (g->coo_by_source) {
+    GG_CUDA(cudaMemcpy(src, g->d_coo_src, 4 * g->coo_len, cudaMemcpyDeviceToHost));
+    GG_CUDA(cudaMemcpy(dst, g->d_coo_dst, 4 * g->coo_len, cudaMemcpyDeviceToHost));
+    return GG_OK;
+  }
+  DevBuf<uint32_t> ds, dd;
+  GG_TRY(ds.alloc(g, g->coo_len + 1));
+  GG_TRY(dd.alloc(g, g->coo_len + 1));
+  if (!tl.empty()) {
+    k_coo_unpack<<<g->num_sms * 4, 256, 0, g->stream>>>(g->coo_tiles.d_tiles, (uint32_t)tl.size(), g->d_coo_src,
+                                                         g->d_coo_dloc, ds.p, dd.p);
+    GG_CUDA(cudaGetLastError());
+  }
+  GG_CUDA(cudaStreamSynchronize(g->stream));
+  GG_CUDA(cudaMemcpy(src, ds.p, 4 * g->coo_len, cudaMemcpyDeviceToHost));
+  GG_CUDA(cudaMemcpy(dst, dd.p, 4 * g->coo_len, cudaMemcpyDeviceToHost));
+  return GG_OK;
+}
+
 int gg_graph_set_profiling(gg_graph_t g, int32_t enable) {
   if (!g) return fail(GG_ERR_INVALID_ARG, "gg_graph_set_profiling: null graph");
   if (enable && !g->prof_ev[0]) {
@@ -870,6 +923,11 @@ int gg_graph_set_tuning(gg_graph_t g, int32_t key, int64_t value) {
       if (value != 0 && value != 1) return fail(GG_ERR_INVALID_ARG, "PageRank graph switch must be 0 or 1");
       g->pr_graph = (int)value;
       return GG_OK;
+    case GG_TUNE_LOOP_WAIT_BUDGET:
+      if (value < 0 || value > (1ll << 22))
+        return fail(GG_ERR_INVALID_ARG, "loop wait budget must be 0..2^22 spins");
+      g->loop_wait_budget = (uint32_t)value;
+      return GG_OK;
     case GG_TUNE_ASYNC_RESULTS:
       if (value != 0 && value != 1) return fail(GG_ERR_INVALID_ARG, "asynchronous results switch must be 0 or 1");
       if (value && !g->copy_stream) {
@@ -911,6 +969,9 @@ int gg_graph_get_tuning(gg_graph_t g, int32_t key, int64_t* value) {
     case GG_TUNE_ASYNC_RESULTS:
       *value = g->async_results;
       return GG_OK;
+    case GG_TUNE_LOOP_WAIT_BUDGET:
+      *value = g->loop_wait_budget;
+      return GG_OK;
     default:
       return fail(GG_ERR_INVALID_ARG, "unknown tuning key %d", key);
   }
@@ -935,6 +996,13 @@ int gg_graph_device_arrays(gg_graph_t g, const uint32_t** oo, const uint32_t** o
   if (oi) *oi = g->out_idx();
   if (io) *io = g->in_off();
   if (ii) *ii = g->in_idx();
+  return GG_OK;
+}
+
+int gg_graph_device_weights(gg_graph_t g, const void** out_w, const void** in_w) {
+  if (!graph_live(g)) return fail(GG_ERR_INVALID_ARG, "gg_graph_device_weights: not a live graph");
+  if (out_w) *out_w = g->wtype == GG_W_NONE ? nullptr : g->out_w();
+  if (in_w) *in_w = g->wtype == GG_W_NONE ? nullptr : g->in_w();
   return GG_OK;
 }
 

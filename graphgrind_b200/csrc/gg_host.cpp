@@ -190,6 +190,81 @@ void hot_first_order(const gg_host_graph* g, const int64_t* starts, int32_t P, u
 
 }  // namespace gg
 
+namespace gg {
+// The deal of VEBO (graphtools/VEBO.C:180-262) over the runs of equal
+// in-degree of the vertices sorted by (in-degree descending, id): runs[i] =
+// (degree, vertices).  Fills perDeg[p * runs + i] (vertices of run i dealt to
+// partition p) and vsize[p].  Zero-degree vertices are not dealt with their
+// run (only the first vertex counts when every degree is zero, as in the
+// reference's group counting) but by the fill that evens out vertex counts.
+int vebo_deal(const std::vector<std::pair<int64_t, int64_t>>& runs, int64_t n, int64_t P, std::vector<int64_t>& perDeg,
+              std::vector<int64_t>& vsize) {
+  const int64_t c = (int64_t)runs.size();
+  int64_t czero = 0, zgrp = 0;
+  std::vector<std::pair<int64_t, int64_t>> perGroup(c, {0, 0});  // (count, degree)
+  for (int64_t a = 0; a < c; a++) {
+    const int64_t deg = runs[a].first, cnt = runs[a].second;
+    if (deg == 0) {
+      czero = cnt;
+      zgrp = a;
+    }
+    perGroup[a].first = deg != 0 ? cnt : (a == 0 ? 1 : 0);
+    if (perGroup[a].first) perGroup[a].second = deg;
+  }
+  std::vector<int64_t> edges(P, 0);
+  vsize.assign(P, 0);
+  perDeg.assign((size_t)P * c, 0);  // [partition][group]
+  auto deal = [&](int64_t p, int64_t grp, int64_t deg, int64_t cnt) {
+    edges[p] += deg * cnt;
+    perDeg[(size_t)p * c + grp] += cnt;
+    vsize[p] += cnt;
+  };
+  for (int64_t i = 0; i < c; i++) {
+    const int64_t deg = perGroup[i].second, same = perGroup[i].first;
+    for (int64_t k = 0; k < same;) {
+      int64_t mx = edges[0], mn = edges[0], mnp = 0;
+      for (int64_t j = 1; j < P; j++) {
+        if (edges[j] < mn) {
+          mn = edges[j];
+          mnp = j;
+        }
+        if (edges[j] > mx) mx = edges[j];
+      }
+      const int64_t remain = (same - k) / P;
+      const int64_t take = (mx - mn > deg && remain > 1) ? remain : 1;
+      deal(mnp, i, deg, take);
+      k += take;
+    }
+  }
+  // zero-degree vertices even out the vertex counts
+  const int64_t avg = n / P, extra = n % P;
+  if (extra == 0 || czero / P != 0) {
+    for (int64_t p = 0; p < P; p++)
+      if (vsize[p] < avg) deal(p, zgrp, 0, avg - vsize[p]);
+    if (extra != 0)
+      for (int64_t p = 0; p < extra; p++) deal(p, zgrp, 0, 1);
+  } else {
+    for (int64_t z = 0; z < czero; z++) {
+      int64_t mn = vsize[0], mnp = 0;
+      for (int64_t p = 1; p < P; p++)
+        if (vsize[p] < mn) {
+          mn = vsize[p];
+          mnp = p;
+        }
+      deal(mnp, zgrp, 0, 1);
+    }
+  }
+  int64_t total = 0;
+  for (int64_t p = 0; p < P; p++) total += vsize[p];
+  if (total != n)
+    return fail(GG_ERR_PARTITION,
+                "gg_vebo: the zero-degree fill places %lld vertices for n=%lld (P=%lld); the reference reads past "
+                "its vertex list here",
+                (long long)total, (long long)n, (long long)P);
+  return GG_OK;
+}
+}  // namespace gg
+
 using namespace gg;
 
 extern "C" {
@@ -678,72 +753,15 @@ int gg_vebo(const gg_host_graph* g, int32_t partitions, uint32_t* new_of_old, in
   std::sort(check.begin(), check.end(), [](const std::pair<int64_t, int64_t>& a, const std::pair<int64_t, int64_t>& b) {
     return a.second > b.second || (a.second == b.second && a.first < b.first);
   });
-  // degree groups: group index of each degree, (count, degree) per group (zero-degree vertices not counted)
-  int64_t c = 1, czero = 0;
-  for (int64_t i = 1; i < n; i++)
-    if (check[i].second != check[i - 1].second) c++;
-  for (int64_t i = 0; i < n; i++)
-    if (check[i].second == 0) czero++;
-  std::vector<int64_t> groupOf((size_t)check[0].second + 1, 0);
-  std::vector<std::pair<int64_t, int64_t>> perGroup(c, {0, 0});
-  int64_t a = 0;
+  // runs of equal degree in the sorted order
+  std::vector<std::pair<int64_t, int64_t>> runs;  // (degree, vertices)
   for (int64_t i = 0; i < n; i++) {
-    if (i > 0 && check[i].second != check[i - 1].second) a++;
-    groupOf[check[i].second] = a;
-    if (i == 0 || check[i].second != 0) {
-      perGroup[a].first++;
-      perGroup[a].second = check[i].second;
-    }
+    if (i == 0 || check[i].second != check[i - 1].second) runs.push_back({check[i].second, 0});
+    runs.back().second++;
   }
-  std::vector<int64_t> edges(P, 0), vsize(P, 0);
-  std::vector<int64_t> perDeg((size_t)P * c, 0);  // [partition][group]
-  auto deal = [&](int64_t p, int64_t grp, int64_t deg, int64_t cnt) {
-    edges[p] += deg * cnt;
-    perDeg[(size_t)p * c + grp] += cnt;
-    vsize[p] += cnt;
-  };
-  for (int64_t i = 0; i < c; i++) {
-    const int64_t deg = perGroup[i].second, same = perGroup[i].first;
-    for (int64_t k = 0; k < same;) {
-      int64_t mx = edges[0], mn = edges[0], mnp = 0;
-      for (int64_t j = 1; j < P; j++) {
-        if (edges[j] < mn) {
-          mn = edges[j];
-          mnp = j;
-        }
-        if (edges[j] > mx) mx = edges[j];
-      }
-      const int64_t remain = (same - k) / P;
-      const int64_t take = (mx - mn > deg && remain > 1) ? remain : 1;
-      deal(mnp, groupOf[deg], deg, take);
-      k += take;
-    }
-  }
-  // zero-degree vertices even out the vertex counts
-  const int64_t avg = n / P, extra = n % P, zgrp = groupOf[0];
-  if (extra == 0 || czero / P != 0) {
-    for (int64_t p = 0; p < P; p++)
-      if (vsize[p] < avg) deal(p, zgrp, 0, avg - vsize[p]);
-    if (extra != 0)
-      for (int64_t p = 0; p < extra; p++) deal(p, zgrp, 0, 1);
-  } else {
-    for (int64_t z = 0; z < czero; z++) {
-      int64_t mn = vsize[0], mnp = 0;
-      for (int64_t p = 1; p < P; p++)
-        if (vsize[p] < mn) {
-          mn = vsize[p];
-          mnp = p;
-        }
-      deal(mnp, zgrp, 0, 1);
-    }
-  }
-  int64_t total = 0;
-  for (int64_t p = 0; p < P; p++) total += vsize[p];
-  if (total != n)
-    return fail(GG_ERR_PARTITION,
-                "gg_vebo: the zero-degree fill places %lld vertices for n=%lld (P=%d); the reference reads past "
-                "its vertex list here",
-                (long long)total, (long long)n, partitions);
+  std::vector<int64_t> perDeg, vsize;
+  GG_TRY_HOST(vebo_deal(runs, n, P, perDeg, vsize));
+  const int64_t c = (int64_t)runs.size();
   std::vector<int64_t> start(P, 0), fill(P, 0);
   for (int64_t p = 1; p < P; p++) start[p] = start[p - 1] + vsize[p - 1];
   std::vector<uint32_t> old_of_new(n);

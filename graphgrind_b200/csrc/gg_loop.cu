@@ -27,7 +27,6 @@ struct BfsLoopState {
   int32_t pad;
 };
 
-constexpr unsigned kBarrierSpin = 1u << 22;
 
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
   unsigned v;
@@ -41,15 +40,16 @@ __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long
   return v;
 }
 
-// All CTAs of the (co-resident) grid arrive; returns false if the wait ran out.
-__device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned target, int* s_ok) {
+// All CTAs of the (co-resident) grid arrive; returns false if the wait ran out
+// (more than `budget` probes of the arrival count, each followed by a short sleep).
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned target, unsigned budget, int* s_ok) {
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
     atomicAdd(bar, 1u);
     int ok = 1;
     for (unsigned it = 0; (int)(ld_acquire_u32(bar) - target) < 0; ++it) {
-      if (it > kBarrierSpin) {
+      if (it >= budget) {
         ok = 0;
         break;
       }
@@ -119,7 +119,8 @@ __global__ void __launch_bounds__(256) k_bfs_push_loop(const uint32_t* __restric
                                                        const uint32_t* __restrict__ idx, int32_t* parents,
                                                        int32_t* levels, uint32_t* q0, uint32_t* q1, uint32_t* eo0,
                                                        uint32_t* eo1, uint32_t n, BfsLoopState* st, int32_t round0,
-                                                       unsigned long long threshold, int32_t max_levels) {
+                                                       unsigned long long threshold, int32_t max_levels,
+                                                       unsigned wait_budget) {
   __shared__ uint32_t s_eo[257];
   __shared__ uint32_t s_v[256];
   __shared__ uint32_t s_beg[256];
@@ -199,7 +200,7 @@ __global__ void __launch_bounds__(256) k_bfs_push_loop(const uint32_t* __restric
       }
     }
     target += gridDim.x;
-    if (!grid_barrier(&st->bar, target, &s_ok)) {
+    if (!grid_barrier(&st->bar, target, wait_budget, &s_ok)) {
       if (tid == 0) atomicExch(&st->exit_reason, -1);
       return;
     }
@@ -210,14 +211,14 @@ __global__ void __launch_bounds__(256) k_bfs_push_loop(const uint32_t* __restric
     if (reason) {
       if (blockIdx.x == 0 && tid == 0) {
         st->levels_done = i + 1;
-        st->exit_reason = reason;
+        atomicCAS(&st->exit_reason, 0, reason);  // a timeout (-1) recorded by any CTA stays
       }
       return;
     }
   }
   if (blockIdx.x == 0 && tid == 0) {
     st->levels_done = max_levels;
-    st->exit_reason = 3;
+    atomicCAS(&st->exit_reason, 0, 3);
   }
 }
 
@@ -270,8 +271,9 @@ int bfs_device_levels(gg_graph_s* g, gg_frontier_s** F, int32_t* parents, int32_
   uint32_t nn = n;
   unsigned long long thr = threshold;
   int32_t cap = 1 << 20;
+  unsigned budget = g->loop_wait_budget;
   void* args[] = {(void*)&off, (void*)&idx, (void*)&parents, (void*)&levels, (void*)&q0, (void*)&q1, (void*)&e0,
-                  (void*)&e1, (void*)&nn, (void*)&d_st, (void*)&round0, (void*)&thr, (void*)&cap};
+                  (void*)&e1, (void*)&nn, (void*)&d_st, (void*)&round0, (void*)&thr, (void*)&cap, (void*)&budget};
   if (e == cudaSuccess)
     e = cudaLaunchCooperativeKernel((const void*)k_bfs_push_loop, grid, 256, args, 0, g->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(&h, d_st, sizeof(h), cudaMemcpyDeviceToHost, g->stream);

@@ -154,6 +154,14 @@ int gg_host_graph_read_gpu(const char* path, int32_t binary, int32_t symmetric,
  * zero-degree fill would place a different number of vertices than n. */
 int gg_vebo(const gg_host_graph* g, int32_t partitions, uint32_t* new_of_old, int64_t* part_sizes,
             gg_host_graph* out);
+/* gg_vebo computed on the GPU (the same arguments, result, bit for bit, and
+ * errors): the in-degree histogram, the (in-degree, id) sort, the runs of
+ * equal degree and the placement and relabelling run on the device; the deal
+ * of the runs to partitions, which depends on every earlier deal, runs on the
+ * host over the runs alone.  The host graph crosses to the device and back;
+ * needs a CUDA device, whose memory it takes is released on return. */
+int gg_vebo_gpu(const gg_host_graph* g, int32_t partitions, uint32_t* new_of_old, int64_t* part_sizes,
+                gg_host_graph* out);
 /* CSC (in-edges) of a host graph: in_offsets n+1, in_indices m, in_weights m. */
 int gg_host_graph_transpose(const gg_host_graph* g, gg_host_graph* out);
 void gg_host_graph_free(gg_host_graph* g);
@@ -196,6 +204,19 @@ int gg_graph_get_info(gg_graph_t g, gg_graph_info* info);
 /* Partition starts (P+1 entries) of the COO partitioner (partitioner::start_of,
  * graphgrind/partitioner.h:153-165). */
 int gg_graph_partition_starts(gg_graph_t g, int64_t* starts);
+/* The partitioned COO as the device holds it (COOPartitionByDest /
+ * COOPartitionBySour + hilbert_sort, graphgrind/graph-numa.h:482-490,
+ * 1116-1171), for inspection: *num_tiles CTA tiles in the order the
+ * persistent kernels take them, tiles[4 t .. 4 t + 3] = {first destination,
+ * destinations, first slot, slots} (for -P source: one entry per source
+ * partition, {first source, sources, first slot, edges}); src/dst[coo_len]
+ * the edge of every slot, 0xffffffff in the padding that rounds a tile up
+ * to 8 slots.  Inside a tile the edges follow the partition's Hilbert (or
+ * CSRDestSort) order at 256-slot granularity and go by destination inside
+ * each 256-slot window.  tiles, src and dst may be NULL (sizes only).
+ * GG_ERR_UNSUPPORTED for a graph without a COO (-v vertex). */
+int gg_graph_coo_layout(gg_graph_t g, uint64_t* num_tiles, uint32_t* tiles, uint64_t* coo_len, uint32_t* src,
+                        uint32_t* dst);
 /* partitioned_graph::transpose (graphgrind/graph-numa.h:721-728): swaps the
  * out/in roles of CSR and CSC for symmetric=0 graphs; the COO partitions are
  * NOT transposed, as in the reference. */
@@ -203,10 +224,17 @@ int gg_graph_transpose(gg_graph_t g);
 /* new_of_old[n]: the device id of every given vertex id (the identity unless
  * the graph was built with a vertex_order). */
 int gg_graph_vertex_order(gg_graph_t g, uint32_t* new_of_old);
-/* Out-degree of every vertex in the current orientation (device pointer). */
+/* Device CSR (out-edges) and CSC (in-edges) of the current orientation, in
+ * the device ids (the vertex array and neighbour lists that
+ * symmetricVertex/asymmetricVertex wrap, graphgrind/graph-numa.h:39-217);
+ * any output may be NULL.  Owned by the graph. */
 int gg_graph_device_arrays(gg_graph_t g, const uint32_t** out_offsets,
                            const uint32_t** out_indices, const uint32_t** in_offsets,
                            const uint32_t** in_indices);
+/* The edge weights beside those lists (int32 or float32 by the graph's
+ * weight_type; getOutWeight/getInWeight, graphgrind/graph-numa.h:63-86),
+ * NULL for an unweighted graph. */
+int gg_graph_device_weights(gg_graph_t g, const void** out_weights, const void** in_weights);
 
 /* ===================================================== vertexSubset API */
 /* partitioned_vertices (graphgrind/ligra-numa.h:91-272). */
@@ -334,7 +362,13 @@ int gg_graph_set_dense_policy(gg_graph_t g, int32_t policy);
  *                         for every such copy (read the arrays after it).
  *                         Pageable arrays are filled before the call
  *                         returns in both modes.  Graphs that keep their
- *                         given ids then hold two n-entry staging arrays */
+ *                         given ids then hold two n-entry staging arrays
+ *   GG_TUNE_LOOP_WAIT_BUDGET  probes of the grid-barrier wait of the device
+ *                         BFS level loop (GG_TUNE_DEVICE_LOOP) before it gives
+ *                         up: 0..2^22 (default 2^22, seconds at most).  When a
+ *                         wait runs out, every CTA returns, and gg_bfs returns
+ *                         GG_ERR_TIMEOUT with the graph left usable; tests set
+ *                         it to 0 to drive that path on a healthy graph */
 #define GG_TUNE_DENSE_POLICY 1
 #define GG_TUNE_COO_KERNEL 2
 #define GG_TUNE_SPARSE_DIV 3
@@ -342,6 +376,7 @@ int gg_graph_set_dense_policy(gg_graph_t g, int32_t policy);
 #define GG_TUNE_CC_ALGO 5
 #define GG_TUNE_PR_GRAPH 6
 #define GG_TUNE_ASYNC_RESULTS 7
+#define GG_TUNE_LOOP_WAIT_BUDGET 8
 int gg_graph_set_tuning(gg_graph_t g, int32_t key, int64_t value);
 int gg_graph_get_tuning(gg_graph_t g, int32_t key, int64_t* value);
 

@@ -59,6 +59,7 @@ for name, args in {
     "or_cc": [C.POINTER(OrGraph), _P, C.POINTER(OrStats)],
     "or_pagerank": [C.POINTER(OrGraph), C.c_int32, C.c_int32, _P, C.POINTER(OrStats)],
     "or_pagerank_delta": [C.POINTER(OrGraph), _P, C.POINTER(OrStats)],
+    "or_pagerank_edges": [C.POINTER(OrGraph), C.c_int32, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int32)],
     "or_spmv": [C.POINTER(OrGraph), _P, _P, C.POINTER(OrStats)],
     "or_bellman_ford": [C.POINTER(OrGraph), C.c_uint32, _P, C.POINTER(OrStats)],
     "or_bc": [C.POINTER(OrGraph), C.c_uint32, _P, _P, C.POINTER(OrStats)],
@@ -149,6 +150,13 @@ class Graph:
         st = self._st()
         assert _lib.or_pagerank(C.byref(self.c), max_iter, int(bit_all), _p(r), C.byref(st)) == 0
         return r, st
+
+    def pagerank_edges(self, max_iter=10, bit_all=False):
+        """(traversed edges, rounds) of pagerank(max_iter, bit_all), counted
+        without the arithmetic (valid while the L1 test does not stop early)."""
+        e, r = C.c_int64(), C.c_int32()
+        assert _lib.or_pagerank_edges(C.byref(self.c), max_iter, int(bit_all), C.byref(e), C.byref(r)) == 0
+        return int(e.value), int(r.value)
 
     def pagerank_delta(self):
         r = np.empty(self.n, np.float64)

@@ -443,6 +443,49 @@ int or_pagerank(const or_graph* g, int32_t max_iter, int32_t bit_all, double* ra
   return 0;
 }
 
+/* The traversed-edge count of or_pagerank without its arithmetic: the
+ * frontier sequence of app/PageRank.C:128-146 (all vertices first, then each
+ * edgeMap's output: every destination of an edge leaving the frontier, since
+ * PR_F::update always returns 1 and cond is cond_true; with bit_all every
+ * vertex sends, app/PageRankBit.C:145), summing each frontier's out-degrees (graphgrind/ligra-numa.h:944-945).  It assumes the
+ * L1 test (:139-140) does not end the loop before max_iter, which holds when
+ * a vertex without in-edges exists: its rank is left out of every later
+ * frontier, so |p_curr - p_next| keeps its 0.15/n there. */
+int or_pagerank_edges(const or_graph* g, int32_t max_iter, int32_t bit_all, int64_t* edges, int32_t* rounds) {
+  if (!g || !edges || !rounds) return -1;
+  const uint32_t n = g->n;
+  uint8_t* cur = (uint8_t*)malloc(n ? n : 1);
+  uint8_t* nxt = (uint8_t*)malloc(n ? n : 1);
+  if (!cur || !nxt) {
+    free(cur);
+    free(nxt);
+    return -2;
+  }
+  memset(cur, 1, n);
+  int all = 1;
+  int64_t total = 0;
+  int32_t r = 0;
+  for (; r < max_iter; r++) {
+    memset(nxt, 0, n);
+    for (uint32_t u = 0; u < n; u++) {
+      /* the frontier's out-degrees count; with bit set (PageRankBit's
+       * output.bit = true) every source sends */
+      if (cur[u]) total += (int64_t)(g->out_off[u + 1] - g->out_off[u]);
+      if (!all && !cur[u]) continue;
+      for (uint32_t j = g->out_off[u]; j < g->out_off[u + 1]; j++) nxt[g->out_idx[j]] = 1;
+    }
+    uint8_t* t = cur;
+    cur = nxt;
+    nxt = t;
+    all = bit_all;
+  }
+  free(cur);
+  free(nxt);
+  *edges = total;
+  *rounds = r;
+  return 0;
+}
+
 /* ============================================================ PageRankDelta */
 /* app/PageRankDelta.C:29-117 */
 typedef struct { double* p; double* delta; double* ngh; const eng_t* e; double damping, added, one_over_n, eps2; } prd_ctx;

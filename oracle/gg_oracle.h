@@ -43,6 +43,9 @@ typedef struct or_stats {
 int or_bfs(const or_graph* g, uint32_t start, int64_t* parents, int32_t* levels, or_stats* st);
 int or_cc(const or_graph* g, int64_t* ids, or_stats* st);
 int or_pagerank(const or_graph* g, int32_t max_iter, int32_t bit_all, double* ranks, or_stats* st);
+/* or_pagerank's traversed edges and rounds, counted without the arithmetic
+ * (valid while the L1 test does not stop the loop early). */
+int or_pagerank_edges(const or_graph* g, int32_t max_iter, int32_t bit_all, int64_t* edges, int32_t* rounds);
 int or_pagerank_delta(const or_graph* g, double* ranks, or_stats* st);
 int or_spmv(const or_graph* g, const double* x, double* y, or_stats* st);
 int or_bellman_ford(const or_graph* g, uint32_t start, int64_t* dist, or_stats* st);

@@ -52,3 +52,25 @@ def test_reference_arm_other_ranks_exit_quietly():
     p = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2"],
                        capture_output=True, text=True, env=env, timeout=300)
     assert p.returncode == 0 and p.stdout.strip() == ""
+
+
+def test_reference_arm_loads_only_the_oracle():
+    """The reference arm builds its graph with the oracle's generator and times
+    the reference's own build: the process maps no library of the product, and
+    its line carries the GPU arm's config block."""
+    import oracle
+    if not all(oracle.ref_available(a) for a in ("BFS", "PR", "SPMV")):
+        pytest.skip("reference binaries not built here")
+    code = ("import json, sys; sys.argv = ['bench.py', '--impl', 'reference', '--scale', '10', '--partitions', '4', "
+            "'--steps', '1', '--warmup', '1', '--no-one-thread']; sys.path.insert(0, %r); import bench; bench.main(); "
+            "maps = open('/proc/self/maps').read(); "
+            "print(json.dumps({'module': 'graphgrind_b200' in sys.modules, 'libgg': 'libgg.so' in maps}))" % ROOT)
+    env = dict(os.environ, OMP_NUM_THREADS="2")
+    p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, timeout=600)
+    assert p.returncode == 0, p.stderr[-2000:]
+    import json
+    line, probe = [json.loads(x) for x in p.stdout.strip().splitlines()[-2:]]
+    assert probe == {"module": False, "libgg": False}
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert line["config"]["n"] == 1024 and line["config"]["partitions"] == 4
+    assert line["reference_detail"]["edges"]["SPMV"] == line["config"]["m"]

@@ -64,3 +64,13 @@ def test_csc_matches_sort():
     assert np.array_equal(in_off[1:], np.cumsum(np.bincount(idx, minlength=hg.n)))
     t = hg.transpose()
     assert np.array_equal(in_off, t.offsets) and np.array_equal(in_idx, t.indices)
+
+
+@pytest.mark.parametrize("sym,bit", [(False, False), (False, True), (True, False)])
+def test_pagerank_edge_count(sym, bit):
+    """The reference-arm edge count equals the full restatement's."""
+    r = oracle.RmatGraph(12, 16, seed=21, symmetric=sym)
+    og = oracle.Graph(r.offsets, r.indices, symmetric=sym)
+    _, st = og.pagerank(10, bit)
+    assert st.rounds == 10
+    assert og.pagerank_edges(10, bit) == (st.edges_traversed, st.rounds)
