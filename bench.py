@@ -212,7 +212,8 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
     hg = make_graph(gg, args.scale, 2, gg.W_FLOAT32)
     log(f"[rank {rank}] generated RMAT-{args.scale}: n={hg.n} m={hg.m} in {time.time() - t0:.1f}s")
     t0 = time.time()
-    g = gg.Graph(hg, partitions=args.partitions, tile_edges=args.tile_edges, vertex_order=args.vertex_order)
+    g = gg.Graph(hg, partitions=args.partitions, tile_edges=args.tile_edges, vertex_order=args.vertex_order,
+                 order=gg.ORDER_HILBERT if args.order == "hilbert" else gg.ORDER_CSR)
     g.set_dense_policy(args.dense_policy)
     g.set_tuning(gg.TUNE_PR_GRAPH, 1 if args.pr_loop == "graph" else 0)
     info = g.info()
@@ -357,7 +358,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
         "config": common_config(args, n, m),
         "parallelism": "replicas" if world > 1 else "single GPU",
         "engine": {"dense_policy": ["reference rule", "csc pull", "coo pull"][args.dense_policy],
-                   "tile_edges": args.tile_edges,
+                   "tile_edges": args.tile_edges, "coo_order": args.order,
                    "pagerank_loop": {"graph": "iterations replayed as one CUDA graph",
                                      "host": "one host round trip per iteration"}[args.pr_loop],
                    "result_copies": {"overlap": "to pinned host arrays on a copy stream, overlapping the next "
@@ -409,7 +410,8 @@ def run_other_apps(gg, hg, g, args):
         r = min(runs, key=lambda x: x.ms)
         out[name] = {"ms": round(r.ms, 3), "rounds": r.rounds, "gteps": round(r.edges_traversed / r.ms / 1e6, 2)}
     hw = make_graph(gg, args.scale, 2, gg.W_INT32)
-    gw = gg.Graph(hw, partitions=args.partitions, tile_edges=args.tile_edges, vertex_order=args.vertex_order)
+    gw = gg.Graph(hw, partitions=args.partitions, tile_edges=args.tile_edges, vertex_order=args.vertex_order,
+                  order=gg.ORDER_HILBERT if args.order == "hilbert" else gg.ORDER_CSR)
     gw.bellman_ford(args.start)
     runs = [gw.bellman_ford(args.start)[1] for _ in range(3)]
     r = min(runs, key=lambda x: x.ms)
@@ -703,6 +705,8 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the library's default runtime knobs")
     ap.add_argument("--no-stress", action="store_true",
                     help="skip the other RMAT-24 apps and the grid / Erdos-Renyi BFS and Components lines")
+    ap.add_argument("--order", choices=["hilbert", "csr"], default="hilbert",
+                    help="COO order inside partitions: Hilbert (EDGES_HILBERT=1) or source-major (CSRDestSort)")
     ap.add_argument("--vertex-order", type=int, default=1, choices=[0, 1],
                     help="device numbering: 0 the given ids, 1 hottest sources first inside each partition")
     ap.add_argument("--tile-edges", type=int, default=1 << 18,

@@ -57,6 +57,10 @@ int scratch_on_current_device(unsigned char** out, int* num_sms) {
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p)
       return gg::fail(GG_ERR_CUDA, "cudaGetSymbolAddress(scratch) on device %d: %s", dev, cudaGetErrorString(e));
+    // the dedup bitmap is zero between calls (each call clears the words its
+    // output set); make it so once, whatever the array held at load
+    GG_CUDA(cudaMemset(p, 0, GG_NOALLOC_SCRATCH_BYTES));
+    GG_CUDA(cudaDeviceSynchronize());
     int sms = 0;
     GG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     g_scratch_addr[dev] = static_cast<unsigned char*>(p);
@@ -89,9 +93,10 @@ extern "C" int gg_bfs_push_step_noalloc(const uint32_t* out_offsets, const uint3
   uint32_t* dedup = reinterpret_cast<uint32_t*>(base + kStatsBytes);
   uint32_t* scan = reinterpret_cast<uint32_t*>(base + kStatsBytes + kDedupBytes);
   uint32_t* bsum = reinterpret_cast<uint32_t*>(base + kStatsBytes + kDedupBytes + kScanBytes);
-  // The array keeps the previous call's contents: clear what must start at zero.
+  // The array keeps the previous call's contents: the counters start at zero
+  // here; the dedup bitmap is zero on entry (cleared at set-up, then by every
+  // call for the vertices it output), so no call pays for an n-bit clear.
   GG_CUDA(cudaMemsetAsync(stats, 0, kStatsBytes, st));
-  GG_CUDA(cudaMemsetAsync(dedup, 0, sizeof(uint32_t) * ((size_t)(n + 31) / 32 + 4), st));
   if (frontier_len > 0) {
     const uint32_t nb = (frontier_len + gg::kScanTile - 1) / gg::kScanTile;
     gg::k_scan_sums<<<nb, gg::kScanThreads, 0, st>>>(frontier, frontier_len, out_offsets, bsum);
@@ -114,6 +119,9 @@ extern "C" int gg_bfs_push_step_noalloc(const uint32_t* out_offsets, const uint3
     f.levels = levels;
     f.round = round;
     gg::k_push<gg::BfsF, false><<<num_sms * 8, gg::kPushThreads, 0, st>>>(p, f);
+    GG_CUDA(cudaGetLastError());
+    // the output's dedup words back to zero for the next call
+    gg::k_clear_dedup<<<num_sms * 4, 256, 0, st>>>(next_frontier, stats + 2, dedup);
     GG_CUDA(cudaGetLastError());
   }
   // next_counts[0] = output frontier size, next_counts[1] = its out-degree sum

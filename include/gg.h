@@ -428,8 +428,9 @@ int gg_host_free_pinned(void* host_ptr);
  * Sizes above GG_NOALLOC_MAX_VERTICES / GG_NOALLOC_MAX_FRONTIER return
  * GG_ERR_SIZE.  The call is asynchronous on `stream`.  All calls share the
  * array: calls that overlap on the GPU race, so issue them in sequence.  The
- * first call on each device looks up the array's device address; make it
- * before any stream capture. */
+ * first call on each device looks up the array's device address and zeroes
+ * the array (a synchronous memset); make it before any stream capture.
+ * Later calls clear only the bitmap words of the vertices they output. */
 #define GG_NOALLOC_MAX_VERTICES (1u << 24)
 #define GG_NOALLOC_MAX_FRONTIER (1u << 19)
 #define GG_NOALLOC_SCRATCH_BYTES ((4u << 20) + (64u << 10))
