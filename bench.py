@@ -213,7 +213,8 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
     log(f"[rank {rank}] generated RMAT-{args.scale}: n={hg.n} m={hg.m} in {time.time() - t0:.1f}s")
     t0 = time.time()
     g = gg.Graph(hg, partitions=args.partitions, tile_edges=args.tile_edges, vertex_order=args.vertex_order,
-                 order=gg.ORDER_HILBERT if args.order == "hilbert" else gg.ORDER_CSR)
+                 order=gg.ORDER_HILBERT if args.order == "hilbert" else gg.ORDER_CSR,
+                 coo_tile_vertices=args.coo_tile_vertices)
     g.set_dense_policy(args.dense_policy)
     g.set_tuning(gg.TUNE_PR_GRAPH, 1 if args.pr_loop == "graph" else 0)
     info = g.info()
@@ -359,6 +360,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
         "parallelism": "replicas" if world > 1 else "single GPU",
         "engine": {"dense_policy": ["reference rule", "csc pull", "coo pull"][args.dense_policy],
                    "tile_edges": args.tile_edges, "coo_order": args.order,
+                   "coo_tile_vertices": args.coo_tile_vertices or 4096,
                    "pagerank_loop": {"graph": "iterations replayed as one CUDA graph",
                                      "host": "one host round trip per iteration"}[args.pr_loop],
                    "result_copies": {"overlap": "to pinned host arrays on a copy stream, overlapping the next "
@@ -411,7 +413,8 @@ def run_other_apps(gg, hg, g, args):
         out[name] = {"ms": round(r.ms, 3), "rounds": r.rounds, "gteps": round(r.edges_traversed / r.ms / 1e6, 2)}
     hw = make_graph(gg, args.scale, 2, gg.W_INT32)
     gw = gg.Graph(hw, partitions=args.partitions, tile_edges=args.tile_edges, vertex_order=args.vertex_order,
-                  order=gg.ORDER_HILBERT if args.order == "hilbert" else gg.ORDER_CSR)
+                  order=gg.ORDER_HILBERT if args.order == "hilbert" else gg.ORDER_CSR,
+                  coo_tile_vertices=args.coo_tile_vertices)
     gw.bellman_ford(args.start)
     runs = [gw.bellman_ford(args.start)[1] for _ in range(3)]
     r = min(runs, key=lambda x: x.ms)
@@ -705,6 +708,8 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the library's default runtime knobs")
     ap.add_argument("--no-stress", action="store_true",
                     help="skip the other RMAT-24 apps and the grid / Erdos-Renyi BFS and Components lines")
+    ap.add_argument("--coo-tile-vertices", type=int, default=0,
+                    help="max destinations per COO tile (0: 4096, the CSC tile width)")
     ap.add_argument("--order", choices=["hilbert", "csr"], default="hilbert",
                     help="COO order inside partitions: Hilbert (EDGES_HILBERT=1) or source-major (CSRDestSort)")
     ap.add_argument("--vertex-order", type=int, default=1, choices=[0, 1],

@@ -67,7 +67,7 @@ class BuildOpts(C.Structure):
     _fields_ = [("num_partitions", C.c_int32), ("balance", C.c_int32), ("part_how", C.c_int32),
                 ("relabel", C.c_int32), ("order", C.c_int32), ("tile_vertices", C.c_int32),
                 ("tile_edges", C.c_int32), ("build_coo", C.c_int32), ("coo_window", C.c_int32),
-                ("coo_dst_window", C.c_int32), ("vertex_order", C.c_int32)]
+                ("coo_dst_window", C.c_int32), ("vertex_order", C.c_int32), ("coo_tile_vertices", C.c_int32)]
 
 
 class TuneTrial(C.Structure):
@@ -511,11 +511,11 @@ class Graph:
 
     def __init__(self, host: HostGraph, partitions=384, balance=BALANCE_EDGE, part_how=PART_DEST, relabel=False,
                  order=ORDER_HILBERT, tile_vertices=0, tile_edges=0, build_coo=0, coo_window=0, coo_dst_window=0,
-                 vertex_order=VORDER_GIVEN):
+                 vertex_order=VORDER_GIVEN, coo_tile_vertices=0):
         self.host = host
         self._deps = weakref.WeakSet()
         o = BuildOpts(partitions, balance, part_how, int(relabel), order, tile_vertices, tile_edges, build_coo,
-                      coo_window, coo_dst_window, vertex_order)
+                      coo_window, coo_dst_window, vertex_order, coo_tile_vertices)
         h = C.c_void_p()
         check(lib.gg_graph_build(C.byref(host.c), C.byref(o), C.byref(h)), "gg_graph_build")
         self.h = h
@@ -833,10 +833,10 @@ def autotune_build(host, app=APP_PAGERANK, start=0, candidates=()):
     """Build `host` under each candidate (dicts of Graph keyword options),
     autotune each, and return (best options dict, best trial dict)."""
     names = ("partitions", "balance", "part_how", "relabel", "order", "tile_vertices", "tile_edges", "build_coo",
-             "coo_window", "coo_dst_window", "vertex_order")
+             "coo_window", "coo_dst_window", "vertex_order", "coo_tile_vertices")
     defaults = dict(partitions=384, balance=BALANCE_EDGE, part_how=PART_DEST, relabel=0, order=ORDER_HILBERT,
                     tile_vertices=0, tile_edges=0, build_coo=0, coo_window=0, coo_dst_window=0,
-                    vertex_order=VORDER_GIVEN)
+                    vertex_order=VORDER_GIVEN, coo_tile_vertices=0)
     cands = (BuildOpts * len(candidates))()
     for i, c in enumerate(candidates):
         d = dict(defaults, **c)

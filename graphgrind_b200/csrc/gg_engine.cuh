@@ -66,6 +66,7 @@ constexpr int kPullSlots = kPullThreads * kPullK;           // 2048 stage slots
 constexpr int kPullChunk = kPullSlots - 8;                  // edges per chunk (8-aligned slack)
 constexpr int kPullStages = 3;
 constexpr int kMaxTileVertices = 4096;
+constexpr int kMaxCooTileVertices = 16384;  // COO tiles (16-bit destination offsets)
 constexpr uint32_t kPad = 0xffffffffu;                      // COO padding source id
 
 constexpr int kPushThreads = 256;

@@ -241,13 +241,14 @@ __global__ void k_coo_keys(const uint32_t* src, const uint32_t* dst, uint64_t m,
 // Second-level order inside a tile: positions keep their 256-edge window of
 // the Hilbert order, and inside a window edges go by destination, so that a
 // thread's 8 consecutive edges form destination runs while the window keeps
-// the Hilbert locality of its sources.  key = window << 12 | local destination.
+// the Hilbert locality of its sources.  key = window << dbits | local
+// destination (dbits covers the tile width).
 __global__ void k_coo_window_keys(const uint4* seg, uint32_t ntiles, const uint32_t* perm, const uint32_t* dst,
-                                  uint32_t window, uint32_t* keys) {
+                                  uint32_t window, uint32_t dbits, uint32_t* keys) {
   for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const uint4 s = seg[t];  // {v0, nv, e0 (CSC), ne}
     for (uint32_t i = threadIdx.x; i < s.w; i += blockDim.x)
-      keys[s.z + i] = ((i / window) << 12) | (dst[perm[s.z + i]] - s.x);
+      keys[s.z + i] = ((i / window) << dbits) | (dst[perm[s.z + i]] - s.x);
   }
 }
 
@@ -283,7 +284,7 @@ static int build_coo(gg_graph_s* g, const uint32_t* h_in_off) {
   const uint32_t n = g->n;
   const uint64_t m = g->m;
   const int P = (int)g->coo_sizes.size();
-  const uint32_t tv = (uint32_t)g->opts.tile_vertices;
+  const uint32_t tv = (uint32_t)g->opts.coo_tile_vertices;
   const uint64_t te = (uint64_t)g->opts.tile_edges;
   std::vector<uint4> segs;  // in vertex order
   for (int p = 0; p < P; ++p)
@@ -296,6 +297,12 @@ static int build_coo(gg_graph_s* g, const uint32_t* h_in_off) {
     pos += (segs[t].w + 7u) & ~7u;
   }
   if (pos + 16 >= (1ull << 31)) return fail(GG_ERR_SIZE, "padded COO exceeds the 2^31-edge sort limit");
+  // 32-bit window keys: the local destination in dbits bits, the window above
+  uint32_t dbits = 1;
+  while ((1u << dbits) < tv) ++dbits;
+  for (const uint4& sg : segs)
+    if (g->opts.coo_window == 0 && (uint64_t)sg.w / (uint64_t)g->opts.coo_dst_window >= (1ull << (32 - dbits)))
+      return fail(GG_ERR_SIZE, "a COO tile of %u edges exceeds the window-key range", sg.w);
   g->coo_len = pos;
   GG_TRY(dev_alloc(g, &g->d_coo_src, pos + 16));
   GG_TRY(dev_alloc(g, &g->d_coo_dloc, pos + 16));
@@ -385,7 +392,7 @@ static int build_coo(gg_graph_s* g, const uint32_t* h_in_off) {
       uint32_t* k32 = reinterpret_cast<uint32_t*>(d_keys);
       uint32_t* k32_out = reinterpret_cast<uint32_t*>(d_keys_out);
       k_coo_window_keys<<<grid, 256>>>(d_segs, (uint32_t)segs.size(), d_perm, d_dst,
-                                       (uint32_t)g->opts.coo_dst_window, k32);
+                                       (uint32_t)g->opts.coo_dst_window, dbits, k32);
       GG_BUILD(cudaGetLastError());
       size_t temp2 = 0;
       GG_BUILD(cub::DeviceSegmentedRadixSort::SortPairs(nullptr, temp2, k32, k32_out, d_perm, d_vals, (int)m,
@@ -598,6 +605,8 @@ static int graph_build(const gg_host_graph* hg_given, const gg_build_opts* opts_
     return fail(GG_ERR_INVALID_ARG, "gg_graph_build: unknown vertex_order %d", o.vertex_order);
   if (o.num_partitions <= 0) o.num_partitions = 384;
   if (o.tile_vertices <= 0 || o.tile_vertices > kMaxTileVertices) o.tile_vertices = kMaxTileVertices;
+  if (o.coo_tile_vertices <= 0) o.coo_tile_vertices = o.tile_vertices;
+  if (o.coo_tile_vertices > kMaxCooTileVertices) o.coo_tile_vertices = kMaxCooTileVertices;
   if (o.tile_edges <= 0) o.tile_edges = 1 << 16;
   if (o.coo_window < 0) o.coo_window = 0;
   if (o.coo_window > 0) o.coo_window = (o.coo_window + kSegBlock - 1) / kSegBlock * kSegBlock;

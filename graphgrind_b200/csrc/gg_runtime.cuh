@@ -216,7 +216,7 @@ int pull_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f
   p.err = g->ws.d_stats + 3;
   if (p.ntiles == 0) return GG_OK;
   constexpr bool kHW = HW;
-  p.tv = (uint32_t)g->opts.tile_vertices;
+  p.tv = (uint32_t)(coo ? g->opts.coo_tile_vertices : g->opts.tile_vertices);
   const size_t smem_coo = pull_smem_bytes(true, kHW, 4, p.tv);
   const size_t smem_csc = pull_smem_bytes(false, kHW, 4);
   // opt in once per device to the largest dynamic shared memory (widest
@@ -225,7 +225,7 @@ int pull_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f
   auto launch = [&](auto kern, size_t smem, DeviceOnce& once) -> int {
     const int ok = once.get(g->device, [&]() {
       return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)pull_smem_bytes(true, kHW, 4, kMaxTileVertices)) == cudaSuccess ? 1 : -1;
+                                  (int)pull_smem_bytes(true, kHW, 4, kMaxCooTileVertices)) == cudaSuccess ? 1 : -1;
     });
     if (ok < 0) return fail(GG_ERR_CUDA, "cudaFuncSetAttribute failed for the dense pull");
     int blocks = 1;
@@ -247,7 +247,7 @@ int pull_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f
       const size_t smem = coo_w_smem_bytes(kHW, stages, 4, p.tv, flags);
       const int ok = once.get(g->device, [&]() {
         return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)coo_w_smem_bytes(kHW, stages, 4, kMaxTileVertices, flags)) == cudaSuccess
+                                    (int)coo_w_smem_bytes(kHW, stages, 4, kMaxCooTileVertices, flags)) == cudaSuccess
                    ? 1
                    : -1;
       });

@@ -70,6 +70,9 @@ typedef struct gg_build_opts {
   int32_t coo_dst_window;   /* GPU: edges per destination-ordered window when
                                coo_window == 0 (multiple of 256; 0 = 256)    */
   int32_t vertex_order;     /* GPU: gg_vertex_order (0 = the given ids)      */
+  int32_t coo_tile_vertices;/* GPU: max destinations per COO tile (<= 16384;
+                               0 = tile_vertices); the CSC tiles keep
+                               tile_vertices                                 */
 } gg_build_opts;
 
 /* Device-side vertex numbering of a graph (gg_build_opts.vertex_order).

@@ -99,3 +99,31 @@ def test_device_coo_orders_on_rmat(gg, sym):
         tiles = _check_layout(gg, g, h, key)
         assert len(tiles) > 32
         g.close()
+
+
+@pytest.mark.parametrize("order", ["hilbert", "csr"])
+@pytest.mark.parametrize("ctv", [8192, 16384])
+def test_wide_coo_tiles(gg, orc, order, ctv):
+    """COO tiles wider than the CSC tiles (coo_tile_vertices up to 16384):
+    the layout keeps its guarantees and every dense-COO application gives
+    the oracle's results."""
+    from conftest import PR_MAX_ABS, PR_REL_L1, rel_l1
+    hg = gg.HostGraph.rmat(16, 16, seed=23, symmetric=False).add_weights(gg.W_FLOAT32, seed=4)
+    o = gg.ORDER_HILBERT if order == "hilbert" else gg.ORDER_CSR
+    key = gg.hilbert_key if order == "hilbert" else (lambda side, x, y: (x << 32) | y)
+    g = gg.Graph(hg, partitions=8, order=o, tile_edges=1 << 20, coo_tile_vertices=ctv)
+    tiles = _check_layout(gg, g, _Host(hg), key)
+    assert int(tiles[:, 1].max()) > 4096
+    g.set_dense_policy(2)  # every dense step on the COO
+    og = orc.Graph.from_host(hg)
+    _, lev, _ = g.bfs(7)
+    np.testing.assert_array_equal(lev, og.bfs(7)[1])
+    r, _ = g.pagerank(10)
+    o_r, _ = og.pagerank(10)
+    assert rel_l1(r, o_r) <= PR_REL_L1 and np.abs(r - o_r).max() <= PR_MAX_ABS
+    ids, _ = g.components()
+    np.testing.assert_array_equal(ids, og.cc()[0])
+    y, _ = g.spmv()
+    oy, _ = og.spmv()
+    assert rel_l1(y, oy) <= 1e-6
+    g.close()
