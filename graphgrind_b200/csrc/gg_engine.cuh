@@ -149,6 +149,7 @@ struct gg_graph_s {
   int device_loop = 1;  // BFS runs consecutive sparse levels in one cooperative launch
   int cc_algo = 0;      // Components on symmetric graphs: 0 label propagation, 1 union-find
   uint32_t loop_wait_budget = 1u << 22;  // spins of the BFS level loop's grid-barrier wait
+  int early_kernel = 1;  // early-exit dense pull: 0 one lane per destination, 1 8-lane groups
   int pr_graph = 1;     // PageRank iterations replayed as one CUDA graph (0: one host round trip per iteration)
   // GG_TUNE_ASYNC_RESULTS: results bound for pinned host memory leave from the
   // given-order arrays on copy_stream, and the call returns without waiting
@@ -1180,6 +1181,84 @@ __global__ void __launch_bounds__(256) k_pull_early(uint32_t n, const uint32_t* 
       atomicOr(next_bits + (b >> 5), word);
       my_cnt += __popc(word);
     }
+  }
+  my_cnt = warp_sum(my_cnt);
+  my_deg = warp_sum(my_deg);
+  if (lane == 0) {
+    if (my_cnt) atomicAdd(stats + 0, my_cnt);
+    if (my_deg) atomicAdd(stats + 1, my_deg);
+  }
+}
+
+// Dense pull with early exit, cooperative form: a warp takes 32 consecutive
+// destinations, keeps those that pass cond (and have in-edges), and walks
+// their in-lists 4 at a time with 8 lanes each, 8 consecutive in-edges per
+// step (one 32-byte read per group).  A destination stops at the first step
+// holding a frontier in-neighbour and takes the first one of that step, so
+// it still takes its first frontier in-neighbour in list order, as the
+// one-lane form does; a hub row is walked 8 edges per step instead of 1.
+template <class F, bool HW, bool ALL>
+__global__ void __launch_bounds__(256) k_pull_early_g(uint32_t n, const uint32_t* off, const uint32_t* idx,
+                                                      const uint32_t* wts, const uint32_t* fr_bits,
+                                                      uint32_t* next_bits, const uint32_t* deg_off,
+                                                      const uint32_t* member_off, unsigned long long* stats,
+                                                      const F f) {
+  __shared__ uint32_t s_cand[8][32];
+  unsigned long long my_cnt = 0, my_deg = 0;
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t grp = lane >> 3, sub = lane & 7;
+  const uint32_t gmask = 0xffu << (grp * 8);
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); b < n; b += stride) {
+    const uint32_t v = (uint32_t)b + lane;
+    bool cand = false;
+    if (v < n && (!member_off || member_off[v + 1] > member_off[v]))
+      cand = off[v + 1] > off[v] && f.cond(v);
+    const uint32_t cm = __ballot_sync(0xffffffffu, cand);
+    if (cand) s_cand[warp][__popc(cm & ((1u << lane) - 1u))] = lane;
+    __syncwarp();
+    const uint32_t nc = __popc(cm);
+    uint32_t found = 0;  // lanes (vertex offsets in the warp's 32) that took a parent
+    for (uint32_t c0 = 0; c0 < nc; c0 += 4) {
+      const uint32_t c = c0 + grp;
+      const bool mine = c < nc;
+      const uint32_t lv = mine ? s_cand[warp][c] : 0u;
+      const uint32_t vv = (uint32_t)b + lv;
+      uint32_t j = mine ? off[vv] + sub : 0u;
+      const uint32_t e1 = mine ? off[vv + 1] : 0u;
+      bool live = mine;
+      while (__any_sync(0xffffffffu, live)) {
+        bool hit = false;
+        uint32_t s = 0;
+        if (live && j < e1) {
+          s = idx[j];
+          hit = ALL || test_bit(fr_bits, s);
+        }
+        const uint32_t hm = __ballot_sync(0xffffffffu, hit) & gmask;
+        if (live) {
+          if (hm) {
+            const uint32_t first = __ffs(hm) - 1;
+            if (lane == first) {
+              if (f.commit(vv, f.gather(s, HW ? wts[j] : 1u))) found |= 1u << lv;
+            }
+            live = false;
+          } else {
+            j += 8;
+            if (j - sub >= e1) live = false;  // the group's next step starts past the row
+          }
+        }
+      }
+    }
+    // every lane's found bits of this warp's 32 destinations
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) found |= __shfl_xor_sync(0xffffffffu, found, o);
+    const bool act = (found >> lane) & 1u;
+    if (act) my_deg += deg_off[v + 1] - deg_off[v];
+    if (lane == 0 && found) {
+      atomicOr(next_bits + (b >> 5), found);
+      my_cnt += __popc(found);
+    }
+    __syncwarp();
   }
   my_cnt = warp_sum(my_cnt);
   my_deg = warp_sum(my_deg);

@@ -338,12 +338,21 @@ template <class F, bool HW>
 int pull_early_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f) {
   const uint32_t* member = g->transposed ? g->d_csc_off : nullptr;
   const int grid = generic_grid(g, g->n);
-  if (in->bit)
+  static_assert(kGenericThreads == 256, "k_pull_early_g stages 8 warps of candidates");
+  if (g->early_kernel == 1) {
+    if (in->bit)
+      k_pull_early_g<F, HW, true><<<grid, kGenericThreads, 0, g->stream>>>(
+          g->n, g->in_off(), g->in_idx(), g->in_w(), nullptr, out->d_bits, g->out_off(), member, g->ws.d_stats, f);
+    else
+      k_pull_early_g<F, HW, false><<<grid, kGenericThreads, 0, g->stream>>>(
+          g->n, g->in_off(), g->in_idx(), g->in_w(), in->d_bits, out->d_bits, g->out_off(), member, g->ws.d_stats, f);
+  } else if (in->bit) {
     k_pull_early<F, HW, true><<<grid, kGenericThreads, 0, g->stream>>>(
         g->n, g->in_off(), g->in_idx(), g->in_w(), nullptr, out->d_bits, g->out_off(), member, g->ws.d_stats, f);
-  else
+  } else {
     k_pull_early<F, HW, false><<<grid, kGenericThreads, 0, g->stream>>>(
         g->n, g->in_off(), g->in_idx(), g->in_w(), in->d_bits, out->d_bits, g->out_off(), member, g->ws.d_stats, f);
+  }
   GG_CUDA(cudaGetLastError());
   g->kernels++;
   return GG_OK;

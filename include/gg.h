@@ -371,7 +371,12 @@ int gg_graph_set_dense_policy(gg_graph_t g, int32_t policy);
  *                         up: 0..2^22 (default 2^22, seconds at most).  When a
  *                         wait runs out, every CTA returns, and gg_bfs returns
  *                         GG_ERR_TIMEOUT with the graph left usable; tests set
- *                         it to 0 to drive that path on a healthy graph */
+ *                         it to 0 to drive that path on a healthy graph
+ *   GG_TUNE_EARLY_KERNEL  the dense pull with early exit (BFS's bottom-up
+ *                         step, edgeMapDenseCSC's break, ligra-numa.h:621-626, 708-713):
+ *                         1 (default) 8 lanes walk a destination's in-list 8
+ *                         edges per step, 4 destinations per warp; 0 one lane
+ *                         per destination, one edge per step */
 #define GG_TUNE_DENSE_POLICY 1
 #define GG_TUNE_COO_KERNEL 2
 #define GG_TUNE_SPARSE_DIV 3
@@ -380,6 +385,7 @@ int gg_graph_set_dense_policy(gg_graph_t g, int32_t policy);
 #define GG_TUNE_PR_GRAPH 6
 #define GG_TUNE_ASYNC_RESULTS 7
 #define GG_TUNE_LOOP_WAIT_BUDGET 8
+#define GG_TUNE_EARLY_KERNEL 9
 int gg_graph_set_tuning(gg_graph_t g, int32_t key, int64_t value);
 int gg_graph_get_tuning(gg_graph_t g, int32_t key, int64_t* value);
 

@@ -253,3 +253,18 @@ def test_apps_with_source_partitions(gg, orc, sym):
         check_float(r, o)
         y, _ = g.spmv()
         check_float(y, og.spmv()[0], rel=1e-6, mx=1e-6 * float(np.abs(og.spmv()[0]).max()))
+
+
+@pytest.mark.parametrize("kernel", [0, 1])
+def test_bfs_early_exit_kernels(gg, rmat14, kernel):
+    """Both forms of the bottom-up (early-exit) dense step give the oracle's
+    levels; parents are frontier in-neighbours one level up."""
+    hg, g, og = rmat14
+    g.set_tuning(gg.TUNE_EARLY_KERNEL, kernel)
+    g.set_dense_policy(1)  # every dense level takes the early-exit CSC pull
+    try:
+        for start in (0, 100, 12345):
+            check_bfs(g, og, start, hg)
+    finally:
+        g.set_tuning(gg.TUNE_EARLY_KERNEL, 1)
+        g.set_dense_policy(0)
