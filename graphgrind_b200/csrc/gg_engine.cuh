@@ -149,7 +149,7 @@ struct gg_graph_s {
   int device_loop = 1;  // BFS runs consecutive sparse levels in one cooperative launch
   int cc_algo = 0;      // Components on symmetric graphs: 0 label propagation, 1 union-find
   uint32_t loop_wait_budget = 1u << 22;  // spins of the BFS level loop's grid-barrier wait
-  int early_kernel = 1;  // early-exit dense pull: 0 one lane per destination, 1 8-lane groups
+  int early_kernel = 0;  // early-exit dense pull: 0 one lane per destination (faster on R-MAT), 1 8-lane groups
   int pr_graph = 1;     // PageRank iterations replayed as one CUDA graph (0: one host round trip per iteration)
   // GG_TUNE_ASYNC_RESULTS: results bound for pinned host memory leave from the
   // given-order arrays on copy_stream, and the call returns without waiting

@@ -374,9 +374,11 @@ int gg_graph_set_dense_policy(gg_graph_t g, int32_t policy);
  *                         it to 0 to drive that path on a healthy graph
  *   GG_TUNE_EARLY_KERNEL  the dense pull with early exit (BFS's bottom-up
  *                         step, edgeMapDenseCSC's break, ligra-numa.h:621-626, 708-713):
- *                         1 (default) 8 lanes walk a destination's in-list 8
- *                         edges per step, 4 destinations per warp; 0 one lane
- *                         per destination, one edge per step */
+ *                         0 (default) one lane per destination, one edge per
+ *                         step; 1 8 lanes walk a destination's in-list 8 edges
+ *                         per step, 4 destinations per warp (faster on long
+ *                         rows, slower on R-MAT-24: 0.67 against 0.46 ms for
+ *                         BFS's three bottom-up levels) */
 #define GG_TUNE_DENSE_POLICY 1
 #define GG_TUNE_COO_KERNEL 2
 #define GG_TUNE_SPARSE_DIV 3

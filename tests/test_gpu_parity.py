@@ -266,5 +266,5 @@ def test_bfs_early_exit_kernels(gg, rmat14, kernel):
         for start in (0, 100, 12345):
             check_bfs(g, og, start, hg)
     finally:
-        g.set_tuning(gg.TUNE_EARLY_KERNEL, 1)
+        g.set_tuning(gg.TUNE_EARLY_KERNEL, 0)
         g.set_dense_policy(0)
