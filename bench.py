@@ -10,10 +10,14 @@ each run through the library's C ABI (gg_bfs / gg_pagerank / gg_spmv).
 
   value  = traversed edges of the step / device time of the three Compute
            loops (CUDA events on the library's stream), graph resident in HBM
-  e2e    = same edges / host wall time of the same C-ABI calls, including the
-           H2D copy of the SpMV input vector from pinned memory and the D2H
-           copies of every result array of the reference's apps (BFS parents,
-           PageRank ranks, SpMV y)
+  e2e    = same edges / host wall time of the K steps' C-ABI calls, including
+           every step's H2D copy of the SpMV input vector from pinned memory
+           and D2H copies of every result array of the reference's apps (BFS
+           parents, PageRank ranks, SpMV y); the copies leave on the
+           library's copy stream while the next application (and the next
+           step) runs, and the clock stops when the last step's copies have
+           arrived (--copies pipeline; --copies overlap makes every step wait
+           for its own copies)
   roofline = the dense-pull kernel of the PageRank iterations: algorithmic
            bytes 8m + 16n per launch over its CUDA-event duration
   cpu_baseline = the reference's own OpenMP build (oracle/_ref, compiled from
@@ -246,7 +250,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
 
     # results leave for the pinned host arrays on the library's copy stream
     # while the next application runs; the step ends when all have arrived
-    g.set_tuning(gg.TUNE_ASYNC_RESULTS, 1 if args.copies == "overlap" else 0)
+    g.set_tuning(gg.TUNE_ASYNC_RESULTS, 0 if args.copies == "wait" else 1)
 
     def step():
         use("bfs")
@@ -255,11 +259,13 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
         _, p = g.pagerank(10, out=ranks.array)
         use("spmv")
         _, s = g.spmv(x.array, out=y.array)
-        g.synchronize()
+        if args.copies != "pipeline":
+            g.synchronize()
         return b, p, s
 
     for _ in range(args.warmup):
         step()
+    g.synchronize()
     if dist:
         dist.barrier()
     gpu_index = os.environ.get("CUDA_VISIBLE_DEVICES", str(local_rank)).split(",")[local_rank] if \
@@ -269,16 +275,19 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
     per_app = {"bfs": [0, 0.0], "pagerank": [0, 0.0], "spmv": [0, 0.0]}
     pr_prof = {"launches": 0, "ms": 0.0}
     pr_kind = None
+    # pipeline: a step's result copies overlap the next step, and the wall
+    # clock stops once the last step's copies have arrived
+    w0 = time.perf_counter()
     for _ in range(args.steps):
-        w0 = time.perf_counter()
         b, p, s = step()
-        wall_s += time.perf_counter() - w0
         for name, r in (("bfs", b), ("pagerank", p), ("spmv", s)):
             per_app[name][0] += r.edges_traversed
             per_app[name][1] += r.ms
             dev_ms += r.ms
             edges += r.edges_traversed
             launches += r.kernels
+    g.synchronize()
+    wall_s = time.perf_counter() - w0
     # per-kernel-class profile of one more step, outside the timed region
     # (profiling records an event pair per edgeMap, so PageRank takes its host
     # loop there instead of the captured graph)
@@ -363,7 +372,10 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
                    "coo_tile_vertices": args.coo_tile_vertices or 4096,
                    "pagerank_loop": {"graph": "iterations replayed as one CUDA graph",
                                      "host": "one host round trip per iteration"}[args.pr_loop],
-                   "result_copies": {"overlap": "to pinned host arrays on a copy stream, overlapping the next "
+                   "result_copies": {"pipeline": "to pinned host arrays on a copy stream, overlapping the next "
+                                                 "application and the next step; the timed region ends after the "
+                                                 "last step's copies (gg_graph_synchronize)",
+                                     "overlap": "to pinned host arrays on a copy stream, overlapping the next "
                                                 "application; the step waits for all (gg_graph_synchronize)",
                                      "wait": "each call returns after its copy"}[args.copies],
                    "vertex_order": ["given ids", "hottest sources first inside each partition (results in the "
@@ -716,9 +728,11 @@ def main():
                     help="device numbering: 0 the given ids, 1 hottest sources first inside each partition")
     ap.add_argument("--tile-edges", type=int, default=1 << 18,
                     help="target edges per CTA tile (gg_autotune_build's choice for this workload)")
-    ap.add_argument("--copies", choices=["overlap", "wait"], default="overlap",
-                    help="result copies to the host overlap the next application (GG_TUNE_ASYNC_RESULTS 1) "
-                         "or finish inside each call")
+    ap.add_argument("--copies", choices=["pipeline", "overlap", "wait"], default="pipeline",
+                    help="result copies to the host overlap the next application and the next step, the clock "
+                         "stopping after the last step's copies (pipeline); overlap the next application, each "
+                         "step waiting for its copies (overlap) (both GG_TUNE_ASYNC_RESULTS 1); or finish inside "
+                         "each call (wait)")
     ap.add_argument("--pr-loop", choices=["graph", "host"], default="graph",
                     help="PageRank iterations as one CUDA graph (GG_TUNE_PR_GRAPH 1) or host-driven")
     ap.add_argument("--traffic", type=float, default=None,

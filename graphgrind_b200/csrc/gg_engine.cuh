@@ -150,6 +150,8 @@ struct gg_graph_s {
   int cc_algo = 0;      // Components on symmetric graphs: 0 label propagation, 1 union-find
   uint32_t loop_wait_budget = 1u << 22;  // spins of the BFS level loop's grid-barrier wait
   int early_kernel = 0;  // early-exit dense pull: 0 one lane per destination (faster on R-MAT), 1 8-lane groups
+  int push_dense_div = 0;  // a dense edgeMap of an early-exit functor pushes into a bitmap when
+                           // the frontier has at most n / push_dense_div vertices (0: never)
   int pr_graph = 1;     // PageRank iterations replayed as one CUDA graph (0: one host round trip per iteration)
   // GG_TUNE_ASYNC_RESULTS: results bound for pinned host memory leave from the
   // given-order arrays on copy_stream, and the call returns without waiting
@@ -1370,6 +1372,66 @@ struct PushParams {
   uint32_t* out_q;          // output queue
   unsigned long long* stats;  // [0] -, [1] out-degree sum, [2] queue length
 };
+
+// Push whose output is a bitmap: the dense edgeMap of a frontier with few
+// vertices but many out-edges (the level after a hub level), where the
+// bottom-up pull would walk every unvisited in-list.  The same per-edge work
+// as k_push (cond && update_atomic); the first winner of a destination sets
+// its bit in p.dedup (here the zeroed output bitmap), and the output's size
+// and out-degree sum are counted per warp, with no queue and no per-warp
+// atomic on one shared counter.
+template <class F, bool HW>
+__global__ void __launch_bounds__(kPushThreads) k_push_bits(const PushParams p, const F f) {
+  __shared__ uint32_t s_q[2];
+  const uint64_t E = *p.total;
+  const int lane = threadIdx.x & 31;
+  unsigned long long my_deg = 0, my_cnt = 0;
+  for (uint64_t c = blockIdx.x; c * kPushEdgesPerCta < E; c += gridDim.x) {
+    const uint32_t e_lo = (uint32_t)(c * kPushEdgesPerCta);
+    const uint64_t e_end = (uint64_t)e_lo + kPushEdgesPerCta;
+    const uint32_t e_hi = (uint32_t)(E < e_end ? E : e_end);
+    if (threadIdx.x < 2) {
+      const uint32_t key = threadIdx.x == 0 ? e_lo : e_hi - 1;
+      uint32_t lo = 0, hi = p.k;  // largest i with offs[i] <= key
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (p.offs[mid] <= key) lo = mid; else hi = mid;
+      }
+      s_q[threadIdx.x] = lo;
+    }
+    __syncthreads();
+    const uint32_t qlo = s_q[0], qhi = s_q[1];
+    const uint32_t iters = (e_hi - e_lo + kPushThreads - 1) / kPushThreads;
+    for (uint32_t it = 0; it < iters; ++it) {
+      const uint32_t e = e_lo + it * kPushThreads + threadIdx.x;
+      if (e < e_hi) {
+        uint32_t lo = qlo, hi = qhi + 1;
+        while (hi - lo > 1) {
+          const uint32_t mid = (lo + hi) >> 1;
+          if (p.offs[mid] <= e) lo = mid; else hi = mid;
+        }
+        const uint32_t s = p.q[lo];
+        const uint32_t ei = p.off[s] + (e - p.offs[lo]);
+        const uint32_t d = p.idx[ei];
+        const uint32_t w = HW ? p.wts[ei] : 1u;
+        if (f.cond(d) && f.update_atomic(s, d, w)) {
+          const uint32_t bit = 1u << (d & 31);
+          if (!(atomicOr(p.dedup + (d >> 5), bit) & bit)) {
+            ++my_cnt;
+            my_deg += p.deg_off[d + 1] - p.deg_off[d];
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  my_deg = warp_sum(my_deg);
+  my_cnt = warp_sum(my_cnt);
+  if (lane == 0) {
+    if (my_cnt) atomicAdd(p.stats + 0, my_cnt);
+    if (my_deg) atomicAdd(p.stats + 1, my_deg);
+  }
+}
 
 template <class F, bool HW>
 __global__ void __launch_bounds__(kPushThreads) k_push(const PushParams p, const F f) {

@@ -936,6 +936,10 @@ int gg_graph_set_tuning(gg_graph_t g, int32_t key, int64_t value) {
       if (value != 0 && value != 1) return fail(GG_ERR_INVALID_ARG, "early-exit kernel must be 0 or 1");
       g->early_kernel = (int)value;
       return GG_OK;
+    case GG_TUNE_PUSH_DENSE_DIV:
+      if (value < 0 || value > (1ll << 30)) return fail(GG_ERR_INVALID_ARG, "push-dense divisor must be 0..2^30");
+      g->push_dense_div = (int)value;
+      return GG_OK;
     case GG_TUNE_LOOP_WAIT_BUDGET:
       if (value < 0 || value > (1ll << 22))
         return fail(GG_ERR_INVALID_ARG, "loop wait budget must be 0..2^22 spins");
@@ -987,6 +991,9 @@ int gg_graph_get_tuning(gg_graph_t g, int32_t key, int64_t* value) {
       return GG_OK;
     case GG_TUNE_EARLY_KERNEL:
       *value = g->early_kernel;
+      return GG_OK;
+    case GG_TUNE_PUSH_DENSE_DIV:
+      *value = g->push_dense_div;
       return GG_OK;
     default:
       return fail(GG_ERR_INVALID_ARG, "unknown tuning key %d", key);

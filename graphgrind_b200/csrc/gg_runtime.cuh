@@ -395,6 +395,42 @@ int push_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f
   return GG_OK;
 }
 
+// Top-down step into a bitmap (k_push_bits): `out` bits zeroed, stats reset.
+template <class F, bool HW>
+int push_bits_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f) {
+  const uint32_t k = (uint32_t)in->dm;
+  const uint32_t nb = (k + kScanTile - 1) / kScanTile;
+  Workspace& ws = g->ws;
+  if (nb > ws.bsum_cap) {
+    if (ws.d_bsum) cudaFree(ws.d_bsum);
+    GG_CUDA(cudaMalloc(&ws.d_bsum, sizeof(uint32_t) * (nb + 32)));
+    ws.bsum_cap = nb;
+  }
+  const uint32_t* off = g->out_off();
+  k_scan_sums<<<nb, kScanThreads, 0, g->stream>>>(in->d_queue, k, off, ws.d_bsum);
+  k_scan_blocks<<<1, 1024, 0, g->stream>>>(ws.d_bsum, nb, ws.d_stats + 5);
+  k_scan_write<<<nb, kScanThreads, 0, g->stream>>>(in->d_queue, k, off, ws.d_bsum, ws.d_scan);
+  PushParams p{};
+  p.q = in->d_queue;
+  p.k = k;
+  p.offs = ws.d_scan;
+  p.total = ws.d_stats + 5;
+  p.off = off;
+  p.idx = g->out_idx();
+  p.wts = g->out_w();
+  p.deg_off = off;
+  p.dedup = out->d_bits;
+  p.out_q = nullptr;
+  p.stats = ws.d_stats;
+  const uint64_t work_ub = std::max<uint64_t>(in->out_edges, 1);
+  const int grid = (int)std::min<uint64_t>((work_ub + kPushEdgesPerCta - 1) / kPushEdgesPerCta + 1,
+                                           (uint64_t)g->num_sms * 8);
+  k_push_bits<F, HW><<<std::max(grid, g->num_sms), kPushThreads, 0, g->stream>>>(p, f);
+  GG_CUDA(cudaGetLastError());
+  g->kernels += 4;
+  return GG_OK;
+}
+
 template <class F>
 int edge_map(gg_graph_s* g, gg_frontier_s* in, const F& f, int64_t threshold, uint32_t flags, gg_frontier_s** out) {
   const int64_t m = (int64_t)g->m;
@@ -441,15 +477,26 @@ int edge_map(gg_graph_s* g, gg_frontier_s* in, const F& f, int64_t threshold, ui
     if (flags & GG_EM_FORCE_CSC) coo = false;
     if ((flags & GG_EM_FORCE_COO) && g->has_coo) coo = true;
     const bool early = !coo && F::kEarlyExit;
+    // a dense step of an early-exit functor from few frontier vertices (a
+    // hub level): push the frontier's out-edges into the output bitmap
+    // instead of walking every unvisited in-list
+    const bool push_bits = early && !in->bit && g->push_dense_div > 0 && !(flags & GG_EM_FORCE_CSC) &&
+                           (uint64_t)fm * (uint64_t)g->push_dense_div <= (uint64_t)g->n;
     // GG_EM_NO_OUTPUT: the caller discards the output, which the COO pull of a
     // sum functor then does not build
     const bool no_out = (flags & GG_EM_NO_OUTPUT) && coo && F::kIdentityCommitNoop;
-    if (!in->bit && !in->has_dense) rc = frontier_to_dense(in);
+    if (push_bits) {
+      if (!in->has_sparse) rc = frontier_to_sparse(in);
+    } else if (!in->bit && !in->has_dense) {
+      rc = frontier_to_dense(in);
+    }
     if (!rc) rc = frontier_ensure_bits(o, true);
     if (!rc) rc = reset_stats(g);
     if (!rc) {
       prof_begin();
-      if (early)
+      if (push_bits)
+        rc = hw ? push_bits_launch<F, true>(g, in, o, f) : push_bits_launch<F, false>(g, in, o, f);
+      else if (early)
         rc = hw ? pull_early_launch<F, true>(g, in, o, f) : pull_early_launch<F, false>(g, in, o, f);
       else
         rc = hw ? pull_launch<F, true>(g, in, o, f, coo, no_out) : pull_launch<F, false>(g, in, o, f, coo, no_out);
@@ -466,7 +513,7 @@ int edge_map(gg_graph_s* g, gg_frontier_s* in, const F& f, int64_t threshold, ui
       o->dm = g->ws.h_stats[0];
       o->out_edges = g->ws.h_stats[1];
       g->last.kind = coo ? 3 : 2;
-      prof_end(early ? 3 : (coo ? 2 : 1), coo ? g->coo_len : g->m);
+      prof_end(push_bits ? 0 : (early ? 3 : (coo ? 2 : 1)), push_bits ? (uint64_t)tot : (coo ? g->coo_len : g->m));
     }
   } else {
     if (!in->has_sparse) rc = frontier_to_sparse(in);

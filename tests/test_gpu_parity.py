@@ -268,3 +268,21 @@ def test_bfs_early_exit_kernels(gg, rmat14, kernel):
     finally:
         g.set_tuning(gg.TUNE_EARLY_KERNEL, 0)
         g.set_dense_policy(0)
+
+
+@pytest.mark.parametrize("div", [0, 256, 1 << 30])
+def test_bfs_dense_levels_pushed_into_bitmap(gg, rmat14, div):
+    """Dense BFS levels from a small frontier run top-down into the output
+    bitmap (GG_TUNE_PUSH_DENSE_DIV; 2^30 takes every dense level that way,
+    0 none): the oracle's levels and traversed-edge counts either way."""
+    hg, g, og = rmat14
+    g.set_tuning(gg.TUNE_PUSH_DENSE_DIV, div)
+    g.set_dense_policy(1)
+    try:
+        for start in (0, 100, 12345):
+            check_bfs(g, og, start, hg)
+            _, _, st = g.bfs(start)
+            assert st.edges_traversed == og.bfs(start)[2].edges_traversed
+    finally:
+        g.set_tuning(gg.TUNE_PUSH_DENSE_DIV, 0)
+        g.set_dense_policy(0)
