@@ -12,6 +12,8 @@ each run through the library's C ABI (gg_bfs / gg_pagerank / gg_spmv).
            loops (CUDA events on the library's stream), graph resident in HBM
   e2e    = same edges / host wall time of the K steps' C-ABI calls, including
            every step's H2D copy of the SpMV input vector from pinned memory
+           (staged with gg_spmv_stage_input, so that it crosses while
+           PageRank runs)
            and D2H copies of every result array of the reference's apps (BFS
            parents, PageRank ranks, SpMV y); the copies leave on the
            library's copy stream while the next application (and the next
@@ -252,13 +254,20 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
     # while the next application runs; the step ends when all have arrived
     g.set_tuning(gg.TUNE_ASYNC_RESULTS, 0 if args.copies == "wait" else 1)
 
+    staged = args.copies != "wait" and args.spmv_input == "staged"
+
     def step():
         use("bfs")
         _, _, b = g.bfs(args.start, out=(par.array, None))  # app/BFS.C's result is Parents
+        if staged:  # SpMV's input crosses PCIe while PageRank runs
+            g.spmv_stage_input(x.array)
         use("pagerank")
         _, p = g.pagerank(10, out=ranks.array)
         use("spmv")
-        _, s = g.spmv(x.array, out=y.array)
+        if staged:
+            _, s = g.spmv_staged(out=y.array)
+        else:
+            _, s = g.spmv(x.array, out=y.array)
         if args.copies != "pipeline":
             g.synchronize()
         return b, p, s
@@ -378,6 +387,8 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
                                      "overlap": "to pinned host arrays on a copy stream, overlapping the next "
                                                 "application; the step waits for all (gg_graph_synchronize)",
                                      "wait": "each call returns after its copy"}[args.copies],
+                   "spmv_input": "uploaded while PageRank runs (gg_spmv_stage_input)" if staged else
+                                 "uploaded by the gg_spmv call",
                    "vertex_order": ["given ids", "hottest sources first inside each partition (results in the "
                                     "given ids)"][args.vertex_order],
                    "autotuned_knobs": knobs or None, "autotune_seconds": round(tune_s, 2)},
@@ -733,6 +744,9 @@ def main():
                          "stopping after the last step's copies (pipeline); overlap the next application, each "
                          "step waiting for its copies (overlap) (both GG_TUNE_ASYNC_RESULTS 1); or finish inside "
                          "each call (wait)")
+    ap.add_argument("--spmv-input", choices=["staged", "call"], default="staged",
+                    help="SpMV's input uploaded while PageRank runs (gg_spmv_stage_input + gg_spmv_staged) or "
+                         "by the gg_spmv call itself")
     ap.add_argument("--pr-loop", choices=["graph", "host"], default="graph",
                     help="PageRank iterations as one CUDA graph (GG_TUNE_PR_GRAPH 1) or host-driven")
     ap.add_argument("--traffic", type=float, default=None,

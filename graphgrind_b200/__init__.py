@@ -158,6 +158,8 @@ _sig("gg_graph_device_arrays", C.c_int, _P, C.POINTER(_P), C.POINTER(_P), C.POIN
 _sig("gg_graph_vertex_order", C.c_int, _P, _P)
 _sig("gg_graph_device_weights", C.c_int, _P, C.POINTER(_P), C.POINTER(_P))
 _sig("gg_graph_coo_layout", C.c_int, _P, C.POINTER(C.c_uint64), _P, C.POINTER(C.c_uint64), _P, _P)
+_sig("gg_spmv_stage_input", C.c_int, _P, _P)
+_sig("gg_spmv_staged", C.c_int, _P, _P, C.POINTER(RunStats))
 _sig("gg_frontier_single", C.c_int, _P, C.c_uint32, C.POINTER(_P))
 _sig("gg_frontier_all", C.c_int, _P, C.POINTER(_P))
 _sig("gg_frontier_empty", C.c_int, _P, C.POINTER(_P))
@@ -234,7 +236,7 @@ EXPORTED = [
     "gg_pagerank_weighted_create", "gg_pagerank_weighted_destroy", "gg_pagerank_weighted_fwd",
     "gg_pagerank_weighted_bwd", "gg_autotune", "gg_autotune_build", "gg_autotune_ppr_k",
     "gg_hot_first_order", "gg_graph_vertex_order", "gg_host_graph_read_gpu", "gg_graph_device_weights",
-    "gg_graph_coo_layout", "gg_vebo_gpu",
+    "gg_graph_coo_layout", "gg_vebo_gpu", "gg_spmv_stage_input", "gg_spmv_staged",
 ]
 
 
@@ -663,6 +665,20 @@ class Graph:
             x = np.ascontiguousarray(x, np.float32)
             xp = _ptr(x)
         check(lib.gg_spmv(self.h, xp, _ptr(y), C.byref(st)), "gg_spmv")
+        return y, _run(st)
+
+    def spmv_stage_input(self, x):
+        """gg_spmv_stage_input: start the upload of x (keep it alive and unchanged
+        until spmv_staged returns; pinned memory overlaps best)."""
+        self._staged = x if isinstance(x, np.ndarray) and x.dtype == np.float32 else np.ascontiguousarray(x, np.float32)
+        check(lib.gg_spmv_stage_input(self.h, _ptr(self._staged)), "gg_spmv_stage_input")
+
+    def spmv_staged(self, out=None):
+        """gg_spmv_staged: SpMV on the staged input; (y, Run)."""
+        y = out if out is not None else np.empty(self.n, np.float32)
+        st = RunStats()
+        check(lib.gg_spmv_staged(self.h, _ptr(y), C.byref(st)), "gg_spmv_staged")
+        self._staged = None
         return y, _run(st)
 
     def bellman_ford(self, start=100):

@@ -1013,8 +1013,26 @@ static int run_pagerank_delta(gg_graph_s* g, float* ranks, gg_run_stats* st) {
   return GG_OK;
 }
 
-// app/SPMV.C:64-92
-static int run_spmv(gg_graph_s* g, const float* x_in, float* y_out, gg_run_stats* st) {
+// An SpMV input uploaded ahead of its gg_spmv_staged call, on the copy
+// stream into given-order array 1, so that the upload overlaps whatever the
+// stream still runs (the previous application).  The copy starts after the
+// work already queued on the stream (which may still read that array) and
+// after the copies already leaving from it (same copy stream).
+static int stage_spmv_input(gg_graph_s* g, const float* x_host) {
+  if (!g->async_results || !g->ws.d_order[1] || !g->copy_stream)
+    return fail(GG_ERR_UNSUPPORTED, "gg_spmv_stage_input needs GG_TUNE_ASYNC_RESULTS 1");
+  if (!g->input_ready) GG_CUDA(cudaEventCreateWithFlags(&g->input_ready, cudaEventDisableTiming));
+  GG_CUDA(cudaEventRecord(g->result_ready, g->stream));
+  GG_CUDA(cudaStreamWaitEvent(g->copy_stream, g->result_ready, 0));
+  GG_CUDA(cudaMemcpyAsync(g->ws.d_order[1], x_host, 4ull * g->n, cudaMemcpyHostToDevice, g->copy_stream));
+  GG_CUDA(cudaEventRecord(g->input_ready, g->copy_stream));
+  g->input_staged = true;
+  return GG_OK;
+}
+
+// app/SPMV.C:64-92.  x_in: host input, or NULL for x = 1/n; staged: the
+// input was uploaded by stage_spmv_input (x_in is then ignored).
+static int run_spmv(gg_graph_s* g, const float* x_in, float* y_out, gg_run_stats* st, bool staged = false) {
   const uint32_t n = g->n;
   g->kernels = 0;
   DevBuf<float> x, y;
@@ -1025,11 +1043,19 @@ static int run_spmv(gg_graph_s* g, const float* x_in, float* y_out, gg_run_stats
   // which the result uses after it (array 0 may still be leaving for the
   // host with an earlier result)
   float* xg = g->relabeled ? reinterpret_cast<float*>(g->ws.d_order[1]) : x.p;
+  if (staged) {
+    GG_CUDA(cudaStreamWaitEvent(g->stream, g->input_ready, 0));
+    g->input_staged = false;
+    x_in = nullptr;
+    xg = reinterpret_cast<float*>(g->ws.d_order[1]);
+  }
   if (x_in && g->relabeled) GG_TRY(slot_write_wait(g, 1));
   if (x_in) GG_CUDA(cudaMemcpyAsync(xg, x_in, 4ull * n, cudaMemcpyHostToDevice, g->stream));
   EventTimer tm(g->stream);
-  if (x_in && g->relabeled) GG_TRY(device_order<float>(g, xg, 1, x.p));
-  if (!x_in) GG_TRY(fill<float>(g, x.p, n, (float)(1 / (double)n)));
+  if ((x_in || staged) && g->relabeled) GG_TRY(device_order<float>(g, xg, 1, x.p));
+  if (staged && !g->relabeled)
+    GG_CUDA(cudaMemcpyAsync(x.p, xg, 4ull * n, cudaMemcpyDeviceToDevice, g->stream));
+  if (!x_in && !staged) GG_TRY(fill<float>(g, x.p, n, (float)(1 / (double)n)));
   // a renumbered graph's sums go straight to the given ids, in array 1 (the
   // input staged there was consumed above)
   float* yd = g->relabeled ? reinterpret_cast<float*>(g->ws.d_order[1]) : y.p;
@@ -1339,6 +1365,15 @@ int gg_pagerank_converge(gg_graph_t g, int32_t max_iter, double eps, float* rank
 int gg_spmv(gg_graph_t g, const float* x, float* y, gg_run_stats* st) {
   if (!g) return fail(GG_ERR_INVALID_ARG, "gg_spmv: null graph");
   return run_spmv(g, x, y, st);
+}
+int gg_spmv_stage_input(gg_graph_t g, const float* x) {
+  if (!graph_live(g) || !x) return fail(GG_ERR_INVALID_ARG, "gg_spmv_stage_input: bad arguments");
+  return stage_spmv_input(g, x);
+}
+int gg_spmv_staged(gg_graph_t g, float* y, gg_run_stats* st) {
+  if (!graph_live(g)) return fail(GG_ERR_INVALID_ARG, "gg_spmv_staged: not a live graph");
+  if (!g->input_staged) return fail(GG_ERR_INVALID_ARG, "gg_spmv_staged: no input staged (gg_spmv_stage_input)");
+  return run_spmv(g, nullptr, y, st, true);
 }
 int gg_bellman_ford(gg_graph_t g, uint32_t start, int32_t* dist, gg_run_stats* st) {
   if (!g || start >= g->n) return fail(GG_ERR_INVALID_ARG, "gg_bellman_ford: bad arguments");

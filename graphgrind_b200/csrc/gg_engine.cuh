@@ -158,6 +158,8 @@ struct gg_graph_s {
   int async_results = 0;
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t result_ready = nullptr;                // on stream: the result to copy is complete
+  cudaEvent_t input_ready = nullptr;                 // on copy_stream: a staged SpMV input has arrived
+  bool input_staged = false;                         // given-order array 1 holds a staged SpMV input
   cudaEvent_t slot_copied[2] = {nullptr, nullptr};  // on copy_stream: the last copy out of ws.d_order[k]
   gg::PrLoop* pr_loop = nullptr;  // created by the first graph-driven PageRank call
   int coo_kernel = 6;  // 0 CTA ring (k_pull), 1 per-warp direct loads, 2/3 per-warp bulk-copy rings, 6 direct loads

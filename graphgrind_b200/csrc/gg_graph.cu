@@ -590,6 +590,7 @@ static void graph_release(gg_graph_s* g) {
   for (auto& e : g->slot_copied)
     if (e) cudaEventDestroy(e);
   if (g->result_ready) cudaEventDestroy(g->result_ready);
+  if (g->input_ready) cudaEventDestroy(g->input_ready);
   if (g->copy_stream) cudaStreamDestroy(g->copy_stream);
   if (g->stream) cudaStreamDestroy(g->stream);
   delete g;

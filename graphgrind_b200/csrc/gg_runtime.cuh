@@ -118,6 +118,10 @@ int given_order(gg_graph_s* g, const T* dev, uint32_t k, DevBuf<T>& tmp, const T
 // the host that still reads it (GG_TUNE_ASYNC_RESULTS) is done.
 inline int slot_write_wait(gg_graph_s* g, int slot) {
   if (g->slot_copied[slot]) GG_CUDA(cudaStreamWaitEvent(g->stream, g->slot_copied[slot], 0));
+  if (slot == 1 && g->input_staged) {  // a staged SpMV input in the array is given up
+    GG_CUDA(cudaStreamWaitEvent(g->stream, g->input_ready, 0));
+    g->input_staged = false;
+  }
   return GG_OK;
 }
 // The same for one 4-byte value per vertex, into the graph's given-order

@@ -487,6 +487,17 @@ int gg_pagerank_converge(gg_graph_t g, int32_t max_iter, double eps, float* rank
 int gg_pagerank_delta(gg_graph_t g, float* ranks, gg_run_stats* st);
 /* app/SPMV.C:64-92 with x = 1/n (x_in == NULL) or x_in[n]: y[n] = A^T-weighted sum. */
 int gg_spmv(gg_graph_t g, const float* x_in, float* y, gg_run_stats* st);
+/* gg_spmv with its input uploaded ahead: gg_spmv_stage_input starts the
+ * upload of x[n] (pinned host memory) on the graph's copy stream after the
+ * work already queued (so it overlaps the preceding call, e.g. a PageRank),
+ * and gg_spmv_staged runs SPMV on it (its device work waits for the
+ * upload).  Needs GG_TUNE_ASYNC_RESULTS 1; x must stay unchanged until
+ * gg_spmv_staged returns; one input is staged at a time (a second stage call
+ * replaces it), and a call in between that stages a result in the same
+ * array (BFS levels, SpMV, BC dependencies) gives it up: gg_spmv_staged then
+ * returns GG_ERR_INVALID_ARG. */
+int gg_spmv_stage_input(gg_graph_t g, const float* x_in);
+int gg_spmv_staged(gg_graph_t g, float* y, gg_run_stats* st);
 /* app/BellmanFord.C:106-145: dist[n] (1073741823 = unreached). */
 int gg_bellman_ford(gg_graph_t g, uint32_t start, int32_t* dist, gg_run_stats* st);
 /* app/BC.C:156-226 single source: dependencies[n], num_paths[n] (forward counts). */

@@ -70,3 +70,36 @@ def test_async_switch(gg, graph):
     with pytest.raises(gg.GGError):
         g.set_tuning(gg.TUNE_ASYNC_RESULTS, 2)
     g.synchronize()
+
+
+def test_staged_spmv_input(gg, graph):
+    """gg_spmv_stage_input uploads SpMV's input on the copy stream while the
+    preceding call still runs; gg_spmv_staged then gives gg_spmv's result.
+    Staging into the array a BFS level output also uses gives the input up,
+    and staging needs the asynchronous mode."""
+    hg, g = graph
+    n = hg.n
+    x = np.random.default_rng(8).random(n, dtype=np.float32)
+    g.set_tuning(gg.TUNE_ASYNC_RESULTS, 0)
+    y0, _ = g.spmv(x)
+    with pytest.raises(gg.GGError) as e:
+        g.spmv_stage_input(x)
+    assert e.value.code == gg.ERR_UNSUPPORTED
+    g.set_tuning(gg.TUNE_ASYNC_RESULTS, 1)
+    xp, yp, rp = gg.PinnedArray(n, np.float32), gg.PinnedArray(n, np.float32), gg.PinnedArray(n, np.float32)
+    xp.array[:] = x
+    for _ in range(3):  # back to back, as a serving loop stages each request's input
+        g.bfs(5)
+        g.spmv_stage_input(xp.array)
+        g.pagerank(10, out=rp.array)  # runs while the input uploads
+        _, run = g.spmv_staged(out=yp.array)
+        g.synchronize()
+        np.testing.assert_allclose(yp.array, y0, rtol=1e-6, atol=1e-7 * np.abs(y0).max())
+        assert run.edges_traversed == hg.m
+    g.spmv_stage_input(xp.array)
+    lev = gg.PinnedArray(n, np.int32)
+    g.bfs(5, out=(np.empty(n, np.int32), lev.array))  # levels are staged in the same array
+    with pytest.raises(gg.GGError) as e:
+        g.spmv_staged(out=yp.array)
+    assert e.value.code == gg.ERR_INVALID_ARG
+    g.synchronize()
