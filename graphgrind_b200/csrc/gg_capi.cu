@@ -193,11 +193,16 @@ static int run_bfs(gg_graph_s* g, uint32_t start, int32_t* parents, int32_t* lev
   GG_TRY(set_one<int32_t>(g, par.p, start, (int32_t)start));
   GG_TRY(set_one<int32_t>(g, lev.p, start, 0));
   FrontierHold F;
-  GG_TRY(gg_frontier_single(g, start, &F.f));
   int32_t round = 0;
   uint64_t trav = 0;
   const int64_t thr = app_threshold(g);
-  while (F.f->dm > 0) {
+  // every level in one cooperative launch (its dense levels pull over the CSC;
+  // a graph told to pull over the COO keeps the host loop for them)
+  if (g->device_loop == 2 && !g->transposed && g->dense_policy != 2)
+    GG_TRY(bfs_device_full(g, start, par.p, lev.p, (uint64_t)thr, &round, &trav));
+  else
+    GG_TRY(gg_frontier_single(g, start, &F.f));
+  while (F.f && F.f->dm > 0) {
     if (g->device_loop && (int64_t)(F.f->dm + F.f->out_edges) <= thr && F.f->out_edges > 0) {
       // sparse levels run on the device until the frontier empties or turns dense
       int32_t levels_run = 0;

@@ -104,7 +104,7 @@ struct Workspace {
   uint32_t bsum_cap = 0;
   double* d_red = nullptr;                // reduction scratch (double)
   double* h_red = nullptr;                // pinned
-  unsigned long long* d_loop = nullptr;   // state of the device-driven level loop (16 words)
+  unsigned long long* d_loop = nullptr;   // state of the device-driven level loops (64 words)
   uint32_t* d_order[2] = {nullptr, nullptr};  // renumbered graphs: n-entry arrays for the given-order copies
 };
 
@@ -146,8 +146,9 @@ struct gg_graph_s {
   cudaEvent_t prof_ev[2] = {nullptr, nullptr};
   int dense_policy = 0;
   int sparse_div = 20;  // the apps' edgeMap threshold is m / sparse_div (app/*.C pass m/20)
-  int device_loop = 1;  // BFS runs consecutive sparse levels in one cooperative launch
+  int device_loop = 2;  // 2: the whole BFS in one cooperative launch; 1: runs of sparse levels; 0: none
   int cc_algo = 0;      // Components on symmetric graphs: 0 label propagation, 1 union-find
+  int loop_ctas_per_sm = 0;  // CTAs per SM of the device BFS loops (capped by occupancy); 0: 4 / 8 by loop
   uint32_t loop_wait_budget = 1u << 22;  // spins of the BFS level loop's grid-barrier wait
   int early_kernel = 0;  // early-exit dense pull: 0 one lane per destination (faster on R-MAT), 1 8-lane groups
   int push_dense_div = 0;  // a dense edgeMap of an early-exit functor pushes into a bitmap when

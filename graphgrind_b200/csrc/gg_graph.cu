@@ -747,7 +747,7 @@ static int graph_build(const gg_host_graph* hg_given, const gg_build_opts* opts_
   GG_CUDA(cudaMemset(g->ws.d_dedup, 0, sizeof(uint32_t) * ((size_t)g->words() + 4)));
   GG_TRY(dev_alloc(g, &g->ws.d_scan, (size_t)n + 4));
   GG_TRY(dev_alloc(g, &g->ws.d_red, 64));
-  GG_TRY(dev_alloc(g, &g->ws.d_loop, 16));
+  GG_TRY(dev_alloc(g, &g->ws.d_loop, 64));
   if (g->relabeled)
     for (auto& a : g->ws.d_order) GG_TRY(dev_alloc(g, &a, (size_t)n + 4));
   GG_CUDA(cudaMallocHost((void**)&g->ws.h_red, 64 * sizeof(double)));
@@ -922,7 +922,7 @@ int gg_graph_set_tuning(gg_graph_t g, int32_t key, int64_t value) {
       g->sparse_div = (int)value;
       return GG_OK;
     case GG_TUNE_DEVICE_LOOP:
-      if (value != 0 && value != 1) return fail(GG_ERR_INVALID_ARG, "device loop switch must be 0 or 1");
+      if (value < 0 || value > 2) return fail(GG_ERR_INVALID_ARG, "device loop switch must be 0, 1 or 2");
       g->device_loop = (int)value;
       return GG_OK;
     case GG_TUNE_CC_ALGO:
@@ -940,6 +940,10 @@ int gg_graph_set_tuning(gg_graph_t g, int32_t key, int64_t value) {
     case GG_TUNE_PUSH_DENSE_DIV:
       if (value < 0 || value > (1ll << 30)) return fail(GG_ERR_INVALID_ARG, "push-dense divisor must be 0..2^30");
       g->push_dense_div = (int)value;
+      return GG_OK;
+    case GG_TUNE_LOOP_CTAS:
+      if (value < 0 || value > 16) return fail(GG_ERR_INVALID_ARG, "loop CTAs per SM must be 0..16");
+      g->loop_ctas_per_sm = (int)value;
       return GG_OK;
     case GG_TUNE_LOOP_WAIT_BUDGET:
       if (value < 0 || value > (1ll << 22))
@@ -995,6 +999,9 @@ int gg_graph_get_tuning(gg_graph_t g, int32_t key, int64_t* value) {
       return GG_OK;
     case GG_TUNE_PUSH_DENSE_DIV:
       *value = g->push_dense_div;
+      return GG_OK;
+    case GG_TUNE_LOOP_CTAS:
+      *value = g->loop_ctas_per_sm;
       return GG_OK;
     default:
       return fail(GG_ERR_INVALID_ARG, "unknown tuning key %d", key);

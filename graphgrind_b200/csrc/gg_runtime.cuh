@@ -170,6 +170,8 @@ int frontier_to_sparse(gg_frontier_s* f);
 void frontier_free(gg_frontier_s* f);
 int bfs_device_levels(gg_graph_s* g, gg_frontier_s** F, int32_t* parents, int32_t* levels, int32_t round0,
                       uint64_t threshold, int32_t* rounds, uint64_t* trav);
+int bfs_device_full(gg_graph_s* g, uint32_t start, int32_t* parents, int32_t* levels, uint64_t threshold,
+                    int32_t* rounds, uint64_t* trav);
 int reset_stats(gg_graph_s* g);
 void pr_loop_free(gg_graph_s* g);  // releases the captured PageRank loop and its buffers
 int read_stats(gg_graph_s* g);  // blocks; checks the device error word

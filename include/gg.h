@@ -336,9 +336,19 @@ int gg_graph_set_dense_policy(gg_graph_t g, int32_t policy);
  *                         default for graphs built with coo_window == 0)
  *   GG_TUNE_SPARSE_DIV    the application loops (gg_bfs ... gg_bc) call edgeMap
  *                         with threshold m / value (20 in the reference apps)
- *   GG_TUNE_DEVICE_LOOP   1 (default): gg_bfs runs consecutive sparse levels in
- *                         one cooperative launch that applies the direction
- *                         rule on the device; 0: one host round trip per level
+ *   GG_TUNE_DEVICE_LOOP   2 (default): gg_bfs runs the whole BFS in one
+ *                         cooperative launch, dense levels bottom-up over the
+ *                         in-edges (first frontier in-neighbour, as
+ *                         edgeMapDenseCSC with BFS_F) and sparse levels
+ *                         top-down, the direction rule and the queue/bitmap
+ *                         conversions done on the device (transposed graphs
+ *                         and dense policy 2 take mode 1); 1: runs of
+ *                         consecutive sparse levels in one cooperative launch
+ *                         each, dense levels from the host; 0: one host round
+ *                         trip per level
+ *   GG_TUNE_LOOP_CTAS     CTAs per SM of those cooperative launches, 0..16
+ *                         (0, the default: 4 for mode 1, 8 for mode 2; capped
+ *                         by the kernel's occupancy)
  *   GG_TUNE_CC_ALGO       0 (default): gg_components runs app/Components.C's
  *                         label propagation through edgeMap; 1: on symmetric
  *                         graphs, a union-find pass over the edges (each root
@@ -397,6 +407,7 @@ int gg_graph_set_dense_policy(gg_graph_t g, int32_t policy);
 #define GG_TUNE_LOOP_WAIT_BUDGET 8
 #define GG_TUNE_EARLY_KERNEL 9
 #define GG_TUNE_PUSH_DENSE_DIV 10
+#define GG_TUNE_LOOP_CTAS 11
 int gg_graph_set_tuning(gg_graph_t g, int32_t key, int64_t value);
 int gg_graph_get_tuning(gg_graph_t g, int32_t key, int64_t* value);
 

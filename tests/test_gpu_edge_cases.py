@@ -167,14 +167,22 @@ def test_traversals(gg, orc, name, policy, vorder):
         assert rel_l1(dep[fin], odep[fin]) <= 1e-4
 
 
+@pytest.mark.parametrize("loop", [0, 1, 2])
 @pytest.mark.parametrize("name", CASES)
-def test_device_loop_off(gg, orc, name):
-    """BFS with one host round trip per level gives the same levels."""
+def test_device_loop_modes(gg, orc, name, loop):
+    """BFS with one host round trip per level (0), with runs of sparse levels
+    in one cooperative launch (1) and with every level in one (2, the
+    default) gives the oracle's levels, rounds and traversed edges, with
+    valid parents."""
     hg, og, pref = _case(gg, orc, name)
     g = gg.Graph(hg, partitions=_partitions(gg, hg, pref))
-    g.set_tuning(gg.TUNE_DEVICE_LOOP, 0)
+    g.set_tuning(gg.TUNE_DEVICE_LOOP, loop)
     for s in _starts(hg):
-        np.testing.assert_array_equal(g.bfs(s)[1], og.bfs(s)[1])
+        par, lev, run = g.bfs(s)
+        _, olev, ost = og.bfs(s)
+        np.testing.assert_array_equal(lev, olev, err_msg=f"bfs from {s}")
+        _check_parents(par, lev, hg, s)
+        assert run.rounds == ost.rounds and run.edges_traversed == ost.edges_traversed
 
 
 @pytest.mark.parametrize("vorder", [0, 1])

@@ -144,9 +144,10 @@ def test_apps_with_each_coo_kernel(gg, orc, coo_kernel, coo_window):
 
 @pytest.mark.parametrize("graph", ["grid", "rmat_sym", "rmat_dir", "rmat_dir_t"])
 def test_bfs_device_loop_matches_host_loop(gg, orc, graph):
-    """BFS with consecutive sparse levels in one cooperative launch gives the
-    per-level host loop's levels, level count and traversed edges (and the
-    oracle's), for every push/pull threshold."""
+    """BFS with consecutive sparse levels in one cooperative launch (1), and
+    with every level in one (2), gives the per-level host loop's levels, level
+    count and traversed edges (and the oracle's), for every push/pull
+    threshold.  Transposed graphs take mode 1's path under mode 2."""
     if graph == "grid":
         hg = gg.HostGraph.grid(96, 0.002, seed=5)
     else:
@@ -157,11 +158,11 @@ def test_bfs_device_loop_matches_host_loop(gg, orc, graph):
         g.transpose()
         oh = hg.transpose()
     og = orc.Graph.from_host(oh)
-    assert g.get_tuning(gg.TUNE_DEVICE_LOOP) == 1
+    assert g.get_tuning(gg.TUNE_DEVICE_LOOP) == 2
     for div in (20, 2, 1000):
         g.set_tuning(gg.TUNE_SPARSE_DIV, div)
-        for start in (0, 77):
-            g.set_tuning(gg.TUNE_DEVICE_LOOP, 1)
+        for start, loop in ((0, 1), (77, 1), (0, 2), (77, 2)):
+            g.set_tuning(gg.TUNE_DEVICE_LOOP, loop)
             par, lev, run = g.bfs(start)
             g.set_tuning(gg.TUNE_DEVICE_LOOP, 0)
             par0, lev0, run0 = g.bfs(start)

@@ -286,3 +286,27 @@ def test_bfs_dense_levels_pushed_into_bitmap(gg, rmat14, div):
     finally:
         g.set_tuning(gg.TUNE_PUSH_DENSE_DIV, 0)
         g.set_dense_policy(0)
+
+
+@pytest.mark.parametrize("ctas", [0, 1, 4, 16])
+def test_bfs_every_level_on_device(gg, rmat14, ctas):
+    """GG_TUNE_DEVICE_LOOP 2 runs the whole BFS in one cooperative launch
+    (bottom-up dense levels, top-down sparse ones, the direction rule and the
+    bitmap-to-queue conversion on the device): the oracle's levels, rounds
+    and traversed edges, at any grid size (GG_TUNE_LOOP_CTAS, capped by
+    occupancy; 0 the default per loop)."""
+    hg, g, og = rmat14
+    g.set_tuning(gg.TUNE_DEVICE_LOOP, 2)
+    g.set_tuning(gg.TUNE_LOOP_CTAS, ctas)
+    try:
+        for start in (0, 100, 12345):
+            check_bfs(g, og, start, hg)
+            _, _, st = g.bfs(start)
+            assert st.edges_traversed == og.bfs(start)[2].edges_traversed
+        for div in (1, 1000):  # every level dense / every level sparse
+            g.set_tuning(gg.TUNE_SPARSE_DIV, div)
+            check_bfs(g, og, 100, hg)
+    finally:
+        g.set_tuning(gg.TUNE_SPARSE_DIV, 20)
+        g.set_tuning(gg.TUNE_DEVICE_LOOP, 2)
+        g.set_tuning(gg.TUNE_LOOP_CTAS, 0)

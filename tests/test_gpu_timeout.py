@@ -1,7 +1,7 @@
 """A bounded device wait driven to expiry on a healthy graph.
 
-The device BFS level loop (GG_TUNE_DEVICE_LOOP) ends every level at a grid
-barrier whose wait is bounded.  With the budget set to 0 probes
+The device BFS loops (GG_TUNE_DEVICE_LOOP 1: consecutive sparse levels, 2:
+every level) end every level at a grid barrier whose wait is bounded.  With the budget set to 0 probes
 (GG_TUNE_LOOP_WAIT_BUDGET, a test knob), every CTA that arrives before the
 last one gives up at once: all CTAs return (the one that passed stops at the
 next barrier), nothing waits on anything that will not come, the kernel
@@ -15,13 +15,15 @@ from conftest import ok_partitions
 pytestmark = pytest.mark.gpu
 
 
+@pytest.mark.parametrize("loop", [1, 2])
 @pytest.mark.parametrize("sym", [True, False])
-def test_loop_barrier_timeout_then_recovery(gg, orc, sym):
+def test_loop_barrier_timeout_then_recovery(gg, orc, sym, loop):
     hg = gg.HostGraph.rmat(14, 16, seed=3, symmetric=sym)
     g = gg.Graph(hg, partitions=ok_partitions(hg, 16))
     og = orc.Graph.from_host(hg)
     _, olev, _ = og.bfs(100)
-    assert g.get_tuning(gg.TUNE_DEVICE_LOOP) == 1
+    assert g.get_tuning(gg.TUNE_DEVICE_LOOP) == 2
+    g.set_tuning(gg.TUNE_DEVICE_LOOP, loop)
     assert g.get_tuning(gg.TUNE_LOOP_WAIT_BUDGET) == 1 << 22
     g.set_tuning(gg.TUNE_LOOP_WAIT_BUDGET, 0)
     for _ in range(2):

@@ -116,11 +116,11 @@ def test_device_loop_and_thresholds(gg, rmat13):
     hg, g, og, _ = rmat13
     for div in (2, 20, 1000):
         g.set_tuning(gg.TUNE_SPARSE_DIV, div)
-        for loop in (0, 1):
+        for loop in (0, 1, 2):
             g.set_tuning(gg.TUNE_DEVICE_LOOP, loop)
             check_bfs(g, og, hg, 77)
     g.set_tuning(gg.TUNE_SPARSE_DIV, 20)
-    g.set_tuning(gg.TUNE_DEVICE_LOOP, 1)
+    g.set_tuning(gg.TUNE_DEVICE_LOOP, 2)
 
 
 def test_batched_forms(gg, rmat13):
