@@ -424,27 +424,38 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
 def run_other_apps(gg, hg, g, args):
     """The rest of the RMAT-24 application list (Components, PageRankDelta with
     eps 1e-7, BellmanFord from the start vertex on uint32 weights in [1,100]),
-    outside the timed step, each the best of 3 device times."""
+    outside the timed step, each the best of 3 device times; unless
+    --no-autotune, each with the runtime knobs the library's autotuner picks
+    for it on its graph (recorded under "knobs")."""
     out = {}
-    ids = np.empty(hg.n, np.int32)
-    ranks = np.empty(hg.n, np.float32)
-    for name, fn in (("components", lambda: g.components()[1]),
-                     ("pagerank_delta", lambda: g.pagerank_delta()[1])):
+
+    def tuned(graph, app):
+        if args.no_autotune:
+            return None
+        best = graph.autotune(app, start=args.start)[0]
+        kb = {k: best[k] for k in ("dense_policy", "coo_kernel", "sparse_div")}
+        graph.set_tuning(gg.TUNE_DENSE_POLICY, kb["dense_policy"])
+        graph.set_tuning(gg.TUNE_COO_KERNEL, kb["coo_kernel"])
+        graph.set_tuning(gg.TUNE_SPARSE_DIV, kb["sparse_div"])
+        return kb
+
+    def measure(name, fn, kb):
         fn()
         runs = [fn() for _ in range(3)]
         r = min(runs, key=lambda x: x.ms)
         out[name] = {"ms": round(r.ms, 3), "rounds": r.rounds, "gteps": round(r.edges_traversed / r.ms / 1e6, 2)}
+        if kb is not None:
+            out[name]["knobs"] = kb
+
+    for name, app, fn in (("components", gg.APP_COMPONENTS, lambda: g.components()[1]),
+                          ("pagerank_delta", gg.APP_PAGERANK_DELTA, lambda: g.pagerank_delta()[1])):
+        measure(name, fn, tuned(g, app))
     hw = make_graph(gg, args.scale, 2, gg.W_INT32)
     gw = gg.Graph(hw, partitions=args.partitions, tile_edges=args.tile_edges, vertex_order=args.vertex_order,
                   order=gg.ORDER_HILBERT if args.order == "hilbert" else gg.ORDER_CSR,
                   coo_tile_vertices=args.coo_tile_vertices)
-    gw.bellman_ford(args.start)
-    runs = [gw.bellman_ford(args.start)[1] for _ in range(3)]
-    r = min(runs, key=lambda x: x.ms)
-    out["bellman_ford"] = {"ms": round(r.ms, 3), "rounds": r.rounds,
-                           "gteps": round(r.edges_traversed / r.ms / 1e6, 2)}
+    measure("bellman_ford", lambda: gw.bellman_ford(args.start)[1], tuned(gw, gg.APP_BELLMAN_FORD))
     gw.close()
-    del ids, ranks
     return out
 
 

@@ -184,6 +184,7 @@ TUNE_LOOP_WAIT_BUDGET = 8
 TUNE_EARLY_KERNEL = 9
 TUNE_PUSH_DENSE_DIV = 10
 TUNE_LOOP_CTAS = 11
+TUNE_ROUND_GRAPH = 12
 APP_BFS, APP_COMPONENTS, APP_PAGERANK, APP_PAGERANK_DELTA, APP_SPMV, APP_BELLMAN_FORD, APP_BC = range(1, 8)
 _sig("gg_vertex_map", C.c_int, _P, _P, C.c_int32, _P)
 _sig("gg_vertex_filter", C.c_int, _P, _P, C.c_int32, _P, C.POINTER(_P))

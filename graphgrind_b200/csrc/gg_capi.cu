@@ -43,6 +43,15 @@ struct FrontierHold {
   }
 };
 
+// Runs of dense COO rounds of BellmanFord and Components as one CUDA graph
+// (defined with the PageRank graph below).
+enum { kRoundLoopBf = 0, kRoundLoopCc = 1 };
+static RoundLoop* round_loop_get(gg_graph_s* g, int app);
+static int32_t* round_loop_array(RoundLoop* L, int i);
+static bool round_takes_coo(const gg_graph_s* g, const gg_frontier_s* f);
+static int round_loop_run(gg_graph_s* g, RoundLoop* L, FrontierHold& F, uint32_t max_rounds, int64_t* round,
+                          uint64_t* trav);
+
 // contrib[s] = val[s] / outdeg(s)   (0 for out-degree 0, never gathered)
 __global__ void k_div_outdeg(uint32_t n, const float* val, const uint32_t* off, float* contrib) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -374,26 +383,39 @@ static int run_cc_union_find(gg_graph_s* g, int32_t* ids_out, gg_run_stats* st) 
 static int run_cc(gg_graph_s* g, int32_t* ids_out, gg_run_stats* st) {
   if (g->cc_algo == 1 && g->symmetric) return run_cc_union_find(g, ids_out, st);
   const uint32_t n = g->n;
+  RoundLoop* L = round_loop_get(g, kRoundLoopCc);  // its arrays, when its graph runs the dense rounds
   g->kernels = 0;
-  DevBuf<int32_t> ids, prev;
-  GG_TRY(ids.alloc(g, n));
-  GG_TRY(prev.alloc(g, n));
+  DevBuf<int32_t> idsb, prevb;
+  int32_t *ids = nullptr, *prev = nullptr;
+  if (L) {
+    ids = round_loop_array(L, 0);
+    prev = round_loop_array(L, 1);
+  } else {
+    GG_TRY(idsb.alloc(g, n));
+    GG_TRY(prevb.alloc(g, n));
+    ids = idsb.p;
+    prev = prevb.p;
+  }
   EventTimer tm(g->stream);
   // IDs[i] = i (app/Components.C:112): the given id, also on a renumbered graph
   if (g->relabeled)
-    GG_CUDA(cudaMemcpyAsync(ids.p, g->d_old_of_new, 4ull * n, cudaMemcpyDeviceToDevice, g->stream));
+    GG_CUDA(cudaMemcpyAsync(ids, g->d_old_of_new, 4ull * n, cudaMemcpyDeviceToDevice, g->stream));
   else
-    k_iota<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>((uint32_t*)ids.p, n);
+    k_iota<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>((uint32_t*)ids, n);
   FrontierHold F;
   GG_TRY(gg_frontier_all(g, &F.f));
-  int rounds = 0;
+  int64_t rounds = 0;
   uint64_t trav = 0;
   while (F.f->dm > 0) {
-    VCcCopy vc{ids.p, prev.p};
+    if (L && round_takes_coo(g, F.f)) {  // dense COO rounds on the device
+      GG_TRY(round_loop_run(g, L, F, n, &rounds, &trav));  // labels only fall: at most n rounds
+      continue;
+    }
+    VCcCopy vc{ids, prev};
     GG_TRY(vertex_map(g, F.f, vc));
     CcF f;
-    f.ids = ids.p;
-    f.prev = prev.p;
+    f.ids = ids;
+    f.prev = prev;
     // A vertex outside the frontier has prevIDs == IDs, unchanged since the
     // round it last was in the frontier, when every out-neighbour took a
     // label <= it; so its value cannot lower any destination, and the dense
@@ -406,11 +428,11 @@ static int run_cc(gg_graph_s* g, int32_t* ids_out, gg_run_stats* st) {
     F.reset(out);
     ++rounds;
   }
-  const int32_t* ids_res = ids.p;
-  GG_TRY(given_order<int32_t>(g, ids.p, 0, &ids_res));
+  const int32_t* ids_res = ids;
+  GG_TRY(given_order<int32_t>(g, ids, 0, &ids_res));
   const double ms = tm.stop();
   GG_TRY(to_host(g, ids_out, ids_res, n));
-  fill_stats(st, ms, rounds, trav, g->kernels);
+  fill_stats(st, ms, (int)rounds, trav, g->kernels);
   return GG_OK;
 }
 
@@ -621,7 +643,7 @@ static int add_conditional(cudaGraph_t graph, cudaGraphNode_t dep, cudaGraphCond
   np.conditional.type = type;
   np.conditional.size = 1;
   cudaGraphNode_t node;
-  GG_CUDA(cudaGraphAddNode(&node, graph, &dep, 1, &np));
+  GG_CUDA(cudaGraphAddNode(&node, graph, dep ? &dep : nullptr, dep ? 1 : 0, &np));
   *body = np.conditional.phGraph_out[0];
   return GG_OK;
 }
@@ -719,6 +741,265 @@ static int pr_loop_get(gg_graph_s* g, bool bit_all, PrLoop** out) {
     std::copy(key, key + 3, L->key);
   }
   *out = L;
+  return GG_OK;
+}
+
+// ------------------------------- dense rounds of BellmanFord and Components
+// The round loops of app/BellmanFord.C:119-140 and app/Components.C:113-124
+// hand each run of rounds that edgeMap sends to the dense COO pull to one
+// CUDA graph, like PageRank's iterations: a while node whose body runs a round
+// from bitmap 0 into bitmap 1 and, under an if node, the next from 1 into 0.
+// A round is the application's edgeMap (the COO pull into the output bitmap,
+// with its count and out-degree sum) and its vertexMap (BellmanFord: Visited
+// reset over the output; Components: prevIDs = IDs over the input, before
+// the pull).  After each round a check kernel counts it, clears the round's
+// input bitmap (the next output) and applies the host loop's tests: stop on
+// an empty output or at the round cap (BellmanFord's n rounds), and hand
+// back to the host when the next edgeMap would not take the dense COO pull
+// (sparse push, CSC pull, or a frontier without out-edges).  The graph, the
+// two bitmaps and the application's two vertex arrays stay with the graph
+// handle.
+struct RoundLoopCtl {
+  unsigned long long trav;       // out-degree sums of the inputs of the rounds after the first
+  unsigned long long dm;         // last output: members
+  unsigned long long out_edges;  //   and their out-degree sum
+  unsigned long long err;        // device error word seen by a check
+  long long threshold;           // edgeMap's threshold (m / div)
+  long long dense_threshold;     // m / 2
+  uint32_t count;                // rounds run
+  uint32_t max_rounds;
+  uint32_t reason;               // 0 running, 1 empty output, 2 round cap, 3 handed back, 4 device error
+  uint32_t coo_always;           // the dense policy pins the COO pull (else the m/2 rule)
+};
+
+struct RoundLoop {
+  int32_t* arr[2] = {nullptr, nullptr};    // BellmanFord: distances, Visited; Components: IDs, prevIDs
+  uint32_t* bits[2] = {nullptr, nullptr};  // frontier bitmaps (round inputs and outputs alternate)
+  RoundLoopCtl* d_ctl = nullptr;
+  RoundLoopCtl* h_ctl = nullptr;  // pinned
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int key[3] = {-1, -1, -1};  // COO kernel, transposed, -P source of the captured graph
+  int per_round = 0;          // kernels per round
+  uint64_t bytes = 0;
+};
+
+void round_loops_free(gg_graph_s* g) {
+  for (RoundLoop*& L : g->round_loop) {
+    if (!L) continue;
+    if (L->exec) cudaGraphExecDestroy(L->exec);
+    if (L->graph) cudaGraphDestroy(L->graph);
+    for (int32_t* a : L->arr) cudaFree(a);
+    for (uint32_t* b : L->bits) cudaFree(b);
+    cudaFree(L->d_ctl);
+    if (L->h_ctl) cudaFreeHost(L->h_ctl);
+    g->device_bytes -= L->bytes;
+    delete L;
+    L = nullptr;
+  }
+}
+
+__global__ void k_round_check(RoundLoopCtl* c, unsigned long long* stats, cudaGraphConditionalHandle h_loop,
+                              cudaGraphConditionalHandle h_odd, int set_odd, uint32_t* clear_bits,
+                              uint32_t clear_words) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < clear_words;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    clear_bits[i] = 0;
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const unsigned long long dm = stats[0], oe = stats[1], err = stats[3];
+  for (int i = 0; i < 8; ++i) stats[i] = 0;  // the next pull's counters and tile counter
+  const uint32_t count = c->count + 1;
+  c->count = count;
+  c->dm = dm;
+  c->out_edges = oe;
+  uint32_t reason = 0;
+  if (err) {
+    c->err = err;
+    reason = 4;
+  } else if (dm == 0) {
+    reason = 1;
+  } else if (count >= c->max_rounds) {
+    reason = 2;
+  } else {
+    const long long fm = (long long)dm, tot = (long long)oe;
+    const bool pull = tot > 0 && fm + tot > c->threshold && (c->coo_always || fm + tot > c->dense_threshold);
+    if (pull)
+      c->trav += oe;
+    else
+      reason = 3;
+  }
+  c->reason = reason;
+  cudaGraphSetConditional(h_loop, reason == 0 ? 1u : 0u);
+  if (set_odd) cudaGraphSetConditional(h_odd, reason == 0 ? 1u : 0u);
+}
+
+// The next edgeMap of a round loop takes the dense COO pull (edge_map's rule
+// for flags 0 and a functor without early exit).
+static bool round_takes_coo(const gg_graph_s* g, const gg_frontier_s* f) {
+  const int64_t fm = (int64_t)f->dm, tot = (int64_t)f->out_edges, m = (int64_t)g->m;
+  if (f->bit || tot == 0 || !g->has_coo || fm + tot <= app_threshold(g)) return false;
+  const bool ref_rule = g->dense_policy == 0 || g->transposed;
+  return ref_rule ? fm + tot > m / 2 : g->dense_policy == 2;
+}
+
+static int32_t* round_loop_array(RoundLoop* L, int i) { return L->arr[i]; }
+
+// One round's launches, from bitmap in_bits into out_bits.
+static int round_launches(gg_graph_s* g, RoundLoop* L, int app, uint32_t* in_bits, uint32_t* out_bits) {
+  gg_frontier_s in{}, out{};
+  in.g = out.g = g;
+  in.n = out.n = g->n;
+  in.has_dense = out.has_dense = true;
+  in.d_bits = in_bits;
+  out.d_bits = out_bits;
+  const bool hw = g->wtype != GG_W_NONE;
+  if (app == kRoundLoopBf) {
+    BfF f;
+    f.sp = L->arr[0];
+    f.visited = L->arr[1];
+    GG_TRY(hw ? (pull_launch<BfF, true>(g, &in, &out, f, true)) : (pull_launch<BfF, false>(g, &in, &out, f, true)));
+    VFill<int32_t> vf{L->arr[1], 0};
+    return vertex_map(g, &out, vf);
+  }
+  VCcCopy vc{L->arr[0], L->arr[1]};
+  GG_TRY(vertex_map(g, &in, vc));
+  CcF f;
+  f.ids = L->arr[0];
+  f.prev = L->arr[1];
+  f.outside_inert = true;  // as run_cc's rounds
+  return pull_launch<CcF, false>(g, &in, &out, f, true);
+}
+
+static int round_loop_capture(gg_graph_s* g, RoundLoop* L, int app) {
+  cudaGraph_t graph = nullptr;
+  GG_CUDA(cudaGraphCreate(&graph, 0));
+  uint32_t *X = L->bits[0], *Y = L->bits[1];
+  cudaGraphConditionalHandle h_loop = 0, h_odd = 0;
+  cudaGraph_t body = nullptr, odd = nullptr;
+  cudaGraphNode_t last = nullptr;
+  const uint32_t words = g->words() + 4;
+  const int k0 = g->kernels;
+  auto check = [&](int set_odd, uint32_t* in_bits) -> int {
+    k_round_check<<<generic_grid(g, words), kGenericThreads, 0, g->stream>>>(L->d_ctl, g->ws.d_stats, h_loop,
+                                                                             h_odd, set_odd, in_bits, words);
+    GG_CUDA(cudaGetLastError());
+    g->kernels++;
+    return GG_OK;
+  };
+  int rc = cudaGraphConditionalHandleCreate(&h_loop, graph, 1, cudaGraphCondAssignDefault) == cudaSuccess
+               ? GG_OK
+               : fail(GG_ERR_CUDA, "round graph: no conditional handle");
+  if (!rc) rc = add_conditional(graph, nullptr, h_loop, cudaGraphCondTypeWhile, &body);
+  if (!rc && cudaGraphConditionalHandleCreate(&h_odd, body, 0, cudaGraphCondAssignDefault) != cudaSuccess)
+    rc = fail(GG_ERR_CUDA, "round graph: no conditional handle");
+  // odd rounds: bitmap 0 into bitmap 1
+  if (!rc)
+    rc = capture_into(g, body, [&]() -> int {
+      GG_TRY(round_launches(g, L, app, X, Y));
+      return check(1, X);
+    }, &last);
+  const int per_round = g->kernels - k0;
+  if (!rc) rc = add_conditional(body, last, h_odd, cudaGraphCondTypeIf, &odd);
+  // even rounds: bitmap 1 into bitmap 0
+  if (!rc)
+    rc = capture_into(g, odd, [&]() -> int {
+      GG_TRY(round_launches(g, L, app, Y, X));
+      return check(0, Y);
+    }, &last);
+  cudaGraphExec_t exec = nullptr;
+  if (!rc && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess)
+    rc = fail(GG_ERR_CUDA, "round graph: instantiation refused");
+  if (rc) {
+    cudaGetLastError();
+    cudaGraphDestroy(graph);
+    return rc;
+  }
+  if (L->exec) cudaGraphExecDestroy(L->exec);
+  if (L->graph) cudaGraphDestroy(L->graph);
+  L->graph = graph;
+  L->exec = exec;
+  L->per_round = per_round;
+  return GG_OK;
+}
+
+// The round loop of app for this graph handle, captured (again) when a knob
+// it depends on changed since; nullptr when rounds stay on the host (switch
+// off, profiling, no COO, or the driver refused the graph: the switch then
+// turns off).
+static RoundLoop* round_loop_get(gg_graph_s* g, int app) {
+  if (!g->round_graph || g->profiling || !g->has_coo || g->m == 0) return nullptr;
+  RoundLoop*& L = g->round_loop[app];
+  if (!L) {
+    L = new (std::nothrow) RoundLoop;
+    if (!L) return nullptr;
+    const uint64_t ab = 4ull * ((uint64_t)g->n + 4), bb = 4ull * ((uint64_t)g->words() + 4);
+    bool ok = true;
+    for (int32_t*& a : L->arr) ok = ok && cudaMalloc((void**)&a, ab) == cudaSuccess;
+    for (uint32_t*& b : L->bits) ok = ok && cudaMalloc((void**)&b, bb) == cudaSuccess;
+    ok = ok && cudaMalloc((void**)&L->d_ctl, sizeof(RoundLoopCtl)) == cudaSuccess;
+    ok = ok && cudaMallocHost((void**)&L->h_ctl, sizeof(RoundLoopCtl)) == cudaSuccess;
+    L->bytes = 2 * ab + 2 * bb + sizeof(RoundLoopCtl);
+    g->device_bytes += L->bytes;
+    if (!ok) {
+      cudaGetLastError();
+      round_loops_free(g);
+      return nullptr;
+    }
+  }
+  const int key[3] = {g->coo_kernel, g->transposed ? 1 : 0, g->coo_by_source ? 1 : 0};
+  if (!L->exec || !std::equal(key, key + 3, L->key)) {
+    L->key[0] = -1;
+    const int k = g->kernels;
+    const int rc = round_loop_capture(g, L, app);
+    g->kernels = k;
+    if (rc) {
+      g->round_graph = 0;  // refused by the driver: the host loop from now on
+      return nullptr;
+    }
+    std::copy(key, key + 3, L->key);
+  }
+  return L;
+}
+
+// Runs dense COO rounds from frontier F (which takes the COO pull) on the
+// device; afterwards F is the last round's output, *round and *trav count
+// the rounds run and their inputs' out-degree sums.
+static int round_loop_run(gg_graph_s* g, RoundLoop* L, FrontierHold& F, uint32_t max_rounds, int64_t* round,
+                          uint64_t* trav) {
+  gg_frontier_s* in = F.f;
+  if (!in->has_dense) GG_TRY(frontier_to_dense(in));
+  const size_t bb = 4ull * (g->words() + 4);
+  GG_CUDA(cudaMemcpyAsync(L->bits[0], in->d_bits, bb, cudaMemcpyDeviceToDevice, g->stream));
+  GG_CUDA(cudaMemsetAsync(L->bits[1], 0, bb, g->stream));
+  GG_TRY(reset_stats(g));
+  RoundLoopCtl& c = *L->h_ctl;
+  c = RoundLoopCtl{};
+  c.threshold = app_threshold(g);
+  c.dense_threshold = (long long)g->m / 2;
+  c.max_rounds = max_rounds;
+  c.coo_always = (g->dense_policy == 0 || g->transposed) ? 0u : 1u;
+  GG_CUDA(cudaMemcpyAsync(L->d_ctl, L->h_ctl, sizeof(RoundLoopCtl), cudaMemcpyHostToDevice, g->stream));
+  GG_CUDA(cudaGraphLaunch(L->exec, g->stream));
+  GG_CUDA(cudaMemcpyAsync(L->h_ctl, L->d_ctl, sizeof(RoundLoopCtl), cudaMemcpyDeviceToHost, g->stream));
+  GG_CUDA(cudaStreamSynchronize(g->stream));
+  if (c.reason == 4) return fail(GG_ERR_TIMEOUT, "device wait budget exhausted (error word %llu)", c.err);
+  if (c.reason < 1 || c.reason > 3 || c.count < 1 || c.count > max_rounds)
+    return fail(GG_ERR_CUDA, "round graph: bad loop state");
+  *round += c.count;
+  *trav += in->out_edges + c.trav;
+  g->kernels += L->per_round * (int)c.count;
+  g->last = gg_edge_map_stats{};
+  g->last.kind = 3;
+  g->last.output_active = c.dm;
+  g->last.output_out_edges = c.out_edges;
+  gg_frontier_s* o = nullptr;
+  GG_TRY(frontier_new(g, &o));
+  F.reset(o);
+  GG_TRY(frontier_ensure_bits(o, false));
+  GG_CUDA(cudaMemcpyAsync(o->d_bits, L->bits[(c.count & 1) ? 1 : 0], bb, cudaMemcpyDeviceToDevice, g->stream));
+  o->has_dense = true;
+  o->dm = c.dm;
+  o->out_edges = c.out_edges;
   return GG_OK;
 }
 
@@ -1087,37 +1368,50 @@ static int run_spmv(gg_graph_s* g, const float* x_in, float* y_out, gg_run_stats
 // app/BellmanFord.C:106-145
 static int run_bf(gg_graph_s* g, uint32_t start, int32_t* dist, gg_run_stats* st) {
   const uint32_t n = g->n;
+  RoundLoop* L = round_loop_get(g, kRoundLoopBf);  // its arrays, when its graph runs the dense rounds
   g->kernels = 0;
-  DevBuf<int32_t> sp, vis;
-  GG_TRY(sp.alloc(g, n));
-  GG_TRY(vis.alloc(g, n));
+  DevBuf<int32_t> spb, visb;
+  int32_t *sp = nullptr, *vis = nullptr;
+  if (L) {
+    sp = round_loop_array(L, 0);
+    vis = round_loop_array(L, 1);
+  } else {
+    GG_TRY(spb.alloc(g, n));
+    GG_TRY(visb.alloc(g, n));
+    sp = spb.p;
+    vis = visb.p;
+  }
   const int32_t inf = 2147483647 / 2;
   EventTimer tm(g->stream);
-  GG_TRY(fill<int32_t>(g, sp.p, n, inf));
-  GG_TRY(set_one<int32_t>(g, sp.p, start, 0));
-  GG_TRY(fill<int32_t>(g, vis.p, n, 0));
+  GG_TRY(fill<int32_t>(g, sp, n, inf));
+  GG_TRY(set_one<int32_t>(g, sp, start, 0));
+  GG_TRY(fill<int32_t>(g, vis, n, 0));
   FrontierHold F;
   GG_TRY(gg_frontier_single(g, start, &F.f));
   int64_t round = 0;
   uint64_t trav = 0;
   while (F.f->dm > 0) {
     if (round == (int64_t)n) {  // negative weight cycle
-      GG_TRY(fill<int32_t>(g, sp.p, n, -inf));
+      GG_TRY(fill<int32_t>(g, sp, n, -inf));
       break;
     }
+    if (L && round_takes_coo(g, F.f)) {  // dense COO rounds on the device
+      GG_TRY(round_loop_run(g, L, F, (uint32_t)((int64_t)n - round), &round, &trav));
+      continue;
+    }
     BfF f;
-    f.sp = sp.p;
-    f.visited = vis.p;
+    f.sp = sp;
+    f.visited = vis;
     trav += F.f->out_edges;
     gg_frontier_s* out = nullptr;
     GG_TRY(edge_map(g, F.f, f, app_threshold(g), 0, &out));
-    VFill<int32_t> vf{vis.p, 0};
+    VFill<int32_t> vf{vis, 0};
     GG_TRY(vertex_map(g, out, vf));
     F.reset(out);
     ++round;
   }
-  const int32_t* res = sp.p;
-  GG_TRY(given_order<int32_t>(g, sp.p, 0, &res));
+  const int32_t* res = sp;
+  GG_TRY(given_order<int32_t>(g, sp, 0, &res));
   const double ms = tm.stop();
   GG_TRY(to_host(g, dist, res, n));
   fill_stats(st, ms, (int)round, trav, g->kernels);

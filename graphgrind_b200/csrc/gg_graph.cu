@@ -552,6 +552,7 @@ static void graph_release(gg_graph_s* g) {
   if (g->stream) cudaStreamSynchronize(g->stream);
   if (g->copy_stream) cudaStreamSynchronize(g->copy_stream);
   pr_loop_free(g);
+  round_loops_free(g);
   for (void* a : g->arrays) cudaFree(a);
   g->arrays.clear();
   cudaFree(g->d_csr_off);
@@ -941,6 +942,10 @@ int gg_graph_set_tuning(gg_graph_t g, int32_t key, int64_t value) {
       if (value < 0 || value > (1ll << 30)) return fail(GG_ERR_INVALID_ARG, "push-dense divisor must be 0..2^30");
       g->push_dense_div = (int)value;
       return GG_OK;
+    case GG_TUNE_ROUND_GRAPH:
+      if (value != 0 && value != 1) return fail(GG_ERR_INVALID_ARG, "round graph switch must be 0 or 1");
+      g->round_graph = (int)value;
+      return GG_OK;
     case GG_TUNE_LOOP_CTAS:
       if (value < 0 || value > 16) return fail(GG_ERR_INVALID_ARG, "loop CTAs per SM must be 0..16");
       g->loop_ctas_per_sm = (int)value;
@@ -1002,6 +1007,9 @@ int gg_graph_get_tuning(gg_graph_t g, int32_t key, int64_t* value) {
       return GG_OK;
     case GG_TUNE_LOOP_CTAS:
       *value = g->loop_ctas_per_sm;
+      return GG_OK;
+    case GG_TUNE_ROUND_GRAPH:
+      *value = g->round_graph;
       return GG_OK;
     default:
       return fail(GG_ERR_INVALID_ARG, "unknown tuning key %d", key);

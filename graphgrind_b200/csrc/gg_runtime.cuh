@@ -174,6 +174,7 @@ int bfs_device_full(gg_graph_s* g, uint32_t start, int32_t* parents, int32_t* le
                     int32_t* rounds, uint64_t* trav);
 int reset_stats(gg_graph_s* g);
 void pr_loop_free(gg_graph_s* g);  // releases the captured PageRank loop and its buffers
+void round_loops_free(gg_graph_s* g);  // the same for the BellmanFord / Components round loops
 int read_stats(gg_graph_s* g);  // blocks; checks the device error word
 
 // -------------------------------------------------------------- edgeMap

@@ -346,6 +346,16 @@ int gg_graph_set_dense_policy(gg_graph_t g, int32_t policy);
  *                         consecutive sparse levels in one cooperative launch
  *                         each, dense levels from the host; 0: one host round
  *                         trip per level
+ *   GG_TUNE_ROUND_GRAPH   1 (default): gg_bellman_ford and gg_components run
+ *                         each stretch of rounds that edgeMap sends to the
+ *                         dense COO pull as one CUDA graph (the round's
+ *                         edgeMap and vertexMap, then a check kernel that
+ *                         applies the loop's tests and the direction rule on
+ *                         the device); the graph and the two n-entry arrays
+ *                         stay with the graph handle.  0: one host round trip
+ *                         per round.  Falls back to 0 by itself when the
+ *                         driver refuses the capture; profiling also takes
+ *                         the host loop
  *   GG_TUNE_LOOP_CTAS     CTAs per SM of those cooperative launches, 0..16
  *                         (0, the default: 4 for mode 1, 8 for mode 2; capped
  *                         by the kernel's occupancy)
@@ -408,6 +418,7 @@ int gg_graph_set_dense_policy(gg_graph_t g, int32_t policy);
 #define GG_TUNE_EARLY_KERNEL 9
 #define GG_TUNE_PUSH_DENSE_DIV 10
 #define GG_TUNE_LOOP_CTAS 11
+#define GG_TUNE_ROUND_GRAPH 12
 int gg_graph_set_tuning(gg_graph_t g, int32_t key, int64_t value);
 int gg_graph_get_tuning(gg_graph_t g, int32_t key, int64_t* value);
 
