@@ -43,14 +43,14 @@ struct FrontierHold {
   }
 };
 
-// Runs of dense COO rounds of BellmanFord and Components as one CUDA graph
-// (defined with the PageRank graph below).
-enum { kRoundLoopBf = 0, kRoundLoopCc = 1 };
+// Runs of dense COO rounds of BellmanFord, Components and PageRankDelta as
+// one CUDA graph (defined with the PageRank graph below).
+enum { kRoundLoopBf = 0, kRoundLoopCc = 1, kRoundLoopPrd = 2 };
 static RoundLoop* round_loop_get(gg_graph_s* g, int app);
-static int32_t* round_loop_array(RoundLoop* L, int i);
+static void* round_loop_array(RoundLoop* L, int i);
 static bool round_takes_coo(const gg_graph_s* g, const gg_frontier_s* f);
 static int round_loop_run(gg_graph_s* g, RoundLoop* L, FrontierHold& F, uint32_t max_rounds, int64_t* round,
-                          uint64_t* trav);
+                          uint64_t* trav, double eps = 0, double* l1 = nullptr);
 
 // contrib[s] = val[s] / outdeg(s)   (0 for out-degree 0, never gathered)
 __global__ void k_div_outdeg(uint32_t n, const float* val, const uint32_t* off, float* contrib) {
@@ -388,8 +388,8 @@ static int run_cc(gg_graph_s* g, int32_t* ids_out, gg_run_stats* st) {
   DevBuf<int32_t> idsb, prevb;
   int32_t *ids = nullptr, *prev = nullptr;
   if (L) {
-    ids = round_loop_array(L, 0);
-    prev = round_loop_array(L, 1);
+    ids = static_cast<int32_t*>(round_loop_array(L, 0));
+    prev = static_cast<int32_t*>(round_loop_array(L, 1));
   } else {
     GG_TRY(idsb.alloc(g, n));
     GG_TRY(prevb.alloc(g, n));
@@ -744,37 +744,47 @@ static int pr_loop_get(gg_graph_s* g, bool bit_all, PrLoop** out) {
   return GG_OK;
 }
 
-// ------------------------------- dense rounds of BellmanFord and Components
-// The round loops of app/BellmanFord.C:119-140 and app/Components.C:113-124
-// hand each run of rounds that edgeMap sends to the dense COO pull to one
-// CUDA graph, like PageRank's iterations: a while node whose body runs a round
-// from bitmap 0 into bitmap 1 and, under an if node, the next from 1 into 0.
-// A round is the application's edgeMap (the COO pull into the output bitmap,
-// with its count and out-degree sum) and its vertexMap (BellmanFord: Visited
-// reset over the output; Components: prevIDs = IDs over the input, before
-// the pull).  After each round a check kernel counts it, clears the round's
-// input bitmap (the next output) and applies the host loop's tests: stop on
-// an empty output or at the round cap (BellmanFord's n rounds), and hand
-// back to the host when the next edgeMap would not take the dense COO pull
-// (sparse push, CSC pull, or a frontier without out-edges).  The graph, the
-// two bitmaps and the application's two vertex arrays stay with the graph
-// handle.
+// ------------------- dense rounds of BellmanFord, Components, PageRankDelta
+// The round loops of app/BellmanFord.C:119-140, app/Components.C:113-124 and
+// app/PageRankDelta.C:141-170 hand each run of rounds whose edgeMap takes the
+// dense COO pull to one CUDA graph, like PageRank's iterations: a while node
+// whose body runs a round from bitmap 0 into bitmap 1 and, under an if node,
+// the next from 1 into 0.  A round is the application's edgeMap (the COO
+// pull, with its output count and out-degree sum) and its vertex step
+// (BellmanFord: Visited reset over the output; Components: prevIDs = IDs over
+// the input, before the pull; PageRankDelta: the vertexFilter over all
+// vertices, whose output is the next frontier, and the epilogue with the L1
+// norm; its pull's own output goes to a third bitmap nobody reads).  After
+// each round a check kernel counts it, clears the round's input bitmap (the
+// next output) and applies the host loop's tests: stop on an empty frontier,
+// at the round cap (BellmanFord's n rounds) or when L1 < eps
+// (PageRankDelta), and hand back to the host when the next edgeMap would not
+// take the dense COO pull (sparse push, CSC pull, or a frontier without
+// out-edges).  The graph, the bitmaps and the application's vertex arrays
+// stay with the graph handle.
 struct RoundLoopCtl {
   unsigned long long trav;       // out-degree sums of the inputs of the rounds after the first
-  unsigned long long dm;         // last output: members
+  unsigned long long dm;         // next frontier: members
   unsigned long long out_edges;  //   and their out-degree sum
   unsigned long long err;        // device error word seen by a check
+  double l1;                     // PageRankDelta: L1 of the last round
+  double eps;                    //   and its stop threshold
   long long threshold;           // edgeMap's threshold (m / div)
   long long dense_threshold;     // m / 2
   uint32_t count;                // rounds run
   uint32_t max_rounds;
-  uint32_t reason;               // 0 running, 1 empty output, 2 round cap, 3 handed back, 4 device error
+  uint32_t reason;               // 0 running, 1 empty frontier or L1 < eps, 2 round cap, 3 handed back, 4 device error
   uint32_t coo_always;           // the dense policy pins the COO pull (else the m/2 rule)
+  uint32_t use_l1;               // stop on L1 < eps
+  uint32_t pad;
 };
 
 struct RoundLoop {
-  int32_t* arr[2] = {nullptr, nullptr};    // BellmanFord: distances, Visited; Components: IDs, prevIDs
-  uint32_t* bits[2] = {nullptr, nullptr};  // frontier bitmaps (round inputs and outputs alternate)
+  // BellmanFord: distances, Visited; Components: IDs, prevIDs; PageRankDelta:
+  // p, Delta, nghSum, contributions (n + 4 entries of 4 bytes each)
+  void* arr[4] = {nullptr, nullptr, nullptr, nullptr};
+  uint32_t* bits[3] = {nullptr, nullptr, nullptr};  // frontiers of the rounds (0, 1); PageRankDelta's pull output (2)
+  unsigned long long* d_fstats = nullptr;  // PageRankDelta: the vertexFilter's count and out-degree sum
   RoundLoopCtl* d_ctl = nullptr;
   RoundLoopCtl* h_ctl = nullptr;  // pinned
   cudaGraph_t graph = nullptr;
@@ -789,8 +799,9 @@ void round_loops_free(gg_graph_s* g) {
     if (!L) continue;
     if (L->exec) cudaGraphExecDestroy(L->exec);
     if (L->graph) cudaGraphDestroy(L->graph);
-    for (int32_t* a : L->arr) cudaFree(a);
+    for (void* a : L->arr) cudaFree(a);
     for (uint32_t* b : L->bits) cudaFree(b);
+    cudaFree(L->d_fstats);
     cudaFree(L->d_ctl);
     if (L->h_ctl) cudaFreeHost(L->h_ctl);
     g->device_bytes -= L->bytes;
@@ -799,24 +810,29 @@ void round_loops_free(gg_graph_s* g) {
   }
 }
 
-__global__ void k_round_check(RoundLoopCtl* c, unsigned long long* stats, cudaGraphConditionalHandle h_loop,
+// fstats: where the round's next frontier was counted (PageRankDelta's
+// vertexFilter), else the pull's own counters in stats; red: the round's L1.
+__global__ void k_round_check(RoundLoopCtl* c, unsigned long long* stats, unsigned long long* fstats,
+                              const double* red, cudaGraphConditionalHandle h_loop,
                               cudaGraphConditionalHandle h_odd, int set_odd, uint32_t* clear_bits,
                               uint32_t clear_words) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < clear_words;
        i += (uint64_t)gridDim.x * blockDim.x)
     clear_bits[i] = 0;
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  const unsigned long long dm = stats[0], oe = stats[1], err = stats[3];
+  const unsigned long long dm = fstats ? fstats[0] : stats[0], oe = fstats ? fstats[1] : stats[1], err = stats[3];
   for (int i = 0; i < 8; ++i) stats[i] = 0;  // the next pull's counters and tile counter
+  if (fstats) fstats[0] = fstats[1] = 0;
   const uint32_t count = c->count + 1;
   c->count = count;
   c->dm = dm;
   c->out_edges = oe;
+  if (c->use_l1) c->l1 = red[0];
   uint32_t reason = 0;
   if (err) {
     c->err = err;
     reason = 4;
-  } else if (dm == 0) {
+  } else if (c->use_l1 ? c->l1 < c->eps : dm == 0) {
     reason = 1;
   } else if (count >= c->max_rounds) {
     reason = 2;
@@ -842,7 +858,7 @@ static bool round_takes_coo(const gg_graph_s* g, const gg_frontier_s* f) {
   return ref_rule ? fm + tot > m / 2 : g->dense_policy == 2;
 }
 
-static int32_t* round_loop_array(RoundLoop* L, int i) { return L->arr[i]; }
+static void* round_loop_array(RoundLoop* L, int i) { return L->arr[i]; }
 
 // One round's launches, from bitmap in_bits into out_bits.
 static int round_launches(gg_graph_s* g, RoundLoop* L, int app, uint32_t* in_bits, uint32_t* out_bits) {
@@ -855,22 +871,48 @@ static int round_launches(gg_graph_s* g, RoundLoop* L, int app, uint32_t* in_bit
   const bool hw = g->wtype != GG_W_NONE;
   if (app == kRoundLoopBf) {
     BfF f;
-    f.sp = L->arr[0];
-    f.visited = L->arr[1];
+    f.sp = static_cast<int32_t*>(L->arr[0]);
+    f.visited = static_cast<int32_t*>(L->arr[1]);
     GG_TRY(hw ? (pull_launch<BfF, true>(g, &in, &out, f, true)) : (pull_launch<BfF, false>(g, &in, &out, f, true)));
-    VFill<int32_t> vf{L->arr[1], 0};
+    VFill<int32_t> vf{f.visited, 0};
     return vertex_map(g, &out, vf);
   }
-  VCcCopy vc{L->arr[0], L->arr[1]};
-  GG_TRY(vertex_map(g, &in, vc));
-  CcF f;
-  f.ids = L->arr[0];
-  f.prev = L->arr[1];
-  f.outside_inert = true;  // as run_cc's rounds
-  return pull_launch<CcF, false>(g, &in, &out, f, true);
+  if (app == kRoundLoopCc) {
+    int32_t* ids = static_cast<int32_t*>(L->arr[0]);
+    int32_t* prev = static_cast<int32_t*>(L->arr[1]);
+    VCcCopy vc{ids, prev};
+    GG_TRY(vertex_map(g, &in, vc));
+    CcF f;
+    f.ids = ids;
+    f.prev = prev;
+    f.outside_inert = true;  // as run_cc's rounds
+    return pull_launch<CcF, false>(g, &in, &out, f, true);
+  }
+  // PageRankDelta: the pull's output (discarded by the application) into the
+  // third bitmap, the vertexFilter over all vertices into out_bits
+  float* p = static_cast<float*>(L->arr[0]);
+  float* delta = static_cast<float*>(L->arr[1]);
+  float* ngh = static_cast<float*>(L->arr[2]);
+  float* contrib = static_cast<float*>(L->arr[3]);
+  out.d_bits = L->bits[2];
+  PrF f;
+  f.contrib = contrib;
+  f.acc_out = ngh;
+  GG_TRY((pull_launch<PrF, false>(g, &in, &out, f, true)));
+  const VPrd vf{p, delta, ngh, 0.85f, 0.01f};
+  k_vertex_filter<VPrd, true><<<generic_grid(g, g->n), kGenericThreads, 0, g->stream>>>(
+      g->n, nullptr, out_bits, g->out_off(), L->d_fstats, vf);
+  GG_CUDA(cudaGetLastError());
+  GG_CUDA(cudaMemsetAsync(g->ws.d_red, 0, sizeof(double), g->stream));
+  k_prd_epilogue<<<generic_grid(g, g->n), kGenericThreads, 0, g->stream>>>(g->n, delta, ngh, g->out_off(), contrib,
+                                                                           g->ws.d_red);
+  GG_CUDA(cudaGetLastError());
+  g->kernels += 2;
+  return GG_OK;
 }
 
 static int round_loop_capture(gg_graph_s* g, RoundLoop* L, int app) {
+  unsigned long long* fstats = app == kRoundLoopPrd ? L->d_fstats : nullptr;
   cudaGraph_t graph = nullptr;
   GG_CUDA(cudaGraphCreate(&graph, 0));
   uint32_t *X = L->bits[0], *Y = L->bits[1];
@@ -880,8 +922,8 @@ static int round_loop_capture(gg_graph_s* g, RoundLoop* L, int app) {
   const uint32_t words = g->words() + 4;
   const int k0 = g->kernels;
   auto check = [&](int set_odd, uint32_t* in_bits) -> int {
-    k_round_check<<<generic_grid(g, words), kGenericThreads, 0, g->stream>>>(L->d_ctl, g->ws.d_stats, h_loop,
-                                                                             h_odd, set_odd, in_bits, words);
+    k_round_check<<<generic_grid(g, words), kGenericThreads, 0, g->stream>>>(
+        L->d_ctl, g->ws.d_stats, fstats, g->ws.d_red, h_loop, h_odd, set_odd, in_bits, words);
     GG_CUDA(cudaGetLastError());
     g->kernels++;
     return GG_OK;
@@ -933,12 +975,17 @@ static RoundLoop* round_loop_get(gg_graph_s* g, int app) {
     L = new (std::nothrow) RoundLoop;
     if (!L) return nullptr;
     const uint64_t ab = 4ull * ((uint64_t)g->n + 4), bb = 4ull * ((uint64_t)g->words() + 4);
+    const int na = app == kRoundLoopPrd ? 4 : 2, nb = app == kRoundLoopPrd ? 3 : 2;
     bool ok = true;
-    for (int32_t*& a : L->arr) ok = ok && cudaMalloc((void**)&a, ab) == cudaSuccess;
-    for (uint32_t*& b : L->bits) ok = ok && cudaMalloc((void**)&b, bb) == cudaSuccess;
+    for (int i = 0; i < na; ++i) ok = ok && cudaMalloc(&L->arr[i], ab) == cudaSuccess;
+    for (int i = 0; i < nb; ++i) ok = ok && cudaMalloc((void**)&L->bits[i], bb) == cudaSuccess;
+    if (app == kRoundLoopPrd) {
+      ok = ok && cudaMalloc((void**)&L->d_fstats, 4 * sizeof(unsigned long long)) == cudaSuccess;
+      ok = ok && cudaMemset(L->d_fstats, 0, 4 * sizeof(unsigned long long)) == cudaSuccess;
+    }
     ok = ok && cudaMalloc((void**)&L->d_ctl, sizeof(RoundLoopCtl)) == cudaSuccess;
     ok = ok && cudaMallocHost((void**)&L->h_ctl, sizeof(RoundLoopCtl)) == cudaSuccess;
-    L->bytes = 2 * ab + 2 * bb + sizeof(RoundLoopCtl);
+    L->bytes = na * ab + nb * bb + sizeof(RoundLoopCtl) + (app == kRoundLoopPrd ? 32 : 0);
     g->device_bytes += L->bytes;
     if (!ok) {
       cudaGetLastError();
@@ -965,7 +1012,7 @@ static RoundLoop* round_loop_get(gg_graph_s* g, int app) {
 // device; afterwards F is the last round's output, *round and *trav count
 // the rounds run and their inputs' out-degree sums.
 static int round_loop_run(gg_graph_s* g, RoundLoop* L, FrontierHold& F, uint32_t max_rounds, int64_t* round,
-                          uint64_t* trav) {
+                          uint64_t* trav, double eps, double* l1) {
   gg_frontier_s* in = F.f;
   if (!in->has_dense) GG_TRY(frontier_to_dense(in));
   const size_t bb = 4ull * (g->words() + 4);
@@ -978,6 +1025,8 @@ static int round_loop_run(gg_graph_s* g, RoundLoop* L, FrontierHold& F, uint32_t
   c.dense_threshold = (long long)g->m / 2;
   c.max_rounds = max_rounds;
   c.coo_always = (g->dense_policy == 0 || g->transposed) ? 0u : 1u;
+  c.use_l1 = l1 ? 1u : 0u;
+  c.eps = eps;
   GG_CUDA(cudaMemcpyAsync(L->d_ctl, L->h_ctl, sizeof(RoundLoopCtl), cudaMemcpyHostToDevice, g->stream));
   GG_CUDA(cudaGraphLaunch(L->exec, g->stream));
   GG_CUDA(cudaMemcpyAsync(L->h_ctl, L->d_ctl, sizeof(RoundLoopCtl), cudaMemcpyDeviceToHost, g->stream));
@@ -987,6 +1036,7 @@ static int round_loop_run(gg_graph_s* g, RoundLoop* L, FrontierHold& F, uint32_t
     return fail(GG_ERR_CUDA, "round graph: bad loop state");
   *round += c.count;
   *trav += in->out_edges + c.trav;
+  if (l1) *l1 = c.l1;
   g->kernels += L->per_round * (int)c.count;
   g->last = gg_edge_map_stats{};
   g->last.kind = 3;
@@ -1241,49 +1291,68 @@ static int run_pagerank_converge(gg_graph_s* g, int32_t max_iter, double eps, fl
 // app/PageRankDelta.C:120-174
 static int run_pagerank_delta(gg_graph_s* g, float* ranks, gg_run_stats* st) {
   const uint32_t n = g->n;
+  RoundLoop* L = round_loop_get(g, kRoundLoopPrd);  // its arrays, when its graph runs the dense rounds
   g->kernels = 0;
-  DevBuf<float> p, delta, ngh, contrib;
-  GG_TRY(p.alloc(g, n));
-  GG_TRY(delta.alloc(g, n));
-  GG_TRY(ngh.alloc(g, n));
-  GG_TRY(contrib.alloc(g, n));
-  const float damping = 0.85f, eps2 = 0.01f;
+  DevBuf<float> pb, deltab, nghb, contribb;
+  float *p = nullptr, *delta = nullptr, *ngh = nullptr, *contrib = nullptr;
+  if (L) {
+    p = static_cast<float*>(round_loop_array(L, 0));
+    delta = static_cast<float*>(round_loop_array(L, 1));
+    ngh = static_cast<float*>(round_loop_array(L, 2));
+    contrib = static_cast<float*>(round_loop_array(L, 3));
+  } else {
+    GG_TRY(pb.alloc(g, n));
+    GG_TRY(deltab.alloc(g, n));
+    GG_TRY(nghb.alloc(g, n));
+    GG_TRY(contribb.alloc(g, n));
+    p = pb.p;
+    delta = deltab.p;
+    ngh = nghb.p;
+    contrib = contribb.p;
+  }
+  const float damping = 0.85f, eps2 = 0.01f;  // the round graph's vertexFilter uses the same constants
   const double eps = 0.0000001;
   const float one_over_n = (float)(1 / (double)n);
   const float added = (float)((1 - 0.85) * (1 / (double)n));
   EventTimer tm(g->stream);
-  GG_TRY(fill<float>(g, p.p, n, 0.0f));
-  GG_TRY(fill<float>(g, delta.p, n, one_over_n));
-  GG_TRY(fill<float>(g, ngh.p, n, 0.0f));
-  k_div_outdeg<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(n, delta.p, g->out_off(), contrib.p);
+  GG_TRY(fill<float>(g, p, n, 0.0f));
+  GG_TRY(fill<float>(g, delta, n, one_over_n));
+  GG_TRY(fill<float>(g, ngh, n, 0.0f));
+  k_div_outdeg<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(n, delta, g->out_off(), contrib);
   g->kernels++;
   FrontierHold F, All;
   GG_TRY(gg_frontier_all(g, &F.f));
   GG_TRY(gg_frontier_all(g, &All.f));
-  int round = 0;
+  int64_t round = 0;
   uint64_t trav = 0;
   for (;;) {
+    if (L && round_takes_coo(g, F.f)) {  // dense COO rounds on the device, each with its L1 test
+      double l1 = 0;
+      GG_TRY(round_loop_run(g, L, F, 0xffffffffu, &round, &trav, eps, &l1));
+      if (l1 < eps) break;
+      continue;
+    }
     ++round;
     PrF f;
-    f.contrib = contrib.p;
-    f.acc_out = ngh.p;
+    f.contrib = contrib;
+    f.acc_out = ngh;
     trav += F.f->out_edges;
     gg_frontier_s* out = nullptr;
     GG_TRY(edge_map(g, F.f, f, app_threshold(g), 0, &out));
     frontier_free(out);
     gg_frontier_s* active = nullptr;
     if (round == 1) {
-      VPrdFirst vf{p.p, delta.p, ngh.p, damping, added, one_over_n, eps2};
+      VPrdFirst vf{p, delta, ngh, damping, added, one_over_n, eps2};
       GG_TRY(vertex_filter(g, All.f, vf, &active));
     } else {
-      VPrd vf{p.p, delta.p, ngh.p, damping, eps2};
+      VPrd vf{p, delta, ngh, damping, eps2};
       GG_TRY(vertex_filter(g, All.f, vf, &active));
     }
     FrontierHold A;
     A.f = active;
     GG_CUDA(cudaMemsetAsync(g->ws.d_red, 0, sizeof(double), g->stream));
-    k_prd_epilogue<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(n, delta.p, ngh.p, g->out_off(),
-                                                                          contrib.p, g->ws.d_red);
+    k_prd_epilogue<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(n, delta, ngh, g->out_off(), contrib,
+                                                                          g->ws.d_red);
     GG_CUDA(cudaGetLastError());
     g->kernels++;
     double l1;
@@ -1291,11 +1360,11 @@ static int run_pagerank_delta(gg_graph_s* g, float* ranks, gg_run_stats* st) {
     if (l1 < eps) break;
     F.reset(A.release());
   }
-  const float* res = p.p;
-  GG_TRY(given_order<float>(g, p.p, 0, &res));
+  const float* res = p;
+  GG_TRY(given_order<float>(g, p, 0, &res));
   const double ms = tm.stop();
   GG_TRY(to_host(g, ranks, res, n));
-  fill_stats(st, ms, round, trav, g->kernels);
+  fill_stats(st, ms, (int)round, trav, g->kernels);
   return GG_OK;
 }
 
@@ -1373,8 +1442,8 @@ static int run_bf(gg_graph_s* g, uint32_t start, int32_t* dist, gg_run_stats* st
   DevBuf<int32_t> spb, visb;
   int32_t *sp = nullptr, *vis = nullptr;
   if (L) {
-    sp = round_loop_array(L, 0);
-    vis = round_loop_array(L, 1);
+    sp = static_cast<int32_t*>(round_loop_array(L, 0));
+    vis = static_cast<int32_t*>(round_loop_array(L, 1));
   } else {
     GG_TRY(spb.alloc(g, n));
     GG_TRY(visb.alloc(g, n));

@@ -164,8 +164,8 @@ struct gg_graph_s {
   bool input_staged = false;                         // given-order array 1 holds a staged SpMV input
   cudaEvent_t slot_copied[2] = {nullptr, nullptr};  // on copy_stream: the last copy out of ws.d_order[k]
   gg::PrLoop* pr_loop = nullptr;  // created by the first graph-driven PageRank call
-  gg::RoundLoop* round_loop[2] = {nullptr, nullptr};  // BellmanFord, Components: created by their first call
-  int round_graph = 1;  // dense COO rounds of BellmanFord / Components as a CUDA graph
+  gg::RoundLoop* round_loop[3] = {nullptr, nullptr, nullptr};  // BellmanFord, Components, PageRankDelta: created by their first call
+  int round_graph = 1;  // dense COO rounds of BellmanFord / Components / PageRankDelta as a CUDA graph
   int coo_kernel = 6;  // 0 CTA ring (k_pull), 1 per-warp direct loads, 2/3 per-warp bulk-copy rings, 6 direct loads
                        // with cross-lane run merging (fastest measured)
   // gg_build_opts.vertex_order: device ids differ from the given ids

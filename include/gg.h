@@ -346,14 +346,16 @@ int gg_graph_set_dense_policy(gg_graph_t g, int32_t policy);
  *                         consecutive sparse levels in one cooperative launch
  *                         each, dense levels from the host; 0: one host round
  *                         trip per level
- *   GG_TUNE_ROUND_GRAPH   1 (default): gg_bellman_ford and gg_components run
- *                         each stretch of rounds that edgeMap sends to the
- *                         dense COO pull as one CUDA graph (the round's
- *                         edgeMap and vertexMap, then a check kernel that
- *                         applies the loop's tests and the direction rule on
- *                         the device); the graph and the two n-entry arrays
- *                         stay with the graph handle.  0: one host round trip
- *                         per round.  Falls back to 0 by itself when the
+ *   GG_TUNE_ROUND_GRAPH   1 (default): gg_bellman_ford, gg_components and
+ *                         gg_pagerank_delta run each stretch of rounds that
+ *                         edgeMap sends to the dense COO pull as one CUDA
+ *                         graph (the round's edgeMap and vertex step, then a
+ *                         check kernel that applies the loop's tests, L1 <
+ *                         eps for PageRankDelta, and the direction rule on
+ *                         the device); the graph and the application's
+ *                         n-entry arrays (two, four for PageRankDelta) stay
+ *                         with the graph handle.  0: one host round trip per
+ *                         round.  Falls back to 0 by itself when the
  *                         driver refuses the capture; profiling also takes
  *                         the host loop
  *   GG_TUNE_LOOP_CTAS     CTAs per SM of those cooperative launches, 0..16

@@ -1,8 +1,10 @@
-"""BellmanFord and Components with their runs of dense COO rounds replayed as
-one CUDA graph (GG_TUNE_ROUND_GRAPH, the default) against the host-driven
-loop and the oracle: identical distances and labels, including the hand-back
+"""BellmanFord, Components and PageRankDelta with their runs of dense COO
+rounds replayed as one CUDA graph (GG_TUNE_ROUND_GRAPH, the default) against
+the host-driven loop and the oracle: identical distances and labels,
+PageRankDelta's ranks within its tolerance (1e-4 relative L1: its pull sums
+in FP32 in an order that varies from run to run), including the hand-back
 to the host when a frontier leaves the dense COO pull (sparse push or CSC
-pull) and BellmanFord's return from the host to the graph.
+pull) and the return from the host to the graph.
 
 Round counts and traversed edges are not compared: within a round both
 applications read values that other threads of the same round may already
@@ -12,7 +14,9 @@ intermediate frontiers depend on timing while the fixed point does not."""
 import numpy as np
 import pytest
 
-from conftest import ok_partitions
+from conftest import PR_MAX_ABS, ok_partitions, rel_l1
+
+PRD_REL_L1 = 1e-4
 
 pytestmark = pytest.mark.gpu
 
@@ -56,6 +60,12 @@ def test_round_graph_matches_host_loop_and_oracle(gg, orc, name, policy, vorder)
     np.testing.assert_array_equal(i1, i0)
     np.testing.assert_array_equal(i1, og.cc()[0])
     assert 1 <= c1.rounds <= hg.n
+    (p1, q1), (p0, q0) = run_both(gg, g, g.pagerank_delta)
+    o, ost = og.pagerank_delta()
+    for r in (p1, p0):
+        assert rel_l1(r, o) <= PRD_REL_L1, rel_l1(r, o)
+        assert np.abs(r.astype(np.float64) - o).max() <= PR_MAX_ABS
+    assert 1 <= q1.rounds <= 10 * ost.rounds
 
 
 def test_round_graph_buffers_stay_with_the_graph(gg, orc):
@@ -73,7 +83,10 @@ def test_round_graph_buffers_stay_with_the_graph(gg, orc):
     g.bellman_ford(77)
     assert g.info().device_bytes == after_bf
     g.components()
-    assert g.info().device_bytes > after_bf
+    after_cc = g.info().device_bytes
+    assert after_cc > after_bf
+    g.pagerank_delta()
+    assert g.info().device_bytes >= after_cc + 4 * 4 * (n + 4) + 3 * 4 * (words + 4)
     with pytest.raises(gg.GGError):
         g.set_tuning(gg.TUNE_ROUND_GRAPH, 2)
     g.close()
