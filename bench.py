@@ -86,7 +86,7 @@ HBM_FALLBACK_GBS = 6650.0
 # DRAM bytes per PageRank-pull launch of the default workload (the merged-run
 # COO kernel with the vertex step at its commits), from one ncu capture
 # (profiles/dram_k_pull_coo_w_pagerank_rmat24.md)
-TRAFFIC_RMAT24_PR_PULL = {1: 2110578176}  # by vertex order
+TRAFFIC_RMAT24_PR_PULL = {(6, 1): 2110578176, (7, 1): 1983904896}  # by (COO kernel, vertex order)
 TRAFFIC_TILE_EDGES = 1 << 18
 
 
@@ -334,7 +334,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
     algo_bytes = pr_bytes
     coo_names = {0: "k_pull (CTA ring)", 1: "k_pull_coo_w", 2: "k_pull_coo_w (2-stage ring)",
                  3: "k_pull_coo_w (3-stage ring)", 4: "k_pull_coo_w (lane-contiguous)", 5: "k_pull_coo_w (prefetch)",
-                 6: "k_pull_coo_w (merged runs)"}
+                 6: "k_pull_coo_w (merged runs)", 7: "k_pull_coo_w (merged runs, cache hints)"}
     kernel_name = coo_names.get(pr_coo_kernel, "k_pull_coo_w") if pr_kind == "coo_pull" else "k_pull_seg"
     if pr_fused:
         kernel_name += " with the vertex step"
@@ -364,9 +364,9 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
                                   "unit": "GB/s", "frac": round(ach / peak, 4)}
     traffic, traffic_src = args.traffic, "--traffic" if args.traffic else None
     if traffic is None and args.scale == 24 and args.partitions == 384 and args.dense_policy == 0 and \
-            args.tile_edges == TRAFFIC_TILE_EDGES and pr_kind == "coo_pull" and pr_coo_kernel == 6 and \
-            args.vertex_order in TRAFFIC_RMAT24_PR_PULL:
-        traffic = TRAFFIC_RMAT24_PR_PULL[args.vertex_order]
+            args.tile_edges == TRAFFIC_TILE_EDGES and pr_kind == "coo_pull" and \
+            (pr_coo_kernel, args.vertex_order) in TRAFFIC_RMAT24_PR_PULL:
+        traffic = TRAFFIC_RMAT24_PR_PULL[(pr_coo_kernel, args.vertex_order)]
         traffic_src = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/dram_k_pull_coo_w_pagerank_rmat24.md"
     achieved = algo_bytes / (pull_ms / 1e3) / 1e9 if pull_ms > 0 else None
     out = {

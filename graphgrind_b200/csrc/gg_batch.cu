@@ -169,11 +169,11 @@ static int run_ppr_k(gg_graph_s* g, int32_t k, int32_t iters, float damping, con
     std::function<void()> f;
     ~Guard() { f(); }
   } guard{cleanup};
-  GG_CUDA(cudaMallocAsync((void**)&T, 4 * nk, g->stream));
-  GG_CUDA(cudaMallocAsync((void**)&XS, 4 * nk, g->stream));
-  GG_CUDA(cudaMallocAsync((void**)&S, 4 * nk, g->stream));
-  GG_CUDA(cudaMallocAsync((void**)&Y, 4 * nk, g->stream));
-  GG_CUDA(cudaMallocAsync((void**)&d_brows, 4 * (brows.size() + 1), g->stream));
+  GG_CUDA(pool_alloc((void**)&T, 4 * nk, g->stream, g->device));
+  GG_CUDA(pool_alloc((void**)&XS, 4 * nk, g->stream, g->device));
+  GG_CUDA(pool_alloc((void**)&S, 4 * nk, g->stream, g->device));
+  GG_CUDA(pool_alloc((void**)&Y, 4 * nk, g->stream, g->device));
+  GG_CUDA(pool_alloc((void**)&d_brows, 4 * (brows.size() + 1), g->stream, g->device));
   if (!brows.empty())
     GG_CUDA(cudaMemcpyAsync(d_brows, brows.data(), 4 * brows.size(), cudaMemcpyHostToDevice, g->stream));
   g->kernels = 0;
@@ -196,7 +196,7 @@ static int run_ppr_k(gg_graph_s* g, int32_t k, int32_t iters, float damping, con
   } else {
     std::vector<uint32_t> dev_seeds(seeds, seeds + k);
     for (auto& v : dev_seeds) v = g->device_id(v);
-    GG_CUDA(cudaMallocAsync((void**)&d_seeds, 4 * k, g->stream));
+    GG_CUDA(pool_alloc((void**)&d_seeds, 4 * k, g->stream, g->device));
     GG_CUDA(cudaMemcpyAsync(d_seeds, dev_seeds.data(), 4 * k, cudaMemcpyHostToDevice, g->stream));
     GG_CUDA(cudaStreamSynchronize(g->stream));  // dev_seeds leaves scope
     cudaEventRecord(ea, g->stream);
@@ -623,12 +623,13 @@ __global__ void k_ms_bc_final(uint32_t n, uint32_t k, const uint32_t* new_of_old
 // Device allocations released (stream-ordered) when the holder leaves scope.
 struct DevAllocs {
   cudaStream_t st;
+  int device;
   std::vector<void*> ptrs;
-  explicit DevAllocs(cudaStream_t s) : st(s) {}
+  DevAllocs(cudaStream_t s, int dev) : st(s), device(dev) {}
   template <class T>
   int get(T** p, uint64_t count) {
     *p = nullptr;
-    GG_CUDA(cudaMallocAsync((void**)p, sizeof(T) * count + 64, st));
+    GG_CUDA(pool_alloc((void**)p, sizeof(T) * count + 64, st, device));
     ptrs.push_back(*p);
     return GG_OK;
   }
@@ -686,7 +687,7 @@ static int run_ms(gg_graph_s* g, int32_t k, const uint32_t* given_sources, bool 
   const uint64_t n64 = (uint64_t)n * 64;
   const uint64_t nk = (uint64_t)n * k;
   const uint64_t kmask = k == 64 ? ~0ull : ((1ull << k) - 1);
-  DevAllocs mem(g->stream);
+  DevAllocs mem(g->stream, g->device);
   uint64_t *seen, *visit, *next, *mask_a, *mask_b, *qmask = nullptr;
   float *sigma = nullptr, *dep = nullptr;
   uint32_t *d_src, *queue, *qdeg, *qoff;

@@ -24,6 +24,35 @@ __device__ __forceinline__ T warp_sum(T v) {
   return v;
 }
 
+// ------------------------------------------------------------ cache hints
+// L2 eviction policies (createpolicy, sm_80+) for loads that carry a
+// .L2::cache_hint operand: evict_first for data read once (a COO edge
+// stream), evict_last for data gathered again and again (source values).
+__device__ __forceinline__ uint64_t l2_policy_evict_first() {
+  uint64_t pol;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ uint64_t l2_policy_evict_last() {
+  uint64_t pol;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+// 16-byte read-only load that bypasses L1 (streamed data), with an L2 policy.
+__device__ __forceinline__ uint4 ld_stream_v4(const void* ptr, uint64_t pol) {
+  uint4 r;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+      : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+      : "l"(ptr), "l"(pol));
+  return r;
+}
+// 4-byte read-only gather kept in L1 and L2 ahead of streamed lines.
+__device__ __forceinline__ float ld_keep_f32(const float* ptr, uint64_t pol) {
+  float r;
+  asm("ld.global.nc.L1::evict_last.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(r) : "l"(ptr), "l"(pol));
+  return r;
+}
+
 // ------------------------------------------------------------ mbarrier
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));

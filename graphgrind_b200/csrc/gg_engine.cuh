@@ -37,6 +37,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+#include <utility>
+
 #include <unordered_set>
 #include <vector>
 
@@ -166,8 +169,8 @@ struct gg_graph_s {
   gg::PrLoop* pr_loop = nullptr;  // created by the first graph-driven PageRank call
   gg::RoundLoop* round_loop[3] = {nullptr, nullptr, nullptr};  // BellmanFord, Components, PageRankDelta: created by their first call
   int round_graph = 1;  // dense COO rounds of BellmanFord / Components / PageRankDelta as a CUDA graph
-  int coo_kernel = 6;  // 0 CTA ring (k_pull), 1 per-warp direct loads, 2/3 per-warp bulk-copy rings, 6 direct loads
-                       // with cross-lane run merging (fastest measured)
+  int coo_kernel = 7;  // 0 CTA ring (k_pull), 1 per-warp direct loads, 2/3 per-warp bulk-copy rings, 6 direct loads
+                       // with cross-lane run merging, 7 the same with cache hints (fastest measured)
   // gg_build_opts.vertex_order: device ids differ from the given ids
   bool relabeled = false;
   std::vector<uint32_t> h_new_of_old, h_old_of_new;
@@ -521,7 +524,16 @@ __host__ __device__ constexpr size_t coo_w_smem_bytes(bool hw, int stages, int v
 // on one address).
 // The pull as a device function, so that a persistent loop kernel can run it
 // once per iteration (k_pull_coo_w is one call of it).
-template <class F, bool HW, bool ALL, int STAGES, bool CONTIG, bool PF, bool NOOUT, bool MERGE>
+// F::gather_pol (a gather that takes an L2 eviction policy), when declared
+template <class F, class = void>
+struct has_gather_pol : std::false_type {};
+template <class F>
+struct has_gather_pol<F, decltype((void)std::declval<const F&>().gather_pol(0u, 0u, 0ull))> : std::true_type {};
+
+// HINT bits of the direct-load pull: 1 the edge stream bypasses L1 and is
+// marked evict-first in L2; 2 the source gathers (functors with gather_pol)
+// are marked evict-last in L1 and L2.
+template <class F, bool HW, bool ALL, int STAGES, bool CONTIG, bool PF, bool NOOUT, bool MERGE, int HINT = 0>
 __device__ __forceinline__ void pull_coo_w_run(const PullParams& p, const F& f) {
   static_assert(!NOOUT || F::kIdentityCommitNoop, "discarding the output needs a no-op identity commit");
   constexpr bool kFin = finishes<F>::value;  // the vertex step runs at the commit (PrFinishF)
@@ -554,6 +566,22 @@ __device__ __forceinline__ void pull_coo_w_run(const PullParams& p, const F& f) 
   uint32_t parity = 0;
   unsigned long long my_cnt = 0, my_deg = 0;
   double my_l1 = 0;
+  constexpr bool kStreamHint = (HINT & 1) != 0 && STAGES == 0 && !CONTIG && !PF;
+  constexpr bool kGatherHint = (HINT & 2) != 0 && has_gather_pol<F>::value;
+  const uint64_t pol_stream = kStreamHint ? l2_policy_evict_first() : 0ull;
+  const uint64_t pol_keep = kGatherHint ? l2_policy_evict_last() : 0ull;
+  auto gather = [&](uint32_t s, uint32_t w) -> V {
+    if constexpr (kGatherHint)
+      return f.gather_pol(s, w, pol_keep);
+    else
+      return f.gather(s, w);
+  };
+  auto ld16 = [&](const void* ptr) -> uint4 {
+    if constexpr (kStreamHint)
+      return ld_stream_v4(ptr, pol_stream);
+    else
+      return __ldg(reinterpret_cast<const uint4*>(ptr));
+  };
 
   for (;;) {
     if (tid == 0) s_tile = (uint32_t)atomicAdd(p.tile_counter, 1ull);
@@ -673,16 +701,16 @@ __device__ __forceinline__ void pull_coo_w_run(const PullParams& p, const F& f) 
         }
       } else if (in) {
         const size_t b0 = (size_t)e0 + (size_t)j * kSegBlock + (size_t)lane * 8;
-        const uint4 a = __ldg(reinterpret_cast<const uint4*>(p.src + b0));
-        const uint4 c = __ldg(reinterpret_cast<const uint4*>(p.src + b0) + 1);
+        const uint4 a = ld16(p.src + b0);
+        const uint4 c = ld16(p.src + b0 + 4);
         sv[0] = a.x; sv[1] = a.y; sv[2] = a.z; sv[3] = a.w;
         sv[4] = c.x; sv[5] = c.y; sv[6] = c.z; sv[7] = c.w;
-        const uint4 q = __ldg(reinterpret_cast<const uint4*>(p.dloc + b0));
+        const uint4 q = ld16(p.dloc + b0);
         dv[0] = q.x & 0xffff; dv[1] = q.x >> 16; dv[2] = q.y & 0xffff; dv[3] = q.y >> 16;
         dv[4] = q.z & 0xffff; dv[5] = q.z >> 16; dv[6] = q.w & 0xffff; dv[7] = q.w >> 16;
         if (HW) {
-          const uint4 u = __ldg(reinterpret_cast<const uint4*>(p.wts + b0));
-          const uint4 v = __ldg(reinterpret_cast<const uint4*>(p.wts + b0) + 1);
+          const uint4 u = ld16(p.wts + b0);
+          const uint4 v = ld16(p.wts + b0 + 4);
           wv[0] = u.x; wv[1] = u.y; wv[2] = u.z; wv[3] = u.w;
           wv[4] = v.x; wv[5] = v.y; wv[6] = v.z; wv[7] = v.w;
         }
@@ -702,7 +730,7 @@ __device__ __forceinline__ void pull_coo_w_run(const PullParams& p, const F& f) 
       V val[8];
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
-        val[k] = vld[k] ? f.gather(sv[k], wv[k]) : F::identity();
+        val[k] = vld[k] ? gather(sv[k], wv[k]) : F::identity();
         if (F::kPositive) vld[k] = vld[k] && !(val[k] < F::identity());
       }
       if constexpr (CONTIG) {
@@ -856,9 +884,9 @@ __device__ __forceinline__ void pull_coo_w_run(const PullParams& p, const F& f) 
 }
 
 template <class F, bool HW, bool ALL, int STAGES, bool CONTIG = false, bool PF = false, bool NOOUT = false,
-          bool MERGE = false>
+          bool MERGE = false, int HINT = 0>
 __global__ void __launch_bounds__(kCooThreads, GG_COO_MIN_BLOCKS) k_pull_coo_w(const PullParams p, const F f) {
-  pull_coo_w_run<F, HW, ALL, STAGES, CONTIG, PF, NOOUT, MERGE>(p, f);
+  pull_coo_w_run<F, HW, ALL, STAGES, CONTIG, PF, NOOUT, MERGE, HINT>(p, f);
 }
 
 // ------------------------------------------ source-partitioned COO (-P source)
@@ -1161,7 +1189,10 @@ __global__ void __launch_bounds__(kSegThreads, 3) k_pull_seg(const SegParams p, 
 }
 
 // Dense pull with early exit (kEarlyExit functors): one lane per destination.
-template <class F, bool HW, bool ALL>
+// VEC: the in-list is read in 16-byte aligned groups of 4 edges (edge arrays
+// are 16-byte aligned and padded past their end) whose frontier tests issue
+// together; the edges are still taken in list order.
+template <class F, bool HW, bool ALL, bool VEC = false>
 __global__ void __launch_bounds__(256) k_pull_early(uint32_t n, const uint32_t* off, const uint32_t* idx,
                                                     const uint32_t* wts, const uint32_t* fr_bits,
                                                     uint32_t* next_bits, const uint32_t* deg_off,
@@ -1174,12 +1205,33 @@ __global__ void __launch_bounds__(256) k_pull_early(uint32_t n, const uint32_t* 
     const uint32_t v = (uint32_t)b + lane;
     bool act = false;
     if (v < n && f.cond(v) && (!member_off || member_off[v + 1] > member_off[v])) {
-      const uint32_t e1 = off[v + 1];
-      for (uint32_t j = off[v]; j < e1; ++j) {
-        const uint32_t s = idx[j];
-        if (ALL || test_bit(fr_bits, s)) {
-          act = f.commit(v, f.gather(s, HW ? wts[j] : 1u));
-          if (act || !f.cond(v)) break;
+      const uint32_t j0 = off[v], e1 = off[v + 1];
+      if constexpr (VEC) {
+        bool done = false;
+        for (uint32_t a = j0 & ~3u; a < e1 && !done; a += 4) {
+          const uint4 q = __ldg(reinterpret_cast<const uint4*>(idx + a));
+          const uint32_t ss[4] = {q.x, q.y, q.z, q.w};
+          bool hit[4];
+#pragma unroll
+          for (int t = 0; t < 4; ++t) {
+            const uint32_t e = a + (uint32_t)t;
+            hit[t] = e >= j0 && e < e1 && (ALL || test_bit(fr_bits, ss[t]));
+          }
+#pragma unroll
+          for (int t = 0; t < 4; ++t) {
+            if (!done && hit[t]) {
+              act = f.commit(v, f.gather(ss[t], HW ? wts[a + t] : 1u));
+              if (act || !f.cond(v)) done = true;
+            }
+          }
+        }
+      } else {
+        for (uint32_t j = j0; j < e1; ++j) {
+          const uint32_t s = idx[j];
+          if (ALL || test_bit(fr_bits, s)) {
+            act = f.commit(v, f.gather(s, HW ? wts[j] : 1u));
+            if (act || !f.cond(v)) break;
+          }
         }
       }
     }

@@ -6,6 +6,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "gg_device.cuh"
+
 namespace gg {
 
 struct MinI32 {
@@ -109,6 +111,10 @@ struct PrT : SumF32 {
   float* acc_out;
   __device__ bool cond(uint32_t) const { return true; }
   __device__ value_t gather(uint32_t s, uint32_t) const { return __ldg(contrib + s); }
+  // gather with an L2 eviction policy (kept ahead of the streamed edges)
+  __device__ value_t gather_pol(uint32_t s, uint32_t, uint64_t pol) const {
+    return gg::ld_keep_f32(contrib + s, pol);
+  }
   __device__ bool commit(uint32_t d, value_t acc) const {
     acc_out[d] += acc;
     return true;
@@ -172,6 +178,9 @@ struct SpmvF : SumF32 {
   __device__ uint32_t yi(uint32_t d) const { return y_map ? __ldg(y_map + d) : d; }
   __device__ bool cond(uint32_t) const { return true; }
   __device__ value_t gather(uint32_t s, uint32_t w) const { return __ldg(x + s) * wv(w); }
+  __device__ value_t gather_pol(uint32_t s, uint32_t w, uint64_t pol) const {
+    return gg::ld_keep_f32(x + s, pol) * wv(w);
+  }
   __device__ bool commit(uint32_t d, value_t acc) const {
     y[yi(d)] += acc;
     return true;

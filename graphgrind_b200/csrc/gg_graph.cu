@@ -22,6 +22,44 @@
 
 namespace gg {
 
+// ------------------------------------------------------------ memory pools
+constexpr int kPoolDevices = 16;
+static std::mutex g_pool_mu;
+static cudaMemPool_t g_pools[kPoolDevices];
+static bool g_pool_failed[kPoolDevices];
+
+static cudaMemPool_t lib_pool(int device) {
+  if (device < 0 || device >= kPoolDevices) return nullptr;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (!g_pools[device] && !g_pool_failed[device]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+      cudaGetLastError();
+      g_pool_failed[device] = true;
+      return nullptr;
+    }
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    g_pools[device] = pool;
+  }
+  return g_pools[device];
+}
+
+cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t s, int device) {
+  cudaMemPool_t pool = lib_pool(device);
+  return pool ? cudaMallocFromPoolAsync(p, bytes, pool, s) : cudaMallocAsync(p, bytes, s);
+}
+
+void pool_trim(int device) {
+  if (device < 0 || device >= kPoolDevices) return;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (g_pools[device]) cudaMemPoolTrimTo(g_pools[device], 0);
+}
+
 static std::mutex g_reg_mu;
 static std::unordered_set<const gg_graph_s*> g_graphs;
 static std::unordered_set<const gg_frontier_s*> g_frontiers;
@@ -62,14 +100,14 @@ int frontier_new(gg_graph_s* g, gg_frontier_s** out) {
 int frontier_ensure_bits(gg_frontier_s* f, bool zero) {
   gg_graph_s* g = f->g;
   const size_t bytes = sizeof(uint32_t) * ((size_t)g->words() + 4);
-  if (!f->d_bits) GG_CUDA(cudaMallocAsync((void**)&f->d_bits, bytes, g->stream));
+  if (!f->d_bits) GG_CUDA(pool_alloc((void**)&f->d_bits, bytes, g->stream, g->device));
   if (zero) GG_CUDA(cudaMemsetAsync(f->d_bits, 0, bytes, g->stream));
   return GG_OK;
 }
 
 int frontier_ensure_queue(gg_frontier_s* f) {
   gg_graph_s* g = f->g;
-  if (!f->d_queue) GG_CUDA(cudaMallocAsync((void**)&f->d_queue, sizeof(uint32_t) * ((size_t)g->n + 4), g->stream));
+  if (!f->d_queue) GG_CUDA(pool_alloc((void**)&f->d_queue, sizeof(uint32_t) * ((size_t)g->n + 4), g->stream, g->device));
   return GG_OK;
 }
 
@@ -807,7 +845,9 @@ int gg_graph_synchronize(gg_graph_t g) {
 int gg_graph_destroy(gg_graph_t g) {
   if (!graph_live(g)) return fail(GG_ERR_INVALID_ARG, "gg_graph_destroy: not a live graph");
   cudaStreamSynchronize(g->stream);
+  const int device = g->device;
   graph_release(g);
+  pool_trim(device);  // only memory no graph holds goes back
   return GG_OK;
 }
 
@@ -915,7 +955,7 @@ int gg_graph_set_tuning(gg_graph_t g, int32_t key, int64_t value) {
     case GG_TUNE_DENSE_POLICY:
       return gg_graph_set_dense_policy(g, (int32_t)value);
     case GG_TUNE_COO_KERNEL:
-      if (value < 0 || value > 6) return fail(GG_ERR_INVALID_ARG, "COO kernel must be 0..6");
+      if (value < 0 || value > 7) return fail(GG_ERR_INVALID_ARG, "COO kernel must be 0..7");
       g->coo_kernel = (int)value;
       return GG_OK;
     case GG_TUNE_SPARSE_DIV:
@@ -935,7 +975,7 @@ int gg_graph_set_tuning(gg_graph_t g, int32_t key, int64_t value) {
       g->pr_graph = (int)value;
       return GG_OK;
     case GG_TUNE_EARLY_KERNEL:
-      if (value != 0 && value != 1) return fail(GG_ERR_INVALID_ARG, "early-exit kernel must be 0 or 1");
+      if (value < 0 || value > 2) return fail(GG_ERR_INVALID_ARG, "early-exit kernel must be 0, 1 or 2");
       g->early_kernel = (int)value;
       return GG_OK;
     case GG_TUNE_PUSH_DENSE_DIV:

@@ -443,10 +443,13 @@ int bfs_device_levels(gg_graph_s* g, gg_frontier_s** F, int32_t* parents, int32_
 // the frontier bitmap bcur and joins bnxt.  *cnt / *deg: this thread's new
 // vertices and their out-degree sum.  Not inlined: the loop then keeps its
 // registers whatever the rest of the level-loop kernel holds.
+// vec: the in-list is read in 16-byte aligned groups of 4 edges (the edge
+// arrays are 16-byte aligned and padded past their end), the group's 4
+// frontier tests issued together; the first hit in list order still wins.
 __device__ __noinline__ void bottom_up_level(const uint32_t* __restrict__ off, const uint32_t* __restrict__ ioff,
                                              const uint32_t* __restrict__ iidx, int32_t* parents, int32_t* levels,
                                              const uint32_t* bcur, uint32_t* bnxt, uint32_t n, int32_t r,
-                                             uint32_t* cnt, uint32_t* deg) {
+                                             uint32_t* cnt, uint32_t* deg, int vec) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t stride = gridDim.x * blockDim.x;  // <= 2^31 threads
   uint32_t c = 0, dg = 0;
@@ -454,14 +457,33 @@ __device__ __noinline__ void bottom_up_level(const uint32_t* __restrict__ off, c
     const uint32_t v = b + lane;
     bool act = false;
     if (v < n && __ldcg(parents + v) == -1) {
-      const uint32_t e1 = ioff[v + 1];
-      for (uint32_t j = ioff[v]; j < e1; ++j) {
-        const uint32_t s = iidx[j];
-        if ((bcur[s >> 5] >> (s & 31)) & 1u) {
-          parents[v] = (int32_t)s;
-          if (levels) levels[v] = r;
-          act = true;
-          break;
+      const uint32_t j0 = ioff[v], e1 = ioff[v + 1];
+      if (vec) {
+        for (uint32_t a = j0 & ~3u; a < e1; a += 4) {
+          const uint4 q = __ldg(reinterpret_cast<const uint4*>(iidx + a));
+          const uint32_t ss[4] = {q.x, q.y, q.z, q.w};
+          int hit = -1;
+#pragma unroll
+          for (int t = 3; t >= 0; --t) {
+            const uint32_t e = a + (uint32_t)t;
+            if (e >= j0 && e < e1 && ((bcur[ss[t] >> 5] >> (ss[t] & 31)) & 1u)) hit = t;
+          }
+          if (hit >= 0) {
+            parents[v] = (int32_t)ss[hit];
+            if (levels) levels[v] = r;
+            act = true;
+            break;
+          }
+        }
+      } else {
+        for (uint32_t j = j0; j < e1; ++j) {
+          const uint32_t s = iidx[j];
+          if ((bcur[s >> 5] >> (s & 31)) & 1u) {
+            parents[v] = (int32_t)s;
+            if (levels) levels[v] = r;
+            act = true;
+            break;
+          }
         }
       }
     }
@@ -516,7 +538,7 @@ __global__ void __launch_bounds__(256, 8) k_bfs_full(const uint32_t* __restrict_
                                                      uint32_t* eo1, uint32_t* bits, uint32_t wstride,
                                                      unsigned long long* cta, uint32_t n, LoopState* st,
                                                      int32_t round0, unsigned long long threshold,
-                                                     int32_t max_levels, unsigned wait_budget) {
+                                                     int32_t max_levels, unsigned wait_budget, int bu_vec) {
   __shared__ uint32_t s_eo[257];
   __shared__ uint32_t s_v[256];
   __shared__ uint32_t s_beg[256];
@@ -560,7 +582,7 @@ __global__ void __launch_bounds__(256, 8) k_bfs_full(const uint32_t* __restrict_
     if (nk + E > threshold) {
       // bottom-up: one lane per destination, the first frontier in-neighbour wins
       uint32_t c32 = 0, dg32 = 0;
-      bottom_up_level(off, ioff, iidx, parents, levels, bcur, bnxt, n, r, &c32, &dg32);
+      bottom_up_level(off, ioff, iidx, parents, levels, bcur, bnxt, n, r, &c32, &dg32, bu_vec);
       unsigned long long c = warp_sum((unsigned long long)c32), dg = warp_sum((unsigned long long)dg32);
       if (lane == 0) {
         s_red[0][warp] = c;
@@ -744,10 +766,11 @@ int bfs_device_full(gg_graph_s* g, uint32_t start, int32_t* parents, int32_t* le
   unsigned long long thr = threshold;
   int32_t cap = n < (uint32_t)INT32_MAX ? (int32_t)n + 1 : INT32_MAX;
   unsigned budget = g->loop_wait_budget;
+  int vec = g->early_kernel == 2 ? 1 : 0;
   void* args[] = {(void*)&off, (void*)&idx, (void*)&ioff, (void*)&iidx, (void*)&parents, (void*)&levels,
                   (void*)&a0,  (void*)&a1,  (void*)&e0,   (void*)&e1,   (void*)&bp,      (void*)&ws,
                   (void*)&cp,  (void*)&nn,  (void*)&d_st, (void*)&round0, (void*)&thr,   (void*)&cap,
-                  (void*)&budget};
+                  (void*)&budget, (void*)&vec};
   GG_CUDA(cudaLaunchCooperativeKernel((const void*)k_bfs_full, grid, 256, args, 0, g->stream));
   LoopState h{};
   GG_CUDA(cudaMemcpyAsync(&h, d_st, sizeof(h), cudaMemcpyDeviceToHost, g->stream));

@@ -34,6 +34,16 @@ struct EventTimer {
   }
 };
 
+// Stream-ordered allocations of the library (temporaries of the
+// applications, frontiers) come from one memory pool per device whose release
+// threshold is unlimited: memory freed back to it stays mapped across stream
+// synchronisations, so the next call reuses it instead of mapping it again
+// (the default pool returns it at every synchronisation).  Devices past the
+// pool table, or a pool the driver refuses, take cudaMallocAsync.
+cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t s, int device);
+// Returns the pool's unused memory of `device` to the system.
+void pool_trim(int device);
+
 // A stream-ordered device allocation released when the holder leaves scope.
 template <class T>
 struct DevBuf {
@@ -41,7 +51,7 @@ struct DevBuf {
   gg_graph_s* g = nullptr;
   int alloc(gg_graph_s* gg_, uint64_t n) {
     g = gg_;
-    GG_CUDA(cudaMallocAsync((void**)&p, sizeof(T) * (n + 4), g->stream));
+    GG_CUDA(pool_alloc((void**)&p, sizeof(T) * (n + 4), g->stream, g->device));
     return GG_OK;
   }
   ~DevBuf() {
@@ -247,7 +257,7 @@ int pull_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f
   if (coo && g->coo_kernel > 0) {  // per-warp COO pull: 0, 2 or 3 staging stages
     static DeviceOnce opted[2][4];
     static DeviceOnce opted_pf[2];
-    static DeviceOnce opted_no[2][2];
+    static DeviceOnce opted_no[3][2];
     static DeviceOnce opted_mg[2];
     constexpr int kFlags = coo_w_flag_bytes<F, false>(), kFlagsNoOut = coo_w_flag_bytes<F, true>();
     auto launch_w = [&](auto kern, int stages, DeviceOnce& once, int flags) -> int {
@@ -276,8 +286,17 @@ int pull_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f
         return all ? launch_w(k_pull_coo_w<F, kHW, true, 0, false, false, true, true>, 0, opted_no[1][1], kFlagsNoOut)
                    : launch_w(k_pull_coo_w<F, kHW, false, 0, false, false, true, true>, 0, opted_no[1][0],
                               kFlagsNoOut);
+      if (no_out && g->coo_kernel == 7)
+        return all ? launch_w(k_pull_coo_w<F, kHW, true, 0, false, false, true, true, 3>, 0, opted_no[2][1],
+                              kFlagsNoOut)
+                   : launch_w(k_pull_coo_w<F, kHW, false, 0, false, false, true, true, 3>, 0, opted_no[2][0],
+                              kFlagsNoOut);
     }
+    static DeviceOnce opted_h[2];
     switch (g->coo_kernel) {
+      case 7:
+        return all ? launch_w(k_pull_coo_w<F, kHW, true, 0, false, false, false, true, 3>, 0, opted_h[1], kFlags)
+                   : launch_w(k_pull_coo_w<F, kHW, false, 0, false, false, false, true, 3>, 0, opted_h[0], kFlags);
       case 6:
         return all ? launch_w(k_pull_coo_w<F, kHW, true, 0, false, false, false, true>, 0, opted_mg[1], kFlags)
                    : launch_w(k_pull_coo_w<F, kHW, false, 0, false, false, false, true>, 0, opted_mg[0], kFlags);
@@ -352,6 +371,13 @@ int pull_early_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, cons
           g->n, g->in_off(), g->in_idx(), g->in_w(), nullptr, out->d_bits, g->out_off(), member, g->ws.d_stats, f);
     else
       k_pull_early_g<F, HW, false><<<grid, kGenericThreads, 0, g->stream>>>(
+          g->n, g->in_off(), g->in_idx(), g->in_w(), in->d_bits, out->d_bits, g->out_off(), member, g->ws.d_stats, f);
+  } else if (g->early_kernel == 2) {
+    if (in->bit)
+      k_pull_early<F, HW, true, true><<<grid, kGenericThreads, 0, g->stream>>>(
+          g->n, g->in_off(), g->in_idx(), g->in_w(), nullptr, out->d_bits, g->out_off(), member, g->ws.d_stats, f);
+    else
+      k_pull_early<F, HW, false, true><<<grid, kGenericThreads, 0, g->stream>>>(
           g->n, g->in_off(), g->in_idx(), g->in_w(), in->d_bits, out->d_bits, g->out_off(), member, g->ws.d_stats, f);
   } else if (in->bit) {
     k_pull_early<F, HW, true><<<grid, kGenericThreads, 0, g->stream>>>(

@@ -92,7 +92,7 @@ int gg_autotune(gg_graph_t g, int32_t app, uint32_t start, gg_tune_trial* trials
   HostBufs bufs(info.n);
   std::vector<gg_tune_trial> tried;
   const bool has_coo = info.num_coo_tiles > 0;
-  std::vector<int> kernels = {6, 1, 5, 0};
+  std::vector<int> kernels = {7, 6, 1, 5, 0};
   if (keep[1] == 4) kernels.push_back(4);  // lane-contiguous pull: graphs built with source-ordered windows
   const int policies[3] = {0, 1, 2};
   const int divs[3] = {20, 10, 40};

@@ -332,8 +332,12 @@ int gg_graph_set_dense_policy(gg_graph_t g, int32_t policy);
  *                         default for graphs built with coo_window > 0),
  *                         5 per-warp direct loads with the next block's edge
  *                         stream prefetched into registers, 6 per-warp direct
- *                         loads with destination runs merged across lanes (the
- *                         default for graphs built with coo_window == 0)
+ *                         loads with destination runs merged across lanes;
+ *                         7 kernel 6 with cache hints (the default for graphs
+ *                         built with coo_window == 0): the edge stream read
+ *                         past L1 and marked evict-first in L2, the source
+ *                         gathers of PageRank and SpMV marked evict-last in
+ *                         L1 and L2
  *   GG_TUNE_SPARSE_DIV    the application loops (gg_bfs ... gg_bc) call edgeMap
  *                         with threshold m / value (20 in the reference apps)
  *   GG_TUNE_DEVICE_LOOP   2 (default): gg_bfs runs the whole BFS in one
@@ -400,7 +404,10 @@ int gg_graph_set_dense_policy(gg_graph_t g, int32_t policy);
  *                         step; 1 8 lanes walk a destination's in-list 8 edges
  *                         per step, 4 destinations per warp (faster on long
  *                         rows, slower on R-MAT-24: 0.67 against 0.46 ms for
- *                         BFS's three bottom-up levels)
+ *                         BFS's three bottom-up levels); 2 one lane per
+ *                         destination reading its in-list 4 edges per 16-byte
+ *                         load, the 4 frontier tests issued together (also in
+ *                         the bottom-up levels of GG_TUNE_DEVICE_LOOP 2)
  *   GG_TUNE_PUSH_DENSE_DIV  a dense edgeMap of BFS (an early-exit functor)
  *                         whose frontier has at most n / value vertices runs
  *                         top-down instead (the frontier's out-edges pushed,

@@ -341,7 +341,7 @@ def test_source_partitions(gg, orc, name):
         _close(g.spmv()[0], og.spmv()[0], rel=1e-6, mx=1e-6)
 
 
-@pytest.mark.parametrize("kernel", [0, 1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("kernel", [0, 1, 2, 3, 4, 5, 6, 7])
 def test_coo_kernels_on_multigraph(gg, orc, kernel):
     """Every COO pull kernel on repeated edges and loops (coo_window builds
     give kernel 4 its lane-contiguous layout)."""

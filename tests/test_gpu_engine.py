@@ -117,15 +117,16 @@ def test_empty_result_cannot_be_mapped_again(gg, sym12):
 
 
 @pytest.mark.parametrize("coo_window", [0, 1024, 100000])
-@pytest.mark.parametrize("coo_kernel", [0, 1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("coo_kernel", [0, 1, 2, 3, 4, 5, 6, 7])
 def test_apps_with_each_coo_kernel(gg, orc, coo_kernel, coo_window):
     """Every COO pull variant (CTA ring, per-warp direct, per-warp 2/3-stage
-    rings, lane-contiguous) on every window order gives the oracle's results
+    rings, lane-contiguous, prefetch, merged runs with and without cache
+    hints) on every window order gives the oracle's results
     when all dense steps use the COO."""
     from conftest import PR_MAX_ABS, PR_REL_L1, rel_l1
     hg = gg.HostGraph.rmat(12, 16, seed=81, symmetric=False).add_weights(gg.W_INT32, seed=2, lo=1, hi=100)
     g = gg.Graph(hg, partitions=ok_partitions(hg, 16), tile_vertices=1024, coo_window=coo_window)
-    assert g.get_tuning(gg.TUNE_COO_KERNEL) == (4 if coo_window else 6)
+    assert g.get_tuning(gg.TUNE_COO_KERNEL) == (4 if coo_window else 7)
     g.set_dense_policy(2)
     g.set_tuning(gg.TUNE_COO_KERNEL, coo_kernel)
     assert g.get_tuning(gg.TUNE_COO_KERNEL) == coo_kernel
@@ -180,7 +181,7 @@ def test_bfs_device_loop_matches_host_loop(gg, orc, graph):
             assert np.all(lev[p] == lev[reached & (lev > 0)] - 1)
 
 
-@pytest.mark.parametrize("kernel", [1, 6])
+@pytest.mark.parametrize("kernel", [1, 6, 7])
 @pytest.mark.parametrize("force", ["coo", "csc", "sparse"])
 def test_spmv_edge_map_without_output(gg, sym12, force, kernel):
     """GG_EM_NO_OUTPUT keeps the SPMV sums; the dense COO pull then returns an

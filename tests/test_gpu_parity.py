@@ -255,18 +255,23 @@ def test_apps_with_source_partitions(gg, orc, sym):
         check_float(y, og.spmv()[0], rel=1e-6, mx=1e-6 * float(np.abs(og.spmv()[0]).max()))
 
 
-@pytest.mark.parametrize("kernel", [0, 1])
-def test_bfs_early_exit_kernels(gg, rmat14, kernel):
-    """Both forms of the bottom-up (early-exit) dense step give the oracle's
+@pytest.mark.parametrize("loop", [0, 2])
+@pytest.mark.parametrize("kernel", [0, 1, 2])
+def test_bfs_early_exit_kernels(gg, rmat14, kernel, loop):
+    """Every form of the bottom-up (early-exit) dense step, from the host
+    (device loop 0) and inside the all-levels launch (2), gives the oracle's
     levels; parents are frontier in-neighbours one level up."""
     hg, g, og = rmat14
+    keep = g.get_tuning(gg.TUNE_DEVICE_LOOP)
     g.set_tuning(gg.TUNE_EARLY_KERNEL, kernel)
+    g.set_tuning(gg.TUNE_DEVICE_LOOP, loop)
     g.set_dense_policy(1)  # every dense level takes the early-exit CSC pull
     try:
         for start in (0, 100, 12345):
             check_bfs(g, og, start, hg)
     finally:
         g.set_tuning(gg.TUNE_EARLY_KERNEL, 0)
+        g.set_tuning(gg.TUNE_DEVICE_LOOP, keep)
         g.set_dense_policy(0)
 
 
