@@ -25,8 +25,7 @@ static int fill(gg_graph_s* g, T* a, uint64_t n, T v) {
 
 template <class T>
 static int set_one(gg_graph_s* g, T* a, uint32_t i, T v) {
-  GG_CUDA(cudaMemcpyAsync(a + i, &v, sizeof(T), cudaMemcpyHostToDevice, g->stream));
-  return GG_OK;
+  return write_small(g, a + i, v);
 }
 
 struct FrontierHold {
@@ -150,12 +149,7 @@ __global__ void k_bc_final(uint32_t n, float* dep, const float* inv) {
     dep[j] = (dep[j] - inv[j]) / inv[j];
 }
 
-static int read_red(gg_graph_s* g, double* v) {
-  GG_CUDA(cudaMemcpyAsync(g->ws.h_red, g->ws.d_red, sizeof(double), cudaMemcpyDeviceToHost, g->stream));
-  GG_CUDA(cudaStreamSynchronize(g->stream));
-  *v = g->ws.h_red[0];
-  return GG_OK;
-}
+static int read_red(gg_graph_s* g, double* v) { return read_small(g, v, g->ws.d_red); }
 
 static void fill_stats(gg_run_stats* st, double ms, int rounds, uint64_t trav, int kernels) {
   if (!st) return;
@@ -171,7 +165,7 @@ static int to_host(gg_graph_s* g, T* host, const T* dev, uint64_t n) {
   // asynchronous results: a result staged in a given-order array leaves on
   // the copy stream into pinned memory, and the call does not wait for it
   int slot = -1;
-  for (int k = 0; k < 2; ++k)
+  for (int k = 0; k < 3; ++k)
     if (g->ws.d_order[k] && reinterpret_cast<const void*>(dev) == g->ws.d_order[k]) slot = k;
   cudaPointerAttributes pa{};
   if (g->async_results && slot >= 0 && cudaPointerGetAttributes(&pa, host) == cudaSuccess &&
@@ -194,21 +188,26 @@ static int run_bfs(gg_graph_s* g, uint32_t start, int32_t* parents, int32_t* lev
   const uint32_t n = g->n;
   g->kernels = 0;
   DevBuf<int32_t> par, lev;
+  // every level in one cooperative launch (its dense levels pull over the CSC;
+  // a graph told to pull over the COO keeps the host loop for them), which
+  // writes levels only when they are asked for
+  const bool full = g->device_loop == 2 && !g->transposed && g->dense_policy != 2;
+  const bool want_lev = levels || !full;
   GG_TRY(par.alloc(g, n));
-  GG_TRY(lev.alloc(g, n));
+  if (want_lev) GG_TRY(lev.alloc(g, n));
   EventTimer tm(g->stream);
   GG_TRY(fill<int32_t>(g, par.p, n, -1));
-  GG_TRY(fill<int32_t>(g, lev.p, n, -1));
   GG_TRY(set_one<int32_t>(g, par.p, start, (int32_t)start));
-  GG_TRY(set_one<int32_t>(g, lev.p, start, 0));
+  if (want_lev) {
+    GG_TRY(fill<int32_t>(g, lev.p, n, -1));
+    GG_TRY(set_one<int32_t>(g, lev.p, start, 0));
+  }
   FrontierHold F;
   int32_t round = 0;
   uint64_t trav = 0;
   const int64_t thr = app_threshold(g);
-  // every level in one cooperative launch (its dense levels pull over the CSC;
-  // a graph told to pull over the COO keeps the host loop for them)
-  if (g->device_loop == 2 && !g->transposed && g->dense_policy != 2)
-    GG_TRY(bfs_device_full(g, start, par.p, lev.p, (uint64_t)thr, &round, &trav));
+  if (full)
+    GG_TRY(bfs_device_full(g, start, par.p, lev.p, (uint64_t)thr));
   else
     GG_TRY(gg_frontier_single(g, start, &F.f));
   while (F.f && F.f->dm > 0) {
@@ -236,17 +235,21 @@ static int run_bfs(gg_graph_s* g, uint32_t start, int32_t* parents, int32_t* lev
   }
   const int32_t* par_out = par.p;
   const int32_t* lev_out = lev.p;
+  const int pslot = g->async_results && g->ws.d_order[2] ? 2 : 0;  // the given-order array of the parents
   if (g->relabeled && parents) {
-    int32_t* tp = reinterpret_cast<int32_t*>(g->ws.d_order[0]);
-    GG_TRY(slot_write_wait(g, 0));
+    int32_t* tp = reinterpret_cast<int32_t*>(g->ws.d_order[pslot]);
+    GG_TRY(slot_write_wait(g, pslot));
     k_ids_to_given<<<generic_grid(g, n), kGenericThreads, 0, g->stream>>>(n, g->d_new_of_old, g->d_old_of_new,
                                                                           par.p, tp);
     g->kernels++;
     par_out = tp;
   }
-  if (parents && !g->relabeled) GG_TRY(given_order<int32_t>(g, par.p, 0, &par_out));
+  if (parents && !g->relabeled) GG_TRY(given_order<int32_t>(g, par.p, pslot, &par_out));
   if (levels) GG_TRY(given_order<int32_t>(g, lev.p, 1, &lev_out));
   const double ms = tm.stop();
+  // the all-levels launch is read back after the device work it feeds was
+  // queued behind it, so that the stream does not idle for the host
+  if (full) GG_TRY(bfs_device_full_result(g, &round, &trav));
   GG_TRY(to_host(g, parents, par_out, n));
   GG_TRY(to_host(g, levels, lev_out, n));
   fill_stats(st, ms, round, trav, g->kernels);
@@ -1027,10 +1030,9 @@ static int round_loop_run(gg_graph_s* g, RoundLoop* L, FrontierHold& F, uint32_t
   c.coo_always = (g->dense_policy == 0 || g->transposed) ? 0u : 1u;
   c.use_l1 = l1 ? 1u : 0u;
   c.eps = eps;
-  GG_CUDA(cudaMemcpyAsync(L->d_ctl, L->h_ctl, sizeof(RoundLoopCtl), cudaMemcpyHostToDevice, g->stream));
+  GG_TRY(write_small(g, L->d_ctl, c));
   GG_CUDA(cudaGraphLaunch(L->exec, g->stream));
-  GG_CUDA(cudaMemcpyAsync(L->h_ctl, L->d_ctl, sizeof(RoundLoopCtl), cudaMemcpyDeviceToHost, g->stream));
-  GG_CUDA(cudaStreamSynchronize(g->stream));
+  GG_TRY(read_small(g, L->h_ctl, L->d_ctl));
   if (c.reason == 4) return fail(GG_ERR_TIMEOUT, "device wait budget exhausted (error word %llu)", c.err);
   if (c.reason < 1 || c.reason > 3 || c.count < 1 || c.count > max_rounds)
     return fail(GG_ERR_CUDA, "round graph: bad loop state");
@@ -1111,18 +1113,18 @@ static int run_pagerank(gg_graph_s* g, int max_iter, int bit_all, float* ranks, 
     c.dense_threshold = m / 2;
     c.max_iter = (uint32_t)max_iter;
     c.coo_always = ref_rule ? 0u : 1u;
-    GG_CUDA(cudaMemcpyAsync(L->d_ctl, L->h_ctl, sizeof(PrLoopCtl), cudaMemcpyHostToDevice, g->stream));
+    GG_TRY(write_small(g, L->d_ctl, c));
     GG_CUDA(cudaGraphLaunch(L->exec, g->stream));
-    GG_CUDA(cudaMemcpyAsync(L->h_ctl, L->d_ctl, sizeof(PrLoopCtl), cudaMemcpyDeviceToHost, g->stream));
-    GG_CUDA(cudaStreamSynchronize(g->stream));
+    GG_TRY(read_small(g, L->h_ctl, L->d_ctl));
     if (c.reason == 4) return fail(GG_ERR_TIMEOUT, "device wait budget exhausted (error word %llu)", c.err);
     if (c.reason < 1 || c.reason > 3 || c.count < 1) return fail(GG_ERR_CUDA, "PageRank graph: bad loop state");
     count = (int)c.count;
     trav = c.trav;
     // the initial pass, then per iteration the pull, the vertex step's pass
-    // (uncovered ranges or the epilogue) and the check
+    // (uncovered ranges or the epilogue) and the check; the control block's
+    // write before the graph and read-back after it
     const int per_iter = 2 + (pr_fused(g) && g->coo_gap_count == 0 ? 0 : 1);
-    g->kernels = 1 + per_iter * count;
+    g->kernels = 1 + per_iter * count + 2;
     g->last = gg_edge_map_stats{};
     g->last.kind = 3;
     g->last.frontier_active = c.in_dm;
@@ -1274,8 +1276,7 @@ static int run_pagerank_converge(gg_graph_s* g, int32_t max_iter, double eps, fl
     k_prc_norm<<<grid, kGenericThreads, 0, g->stream>>>(n, p_curr, p_next, red + 2, g->out_off(), contrib.p);
     GG_CUDA(cudaGetLastError());
     g->kernels += 3;
-    GG_CUDA(cudaMemcpyAsync(g->ws.h_red, red, 3 * sizeof(double), cudaMemcpyDeviceToHost, g->stream));
-    GG_CUDA(cudaStreamSynchronize(g->stream));
+    GG_TRY(read_small(g, g->ws.h_red, red, 3));
     L1 = g->ws.h_red[1];
     ++count;
     std::swap(p_curr, p_next);

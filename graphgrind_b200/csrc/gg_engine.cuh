@@ -98,6 +98,9 @@ struct SegIndex {
   uint64_t nrows = 0;
 };
 
+// Size of Workspace::h_map, the largest control block read back through it.
+constexpr size_t kMapBytes = 4096;
+
 struct Workspace {
   unsigned long long* d_stats = nullptr;  // [0] count [1] outdeg [2] queue len [3] err [4] tile ctr [5] total edges
   unsigned long long* h_stats = nullptr;  // pinned mirror
@@ -108,7 +111,12 @@ struct Workspace {
   double* d_red = nullptr;                // reduction scratch (double)
   double* h_red = nullptr;                // pinned
   unsigned long long* d_loop = nullptr;   // state of the device-driven level loops (64 words)
-  uint32_t* d_order[2] = {nullptr, nullptr};  // renumbered graphs: n-entry arrays for the given-order copies
+  uint32_t* h_map = nullptr;              // pinned host block (kMapBytes) that kernels write directly
+  uint32_t* d_map = nullptr;              //   and its device address
+  // renumbered graphs: n-entry arrays for the given-order copies (0, 1); with
+  // GG_TUNE_ASYNC_RESULTS also BFS's parents (2), so that they need not wait
+  // for the copy out of array 0 of the application before
+  uint32_t* d_order[3] = {nullptr, nullptr, nullptr};
 };
 
 struct PrLoop;  // PageRank iterations captured as a CUDA graph (buffers, graph, control block)
@@ -165,7 +173,7 @@ struct gg_graph_s {
   cudaEvent_t result_ready = nullptr;                // on stream: the result to copy is complete
   cudaEvent_t input_ready = nullptr;                 // on copy_stream: a staged SpMV input has arrived
   bool input_staged = false;                         // given-order array 1 holds a staged SpMV input
-  cudaEvent_t slot_copied[2] = {nullptr, nullptr};  // on copy_stream: the last copy out of ws.d_order[k]
+  cudaEvent_t slot_copied[3] = {nullptr, nullptr, nullptr};  // on copy_stream: the last copy out of ws.d_order[k]
   gg::PrLoop* pr_loop = nullptr;  // created by the first graph-driven PageRank call
   gg::RoundLoop* round_loop[3] = {nullptr, nullptr, nullptr};  // BellmanFord, Components, PageRankDelta: created by their first call
   int round_graph = 1;  // dense COO rounds of BellmanFord / Components / PageRankDelta as a CUDA graph

@@ -49,6 +49,10 @@ static cudaMemPool_t lib_pool(int device) {
   return g_pools[device];
 }
 
+__global__ void k_get_words(uint32_t* dst, const uint32_t* src, uint32_t words) {
+  for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) dst[i] = __ldcg(src + i);
+}
+
 cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t s, int device) {
   cudaMemPool_t pool = lib_pool(device);
   return pool ? cudaMallocFromPoolAsync(p, bytes, pool, s) : cudaMallocAsync(p, bytes, s);
@@ -183,9 +187,7 @@ int reset_stats(gg_graph_s* g) {
 }
 
 int read_stats(gg_graph_s* g) {
-  GG_CUDA(cudaMemcpyAsync(g->ws.h_stats, g->ws.d_stats, sizeof(unsigned long long) * 8, cudaMemcpyDeviceToHost,
-                          g->stream));
-  GG_CUDA(cudaStreamSynchronize(g->stream));
+  GG_TRY(read_small(g, g->ws.h_stats, g->ws.d_stats, 8));
   if (g->ws.h_stats[3])
     return fail(GG_ERR_TIMEOUT, "device wait budget exhausted (error word %llu)", (unsigned long long)g->ws.h_stats[3]);
   return GG_OK;
@@ -624,6 +626,7 @@ static void graph_release(gg_graph_s* g) {
   for (auto* a : g->ws.d_order) cudaFree(a);
   if (g->ws.h_stats) cudaFreeHost(g->ws.h_stats);
   if (g->ws.h_red) cudaFreeHost(g->ws.h_red);
+  if (g->ws.h_map) cudaFreeHost(g->ws.h_map);
   for (auto& e : g->prof_ev)
     if (e) cudaEventDestroy(e);
   for (auto& e : g->slot_copied)
@@ -788,14 +791,10 @@ static int graph_build(const gg_host_graph* hg_given, const gg_build_opts* opts_
   GG_TRY(dev_alloc(g, &g->ws.d_red, 64));
   GG_TRY(dev_alloc(g, &g->ws.d_loop, 64));
   if (g->relabeled)
-    for (auto& a : g->ws.d_order) GG_TRY(dev_alloc(g, &a, (size_t)n + 4));
+    for (int k = 0; k < 2; ++k) GG_TRY(dev_alloc(g, &g->ws.d_order[k], (size_t)n + 4));
   GG_CUDA(cudaMallocHost((void**)&g->ws.h_red, 64 * sizeof(double)));
-  // keep stream-ordered allocations (frontiers) cached in the pool
-  cudaMemPool_t pool;
-  if (cudaDeviceGetDefaultMemPool(&pool, g->device) == cudaSuccess) {
-    uint64_t thr = UINT64_MAX;
-    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
-  }
+  GG_CUDA(cudaHostAlloc((void**)&g->ws.h_map, kMapBytes, cudaHostAllocMapped));
+  GG_CUDA(cudaHostGetDevicePointer((void**)&g->ws.d_map, g->ws.h_map, 0));
   GG_CUDA(cudaDeviceSynchronize());
   return GG_OK;
 }
@@ -1002,8 +1001,9 @@ int gg_graph_set_tuning(gg_graph_t g, int32_t key, int64_t value) {
         GG_CUDA(cudaEventCreateWithFlags(&g->result_ready, cudaEventDisableTiming));
         for (auto& e : g->slot_copied) GG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
       }
-      if (value && !g->ws.d_order[0])  // results of graphs with their given ids are staged there too
-        for (auto& a : g->ws.d_order) GG_TRY(dev_alloc(g, &a, (size_t)g->n + 4));
+      if (value)  // results of graphs with their given ids are staged there too; BFS's parents in array 2
+        for (auto& a : g->ws.d_order)
+          if (!a) GG_TRY(dev_alloc(g, &a, (size_t)g->n + 4));
       if (!value && g->copy_stream) GG_CUDA(cudaStreamSynchronize(g->copy_stream));
       g->async_results = (int)value;
       return GG_OK;
@@ -1091,8 +1091,7 @@ int gg_frontier_single(gg_graph_t g, uint32_t v, gg_frontier_t* out) {
   gg_frontier_s* f;
   GG_TRY(frontier_new(g, &f));
   int rc = frontier_ensure_queue(f);
-  if (!rc && cudaMemcpyAsync(f->d_queue, &v, 4, cudaMemcpyHostToDevice, g->stream) != cudaSuccess)
-    rc = fail(GG_ERR_CUDA, "frontier upload failed");
+  if (!rc) rc = write_small(g, f->d_queue, v);
   if (rc) {
     frontier_free(f);
     return rc;

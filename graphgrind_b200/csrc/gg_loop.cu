@@ -388,13 +388,14 @@ int bfs_device_levels(gg_graph_s* g, gg_frontier_s** F, int32_t* parents, int32_
                   (void*)&e1, (void*)&nn, (void*)&d_st, (void*)&round0, (void*)&thr, (void*)&cap, (void*)&budget};
   if (e == cudaSuccess)
     e = cudaLaunchCooperativeKernel((const void*)k_bfs_push_loop, grid, 256, args, 0, g->stream);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&h, d_st, sizeof(h), cudaMemcpyDeviceToHost, g->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+  int rr = GG_OK;
+  if (e == cudaSuccess) rr = read_small(g, &h, d_st);
   g->kernels += 2;
-  if (e != cudaSuccess || h.exit_reason < 0) {
+  if (e != cudaSuccess || rr != GG_OK || h.exit_reason < 0) {
     frontier_free(fa);
     frontier_free(fb);
     if (e != cudaSuccess) return fail(GG_ERR_CUDA, "BFS level loop: %s", cudaGetErrorString(e));
+    if (rr != GG_OK) return rr;
     return fail(GG_ERR_TIMEOUT, "BFS level loop: a grid barrier wait ran out");
   }
   const int32_t L = h.levels_done;
@@ -717,12 +718,11 @@ __global__ void __launch_bounds__(256, 8) k_bfs_full(const uint32_t* __restrict_
   }
 }
 
-// Runs every level of the BFS from `start` in one cooperative launch
-// (k_bfs_full); parents/levels hold the source's entries already.  *rounds is
-// the number of edgeMap rounds (the last one finds nothing), *trav the
-// out-degree sum of the frontiers processed.
-int bfs_device_full(gg_graph_s* g, uint32_t start, int32_t* parents, int32_t* levels, uint64_t threshold,
-                    int32_t* rounds, uint64_t* trav) {
+// Enqueues every level of the BFS from `start` as one cooperative launch
+// (k_bfs_full) on the graph's stream and returns without waiting;
+// parents/levels hold the source's entries already (levels may be null).
+// bfs_device_full_result reads the outcome once the stream has passed it.
+int bfs_device_full(gg_graph_s* g, uint32_t start, int32_t* parents, int32_t* levels, uint64_t threshold) {
   const uint32_t n = g->n;
   static DeviceOnce occ;
   const int per_sm = occ.get(g->device, [dev = g->device]() {
@@ -772,10 +772,16 @@ int bfs_device_full(gg_graph_s* g, uint32_t start, int32_t* parents, int32_t* le
                   (void*)&cp,  (void*)&nn,  (void*)&d_st, (void*)&round0, (void*)&thr,   (void*)&cap,
                   (void*)&budget, (void*)&vec};
   GG_CUDA(cudaLaunchCooperativeKernel((const void*)k_bfs_full, grid, 256, args, 0, g->stream));
-  LoopState h{};
-  GG_CUDA(cudaMemcpyAsync(&h, d_st, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
-  GG_CUDA(cudaStreamSynchronize(g->stream));
   g->kernels += 2;
+  return GG_OK;
+}
+
+// The outcome of the BFS bfs_device_full enqueued (synchronises the stream):
+// *rounds, the number of edgeMap rounds (the last one finds nothing), *trav,
+// the out-degree sum of the frontiers processed.
+int bfs_device_full_result(gg_graph_s* g, int32_t* rounds, uint64_t* trav) {
+  LoopState h{};
+  GG_TRY(read_small(g, &h, reinterpret_cast<const LoopState*>(g->ws.d_loop)));
   if (h.exit_reason < 0) return fail(GG_ERR_TIMEOUT, "BFS loop: a grid barrier wait ran out");
   if (h.exit_reason != 1)
     return fail(GG_ERR_CUDA, "BFS loop: stopped without an empty frontier (reason %d)", h.exit_reason);

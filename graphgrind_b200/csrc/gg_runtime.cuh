@@ -4,6 +4,7 @@
 #pragma once
 #include <algorithm>
 #include <atomic>
+#include <cstring>
 
 #include "gg_engine.cuh"
 #include "gg_functors.cuh"
@@ -43,6 +44,43 @@ struct EventTimer {
 cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t s, int device);
 // Returns the pool's unused memory of `device` to the system.
 void pool_trim(int device);
+
+// ------------------------------------------------ small control transfers
+// Loop states, statistics and reductions are read back (and loop control
+// blocks written) by one-warp kernels through the graph's mapped pinned block
+// instead of cudaMemcpyAsync: a small copy on a copy engine waits behind the
+// large result copies that GG_TUNE_ASYNC_RESULTS leaves in flight (a 64 MiB
+// copy takes about 1.2 ms over PCIe), while a kernel's stores to mapped host
+// memory do not.
+__global__ void k_get_words(uint32_t* dst, const uint32_t* src, uint32_t words);
+template <class T>
+__global__ void k_put(T* dst, const T v) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *dst = v;
+}
+// Copies `count` values of T from device memory to `host` (any host memory)
+// after the graph's stream has reached this point; synchronises the stream.
+template <class T>
+int read_small(gg_graph_s* g, T* host, const T* dev, size_t count = 1) {
+  static_assert(sizeof(T) % 4 == 0, "control values are whole 32-bit words");
+  const size_t bytes = sizeof(T) * count;
+  if (bytes > kMapBytes) return fail(GG_ERR_INVALID_ARG, "control block of %zu bytes exceeds the mapped block", bytes);
+  k_get_words<<<1, 128, 0, g->stream>>>(g->ws.d_map, reinterpret_cast<const uint32_t*>(dev), (uint32_t)(bytes / 4));
+  GG_CUDA(cudaGetLastError());
+  g->kernels++;
+  GG_CUDA(cudaStreamSynchronize(g->stream));
+  std::memcpy(host, g->ws.h_map, bytes);
+  return GG_OK;
+}
+// Writes one T to device memory in stream order (the value travels as a
+// kernel argument).
+template <class T>
+int write_small(gg_graph_s* g, T* dev, const T& v) {
+  static_assert(sizeof(T) <= 1024, "control blocks travel as kernel arguments");
+  k_put<T><<<1, 32, 0, g->stream>>>(dev, v);
+  GG_CUDA(cudaGetLastError());
+  g->kernels++;
+  return GG_OK;
+}
 
 // A stream-ordered device allocation released when the holder leaves scope.
 template <class T>
@@ -180,8 +218,8 @@ int frontier_to_sparse(gg_frontier_s* f);
 void frontier_free(gg_frontier_s* f);
 int bfs_device_levels(gg_graph_s* g, gg_frontier_s** F, int32_t* parents, int32_t* levels, int32_t round0,
                       uint64_t threshold, int32_t* rounds, uint64_t* trav);
-int bfs_device_full(gg_graph_s* g, uint32_t start, int32_t* parents, int32_t* levels, uint64_t threshold,
-                    int32_t* rounds, uint64_t* trav);
+int bfs_device_full(gg_graph_s* g, uint32_t start, int32_t* parents, int32_t* levels, uint64_t threshold);
+int bfs_device_full_result(gg_graph_s* g, int32_t* rounds, uint64_t* trav);
 int reset_stats(gg_graph_s* g);
 void pr_loop_free(gg_graph_s* g);  // releases the captured PageRank loop and its buffers
 void round_loops_free(gg_graph_s* g);  // the same for the BellmanFord / Components round loops

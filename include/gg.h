@@ -390,8 +390,11 @@ int gg_graph_set_dense_policy(gg_graph_t g, int32_t policy);
  *                         the next call's work; gg_graph_synchronize waits
  *                         for every such copy (read the arrays after it).
  *                         Pageable arrays are filled before the call
- *                         returns in both modes.  Graphs that keep their
- *                         given ids then hold two n-entry staging arrays
+ *                         returns in both modes.  The mode holds three
+ *                         n-entry staging arrays per graph (BFS's parents
+ *                         have one of their own); small control results
+ *                         (loop states, statistics) never take a copy engine,
+ *                         so the calls do not wait behind these copies
  *   GG_TUNE_LOOP_WAIT_BUDGET  probes of the grid-barrier wait of the device
  *                         BFS level loop (GG_TUNE_DEVICE_LOOP) before it gives
  *                         up: 0..2^22 (default 2^22, seconds at most).  When a

@@ -35,18 +35,22 @@ def test_async_results_match_sync(gg, graph):
     x = np.random.default_rng(2).random(n, dtype=np.float32)
     g.set_tuning(gg.TUNE_ASYNC_RESULTS, 0)
     lev0, r10_0, r3_0, y0, ids0 = reference_results(g, x)
+    lev7 = g.bfs(7)[1]
     g.set_tuning(gg.TUNE_ASYNC_RESULTS, 1)
     assert g.get_tuning(gg.TUNE_ASYNC_RESULTS) == 1
     par, lev = gg.PinnedArray(n, np.int32), gg.PinnedArray(n, np.int32)
+    par7 = gg.PinnedArray(n, np.int32)
     r10, r3 = gg.PinnedArray(n, np.float32), gg.PinnedArray(n, np.float32)
     xin, y = gg.PinnedArray(n, np.float32), gg.PinnedArray(n, np.float32)
     xin.array[:] = x
     for rep in range(3):
-        for a in (par, lev, r10, r3, y):
+        for a in (par, lev, r10, r3, y, par7):
             a.array.fill(-7)
-        # back to back, no wait: both PageRank results and the BFS parents are
-        # staged in the same given-order array, the SpMV input in the other
+        # back to back, no wait: both PageRank results are staged in the same
+        # given-order array, both BFS parents in a third, the SpMV input and
+        # the BFS levels in the second
         g.bfs(5, out=(par.array, lev.array))
+        g.bfs(7, out=(par7.array, None))
         g.pagerank(10, out=r10.array)
         g.pagerank(3, out=r3.array)
         g.spmv(xin.array, out=y.array)
@@ -56,6 +60,8 @@ def test_async_results_match_sync(gg, graph):
         np.testing.assert_array_equal(lev.array, lev0)
         reached = lev.array >= 0
         assert np.all(par.array[~reached] == -1) and np.all(par.array[reached] >= 0)
+        reached7 = lev7 >= 0
+        assert np.all(par7.array[~reached7] == -1) and np.all(par7.array[reached7] >= 0)
         assert rel_l1(r10.array, r10_0.astype(np.float64)) <= PR_REL_L1
         assert rel_l1(r3.array, r3_0.astype(np.float64)) <= PR_REL_L1
         assert rel_l1(r3.array, r10.array.astype(np.float64)) > 1e-4  # not the other result

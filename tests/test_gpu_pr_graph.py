@@ -15,10 +15,11 @@ def graph_kernels(gg, g, rounds):
     """Kernels of a run that the captured graph finished: the initial pass,
     then per iteration the pull, the check and, unless the pull's commits ran
     the vertex step over every vertex, one more pass (the uncovered ranges,
-    or the epilogue)."""
+    or the epilogue); and the one-warp kernels that write the loop's control
+    block before the graph and read it back after."""
     fused = g.get_tuning(gg.TUNE_COO_KERNEL) > 0
     per_iter = 2 if fused and g.info().num_coo_gaps == 0 else 3
-    return 1 + per_iter * rounds
+    return 1 + per_iter * rounds + 2
 
 
 def check_ranks(r, o):
