@@ -441,7 +441,8 @@ int bfs_device_levels(gg_graph_s* g, gg_frontier_s** F, int32_t* parents, int32_
 // level before the current is cleared while the current level runs.
 // One bottom-up level, this CTA's share (warps over 32-vertex groups, grid
 // stride): a vertex without a parent takes its first in-neighbour that is in
-// the frontier bitmap bcur and joins bnxt.  *cnt / *deg: this thread's new
+// the frontier bitmap bcur and joins bnxt.  The next group's parent words and
+// in-list bounds are loaded before the current group walks its in-lists.  *cnt / *deg: this thread's new
 // vertices and their out-degree sum.  Not inlined: the loop then keeps its
 // registers whatever the rest of the level-loop kernel holds.
 // vec: the in-list is read in 16-byte aligned groups of 4 edges (the edge
@@ -454,11 +455,31 @@ __device__ __noinline__ void bottom_up_level(const uint32_t* __restrict__ off, c
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t stride = gridDim.x * blockDim.x;  // <= 2^31 threads
   uint32_t c = 0, dg = 0;
-  for (uint32_t b = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); b < n; b += stride) {
+  uint32_t b = blockIdx.x * blockDim.x + (threadIdx.x & ~31u);
+  // a lane's parent word and in-list bounds are loaded one group ahead, so
+  // that they arrive while the group before walks its in-lists (a vertex is
+  // this lane's alone during a bottom-up level: nobody else writes its parent)
+  auto load = [&](uint32_t bb, int32_t& pv, uint32_t& j0, uint32_t& e1) {
+    const uint32_t v = bb + lane;
+    pv = 0;
+    j0 = e1 = 0;
+    if (v < n) {
+      pv = __ldcg(parents + v);
+      j0 = ioff[v];
+      e1 = ioff[v + 1];
+    }
+  };
+  int32_t pv = 0;
+  uint32_t j0 = 0, e1 = 0;
+  if (b < n) load(b, pv, j0, e1);
+  for (; b < n; b += stride) {
+    const bool last = b > n - 1 - stride;  // b + stride would pass n (or wrap)
+    int32_t pv2 = 0;
+    uint32_t j2 = 0, e2 = 0;
+    if (!last) load(b + stride, pv2, j2, e2);
     const uint32_t v = b + lane;
     bool act = false;
-    if (v < n && __ldcg(parents + v) == -1) {
-      const uint32_t j0 = ioff[v], e1 = ioff[v + 1];
+    if (v < n && pv == -1) {
       if (vec) {
         for (uint32_t a = j0 & ~3u; a < e1; a += 4) {
           const uint4 q = __ldg(reinterpret_cast<const uint4*>(iidx + a));
@@ -494,7 +515,10 @@ __device__ __noinline__ void bottom_up_level(const uint32_t* __restrict__ off, c
       atomicOr(bnxt + (b >> 5), word);
       c += __popc(word);
     }
-    if (b > n - 1 - stride) break;  // b + stride would pass n (or wrap)
+    if (last) break;
+    pv = pv2;
+    j0 = j2;
+    e1 = e2;
   }
   *cnt = c;
   *deg = dg;
