@@ -162,7 +162,8 @@ struct gg_graph_s {
   int cc_algo = 0;      // Components on symmetric graphs: 0 label propagation, 1 union-find
   int loop_ctas_per_sm = 0;  // CTAs per SM of the device BFS loops (capped by occupancy); 0: 4 / 8 by loop
   uint32_t loop_wait_budget = 1u << 22;  // spins of the BFS level loop's grid-barrier wait
-  int early_kernel = 0;  // early-exit dense pull: 0 one lane per destination (faster on R-MAT), 1 8-lane groups
+  int early_kernel = 2;  // early-exit dense pull: 0 one lane per destination, 1 8-lane groups, 2 one lane per
+                         // destination reading 4 in-edges per load (fastest on R-MAT)
   int push_dense_div = 0;  // a dense edgeMap of an early-exit functor pushes into a bitmap when
                            // the frontier has at most n / push_dense_div vertices (0: never)
   int pr_graph = 1;     // PageRank iterations replayed as one CUDA graph (0: one host round trip per iteration)

@@ -441,8 +441,7 @@ int bfs_device_levels(gg_graph_s* g, gg_frontier_s** F, int32_t* parents, int32_
 // level before the current is cleared while the current level runs.
 // One bottom-up level, this CTA's share (warps over 32-vertex groups, grid
 // stride): a vertex without a parent takes its first in-neighbour that is in
-// the frontier bitmap bcur and joins bnxt.  The next group's parent words and
-// in-list bounds are loaded before the current group walks its in-lists.  *cnt / *deg: this thread's new
+// the frontier bitmap bcur and joins bnxt.  *cnt / *deg: this thread's new
 // vertices and their out-degree sum.  Not inlined: the loop then keeps its
 // registers whatever the rest of the level-loop kernel holds.
 // vec: the in-list is read in 16-byte aligned groups of 4 edges (the edge
@@ -456,9 +455,10 @@ __device__ __noinline__ void bottom_up_level(const uint32_t* __restrict__ off, c
   const uint32_t stride = gridDim.x * blockDim.x;  // <= 2^31 threads
   uint32_t c = 0, dg = 0;
   uint32_t b = blockIdx.x * blockDim.x + (threadIdx.x & ~31u);
-  // a lane's parent word and in-list bounds are loaded one group ahead, so
-  // that they arrive while the group before walks its in-lists (a vertex is
-  // this lane's alone during a bottom-up level: nobody else writes its parent)
+  // Loads run ahead of the walk: a lane's parent word and in-list bounds two
+  // groups ahead, its first in-neighbour one group ahead, so that they arrive
+  // while the current group walks its in-lists (a vertex is this lane's alone
+  // during a bottom-up level: nobody else writes its parent).
   auto load = [&](uint32_t bb, int32_t& pv, uint32_t& j0, uint32_t& e1) {
     const uint32_t v = bb + lane;
     pv = 0;
@@ -469,26 +469,37 @@ __device__ __noinline__ void bottom_up_level(const uint32_t* __restrict__ off, c
       e1 = ioff[v + 1];
     }
   };
-  int32_t pv = 0;
-  uint32_t j0 = 0, e1 = 0;
+  auto first = [&](int32_t pv, uint32_t j0, uint32_t e1) -> uint32_t {
+    return (pv == -1 && j0 < e1) ? iidx[j0] : 0u;
+  };
+  // groups b (pv, j0, e1, s0) and b + stride (pv1, j1, e11)
+  int32_t pv = 0, pv1 = 0;
+  uint32_t j0 = 0, e1 = 0, j1 = 0, e11 = 0, s0 = 0;
   if (b < n) load(b, pv, j0, e1);
+  if ((uint64_t)b + stride < n) load(b + stride, pv1, j1, e11);
+  if (b < n) s0 = first(pv, j0, e1);
   for (; b < n; b += stride) {
-    const bool last = b > n - 1 - stride;  // b + stride would pass n (or wrap)
+    const bool last = (uint64_t)b + stride >= n;  // no group after this one
     int32_t pv2 = 0;
-    uint32_t j2 = 0, e2 = 0;
-    if (!last) load(b + stride, pv2, j2, e2);
+    uint32_t j2 = 0, e2 = 0, s1 = 0;
+    if ((uint64_t)b + 2ull * stride < n) load(b + 2 * stride, pv2, j2, e2);
+    if (!last) s1 = first(pv1, j1, e11);
     const uint32_t v = b + lane;
     bool act = false;
-    if (v < n && pv == -1) {
-      if (vec) {
-        for (uint32_t a = j0 & ~3u; a < e1; a += 4) {
+    if (v < n && pv == -1 && j0 < e1) {
+      if ((bcur[s0 >> 5] >> (s0 & 31)) & 1u) {
+        parents[v] = (int32_t)s0;
+        if (levels) levels[v] = r;
+        act = true;
+      } else if (vec) {
+        for (uint32_t a = (j0 + 1) & ~3u; a < e1; a += 4) {
           const uint4 q = __ldg(reinterpret_cast<const uint4*>(iidx + a));
           const uint32_t ss[4] = {q.x, q.y, q.z, q.w};
           int hit = -1;
 #pragma unroll
           for (int t = 3; t >= 0; --t) {
             const uint32_t e = a + (uint32_t)t;
-            if (e >= j0 && e < e1 && ((bcur[ss[t] >> 5] >> (ss[t] & 31)) & 1u)) hit = t;
+            if (e > j0 && e < e1 && ((bcur[ss[t] >> 5] >> (ss[t] & 31)) & 1u)) hit = t;
           }
           if (hit >= 0) {
             parents[v] = (int32_t)ss[hit];
@@ -498,7 +509,7 @@ __device__ __noinline__ void bottom_up_level(const uint32_t* __restrict__ off, c
           }
         }
       } else {
-        for (uint32_t j = j0; j < e1; ++j) {
+        for (uint32_t j = j0 + 1; j < e1; ++j) {
           const uint32_t s = iidx[j];
           if ((bcur[s >> 5] >> (s & 31)) & 1u) {
             parents[v] = (int32_t)s;
@@ -516,9 +527,13 @@ __device__ __noinline__ void bottom_up_level(const uint32_t* __restrict__ off, c
       c += __popc(word);
     }
     if (last) break;
-    pv = pv2;
-    j0 = j2;
-    e1 = e2;
+    pv = pv1;
+    j0 = j1;
+    e1 = e11;
+    s0 = s1;
+    pv1 = pv2;
+    j1 = j2;
+    e11 = e2;
   }
   *cnt = c;
   *deg = dg;

@@ -403,14 +403,15 @@ int gg_graph_set_dense_policy(gg_graph_t g, int32_t policy);
  *                         it to 0 to drive that path on a healthy graph
  *   GG_TUNE_EARLY_KERNEL  the dense pull with early exit (BFS's bottom-up
  *                         step, edgeMapDenseCSC's break, ligra-numa.h:621-626, 708-713):
- *                         0 (default) one lane per destination, one edge per
- *                         step; 1 8 lanes walk a destination's in-list 8 edges
- *                         per step, 4 destinations per warp (faster on long
- *                         rows, slower on R-MAT-24: 0.67 against 0.46 ms for
- *                         BFS's three bottom-up levels); 2 one lane per
+ *                         0 one lane per destination, one edge per step; 1 8
+ *                         lanes walk a destination's in-list 8 edges per step,
+ *                         4 destinations per warp (faster on long rows, slower
+ *                         on R-MAT-24: 0.67 against 0.46 ms for BFS's three
+ *                         bottom-up levels); 2 (default) one lane per
  *                         destination reading its in-list 4 edges per 16-byte
  *                         load, the 4 frontier tests issued together (also in
- *                         the bottom-up levels of GG_TUNE_DEVICE_LOOP 2)
+ *                         the bottom-up levels of GG_TUNE_DEVICE_LOOP 2: BFS
+ *                         on R-MAT-24 0.453 against 0.473 ms with 0)
  *   GG_TUNE_PUSH_DENSE_DIV  a dense edgeMap of BFS (an early-exit functor)
  *                         whose frontier has at most n / value vertices runs
  *                         top-down instead (the frontier's out-edges pushed,

@@ -263,6 +263,7 @@ def test_bfs_early_exit_kernels(gg, rmat14, kernel, loop):
     levels; parents are frontier in-neighbours one level up."""
     hg, g, og = rmat14
     keep = g.get_tuning(gg.TUNE_DEVICE_LOOP)
+    keep_kernel = g.get_tuning(gg.TUNE_EARLY_KERNEL)
     g.set_tuning(gg.TUNE_EARLY_KERNEL, kernel)
     g.set_tuning(gg.TUNE_DEVICE_LOOP, loop)
     g.set_dense_policy(1)  # every dense level takes the early-exit CSC pull
@@ -270,7 +271,7 @@ def test_bfs_early_exit_kernels(gg, rmat14, kernel, loop):
         for start in (0, 100, 12345):
             check_bfs(g, og, start, hg)
     finally:
-        g.set_tuning(gg.TUNE_EARLY_KERNEL, 0)
+        g.set_tuning(gg.TUNE_EARLY_KERNEL, keep_kernel)
         g.set_tuning(gg.TUNE_DEVICE_LOOP, keep)
         g.set_dense_policy(0)
 
