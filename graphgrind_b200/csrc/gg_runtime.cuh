@@ -132,19 +132,46 @@ inline int generic_grid(const gg_graph_s* g, uint64_t work) {
 // orders at their boundary.  The renumbering stays inside partitions, so both
 // directions read and write within one partition's stretch of the array.
 // to_given: out[u] = in[new_of_old[u]];  to_device: out[i] = in[old_of_new[i]].
+// Each thread takes kPermIlp entries a grid stride apart per round, their
+// loads issued together (the map read, then the gather it feeds).
+constexpr int kPermIlp = 4;
 template <class T>
 __global__ void k_permute_rows(uint32_t n, uint32_t k, const uint32_t* map, const T* in, T* out) {
   const uint64_t total = (uint64_t)n * k;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x)
-    out[i] = in[(uint64_t)map[i / k] * k + i % k];
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < total; i0 += kPermIlp * stride) {
+    uint64_t src[kPermIlp];
+#pragma unroll
+    for (int t = 0; t < kPermIlp; ++t) {
+      const uint64_t i = i0 + t * stride;
+      src[t] = i < total ? (uint64_t)map[i / k] * k + i % k : 0;
+    }
+    T val[kPermIlp];
+#pragma unroll
+    for (int t = 0; t < kPermIlp; ++t) val[t] = i0 + t * stride < total ? in[src[t]] : T();
+#pragma unroll
+    for (int t = 0; t < kPermIlp; ++t)
+      if (i0 + t * stride < total) out[i0 + t * stride] = val[t];
+  }
 }
 // vertex ids held as values (BFS parents): the given id of the value, for the
 // given vertex u
 static __global__ void k_ids_to_given(uint32_t n, const uint32_t* new_of_old, const uint32_t* old_of_new,
                                const int32_t* in, int32_t* out) {
-  for (uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; u < n; u += (uint64_t)gridDim.x * blockDim.x) {
-    const int32_t v = in[new_of_old[u]];
-    out[u] = v < 0 ? v : (int32_t)old_of_new[v];
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t u0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; u0 < n; u0 += kPermIlp * stride) {
+    uint32_t w[kPermIlp];
+#pragma unroll
+    for (int t = 0; t < kPermIlp; ++t) w[t] = u0 + t * stride < n ? new_of_old[u0 + t * stride] : 0u;
+    int32_t v[kPermIlp];
+#pragma unroll
+    for (int t = 0; t < kPermIlp; ++t) v[t] = u0 + t * stride < n ? in[w[t]] : -1;
+    uint32_t gv[kPermIlp];
+#pragma unroll
+    for (int t = 0; t < kPermIlp; ++t) gv[t] = v[t] >= 0 ? old_of_new[v[t]] : 0u;
+#pragma unroll
+    for (int t = 0; t < kPermIlp; ++t)
+      if (u0 + t * stride < n) out[u0 + t * stride] = v[t] < 0 ? v[t] : (int32_t)gv[t];
   }
 }
 
