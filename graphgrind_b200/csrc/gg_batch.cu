@@ -326,6 +326,7 @@ __global__ void __launch_bounds__(256, GG_MS_MIN_BLOCKS) k_ms_pull(MsPull p) {
     const uint64_t e0 = b * kSegBlock;
     // rows touching the block: slot 0 continues from the previous block, one slot per head
     const uint32_t h0 = __ldg(p.blk + b), nr = __ldg(p.blk + b + 1) - h0 + 1;
+    bool live = false;  // some row of the block still takes bits
     for (uint32_t i = lane; i < nr; i += 32) {
       uint64_t f = 0;
       uint32_t x = 0;
@@ -335,7 +336,11 @@ __global__ void __launch_bounds__(256, GG_MS_MIN_BLOCKS) k_ms_pull(MsPull p) {
       }
       s_row[warp][i] = x;
       s_filt[warp][i] = f;
+      live = live || f != 0;
     }
+    // every row filtered out (forward: reached from all sources): no edge of
+    // the block can set a bit or move a value
+    if (!__any_sync(0xffffffffu, live)) continue;
     __syncwarp();
     const uint64_t nb = e0 + kSegBlock;
     const bool ends_block = nb >= p.m || (__ldg(p.head + (nb >> 5)) & 1u);
@@ -349,7 +354,7 @@ __global__ void __launch_bounds__(256, GG_MS_MIN_BLOCKS) k_ms_pull(MsPull p) {
       const uint64_t e = e0 + 32 * i + lane;
       const uint32_t rel = running + __popc(hw & lanemask_le);
       const uint64_t f = s_filt[warp][rel];
-      const uint32_t y = e < p.m ? __ldg(p.idx + e) : 0u;
+      const uint32_t y = (e < p.m && f) ? __ldg(p.idx + e) : 0u;  // edges of filtered rows are not read
       uint64_t x = (e < p.m && f) ? (__ldg(p.edge_mask + y) & f) : 0ull;
       if (VALS) {
         s_em[warp][32 * i + lane] = x;
