@@ -162,8 +162,9 @@ struct gg_graph_s {
   int cc_algo = 0;      // Components on symmetric graphs: 0 label propagation, 1 union-find
   int loop_ctas_per_sm = 0;  // CTAs per SM of the device BFS loops (capped by occupancy); 0: 4 / 8 by loop
   uint32_t loop_wait_budget = 1u << 22;  // spins of the BFS level loop's grid-barrier wait
-  int early_kernel = 2;  // early-exit dense pull: 0 one lane per destination, 1 8-lane groups, 2 one lane per
-                         // destination reading 4 in-edges per load (fastest on R-MAT)
+  int early_kernel = 3;  // early-exit dense pull: 0 one lane per destination, 1 8-lane groups, 2 one lane per
+                         // destination reading 4 in-edges per load, 3 the same over in-lists with hub sources
+                         // first (fastest on R-MAT)
   int push_dense_div = 0;  // a dense edgeMap of an early-exit functor pushes into a bitmap when
                            // the frontier has at most n / push_dense_div vertices (0: never)
   int pr_graph = 1;     // PageRank iterations replayed as one CUDA graph (0: one host round trip per iteration)
@@ -178,6 +179,9 @@ struct gg_graph_s {
   gg::PrLoop* pr_loop = nullptr;  // created by the first graph-driven PageRank call
   gg::RoundLoop* round_loop[3] = {nullptr, nullptr, nullptr};  // BellmanFord, Components, PageRankDelta: created by their first call
   int round_graph = 1;  // dense COO rounds of BellmanFord / Components / PageRankDelta as a CUDA graph
+  // GG_TUNE_EARLY_KERNEL 3's in-lists (the CSC's, each by descending source
+  // out-degree), built by the first all-levels BFS (m_pad entries)
+  uint32_t* d_bu_idx = nullptr;
   int coo_kernel = 7;  // 0 CTA ring (k_pull), 1 per-warp direct loads, 2/3 per-warp bulk-copy rings, 6 direct loads
                        // with cross-lane run merging, 7 the same with cache hints (fastest measured)
   // gg_build_opts.vertex_order: device ids differ from the given ids

@@ -320,6 +320,39 @@ __global__ void k_coo_scatter(const uint4* seg, const uint32_t* pad_start, uint3
   }
 }
 
+// ---------------------------------------- in-lists for the bottom-up BFS
+// key of a CSC edge: the complement of its source's out-degree, so that an
+// ascending sort puts the sources with the most out-edges first
+__global__ void k_bu_keys(const uint32_t* src, uint64_t m, const uint32_t* out_off, uint32_t* keys) {
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t s = src[e];
+    keys[e] = ~(out_off[s + 1] - out_off[s]);
+  }
+}
+
+int build_bu_index(gg_graph_s* g) {
+  if (g->d_bu_idx) return GG_OK;
+  const uint64_t m = g->m;
+  const uint32_t n = g->n;
+  if (m >= (1ull << 31)) return fail(GG_ERR_UNSUPPORTED, "bottom-up in-lists: more than 2^31 edges");
+  GG_TRY(dev_alloc(g, &g->d_bu_idx, g->m_pad));
+  GG_CUDA(cudaMemsetAsync(g->d_bu_idx + m, 0, 4ull * (g->m_pad - m), g->stream));
+  if (m == 0) return GG_OK;
+  DevBuf<uint32_t> keys, keys_out;
+  GG_TRY(keys.alloc(g, m));
+  GG_TRY(keys_out.alloc(g, m));
+  k_bu_keys<<<generic_grid(g, m), kGenericThreads, 0, g->stream>>>(g->d_csc_idx, m, g->d_csr_off, keys.p);
+  GG_CUDA(cudaGetLastError());
+  size_t temp = 0;
+  GG_CUDA(cub::DeviceSegmentedSort::StableSortPairs(nullptr, temp, keys.p, keys_out.p, g->d_csc_idx, g->d_bu_idx,
+                                                     (int)m, (int)n, g->d_csc_off, g->d_csc_off + 1, g->stream));
+  DevBuf<unsigned char> tmp;
+  GG_TRY(tmp.alloc(g, temp));
+  GG_CUDA(cub::DeviceSegmentedSort::StableSortPairs(tmp.p, temp, keys.p, keys_out.p, g->d_csc_idx, g->d_bu_idx,
+                                                     (int)m, (int)n, g->d_csc_off, g->d_csc_off + 1, g->stream));
+  return GG_OK;
+}
+
 static int build_coo(gg_graph_s* g, const uint32_t* h_in_off) {
   const uint32_t n = g->n;
   const uint64_t m = g->m;
@@ -621,6 +654,7 @@ static void graph_release(gg_graph_s* g) {
   cudaFree(g->ws.d_bsum);
   cudaFree(g->ws.d_red);
   cudaFree(g->ws.d_loop);
+  cudaFree(g->d_bu_idx);
   cudaFree(g->d_new_of_old);
   cudaFree(g->d_old_of_new);
   for (auto* a : g->ws.d_order) cudaFree(a);
@@ -974,7 +1008,7 @@ int gg_graph_set_tuning(gg_graph_t g, int32_t key, int64_t value) {
       g->pr_graph = (int)value;
       return GG_OK;
     case GG_TUNE_EARLY_KERNEL:
-      if (value < 0 || value > 2) return fail(GG_ERR_INVALID_ARG, "early-exit kernel must be 0, 1 or 2");
+      if (value < 0 || value > 3) return fail(GG_ERR_INVALID_ARG, "early-exit kernel must be 0..3");
       g->early_kernel = (int)value;
       return GG_OK;
     case GG_TUNE_PUSH_DENSE_DIV:

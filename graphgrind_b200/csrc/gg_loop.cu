@@ -792,7 +792,11 @@ int bfs_device_full(gg_graph_s* g, uint32_t start, int32_t* parents, int32_t* le
   const uint32_t* off = g->out_off();
   const uint32_t* idx = g->out_idx();
   const uint32_t* ioff = g->in_off();
-  const uint32_t* iidx = g->in_idx();
+  // the bottom-up levels walk the in-lists hub sources first (same edges,
+  // other order: a vertex then meets a frontier in-neighbour sooner)
+  const bool hubs_first = g->early_kernel == 3;
+  if (hubs_first && !g->d_bu_idx) GG_TRY(build_bu_index(g));
+  const uint32_t* iidx = hubs_first ? g->d_bu_idx : g->in_idx();
   uint32_t* a0 = q0.p;
   uint32_t* a1 = q1.p;
   uint32_t* e0 = eo0.p;
@@ -805,7 +809,7 @@ int bfs_device_full(gg_graph_s* g, uint32_t start, int32_t* parents, int32_t* le
   unsigned long long thr = threshold;
   int32_t cap = n < (uint32_t)INT32_MAX ? (int32_t)n + 1 : INT32_MAX;
   unsigned budget = g->loop_wait_budget;
-  int vec = g->early_kernel == 2 ? 1 : 0;
+  int vec = g->early_kernel >= 2 ? 1 : 0;
   void* args[] = {(void*)&off, (void*)&idx, (void*)&ioff, (void*)&iidx, (void*)&parents, (void*)&levels,
                   (void*)&a0,  (void*)&a1,  (void*)&e0,   (void*)&e1,   (void*)&bp,      (void*)&ws,
                   (void*)&cp,  (void*)&nn,  (void*)&d_st, (void*)&round0, (void*)&thr,   (void*)&cap,

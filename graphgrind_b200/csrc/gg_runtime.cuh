@@ -246,6 +246,9 @@ void frontier_free(gg_frontier_s* f);
 int bfs_device_levels(gg_graph_s* g, gg_frontier_s** F, int32_t* parents, int32_t* levels, int32_t round0,
                       uint64_t threshold, int32_t* rounds, uint64_t* trav);
 int bfs_device_full(gg_graph_s* g, uint32_t start, int32_t* parents, int32_t* levels, uint64_t threshold);
+// The CSC's in-lists with each one's sources by descending out-degree (ties by
+// id), for BFS's bottom-up levels; built once per graph (g->d_bu_idx).
+int build_bu_index(gg_graph_s* g);
 int bfs_device_full_result(gg_graph_s* g, int32_t* rounds, uint64_t* trav);
 int reset_stats(gg_graph_s* g);
 void pr_loop_free(gg_graph_s* g);  // releases the captured PageRank loop and its buffers
@@ -437,7 +440,7 @@ int pull_early_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, cons
     else
       k_pull_early_g<F, HW, false><<<grid, kGenericThreads, 0, g->stream>>>(
           g->n, g->in_off(), g->in_idx(), g->in_w(), in->d_bits, out->d_bits, g->out_off(), member, g->ws.d_stats, f);
-  } else if (g->early_kernel == 2) {
+  } else if (g->early_kernel >= 2) {
     if (in->bit)
       k_pull_early<F, HW, true, true><<<grid, kGenericThreads, 0, g->stream>>>(
           g->n, g->in_off(), g->in_idx(), g->in_w(), nullptr, out->d_bits, g->out_off(), member, g->ws.d_stats, f);

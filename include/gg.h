@@ -407,11 +407,18 @@ int gg_graph_set_dense_policy(gg_graph_t g, int32_t policy);
  *                         lanes walk a destination's in-list 8 edges per step,
  *                         4 destinations per warp (faster on long rows, slower
  *                         on R-MAT-24: 0.67 against 0.46 ms for BFS's three
- *                         bottom-up levels); 2 (default) one lane per
- *                         destination reading its in-list 4 edges per 16-byte
- *                         load, the 4 frontier tests issued together (also in
- *                         the bottom-up levels of GG_TUNE_DEVICE_LOOP 2: BFS
- *                         on R-MAT-24 0.453 against 0.473 ms with 0)
+ *                         bottom-up levels); 2 one lane per destination
+ *                         reading its in-list 4 edges per 16-byte load, the 4
+ *                         frontier tests issued together (also in the
+ *                         bottom-up levels of GG_TUNE_DEVICE_LOOP 2: BFS on
+ *                         R-MAT-24 0.453 against 0.473 ms with 0); 3
+ *                         (default) as 2, and the bottom-up levels of
+ *                         GG_TUNE_DEVICE_LOOP 2 walk a copy of the in-lists
+ *                         with each list's sources by descending out-degree
+ *                         (a vertex meets a frontier in-neighbour sooner:
+ *                         0.438 against 0.452 ms); the first such BFS builds
+ *                         the copy (one segmented sort), which stays with the
+ *                         graph: 4 bytes per edge
  *   GG_TUNE_PUSH_DENSE_DIV  a dense edgeMap of BFS (an early-exit functor)
  *                         whose frontier has at most n / value vertices runs
  *                         top-down instead (the frontier's out-edges pushed,

@@ -256,7 +256,7 @@ def test_apps_with_source_partitions(gg, orc, sym):
 
 
 @pytest.mark.parametrize("loop", [0, 2])
-@pytest.mark.parametrize("kernel", [0, 1, 2])
+@pytest.mark.parametrize("kernel", [0, 1, 2, 3])
 def test_bfs_early_exit_kernels(gg, rmat14, kernel, loop):
     """Every form of the bottom-up (early-exit) dense step, from the host
     (device loop 0) and inside the all-levels launch (2), gives the oracle's
