@@ -1268,7 +1268,7 @@ static int run_pagerank_converge(gg_graph_s* g, int32_t max_iter, double eps, fl
     f.contrib = contrib.p;
     f.acc_out = p_next;
     gg_frontier_s* out = nullptr;
-    GG_TRY(edge_map(g, F.f, f, app_threshold(g), GG_EM_NO_OUTPUT, &out));  // output.del()
+    GG_TRY(edge_map(g, F.f, f, app_threshold(g), GG_EM_NO_OUTPUT | kEmNoWait, &out));  // output.del(); read_small waits
     frontier_free(out);
     GG_CUDA(cudaMemsetAsync(red, 0, 3 * sizeof(double), g->stream));
     k_prc_sum<<<grid, kGenericThreads, 0, g->stream>>>(n, p_next, red);
@@ -1425,7 +1425,7 @@ static int run_spmv(gg_graph_s* g, const float* x_in, float* y_out, gg_run_stats
   f.float_w = g->wtype == GG_W_FLOAT32;
   f.y_map = g->relabeled ? g->d_old_of_new : nullptr;
   gg_frontier_s* out = nullptr;
-  GG_TRY(edge_map(g, F.f, f, app_threshold(g), GG_EM_NO_OUTPUT, &out));  // output.del()
+  GG_TRY(edge_map(g, F.f, f, app_threshold(g), GG_EM_NO_OUTPUT | kEmNoWait, &out));  // output.del(); tm.stop() waits
   frontier_free(out);
   const float* res = yd;
   if (!g->relabeled) GG_TRY(given_order<float>(g, y.p, 1, &res));
@@ -1576,6 +1576,7 @@ int gg_edge_map(gg_graph_t g, gg_frontier_t in, int32_t fid, const void* args, i
                 gg_frontier_t* out) {
   if (!graph_live(g) || !frontier_live(in) || !out || !args || in->g != g)
     return fail(GG_ERR_INVALID_ARG, "gg_edge_map: bad arguments");
+  flags &= GG_EM_FORCE_SPARSE | GG_EM_FORCE_CSC | GG_EM_FORCE_COO | GG_EM_NO_OUTPUT;  // the C ABI's bits
   switch (fid) {
     case GG_F_BFS: {
       const gg_bfs_args* a = (const gg_bfs_args*)args;

@@ -532,6 +532,11 @@ int push_bits_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const
   return GG_OK;
 }
 
+// Internal edge_map flag (beside the GG_EM_* bits of the C ABI, which
+// gg_edge_map passes on alone): with GG_EM_NO_OUTPUT, the caller waits for the
+// stream itself, so the call need not.
+constexpr uint32_t kEmNoWait = 0x80000000u;
+
 template <class F>
 int edge_map(gg_graph_s* g, gg_frontier_s* in, const F& f, int64_t threshold, uint32_t flags, gg_frontier_s** out) {
   const int64_t m = (int64_t)g->m;
@@ -603,7 +608,17 @@ int edge_map(gg_graph_s* g, gg_frontier_s* in, const F& f, int64_t threshold, ui
         rc = hw ? pull_launch<F, true>(g, in, o, f, coo, no_out) : pull_launch<F, false>(g, in, o, f, coo, no_out);
       if (g->profiling) cudaEventRecord(g->prof_ev[1], g->stream);
     }
-    if (!rc) rc = read_stats(g);
+    // an output nobody reads from a pull without waits (the direct-load COO
+    // kernels; only the bulk-copy rings, 0/2/3, can set the error word), for
+    // an application that synchronises later itself (kEmNoWait): no
+    // statistics to read, and the stream goes on without a host round trip
+    const bool skip_stats = no_out && (flags & kEmNoWait) && g->coo_kernel != 0 && g->coo_kernel != 2 &&
+                            g->coo_kernel != 3;
+    if (!rc && skip_stats && g->profiling) {
+      if (cudaEventSynchronize(g->prof_ev[1]) != cudaSuccess) rc = fail(GG_ERR_CUDA, "edgeMap: profiling event");
+    } else if (!rc && !skip_stats) {
+      rc = read_stats(g);
+    }
     if (!rc && no_out) {  // an output nobody reads: empty
       o->dm = 0;
       o->out_edges = 0;
