@@ -545,7 +545,8 @@ struct has_gather_pol<F, decltype((void)std::declval<const F&>().gather_pol(0u, 
 
 // HINT bits of the direct-load pull: 1 the edge stream bypasses L1 and is
 // marked evict-first in L2; 2 the source gathers (functors with gather_pol)
-// are marked evict-last in L1 and L2.
+// are marked evict-last in L1 and L2; 4 a vertex step at the commits
+// (PrFinishF) issues the loads of four 32-vertex groups before it uses them.
 template <class F, bool HW, bool ALL, int STAGES, bool CONTIG, bool PF, bool NOOUT, bool MERGE, int HINT = 0>
 __device__ __forceinline__ void pull_coo_w_run(const PullParams& p, const F& f) {
   static_assert(!NOOUT || F::kIdentityCommitNoop, "discarding the output needs a no-op identity commit");
@@ -843,6 +844,48 @@ __device__ __forceinline__ void pull_coo_w_run(const PullParams& p, const F& f) 
       continue;
     }
     const uint32_t base0 = v0 & ~31u;
+    if constexpr (kFin && (HINT & 4)) {
+      // the vertex step of kCommitAhead 32-vertex groups per round: every
+      // group's loads (degree bounds, rank, previous rank, frontier word)
+      // are issued before the first group's arithmetic and stores
+      constexpr int kCommitAhead = 4;
+      for (uint32_t b0 = base0 + (uint32_t)warp * 32u; b0 < v0 + nv; b0 += kCommitAhead * kCooThreads) {
+        typename F::FinishIn x[kCommitAhead];
+        uint32_t dg[kCommitAhead];
+        bool inr[kCommitAhead];
+#pragma unroll
+        for (int u = 0; u < kCommitAhead; ++u) {
+          const uint32_t v = b0 + (uint32_t)u * kCooThreads + (uint32_t)lane;
+          inr[u] = v >= v0 && v < v0 + nv;
+          dg[u] = 0;
+          if (inr[u]) {
+            dg[u] = __ldg(p.deg_off + v + 1) - __ldg(p.deg_off + v);
+            x[u] = f.finish_load(v);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < kCommitAhead; ++u) {
+          const uint32_t bb = b0 + (uint32_t)u * kCooThreads;
+          if (bb >= v0 + nv) break;  // warp-uniform
+          const uint32_t v = bb + (uint32_t)lane;
+          bool act = false;
+          if (inr[u]) {
+            const uint32_t l = v - v0;
+            const bool touched = s_acc[l] != F::identity();
+            my_l1 += f.finish_apply(v, x[u], touched, s_acc[l], dg[u]);
+            act = touched;
+          }
+          const uint32_t word = __ballot_sync(0xffffffffu, act);
+          if (act) my_deg += dg[u];
+          if (lane == 0 && word) {
+            atomicOr(p.next_bits + (bb >> 5), word);
+            my_cnt += __popc(word);
+          }
+        }
+      }
+      __syncthreads();
+      continue;
+    }
     for (uint32_t bb = base0 + (uint32_t)warp * 32u; bb < v0 + nv; bb += kCooThreads) {
       const uint32_t v = bb + (uint32_t)lane;
       bool act = false;

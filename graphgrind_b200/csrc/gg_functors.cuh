@@ -150,13 +150,28 @@ struct PrFinishF : PrT<true> {
   // vertex v of the tile: s = its accumulated sum (touched: s came from an
   // edge), d = its out-degree; returns its L1 term
   __device__ float finish(uint32_t v, bool touched, float s, uint32_t d) const {
-    float pn = acc_out[v];
+    return finish_apply(v, finish_load(v), touched, s, d);
+  }
+  // The vertex step split into its loads and the rest, so that a caller can
+  // issue the loads of several vertices before it needs any of them.
+  struct FinishIn {
+    float acc, prev;
+    bool in;
+  };
+  __device__ FinishIn finish_load(uint32_t v) const {
+    FinishIn x;
+    x.acc = acc_out[v];
+    x.prev = p_prev[v];
+    x.in = !fbits || ((fbits[v >> 5] >> (v & 31)) & 1u);
+    return x;
+  }
+  __device__ float finish_apply(uint32_t v, const FinishIn& x, bool touched, float s, uint32_t d) const {
+    float pn = x.acc;
     if (touched) pn += s;
-    const bool in = !fbits || ((fbits[v >> 5] >> (v & 31)) & 1u);
-    if (in) pn = damping * pn + added;
-    const float diff = fabsf(p_prev[v] - pn);
+    if (x.in) pn = damping * pn + added;
+    const float diff = fabsf(x.prev - pn);
     acc_out[v] = pn;
-    p_prev[v] = in ? 0.0f : diff;
+    p_prev[v] = x.in ? 0.0f : diff;
     contrib_next[v] = d ? ((!masked || touched) ? pn / (float)d : -1.0f) : 0.0f;
     return diff;
   }

@@ -363,8 +363,8 @@ int pull_launch(gg_graph_s* g, gg_frontier_s* in, gg_frontier_s* out, const F& f
     static DeviceOnce opted_h[2];
     switch (g->coo_kernel) {
       case 7:
-        return all ? launch_w(k_pull_coo_w<F, kHW, true, 0, false, false, false, true, 3>, 0, opted_h[1], kFlags)
-                   : launch_w(k_pull_coo_w<F, kHW, false, 0, false, false, false, true, 3>, 0, opted_h[0], kFlags);
+        return all ? launch_w(k_pull_coo_w<F, kHW, true, 0, false, false, false, true, 7>, 0, opted_h[1], kFlags)
+                   : launch_w(k_pull_coo_w<F, kHW, false, 0, false, false, false, true, 7>, 0, opted_h[0], kFlags);
       case 6:
         return all ? launch_w(k_pull_coo_w<F, kHW, true, 0, false, false, false, true>, 0, opted_mg[1], kFlags)
                    : launch_w(k_pull_coo_w<F, kHW, false, 0, false, false, false, true>, 0, opted_mg[0], kFlags);

@@ -337,7 +337,8 @@ int gg_graph_set_dense_policy(gg_graph_t g, int32_t policy);
  *                         built with coo_window == 0): the edge stream read
  *                         past L1 and marked evict-first in L2, the source
  *                         gathers of PageRank and SpMV marked evict-last in
- *                         L1 and L2
+ *                         L1 and L2; PageRank's vertex step at the commits
+ *                         loads four 32-vertex groups ahead
  *   GG_TUNE_SPARSE_DIV    the application loops (gg_bfs ... gg_bc) call edgeMap
  *                         with threshold m / value (20 in the reference apps)
  *   GG_TUNE_DEVICE_LOOP   2 (default): gg_bfs runs the whole BFS in one
