@@ -86,7 +86,7 @@ HBM_FALLBACK_GBS = 6650.0
 # DRAM bytes per PageRank-pull launch of the default workload (the merged-run
 # COO kernel with the vertex step at its commits), from one ncu capture
 # (profiles/dram_k_pull_coo_w_pagerank_rmat24.md)
-TRAFFIC_RMAT24_PR_PULL = {(6, 1): 2110578176, (7, 1): 1983904896}  # by (COO kernel, vertex order)
+TRAFFIC_RMAT24_PR_PULL = {(6, 1): 2110578176, (7, 1): 1982974208}  # by (COO kernel, vertex order)
 TRAFFIC_TILE_EDGES = 1 << 18
 
 
