@@ -335,21 +335,34 @@ int build_bu_index(gg_graph_s* g) {
   const uint64_t m = g->m;
   const uint32_t n = g->n;
   if (m >= (1ull << 31)) return fail(GG_ERR_UNSUPPORTED, "bottom-up in-lists: more than 2^31 edges");
-  GG_TRY(dev_alloc(g, &g->d_bu_idx, g->m_pad));
-  GG_CUDA(cudaMemsetAsync(g->d_bu_idx + m, 0, 4ull * (g->m_pad - m), g->stream));
-  if (m == 0) return GG_OK;
-  DevBuf<uint32_t> keys, keys_out;
-  GG_TRY(keys.alloc(g, m));
-  GG_TRY(keys_out.alloc(g, m));
-  k_bu_keys<<<generic_grid(g, m), kGenericThreads, 0, g->stream>>>(g->d_csc_idx, m, g->d_csr_off, keys.p);
-  GG_CUDA(cudaGetLastError());
-  size_t temp = 0;
-  GG_CUDA(cub::DeviceSegmentedSort::StableSortPairs(nullptr, temp, keys.p, keys_out.p, g->d_csc_idx, g->d_bu_idx,
-                                                     (int)m, (int)n, g->d_csc_off, g->d_csc_off + 1, g->stream));
-  DevBuf<unsigned char> tmp;
-  GG_TRY(tmp.alloc(g, temp));
-  GG_CUDA(cub::DeviceSegmentedSort::StableSortPairs(tmp.p, temp, keys.p, keys_out.p, g->d_csc_idx, g->d_bu_idx,
-                                                     (int)m, (int)n, g->d_csc_off, g->d_csc_off + 1, g->stream));
+  uint32_t* out = nullptr;
+  GG_TRY(dev_alloc(g, &out, g->m_pad));
+  // the copy is kept only once it is complete
+  auto build = [&]() -> int {
+    GG_CUDA(cudaMemsetAsync(out + m, 0, 4ull * (g->m_pad - m), g->stream));
+    if (m == 0) return GG_OK;
+    DevBuf<uint32_t> keys, keys_out;
+    GG_TRY(keys.alloc(g, m));
+    GG_TRY(keys_out.alloc(g, m));
+    k_bu_keys<<<generic_grid(g, m), kGenericThreads, 0, g->stream>>>(g->d_csc_idx, m, g->d_csr_off, keys.p);
+    GG_CUDA(cudaGetLastError());
+    size_t temp = 0;
+    GG_CUDA(cub::DeviceSegmentedSort::StableSortPairs(nullptr, temp, keys.p, keys_out.p, g->d_csc_idx, out, (int)m,
+                                                       (int)n, g->d_csc_off, g->d_csc_off + 1, g->stream));
+    DevBuf<unsigned char> tmp;
+    GG_TRY(tmp.alloc(g, temp));
+    GG_CUDA(cub::DeviceSegmentedSort::StableSortPairs(tmp.p, temp, keys.p, keys_out.p, g->d_csc_idx, out, (int)m,
+                                                       (int)n, g->d_csc_off, g->d_csc_off + 1, g->stream));
+    return GG_OK;
+  };
+  const int rc = build();
+  if (rc) {
+    cudaStreamSynchronize(g->stream);
+    cudaFree(out);
+    g->device_bytes -= 4ull * g->m_pad;
+    return rc;
+  }
+  g->d_bu_idx = out;
   return GG_OK;
 }
 

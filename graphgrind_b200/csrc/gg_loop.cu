@@ -794,9 +794,10 @@ int bfs_device_full(gg_graph_s* g, uint32_t start, int32_t* parents, int32_t* le
   const uint32_t* ioff = g->in_off();
   // the bottom-up levels walk the in-lists hub sources first (same edges,
   // other order: a vertex then meets a frontier in-neighbour sooner)
-  const bool hubs_first = g->early_kernel == 3;
-  if (hubs_first && !g->d_bu_idx) GG_TRY(build_bu_index(g));
-  const uint32_t* iidx = hubs_first ? g->d_bu_idx : g->in_idx();
+  // (graphs the copy cannot be built for, past 2^31 edges or without the
+  // memory, walk the CSC's own in-lists)
+  if (g->early_kernel == 3 && !g->d_bu_idx && build_bu_index(g) != GG_OK) cudaGetLastError();
+  const uint32_t* iidx = g->early_kernel == 3 && g->d_bu_idx ? g->d_bu_idx : g->in_idx();
   uint32_t* a0 = q0.p;
   uint32_t* a1 = q1.p;
   uint32_t* e0 = eo0.p;
