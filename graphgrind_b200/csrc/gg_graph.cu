@@ -111,7 +111,8 @@ int frontier_ensure_bits(gg_frontier_s* f, bool zero) {
 
 int frontier_ensure_queue(gg_frontier_s* f) {
   gg_graph_s* g = f->g;
-  if (!f->d_queue) GG_CUDA(pool_alloc((void**)&f->d_queue, sizeof(uint32_t) * ((size_t)g->n + 4), g->stream, g->device));
+  if (!f->d_queue)
+    GG_CUDA(pool_alloc((void**)&f->d_queue, sizeof(uint32_t) * ((size_t)g->n + 4), g->stream, g->device));
   return GG_OK;
 }
 

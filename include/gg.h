@@ -419,7 +419,9 @@ int gg_graph_set_dense_policy(gg_graph_t g, int32_t policy);
  *                         (a vertex meets a frontier in-neighbour sooner:
  *                         0.438 against 0.452 ms); the first such BFS builds
  *                         the copy (one segmented sort), which stays with the
- *                         graph: 4 bytes per edge
+ *                         graph: 4 bytes per edge (a graph past 2^31 edges,
+ *                         or one the copy does not fit beside, walks the
+ *                         CSC's own in-lists)
  *   GG_TUNE_PUSH_DENSE_DIV  a dense edgeMap of BFS (an early-exit functor)
  *                         whose frontier has at most n / value vertices runs
  *                         top-down instead (the frontier's out-edges pushed,
